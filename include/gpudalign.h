@@ -1,0 +1,120 @@
+/* gpudalign.h -- C ABI of the sm_100a daligner overlap path (libgpudalign.so).
+ *
+ * The entry points mirror the reference's inner C interface of the path, so that the
+ * reference driver (dalign/daligner.c main) or any FFI can call the GPU path in place of
+ * dalign/filter.c + dalign/align.c.  All pointers are plain host pointers; no CUDA or
+ * torch types cross this boundary.  Every function returns 0 (or a count >= 0) on
+ * success and -1 on failure, with the message in gd_last_error(); nothing exits the
+ * process (the reference calls exit(1) instead, dalign/filter.c:2135-2145).
+ *
+ * One context = one GPU (the device current at gd_create) and one host thread.
+ */
+#ifndef GPUDALIGN_H
+#define GPUDALIGN_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gd_context gd_context;
+
+/* A DB block in host memory, laid out like the reference's Read_All_Sequences result
+ * (db/DB.c:1349-1410): bases[-1] == 4, read i at bases[boff[i]] .. bases[boff[i]+rlen[i]-1],
+ * bases[boff[i]+rlen[i]] == 4.  mask_anno/mask_data (optional) give per read the masked
+ * (begin,end) intervals of the -m tracks: read i's pairs are mask_data[mask_anno[i] ..
+ * mask_anno[i+1]) (the converted track layout of dalign/daligner.c:425-428). */
+typedef struct
+{
+    const uint8_t* bases;
+    const int64_t* boff; /* [nreads+1] */
+    const int32_t* rlen; /* [nreads]   */
+    int32_t nreads;
+    int32_t maxlen;
+    int64_t totlen;
+    int32_t ufirst;
+    const int64_t* mask_anno;
+    const int32_t* mask_data;
+} gd_block;
+
+/* One overlap as the .las file stores it (Overlap minus its trace pointer,
+ * dalign/align.h:307-312, written by Write_Overlap dalign/align.c:3345-3350). */
+typedef struct
+{
+    int32_t tlen, diffs, abpos, bbpos, aepos, bepos;
+    uint32_t flags;
+    int32_t aread, bread, pad;
+    uint64_t toff; /* offset of this record's trace bytes in the trace array */
+} gd_overlap;
+
+typedef struct
+{
+    int64_t kmers[3];     /* index sizes of slots A, B, complement-B */
+    int64_t hits[2];      /* hits of the last N and C Match_Filter calls */
+    int64_t groups[2];    /* pair groups with >= ceil(h/k) hits */
+    int64_t seeds[2];     /* Local_Alignment calls */
+    int64_t cells[2];     /* wave cells (sum of wave widths, dalign/align.c:957-963) */
+    int64_t records;      /* overlaps in the buffer */
+    int32_t limit[2];     /* k-mer pair cap used (dalign/filter.c:2107-2174) */
+    double ms_index[3];   /* device time of Sort_Kmers per slot */
+    double ms_merge[2];   /* device time of merge + hit sort */
+    double ms_align[2];   /* device time of seed scan + alignment */
+} gd_stats;
+
+/* Context on the current CUDA device. */
+gd_context* gd_create(void);
+void gd_destroy(gd_context* ctx);
+const char* gd_last_error(void);
+
+/* Set_Filter_Params (dalign/filter.c:119-139). */
+int gd_set_filter_params(gd_context* ctx, int kmer, int binshift, int suppress, int hitmin);
+
+/* New_Align_Spec (dalign/align.c:214-279) with the HEIDELBERG flags it takes. */
+int gd_new_align_spec(gd_context* ctx, double ave_corr, int trace_space, const float freq[4], int symmetric,
+                      int only_identity, int no_trace_points);
+
+/* The globals daligner's main shares with filter.c (dalign/daligner.c:60-71):
+ * MINOVER (already doubled, :836), IDENTITY, MEM_LIMIT in bytes (0 = uncapped). */
+int gd_set_globals(gd_context* ctx, int minover, int identity, uint64_t mem_limit);
+
+/* Copy a block to the device into slot 0 (A), 1 (B) or 2 (complemented B). */
+int gd_load_block(gd_context* ctx, int slot, const gd_block* block);
+
+/* Sort_Kmers (dalign/filter.c:698-903): builds the sorted k-mer index of a loaded slot on
+ * the device; returns its length. */
+int64_t gd_sort_kmers(gd_context* ctx, int slot);
+
+/* Copies the sorted index of a slot to the host (code, read, rpos); returns its length. */
+int64_t gd_get_kmers(gd_context* ctx, int slot, uint64_t* code, int32_t* read, int32_t* rpos, int64_t cap);
+
+/* Match_Filter (dalign/filter.c:1997-2407): A (slot 0) against bslot in orientation comp;
+ * self != 0 when A and B are the same block (aname == bname in the reference).
+ * Appends the overlaps it finds to the context's overlap buffer. */
+int gd_match_filter(gd_context* ctx, int bslot, int comp, int self);
+
+/* The sorted hits of the last gd_match_filter (rows diag, apos, aread, bread), for tests. */
+int64_t gd_get_hits(gd_context* ctx, int32_t* rows4, int64_t cap);
+
+/* Overlap buffer: count, copy out (sorted as SORT_OVL, dalign/align.c:5786-5813), write
+ * .las files as Write_Overlap_Buffer does (dalign/align.c:5815-6043), reset. */
+int64_t gd_num_overlaps(gd_context* ctx, int64_t* trace_bytes);
+int64_t gd_get_overlaps(gd_context* ctx, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap);
+int gd_write_overlap_buffer(gd_context* ctx, int run_id, const char* ablock, const char* bblock, int last_read);
+int gd_reset_overlap_buffer(gd_context* ctx);
+
+int gd_get_stats(gd_context* ctx, gd_stats* st);
+
+/* Local_Alignment (dalign/align.c:1922-2060) for a batch of seeds on the device.
+ * Sequences are host buffers in gd_block layout; per seed: read offsets into abases /
+ * bbases, lengths, diagonal and anti-diagonal.  out12 receives per seed the A-path
+ * {abpos,bbpos,aepos,bepos,diffs,tlen} then the B-path; traces land at
+ * trace + seed*trstride (A) and + trstride/2 (B); cells per seed in cells. */
+int gd_local_alignment_batch(gd_context* ctx, const uint8_t* abases, int64_t alen_total, const uint8_t* bbases,
+                             int64_t blen_total, const int64_t* aoff, const int32_t* alen, const int64_t* boff,
+                             const int32_t* blen, const int32_t* diag, const int32_t* anti, int nseeds, int comp,
+                             int32_t* out12, uint16_t* trace, int trstride, int64_t* cells);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

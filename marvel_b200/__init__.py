@@ -1,0 +1,266 @@
+"""marvel_b200 -- daligner's overlap path on B200 (sm_100a), behind a C ABI.
+
+The product is ``libgpudalign.so`` (CUDA kernels + host orchestration, ``include/gpudalign.h``)
+and the ``daligner_gpu`` command-line driver.  This module is the thin Python binding used
+by tests and benchmarks: it loads the in-tree shared library with ctypes and exposes the
+reference's operator interface of the path (dalign/filter.h:67-73, dalign/align.h:160-344):
+
+    ctx = Context()
+    ctx.set_filter_params(k, w, t, h)          # Set_Filter_Params
+    ctx.new_align_spec(e, s, freq, ...)        # New_Align_Spec
+    ctx.load_block(slot, block); ctx.sort_kmers(slot)    # Sort_Kmers
+    ctx.match_filter(bslot, comp, self)        # Match_Filter
+    ctx.write_overlap_buffer(...)              # Write_Overlap_Buffer
+
+There is no CPU path: without a CUDA device ``Context()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import dazzdb
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libgpudalign.so")
+_lib = None
+
+
+class GdBlock(C.Structure):
+    _fields_ = [("bases", C.c_void_p), ("boff", C.c_void_p), ("rlen", C.c_void_p), ("nreads", C.c_int32),
+                ("maxlen", C.c_int32), ("totlen", C.c_int64), ("ufirst", C.c_int32),
+                ("mask_anno", C.c_void_p), ("mask_data", C.c_void_p)]
+
+
+class GdOverlap(C.Structure):
+    _fields_ = [("tlen", C.c_int32), ("diffs", C.c_int32), ("abpos", C.c_int32), ("bbpos", C.c_int32),
+                ("aepos", C.c_int32), ("bepos", C.c_int32), ("flags", C.c_uint32), ("aread", C.c_int32),
+                ("bread", C.c_int32), ("pad", C.c_int32), ("toff", C.c_uint64)]
+
+
+OVL_DTYPE = np.dtype([("tlen", "<i4"), ("diffs", "<i4"), ("abpos", "<i4"), ("bbpos", "<i4"), ("aepos", "<i4"),
+                      ("bepos", "<i4"), ("flags", "<u4"), ("aread", "<i4"), ("bread", "<i4"), ("pad", "<i4"),
+                      ("toff", "<u8")])
+assert OVL_DTYPE.itemsize == C.sizeof(GdOverlap)
+
+
+class GdStats(C.Structure):
+    _fields_ = [("kmers", C.c_int64 * 3), ("hits", C.c_int64 * 2), ("groups", C.c_int64 * 2),
+                ("seeds", C.c_int64 * 2), ("cells", C.c_int64 * 2), ("records", C.c_int64),
+                ("limit", C.c_int32 * 2), ("ms_index", C.c_double * 3), ("ms_merge", C.c_double * 2),
+                ("ms_align", C.c_double * 2)]
+
+
+# exported symbols of include/gpudalign.h
+SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "gd_new_align_spec",
+           "gd_set_globals", "gd_load_block", "gd_sort_kmers", "gd_get_kmers", "gd_match_filter", "gd_get_hits",
+           "gd_num_overlaps", "gd_get_overlaps", "gd_write_overlap_buffer", "gd_reset_overlap_buffer",
+           "gd_get_stats", "gd_local_alignment_batch"]
+
+
+def lib():
+    """Loads the in-tree libgpudalign.so (built by marvel_b200/build.py); fails loudly if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise RuntimeError(f"{LIBPATH} is missing: build it with `python marvel_b200/build.py`")
+    L = C.CDLL(LIBPATH)
+    L.gd_create.restype = C.c_void_p
+    L.gd_destroy.argtypes = [C.c_void_p]
+    L.gd_last_error.restype = C.c_char_p
+    L.gd_set_filter_params.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.gd_new_align_spec.argtypes = [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int]
+    L.gd_set_globals.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64]
+    L.gd_load_block.argtypes = [C.c_void_p, C.c_int, C.POINTER(GdBlock)]
+    L.gd_sort_kmers.argtypes = [C.c_void_p, C.c_int]
+    L.gd_sort_kmers.restype = C.c_int64
+    L.gd_get_kmers.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+    L.gd_get_kmers.restype = C.c_int64
+    L.gd_match_filter.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    L.gd_get_hits.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    L.gd_get_hits.restype = C.c_int64
+    L.gd_num_overlaps.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.gd_num_overlaps.restype = C.c_int64
+    L.gd_get_overlaps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
+    L.gd_get_overlaps.restype = C.c_int64
+    L.gd_write_overlap_buffer.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
+    L.gd_reset_overlap_buffer.argtypes = [C.c_void_p]
+    L.gd_get_stats.argtypes = [C.c_void_p, C.POINTER(GdStats)]
+    L.gd_local_alignment_batch.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                           C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    _lib = L
+    return L
+
+
+class GpuError(RuntimeError):
+    pass
+
+
+def _check(rc):
+    if rc < 0:
+        raise GpuError(lib().gd_last_error().decode())
+    return rc
+
+
+class _BlockRef:
+    def __init__(self, blk: dazzdb.Block):
+        self.bases = np.ascontiguousarray(blk.bases, dtype=np.uint8)
+        self.boff = np.ascontiguousarray(blk.boff, dtype=np.int64)
+        self.rlen = np.ascontiguousarray(blk.rlen, dtype=np.int32)
+        s = GdBlock()
+        s.bases = self.bases.ctypes.data + 1
+        s.boff = self.boff.ctypes.data
+        s.rlen = self.rlen.ctypes.data
+        s.nreads = blk.nreads
+        s.maxlen = blk.maxlen
+        s.totlen = blk.totlen
+        s.ufirst = blk.ufirst
+        if blk.mask is not None:
+            anno = [0]
+            data = []
+            for iv in blk.mask:
+                for a, b in iv:
+                    data += [a, b]
+                anno.append(len(data))
+            self.anno = np.array(anno, dtype=np.int64)
+            self.data = np.array(data + [0], dtype=np.int32)
+            s.mask_anno = self.anno.ctypes.data
+            s.mask_data = self.data.ctypes.data
+        self.s = s
+
+
+class Context:
+    """One GPU context of the overlap path (the current CUDA device)."""
+
+    def __init__(self):
+        L = lib()
+        self.h = L.gd_create()
+        if not self.h:
+            raise GpuError(L.gd_last_error().decode())
+        self.tspace = 100
+
+    def close(self):
+        if self.h:
+            lib().gd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_filter_params(self, kmer=14, binshift=6, suppress=0, hitmin=35):
+        _check(lib().gd_set_filter_params(self.h, kmer, binshift, suppress, hitmin))
+
+    def new_align_spec(self, ave_corr, trace_space, freq, symmetric=True, only_identity=False, no_trace=False):
+        f = (C.c_float * 4)(*[float(x) for x in freq])
+        self.tspace = trace_space
+        _check(lib().gd_new_align_spec(self.h, ave_corr, trace_space, f, int(symmetric), int(only_identity),
+                                       int(no_trace)))
+
+    def set_globals(self, minover=2000, identity=False, mem_limit=0):
+        _check(lib().gd_set_globals(self.h, minover, int(identity), int(mem_limit)))
+
+    def load_block(self, slot, blk):
+        r = _BlockRef(blk)
+        _check(lib().gd_load_block(self.h, slot, C.byref(r.s)))
+
+    def sort_kmers(self, slot):
+        return _check(lib().gd_sort_kmers(self.h, slot))
+
+    def get_kmers(self, slot, n):
+        code = np.zeros(max(n, 1), np.uint64)
+        read = np.zeros(max(n, 1), np.int32)
+        rpos = np.zeros(max(n, 1), np.int32)
+        k = _check(lib().gd_get_kmers(self.h, slot, code.ctypes.data, read.ctypes.data, rpos.ctypes.data, n))
+        return code[:k], read[:k], rpos[:k]
+
+    def match_filter(self, bslot, comp, self_cmp):
+        _check(lib().gd_match_filter(self.h, bslot, int(comp), int(self_cmp)))
+
+    def get_hits(self):
+        n = _check(lib().gd_get_hits(self.h, None, 0))
+        rows = np.zeros((max(n, 1), 4), np.int32)
+        _check(lib().gd_get_hits(self.h, rows.ctypes.data, n))
+        return rows[:n]
+
+    def overlaps(self):
+        tb = C.c_int64()
+        n = _check(lib().gd_num_overlaps(self.h, C.byref(tb)))
+        recs = np.zeros(max(n, 1), OVL_DTYPE)
+        tr = np.zeros(max(tb.value, 1), np.uint8)
+        k = _check(lib().gd_get_overlaps(self.h, recs.ctypes.data, tr.ctypes.data, n, tb.value))
+        return recs[:k], tr
+
+    def write_overlap_buffer(self, run_id, ablock, bblock, last_read):
+        _check(lib().gd_write_overlap_buffer(self.h, run_id, ablock.encode(), bblock.encode(), last_read))
+
+    def reset_overlap_buffer(self):
+        _check(lib().gd_reset_overlap_buffer(self.h))
+
+    def stats(self):
+        st = GdStats()
+        _check(lib().gd_get_stats(self.h, C.byref(st)))
+        return {k: (list(getattr(st, k)) if hasattr(getattr(st, k), "__len__") else getattr(st, k))
+                for k, _ in GdStats._fields_}
+
+    def local_alignment_batch(self, abases, aoff, alen, bbases, boff, blen, diag, anti, comp, trstride=None):
+        n = len(diag)
+        if trstride is None:
+            trstride = 2 * (4 * (int(max(np.max(alen), np.max(blen))) // self.tspace + 2) + 16)
+        out = np.zeros((n, 12), np.int32)
+        tr = np.zeros((n, trstride), np.uint16)
+        cells = np.zeros(n, np.int64)
+        abases = np.ascontiguousarray(abases, np.uint8)
+        bbases = np.ascontiguousarray(bbases, np.uint8)
+        arrs = [np.ascontiguousarray(x, t) for x, t in ((aoff, np.int64), (alen, np.int32), (boff, np.int64),
+                                                         (blen, np.int32), (diag, np.int32), (anti, np.int32))]
+        _check(lib().gd_local_alignment_batch(self.h, abases.ctypes.data, abases.size, bbases.ctypes.data,
+                                              bbases.size, *[a.ctypes.data for a in arrs], n, int(comp),
+                                              out.ctypes.data, tr.ctypes.data, trstride, cells.ctypes.data))
+        return out, tr, cells
+
+
+def daligner_block(ctx: Context, A: dazzdb.Block, B: dazzdb.Block | None = None, *, k=14, w=6, h=35, t=0, e=0.70,
+                   l=1000, s=100, M=32, symmetric=True, identity=False, only_identity=False, no_trace=False):
+    """One daligner block comparison on the GPU (dalign/daligner.c:957-1014): A against B
+    (or against itself when B is None) in both orientations.  Returns the overlap buffer
+    as (records, trace bytes), sorted like the .las file."""
+    self_cmp = B is None
+    ctx.set_filter_params(k, w, t, h)
+    ctx.new_align_spec(e, s, A.freq, symmetric and True, only_identity, no_trace)
+    ctx.set_globals(2 * l, identity or only_identity, int(M) * 0x40000000)
+    ctx.reset_overlap_buffer()
+    ctx.load_block(0, A)
+    ctx.sort_kmers(0)
+    if self_cmp:
+        ctx.match_filter(0, 0, 1)
+        Bc = dazzdb.complement_block(A)
+    else:
+        ctx.load_block(1, B)
+        ctx.sort_kmers(1)
+        ctx.match_filter(1, 0, 0)
+        Bc = dazzdb.complement_block(B)
+    ctx.load_block(2, Bc)
+    ctx.sort_kmers(2)
+    ctx.match_filter(2, 1, int(self_cmp))
+    return ctx.overlaps()
+
+
+def write_las(path, recs, trace, tspace):
+    """Writes records (OVL_DTYPE, already sorted) and their trace bytes as a .las file."""
+    tb = 1 if tspace <= 125 else 2
+    with open(path, "wb") as f:
+        f.write(np.int64(recs.size).tobytes())
+        f.write(np.int32(tspace).tobytes())
+        for r in recs:
+            f.write(np.array([r["tlen"], r["diffs"], r["abpos"], r["bbpos"], r["aepos"], r["bepos"]], "<i4").tobytes())
+            f.write(np.uint32(r["flags"]).tobytes())
+            f.write(np.array([r["aread"], r["bread"], 0], "<i4").tobytes())
+            o = int(r["toff"])
+            f.write(trace[o:o + int(r["tlen"]) * tb].tobytes())

@@ -1,0 +1,1614 @@
+// gd_align.cu -- seed scan and adaptive-wave local alignment, one warp per (aread, bread) pair.
+//
+// Restates dalign/filter.c report_thread (:1617-1989) and dalign/align.c Local_Alignment
+// (:1922-2060) with forward_wave (:369-1110) and reverse_wave (:1114-1916).
+//
+// GPU mapping.  A warp owns one pair group of the sorted hit list.  The panel band scores
+// are built lane-parallel (match-any groups per diagonal band), candidate seeds are taken
+// in hit order, and each fired seed runs the O(ND) wave with lanes over diagonals: the
+// wave vectors V (furthest anti-diagonal), T (60-column match bit vector; its popcount is
+// the reference's M), HA/HB (pebble heads), NA/NB (next trace-point marks) live in a
+// per-warp shared-memory ring indexed by diagonal.  Each wave reads the previous wave for
+// diagonals k-1, k, k+1, keeps the new values in registers (up to 32*WAVE_CHUNKS
+// diagonals), and writes them back after a __syncwarp, which is the reference's
+// in-place update order.  The reference's sequential "c > besta" scan over diagonals
+// becomes a warp prefix-max in scan order; its clip bookkeeping becomes ballots.  Pebbles
+// go to a per-warp global arena; the two trace-point chains are unwound by lane 0.
+// Match extension compares 8 bases per step with 64-bit XOR windows.
+#include "gd_align.cuh"
+
+#include <climits>
+
+namespace gd
+{
+
+#define PATH_TOP 0x1000000000000000ull
+#define PATH_INT 0x0fffffffffffffffull
+#define MASK61 0x1fffffffffffffffull
+#define TRIM_LEN 15
+#define TRIM_MASK 0x7fff
+#define TRIM_MLAG 200
+#define WAVE_LAG 30
+#define PANEL_SIZE 50000
+#define PANEL_OVERLAP 10000
+#define RM (RING - 1)
+#define SENT4 0x0404040404040404ull
+
+struct WaveSmem
+{
+    unsigned long long T[RING];
+    int V[RING], HA[RING], HB[RING], NA[RING], NB[RING];
+};
+
+struct LAPath
+{
+    int abpos, bbpos, aepos, bepos, diffs, tlen, toff, pad;
+};
+
+struct WarpSmem
+{
+    WaveSmem ws;
+    LAPath ap, bp;
+    int span_lo, span_hi;
+};
+
+struct WarpCtx
+{
+    WarpSmem* sm;
+    int4* peb;
+    int pcap;
+    uint16_t* pts;
+    int ptscap;
+    DevStatus* st;
+    int lane;
+    int err;
+    int item;
+    long long cells;
+};
+
+__device__ __forceinline__ uint64_t ld8u(const uint8_t* p)
+{
+    uintptr_t a = (uintptr_t)p;
+    const uint64_t* q = (const uint64_t*)(a & ~(uintptr_t)7);
+    unsigned sh = (unsigned)(a & 7) * 8;
+    uint64_t lo = __ldg(q);
+    if (!sh)
+        return lo;
+    uint64_t hi = __ldg(q + 1);
+    return (lo >> sh) | (hi << (64 - sh));
+}
+
+// Extend the match on diagonal k from b-position y forward (FWD) or backward.
+// Returns the new y; sets bend/aend like the reference's snake loop (align.c:798-824).
+template <bool FWD>
+__device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, int y, int k, int lim, bool& bend,
+                                     bool& aend)
+{
+    if (FWD)
+    {
+        // the 4 after every read stops the extension; the cap only guards against a bad pointer
+        for (int guard = (lim >> 3) + 2; guard > 0; guard--)
+        {
+            uint64_t wb = ld8u(bseq + y), wa = ld8u(aseq + y + k);
+            uint64_t stop = (wa ^ wb) | (wb & SENT4);
+            if (stop)
+            {
+                y += (__ffsll((long long)stop) - 1) >> 3;
+                break;
+            }
+            y += 8;
+        }
+        int cb = __ldg(bseq + y);
+        bend = (cb == 4);
+        aend = !bend && (__ldg(aseq + y + k) == 4);
+    }
+    else
+    {
+        for (int guard = (lim >> 3) + 2; guard > 0; guard--)
+        {
+            uint64_t wb = ld8u(bseq + y - 8), wa = ld8u(aseq + y + k - 8);
+            uint64_t stop = (wa ^ wb) | (wb & SENT4);
+            if (stop)
+            {
+                y -= __clzll((long long)stop) >> 3;
+                break;
+            }
+            y -= 8;
+        }
+        int cb = __ldg(bseq + y - 1);
+        bend = (cb == 4);
+        aend = !bend && (__ldg(aseq + y + k - 1) == 4);
+    }
+    return y;
+}
+
+__device__ __forceinline__ int warp_max_incl(int v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int t = __shfl_up_sync(GD_FULL, v, o);
+        if (lane >= o)
+            v = max(v, t);
+    }
+    return v;
+}
+
+// uniform single-pebble allocation (all lanes call, lane 0 writes)
+__device__ __forceinline__ int peb_one(WarpCtx& w, int& npeb, int ptr, int diag, int diff, int mark)
+{
+    int idx = npeb++;
+    if (idx >= w.pcap)
+    {
+        if (!w.err && w.lane == 0)
+            gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
+        w.err = 1;
+        return 0;
+    }
+    if (w.lane == 0)
+        w.peb[idx] = make_int4(ptr, diag, diff, mark);
+    return idx;
+}
+
+// forward_wave (FWD) / reverse_wave (!FWD) restated, with lanes over diagonals.
+template <bool FWD>
+__device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0, int alen, int blen,
+                     int comp, LAPath* apath, LAPath* bpath, int* mind, int maxd, int mida, int minp, int maxp,
+                     uint16_t* atrace, uint16_t* btrace)
+{
+    WaveSmem& R = w.sm->ws;
+    const int lane = w.lane;
+    const int TS = P.tspace;
+    const int S = FWD ? 1 : -1;
+    const int VNONE = FWD ? -1 : INT_MAX;
+    int hgh = maxd, low = *mind, dif = 0;
+    const int boff = comp ? blen % TS : 0;
+    int more = 1;
+    int aclip = FWD ? INT_MAX : -INT_MAX;
+    int bclip = FWD ? -INT_MAX : INT_MAX;
+    int besta, besty, trima, trimy, trimd, trimha, trimhb;
+    int morea, morey, mored, moreha, morehb, morem, lasta;
+    besta = trima = morea = lasta = mida;
+    besty = trimy = morey = (mida - hgh) >> 1;
+    trimd = mored = 0;
+    trimha = moreha = 0;
+    trimhb = morehb = 1;
+    morem = -1;
+    int npeb = 0;
+    // the reverse wave compares the bases just before the point (align.c:1117-1118)
+    const uint8_t* as = FWD ? aseq0 : aseq0 - 1;
+    const uint8_t* bs = FWD ? bseq0 : bseq0 - 1;
+
+    if (low != hgh)
+    {
+        if (lane == 0)
+            gd_fail(w.st, GD_ERR_BAND_WIDTH, w.item, -1);
+        w.err = 1;
+        return;
+    }
+
+    // ---- 0-wave from the seed point on its single diagonal
+    {
+        int k = hgh;
+        int y = (mida - k) >> 1;
+        int ha, hb, na, nb;
+        if (FWD)
+        {
+            na = ((y + k) / TS) * TS;
+            ha = peb_one(w, npeb, -1, k, 0, na);
+            na += TS;
+            nb = ((y + (TS - boff)) / TS - 1) * TS + boff;
+            hb = peb_one(w, npeb, -1, k, 0, nb);
+            nb += TS;
+        }
+        else
+        {
+            na = ((y + k + TS - 1) / TS - 1) * TS;
+            ha = peb_one(w, npeb, -1, k, 0, y + k);
+            nb = ((y + (TS - boff) - 1) / TS - 1) * TS + boff;
+            hb = peb_one(w, npeb, -1, k, 0, y);
+        }
+        bool bend, aend;
+        y = snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
+        if (bend)
+        {
+            more = 0;
+            bclip = FWD ? max(bclip, k) : min(bclip, k);
+        }
+        if (aend)
+        {
+            more = 0;
+            aclip = k;
+        }
+        int c = (y << 1) + k;
+        if (FWD)
+        {
+            while (y + k >= na)
+            {
+                ha = peb_one(w, npeb, ha, k, 0, na);
+                na += TS;
+            }
+            while (y >= nb)
+            {
+                hb = peb_one(w, npeb, hb, k, 0, nb);
+                nb += TS;
+            }
+        }
+        else
+        {
+            while (y + k <= na)
+            {
+                ha = peb_one(w, npeb, ha, k, 0, na);
+                na -= TS;
+            }
+            while (y <= nb)
+            {
+                hb = peb_one(w, npeb, hb, k, 0, nb);
+                nb -= TS;
+            }
+        }
+        if (FWD ? (c > besta) : (c < besta))
+        {
+            besta = trima = lasta = c;
+            besty = trimy = y;
+            trimha = ha;
+            trimhb = hb;
+        }
+        if (lane == 0)
+        {
+            R.V[k & RM] = c;
+            R.T[k & RM] = PATH_INT;
+            R.HA[k & RM] = ha;
+            R.HB[k & RM] = hb;
+            R.NA[k & RM] = na;
+            R.NB[k & RM] = nb;
+        }
+        __syncwarp();
+    }
+    if (w.err)
+        return;
+
+    auto clip_block = [&]() {
+        if (!more)
+        {
+            if (__ldg(bs + besty) != 4 && __ldg(as + besta - besty) != 4)
+                more = 1;
+            if (FWD ? (hgh >= aclip) : (low <= aclip))
+            {
+                if (FWD)
+                    hgh = aclip - 1;
+                else
+                    low = aclip + 1;
+                int Mc = __popcll(R.T[aclip & RM] & MASK61);
+                if (morem <= Mc)
+                {
+                    morem = Mc;
+                    morea = R.V[aclip & RM];
+                    morey = (morea - aclip) / 2;
+                    mored = dif;
+                    moreha = R.HA[aclip & RM];
+                    morehb = R.HB[aclip & RM];
+                }
+            }
+            if (FWD ? (low <= bclip) : (hgh >= bclip))
+            {
+                if (FWD)
+                    low = bclip + 1;
+                else
+                    hgh = bclip - 1;
+                int Mc = __popcll(R.T[bclip & RM] & MASK61);
+                if (morem <= Mc)
+                {
+                    morem = Mc;
+                    morea = R.V[bclip & RM];
+                    morey = (morea - bclip) / 2;
+                    mored = dif;
+                    moreha = R.HA[bclip & RM];
+                    morehb = R.HB[bclip & RM];
+                }
+            }
+            aclip = FWD ? INT_MAX : -INT_MAX;
+            bclip = FWD ? -INT_MAX : INT_MAX;
+        }
+    };
+    clip_block();
+
+    const unsigned lt = lanemask_lt();
+    const int PATH_AVE = P.ave_path;
+
+    // ---- successive waves
+    while (more && (FWD ? (lasta >= besta - TRIM_MLAG) : (lasta <= besta + TRIM_MLAG)))
+    {
+        low -= 1;
+        hgh += 1;
+        bool newlow = low >= minp;
+        if (!newlow)
+            low += 1;
+        bool newhgh = hgh <= maxp;
+        if (lane == 0)
+        {
+            if (newlow)
+            {
+                R.NA[low & RM] = R.NA[(low + 1) & RM];
+                R.NB[low & RM] = R.NB[(low + 1) & RM];
+                R.V[low & RM] = VNONE;
+            }
+            if (newhgh)
+            {
+                R.NA[hgh & RM] = R.NA[(hgh - 1) & RM];
+                R.NB[hgh & RM] = R.NB[(hgh - 1) & RM];
+                R.V[hgh & RM] = VNONE;
+            }
+        }
+        if (!newhgh)
+            hgh -= 1;
+        dif += 1;
+        if (dif > alen + blen + 2)  // the edit distance cannot exceed alen + blen
+        {
+            if (lane == 0)
+                gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
+            w.err = 1;
+            return;
+        }
+        if (lane == 0)
+        {
+            R.V[(hgh + 1) & RM] = VNONE;
+            R.V[(low - 1) & RM] = VNONE;
+        }
+        __syncwarp();
+        const int width = hgh - low + 1;
+        if (width <= 0 || width > 32 * WAVE_CHUNKS)
+        {
+            if (lane == 0)
+                gd_fail(w.st, width <= 0 ? GD_ERR_EMPTY_BAND : GD_ERR_BAND_WIDTH, w.item, width);
+            w.err = 1;
+            return;
+        }
+        const int nch = (width + 31) >> 5;
+        int rc[WAVE_CHUNKS], rha[WAVE_CHUNKS], rhb[WAVE_CHUNKS], rna[WAVE_CHUNKS], rnb[WAVE_CHUNKS];
+        unsigned long long rb[WAVE_CHUNKS];
+#pragma unroll
+        for (int ch = 0; ch < WAVE_CHUNKS; ch++)
+        {
+            if (ch >= nch)
+                break;
+            const int p = ch * 32 + lane;
+            const bool valid = p < width;
+            const int k = FWD ? hgh - p : low + p;
+            int c = 0, y = 0, ha = 0, hb = 0, na = 0, nb = 0;
+            unsigned long long b = 0;
+            bool bend = false, aend = false;
+            if (valid)
+            {
+                // choose the furthest of the three predecessors (align.c:748-797)
+                int vP = R.V[(k + S) & RM], vC = R.V[k & RM], vN = R.V[(k - S) & RM];
+                int wP = FWD ? vP : -vP, wC = FWD ? vC : -vC, wN = FWD ? vN : -vN;
+                int ks, vs, step;
+                if (wC < wN)
+                {
+                    if (wN < wP)
+                    {
+                        ks = k + S;
+                        vs = vP;
+                    }
+                    else
+                    {
+                        ks = k - S;
+                        vs = vN;
+                    }
+                    step = 1;
+                }
+                else if (wC < wP)
+                {
+                    ks = k + S;
+                    vs = vP;
+                    step = 1;
+                }
+                else
+                {
+                    ks = k;
+                    vs = vC;
+                    step = 2;
+                }
+                c = vs + S * step;
+                b = R.T[ks & RM] << 1;
+                ha = R.HA[ks & RM];
+                hb = R.HB[ks & RM];
+                y = (c - k) >> 1;
+                int y0 = y;
+                y = snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
+                int L = FWD ? (y - y0) : (y0 - y);
+                b = (L >= 61) ? ~0ull : ((b << L) | ((1ull << L) - 1ull));
+                c = (y << 1) + k;
+                na = R.NA[k & RM];
+                nb = R.NB[k & RM];
+            }
+            // A trace points (align.c:826-852)
+            while (true)
+            {
+                bool need = valid && (FWD ? (y + k >= na) : (y + k <= na));
+                if (!__any_sync(GD_FULL, need))
+                    break;
+                bool create = need && (FWD ? (w.peb[ha].w < na) : (w.peb[ha].w > na));
+                unsigned cm = __ballot_sync(GD_FULL, create);
+                if (cm)
+                {
+                    int base = npeb;
+                    npeb += __popc(cm);
+                    if (npeb > w.pcap)
+                    {
+                        if (lane == 0)
+                            gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
+                        w.err = 1;
+                        return;
+                    }
+                    if (create)
+                    {
+                        int idx = base + __popc(cm & lt);
+                        w.peb[idx] = make_int4(ha, k, dif, na);
+                        ha = idx;
+                    }
+                }
+                if (need)
+                    na += FWD ? TS : -TS;
+            }
+            // B trace points (align.c:854-878)
+            while (true)
+            {
+                bool need = valid && (FWD ? (y >= nb) : (y <= nb));
+                if (!__any_sync(GD_FULL, need))
+                    break;
+                bool create = need && (FWD ? (w.peb[hb].w < nb) : (w.peb[hb].w > nb));
+                unsigned cm = __ballot_sync(GD_FULL, create);
+                if (cm)
+                {
+                    int base = npeb;
+                    npeb += __popc(cm);
+                    if (npeb > w.pcap)
+                    {
+                        if (lane == 0)
+                            gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
+                        w.err = 1;
+                        return;
+                    }
+                    if (create)
+                    {
+                        int idx = base + __popc(cm & lt);
+                        w.peb[idx] = make_int4(hb, k, dif, nb);
+                        hb = idx;
+                    }
+                }
+                if (need)
+                    nb += FWD ? TS : -TS;
+            }
+            rc[ch] = c;
+            rb[ch] = b;
+            rha[ch] = ha;
+            rhb[ch] = hb;
+            rna[ch] = na;
+            rnb[ch] = nb;
+
+            // clip bookkeeping: bclip = first B-end in scan order, aclip = last A-end
+            unsigned bm = __ballot_sync(GD_FULL, valid && bend);
+            if (bm)
+            {
+                int pb = ch * 32 + __ffs(bm) - 1;
+                int kb = FWD ? hgh - pb : low + pb;
+                bclip = FWD ? max(bclip, kb) : min(bclip, kb);
+                more = 0;
+            }
+            unsigned amk = __ballot_sync(GD_FULL, valid && aend);
+            if (amk)
+            {
+                int pa = ch * 32 + 31 - __clz(amk);
+                aclip = FWD ? hgh - pa : low + pa;
+                more = 0;
+            }
+
+            // best point: every new maximum in scan order is a record (align.c:880-897)
+            int wv = valid ? (FWD ? c : -c) : INT_MIN;
+            int incl = warp_max_incl(wv, lane);
+            int excl = __shfl_up_sync(GD_FULL, incl, 1);
+            if (lane == 0)
+                excl = INT_MIN;
+            int wbest = FWD ? besta : -besta;
+            bool rec = valid && wv > max(wbest, excl);
+            unsigned recm = __ballot_sync(GD_FULL, rec);
+            if (recm)
+            {
+                int j = 31 - __clz(recm);
+                besta = __shfl_sync(GD_FULL, c, j);
+                besty = __shfl_sync(GD_FULL, y, j);
+                bool p1 = rec && (__popcll(b & MASK61) >= PATH_AVE);
+                unsigned m1 = __ballot_sync(GD_FULL, p1);
+                if (m1)
+                {
+                    int j1 = 31 - __clz(m1);
+                    lasta = __shfl_sync(GD_FULL, c, j1);
+                    bool p2 = false;
+                    if (p1)
+                    {
+                        int lo15 = (int)(b & TRIM_MASK), hi15 = (int)((b >> TRIM_LEN) & TRIM_MASK);
+                        p2 = (__ldg(P.table + lo15) >= 0) && (__ldg(P.table + hi15) + __ldg(P.score + lo15) >= 0);
+                    }
+                    unsigned m2 = __ballot_sync(GD_FULL, p2);
+                    if (m2)
+                    {
+                        int j2 = 31 - __clz(m2);
+                        trima = __shfl_sync(GD_FULL, c, j2);
+                        trimy = __shfl_sync(GD_FULL, y, j2);
+                        trimd = dif;
+                        trimha = __shfl_sync(GD_FULL, ha, j2);
+                        trimhb = __shfl_sync(GD_FULL, hb, j2);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int ch = 0; ch < WAVE_CHUNKS; ch++)
+        {
+            if (ch >= nch)
+                break;
+            int p = ch * 32 + lane;
+            if (p < width)
+            {
+                int k = FWD ? hgh - p : low + p;
+                R.V[k & RM] = rc[ch];
+                R.T[k & RM] = rb[ch];
+                R.HA[k & RM] = rha[ch];
+                R.HB[k & RM] = rhb[ch];
+                R.NA[k & RM] = rna[ch];
+                R.NB[k & RM] = rnb[ch];
+            }
+        }
+        __syncwarp();
+        clip_block();
+
+        // drop diagonals more than WAVE_LAG behind the best (align.c:946-955)
+        {
+            int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
+            int w2 = hgh - low + 1;
+            int nl = INT_MAX, nh = INT_MIN;
+            for (int base = 0; base < w2; base += 32)
+            {
+                int k = low + base + lane;
+                bool good = (base + lane < w2) && (FWD ? (R.V[k & RM] >= n) : (R.V[k & RM] <= n));
+                unsigned gm = __ballot_sync(GD_FULL, good);
+                if (gm)
+                {
+                    nl = min(nl, low + base + __ffs(gm) - 1);
+                    nh = max(nh, low + base + 31 - __clz(gm));
+                }
+            }
+            if (nh != INT_MIN)
+            {
+                hgh = nh;
+                low = nl;
+            }
+            else
+                hgh = low - 1;
+        }
+        w.cells += hgh - low + 1;
+    }
+
+    // ---- trace points of both paths from the pebble chains (align.c:970-1106, 1710-1902)
+    if (lane == 0)
+    {
+        int4* cells = w.peb;
+        int atlen = 0, btlen = 0, trimx, a, b, k, h, d, e;
+        if (morem >= 0)
+        {
+            trimx = morea - morey;
+            trimy = morey;
+            trimd = mored;
+            trimha = moreha;
+            trimhb = morehb;
+        }
+        else
+            trimx = trima - trimy;
+
+        a = -1;
+        for (h = trimha; h >= 0; h = b)
+        {
+            b = cells[h].x;
+            cells[h].x = a;
+            a = h;
+        }
+        h = a;
+        if (FWD)
+        {
+            k = cells[h].y;
+            b = (mida - k) / 2;
+            e = 0;
+            for (h = cells[h].x; h >= 0; h = cells[h].x)
+            {
+                k = cells[h].y;
+                a = cells[h].w - k;
+                d = cells[h].z;
+                atrace[atlen++] = (uint16_t)(d - e);
+                atrace[atlen++] = (uint16_t)(a - b);
+                b = a;
+                e = d;
+            }
+            if (b + k != trimx)
+            {
+                atrace[atlen++] = (uint16_t)(trimd - e);
+                atrace[atlen++] = (uint16_t)(trimy - b);
+            }
+            else if (b != trimy)
+            {
+                atrace[atlen - 1] = (uint16_t)(atrace[atlen - 1] + (trimy - b));
+                atrace[atlen - 2] = (uint16_t)(atrace[atlen - 2] + (trimd - e));
+            }
+        }
+        else
+        {
+            k = cells[h].y;
+            b = cells[h].w - k;
+            e = 0;
+            if ((b + k) % TS != 0)
+            {
+                h = cells[h].x;
+                if (h < 0)
+                {
+                    a = trimy;
+                    d = trimd;
+                }
+                else
+                {
+                    k = cells[h].y;
+                    a = cells[h].w - k;
+                    d = cells[h].z;
+                }
+                if (apath->tlen == 0)
+                {
+                    atrace[--atlen] = (uint16_t)(b - a);
+                    atrace[--atlen] = (uint16_t)(d - e);
+                }
+                else
+                {
+                    atrace[1] = (uint16_t)(atrace[1] + (b - a));
+                    atrace[0] = (uint16_t)(atrace[0] + (d - e));
+                }
+                b = a;
+                e = d;
+            }
+            if (h >= 0)
+            {
+                for (h = cells[h].x; h >= 0; h = cells[h].x)
+                {
+                    k = cells[h].y;
+                    a = cells[h].w - k;
+                    atrace[--atlen] = (uint16_t)(b - a);
+                    d = cells[h].z;
+                    atrace[--atlen] = (uint16_t)(d - e);
+                    b = a;
+                    e = d;
+                }
+                if (b + k != trimx)
+                {
+                    atrace[--atlen] = (uint16_t)(b - trimy);
+                    atrace[--atlen] = (uint16_t)(trimd - e);
+                }
+                else if (b != trimy)
+                {
+                    atrace[atlen + 1] = (uint16_t)(atrace[atlen + 1] + (b - trimy));
+                    atrace[atlen] = (uint16_t)(atrace[atlen] + (trimd - e));
+                }
+            }
+        }
+
+        a = -1;
+        for (h = trimhb; h >= 0; h = b)
+        {
+            b = cells[h].x;
+            cells[h].x = a;
+            a = h;
+        }
+        h = a;
+        if (FWD)
+        {
+            k = cells[h].y;
+            b = (mida + k) / 2;
+            e = 0;
+            low = k;
+            for (h = cells[h].x; h >= 0; h = cells[h].x)
+            {
+                k = cells[h].y;
+                a = cells[h].w + k;
+                d = cells[h].z;
+                btrace[btlen++] = (uint16_t)(d - e);
+                btrace[btlen++] = (uint16_t)(a - b);
+                b = a;
+                e = d;
+            }
+            if (b - k != trimy)
+            {
+                btrace[btlen++] = (uint16_t)(trimd - e);
+                btrace[btlen++] = (uint16_t)(trimx - b);
+            }
+            else if (b != trimx)
+            {
+                btrace[btlen - 1] = (uint16_t)(btrace[btlen - 1] + (trimx - b));
+                btrace[btlen - 2] = (uint16_t)(btrace[btlen - 2] + (trimd - e));
+            }
+            apath->aepos = trimx;
+            apath->bepos = trimy;
+            apath->diffs = trimd;
+            apath->tlen = atlen;
+            apath->toff = (int)(atrace - w.pts);
+            if (comp)
+            {
+                bpath->abpos = blen - apath->bepos;
+                bpath->bbpos = alen - apath->aepos;
+            }
+            else
+            {
+                bpath->aepos = apath->bepos;
+                bpath->bepos = apath->aepos;
+            }
+            bpath->diffs = trimd;
+            bpath->tlen = btlen;
+            bpath->toff = (int)(btrace - w.pts);
+            w.sm->span_lo = low;
+        }
+        else
+        {
+            k = cells[h].y;
+            b = cells[h].w + k;
+            e = 0;
+            if ((b - k) % TS != boff)
+            {
+                h = cells[h].x;
+                if (h < 0)
+                {
+                    a = trimx;
+                    d = trimd;
+                }
+                else
+                {
+                    k = cells[h].y;
+                    a = cells[h].w + k;
+                    d = cells[h].z;
+                }
+                if (bpath->tlen == 0)
+                {
+                    btrace[--btlen] = (uint16_t)(b - a);
+                    btrace[--btlen] = (uint16_t)(b - a);  // sic: align.c:1861-1862 stores b-a twice
+                }
+                else
+                {
+                    btrace[1] = (uint16_t)(btrace[1] + (b - a));
+                    btrace[0] = (uint16_t)(btrace[0] + (d - e));
+                }
+                b = a;
+                e = d;
+            }
+            if (h >= 0)
+            {
+                for (h = cells[h].x; h >= 0; h = cells[h].x)
+                {
+                    k = cells[h].y;
+                    a = cells[h].w + k;
+                    btrace[--btlen] = (uint16_t)(b - a);
+                    d = cells[h].z;
+                    btrace[--btlen] = (uint16_t)(d - e);
+                    b = a;
+                    e = d;
+                }
+                if (b - k != trimy)
+                {
+                    btrace[--btlen] = (uint16_t)(b - trimx);
+                    btrace[--btlen] = (uint16_t)(trimd - e);
+                }
+                else if (b != trimx)
+                {
+                    btrace[btlen + 1] = (uint16_t)(btrace[btlen + 1] + (b - trimx));
+                    btrace[btlen] = (uint16_t)(btrace[btlen] + (trimd - e));
+                }
+            }
+            apath->abpos = trimx;
+            apath->bbpos = trimy;
+            apath->diffs = apath->diffs + trimd;
+            apath->tlen = apath->tlen - atlen;
+            apath->toff = (int)(atrace + atlen - w.pts);
+            if (comp)
+            {
+                bpath->aepos = blen - apath->bbpos;
+                bpath->bepos = alen - apath->abpos;
+            }
+            else
+            {
+                bpath->abpos = apath->bbpos;
+                bpath->bbpos = apath->abpos;
+            }
+            bpath->diffs = bpath->diffs + trimd;
+            bpath->tlen = bpath->tlen - btlen;
+            bpath->toff = (int)(btrace + btlen - w.pts);
+        }
+    }
+    __syncwarp();
+    if (FWD)
+        *mind = w.sm->span_lo;
+}
+
+// Local_Alignment from one seed (diag, anti) with lbord = hbord = -1 (align.c:1922-2060).
+__device__ void local_alignment(WarpCtx& w, const AlignParams& P, const uint8_t* aseq, const uint8_t* bseq, int alen,
+                                int blen, int comp, int diag, int anti)
+{
+    const int TS = P.tspace;
+    int maxtp = 2 * (max(alen, blen) / TS + 2);
+    if (4 * maxtp + 16 > w.ptscap)
+    {
+        if (w.lane == 0)
+            gd_fail(w.st, GD_ERR_TRACE, w.item, maxtp);
+        w.err = 1;
+        return;
+    }
+    uint16_t* atrace = w.pts + maxtp;
+    uint16_t* btrace = atrace + 2 * maxtp;
+    LAPath* ap = &w.sm->ap;
+    LAPath* bp = &w.sm->bp;
+    int low = diag, hgh = diag;
+    bool selfie = (aseq == bseq);
+    int minp = (selfie && low >= 0) ? 1 : -INT_MAX;
+    int maxp = (selfie && hgh <= 0) ? -1 : INT_MAX;
+    if (w.lane == 0)
+    {
+        ap->tlen = bp->tlen = 0;
+        ap->diffs = bp->diffs = 0;
+    }
+    __syncwarp();
+    wave<true>(w, P, aseq, bseq, alen, blen, comp, ap, bp, &low, hgh, anti, minp, maxp, atrace, btrace);
+    if (w.err)
+        return;
+    wave<false>(w, P, aseq, bseq, alen, blen, comp, ap, bp, &low, low, anti, minp, maxp, atrace, btrace);
+    if (w.err)
+        return;
+    if (comp && w.lane == 0)
+    {
+        uint16_t* tr = w.pts + bp->toff;
+        int i = bp->tlen - 2, j = 0;
+        while (j < i)
+        {
+            uint16_t t = tr[i];
+            tr[i] = tr[j];
+            tr[j] = t;
+            t = tr[i + 1];
+            tr[i + 1] = tr[j + 1];
+            tr[j + 1] = t;
+            i -= 2;
+            j += 2;
+        }
+    }
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
+// per-pair redundancy handling (Entwine / Fusion / Handle_Redundancies, filter.c:1249-1566),
+// lane 0 only: O(n^2) over the few paths of one pair.
+// ------------------------------------------------------------------------------------------
+
+struct PairBuf
+{
+    MPath* am;
+    MPath* bm;
+    uint16_t* tb;
+    int ttop, tcap;
+    int err;
+};
+
+__device__ int entwine(const MPath* jpath, const MPath* kpath, const uint16_t* tb, int TS, int* where)
+{
+    int ac, b2, y2, ae, i, j, k, den = 0, min = 10000;
+    const uint16_t* ktrace = tb + kpath->toff;
+    const uint16_t* jtrace = tb + jpath->toff;
+    y2 = jpath->bbpos;
+    j = jpath->abpos / TS;
+    b2 = kpath->bbpos;
+    k = kpath->abpos / TS;
+    if (j < k)
+    {
+        ac = k * TS;
+        j = 1 + 2 * (k - j);
+        k = 1;
+        for (i = 1; i < j; i += 2)
+            y2 += jtrace[i];
+    }
+    else
+    {
+        ac = j * TS;
+        k = 1 + 2 * (j - k);
+        j = 1;
+        for (i = 1; i < k; i += 2)
+            b2 += ktrace[i];
+    }
+    ae = jpath->aepos;
+    if (ae > kpath->aepos)
+        ae = kpath->aepos;
+    while (1)
+    {
+        ac += TS;
+        if (ac >= ae)
+            break;
+        y2 += jtrace[j];
+        b2 += ktrace[k];
+        j += 2;
+        k += 2;
+        i = abs(y2 - b2);
+        if (i <= min)
+        {
+            min = i;
+            if (i == 0)
+                *where = ac;
+        }
+        den += 1;
+    }
+    return den == 0 ? -1 : min;
+}
+
+__device__ void fusion(MPath* p1, int ap, const MPath* p2, PairBuf& pb, int TS)
+{
+    int k1 = 2 * ((ap / TS) - (p1->abpos / TS));
+    int k2 = 2 * ((ap / TS) - (p2->abpos / TS));
+    int len = k1 + (p2->tlen - k2), diff = 0, k;
+    if (pb.ttop + len > pb.tcap)
+    {
+        pb.err = 1;
+        return;
+    }
+    int base = pb.ttop;
+    pb.ttop += len;
+    uint16_t* trace = pb.tb + base;
+    len = 0;
+    if (k1 > 0)
+    {
+        const uint16_t* t = pb.tb + p1->toff;
+        for (k = 0; k < k1; k += 2)
+        {
+            trace[len++] = t[k];
+            trace[len++] = t[k + 1];
+            diff += t[k];
+        }
+    }
+    if (k2 < p2->tlen)
+    {
+        const uint16_t* t = pb.tb + p2->toff;
+        for (k = k2; k < p2->tlen; k += 2)
+        {
+            trace[len++] = t[k];
+            trace[len++] = t[k + 1];
+            diff += t[k];
+        }
+    }
+    p1->aepos = p2->aepos;
+    p1->bepos = p2->bepos;
+    p1->diffs = diff;
+    p1->toff = base;
+    p1->tlen = len;
+}
+
+__device__ int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, PairBuf& pb, int TS, int comp)
+{
+    int j, k, no = 0, dist, awhen = 0, bwhen = 0;
+    bool hasB = (bmatch != nullptr);
+    for (j = 1; j < novls; j++)
+    {
+        MPath* jpath = amatch + j;
+        for (k = no; k >= 0; k--)
+        {
+            MPath* kpath = amatch + k;
+            if (jpath->abpos < kpath->abpos)
+            {
+                if (kpath->abpos <= jpath->aepos && kpath->bbpos <= jpath->bepos)
+                {
+                    dist = entwine(jpath, kpath, pb.tb, TS, &awhen);
+                    if (dist == 0)
+                    {
+                        if (kpath->aepos > jpath->aepos)
+                        {
+                            if (hasB)
+                            {
+                                if (comp)
+                                {
+                                    dist = entwine(bmatch + k, bmatch + j, pb.tb, TS, &bwhen);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(jpath, awhen, kpath, pb, TS);
+                                    amatch[k] = *jpath;
+                                    fusion(bmatch + k, bwhen, bmatch + j, pb, TS);
+                                }
+                                else
+                                {
+                                    dist = entwine(bmatch + j, bmatch + k, pb.tb, TS, &bwhen);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(jpath, awhen, kpath, pb, TS);
+                                    amatch[k] = *jpath;
+                                    fusion(bmatch + j, bwhen, bmatch + k, pb, TS);
+                                    bmatch[k] = bmatch[j];
+                                }
+                            }
+                            else
+                            {
+                                fusion(jpath, awhen, kpath, pb, TS);
+                                amatch[k] = *jpath;
+                            }
+                        }
+                        else
+                        {
+                            amatch[k] = *jpath;
+                            if (hasB)
+                                bmatch[k] = bmatch[j];
+                        }
+                        break;
+                    }
+                }
+            }
+            else
+            {
+                if (jpath->abpos <= kpath->aepos && jpath->bbpos <= kpath->bepos)
+                {
+                    dist = entwine(kpath, jpath, pb.tb, TS, &awhen);
+                    if (dist == 0)
+                    {
+                        if (kpath->abpos == jpath->abpos)
+                        {
+                            if (kpath->aepos < jpath->aepos)
+                            {
+                                amatch[k] = *jpath;
+                                if (hasB)
+                                    bmatch[k] = bmatch[j];
+                            }
+                        }
+                        else if (jpath->aepos > kpath->aepos)
+                        {
+                            if (hasB)
+                            {
+                                if (comp)
+                                {
+                                    dist = entwine(bmatch + j, bmatch + k, pb.tb, TS, &bwhen);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(kpath, awhen, jpath, pb, TS);
+                                    fusion(bmatch + j, bwhen, bmatch + k, pb, TS);
+                                    bmatch[k] = bmatch[j];
+                                }
+                                else
+                                {
+                                    dist = entwine(bmatch + k, bmatch + j, pb.tb, TS, &bwhen);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(kpath, awhen, jpath, pb, TS);
+                                    fusion(bmatch + k, bwhen, bmatch + j, pb, TS);
+                                }
+                            }
+                            else
+                                fusion(kpath, awhen, jpath, pb, TS);
+                        }
+                        break;
+                    }
+                }
+            }
+        }
+        if (k < 0)
+        {
+            no += 1;
+            amatch[no] = *jpath;
+            if (hasB)
+                bmatch[no] = bmatch[j];
+        }
+    }
+    return no + 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// the pair kernel
+// ------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ int hit_apos(uint64_t key, const HitBits& hb)
+{
+    return (int)(key & ((1ull << hb.pbits) - 1));
+}
+
+// first index in [lo, hi) whose apos exceeds x (apos ascending within a pair)
+__device__ __forceinline__ int first_above(const uint64_t* hkey, int lo, int hi, int x, const HitBits& hb)
+{
+    while (lo < hi)
+    {
+        int m = (lo + hi) >> 1;
+        if (hit_apos(hkey[m], hb) <= x)
+            lo = m + 1;
+        else
+            hi = m;
+    }
+    return lo;
+}
+
+__device__ void store_path(WarpCtx& w, const LAPath& lp, MPath* dst, PairBuf& pb)
+{
+    // all lanes: copy the trace into the pair buffer
+    if (pb.ttop + lp.tlen > pb.tcap)
+    {
+        pb.err = 1;
+        return;
+    }
+    for (int i = w.lane; i < lp.tlen; i += 32)
+        pb.tb[pb.ttop + i] = w.pts[lp.toff + i];
+    if (w.lane == 0)
+    {
+        dst->toff = pb.ttop;
+        dst->tlen = lp.tlen;
+        dst->diffs = lp.diffs;
+        dst->abpos = lp.abpos;
+        dst->bbpos = lp.bbpos;
+        dst->aepos = lp.aepos;
+        dst->bepos = lp.bepos;
+    }
+    pb.ttop += lp.tlen;
+}
+
+__device__ void emit_paths(WarpCtx& w, const AlignParams& P, const MPath* m, int n, const uint16_t* tb, int aread,
+                           int bread, AlignOut& out)
+{
+    if (n <= 0)
+        return;
+    int tlen_tot = 0;
+    if (!P.no_trace)
+        for (int i = 0; i < n; i++)
+            tlen_tot += m[i].tlen;
+    int tbytes = P.trace8 ? 1 : 2;
+    unsigned long long r0 = 0, t0 = 0;
+    if (w.lane == 0)
+    {
+        r0 = atomicAdd(&out.counters[0], (unsigned long long)n);
+        t0 = atomicAdd(&out.counters[1], (unsigned long long)tlen_tot * tbytes);
+    }
+    r0 = __shfl_sync(GD_FULL, r0, 0);
+    t0 = __shfl_sync(GD_FULL, t0, 0);
+    if (r0 + n > out.rcap || t0 + (unsigned long long)tlen_tot * tbytes > out.tcap)
+        return;  // the host sees the counters past capacity and re-runs with more room
+    unsigned long long toff = t0;
+    for (int i = 0; i < n; i++)
+    {
+        int tl = P.no_trace ? 0 : m[i].tlen;
+        if (w.lane == 0)
+        {
+            OutRec o;
+            o.tlen = tl;
+            o.diffs = m[i].diffs;
+            o.abpos = m[i].abpos;
+            o.bbpos = m[i].bbpos;
+            o.aepos = m[i].aepos;
+            o.bepos = m[i].bepos;
+            o.flags = (uint32_t)P.comp;
+            o.aread = aread;
+            o.bread = bread;
+            o.pad = 0;
+            o.toff = toff;
+            out.rec[r0 + i] = o;
+        }
+        const uint16_t* src = tb + m[i].toff;
+        if (P.trace8)
+            for (int j = w.lane; j < tl; j += 32)
+                out.trace[toff + j] = (uint8_t)src[j];  // Compress_TraceTo8 (align.c:3352-3360)
+        else
+            for (int j = w.lane; j < tl; j += 32)
+            {
+                out.trace[toff + 2 * j] = (uint8_t)(src[j] & 0xff);
+                out.trace[toff + 2 * j + 1] = (uint8_t)(src[j] >> 8);
+            }
+        toff += (unsigned long long)tl * tbytes;
+    }
+}
+
+__global__ void __launch_bounds__(ALIGN_WARPS * 32)
+    k_align_pairs(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
+                  const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
+                  AlignScratch sc, AlignOut out, unsigned* queue, DevStatus* st)
+{
+    __shared__ WarpSmem smem[ALIGN_WARPS];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int gw = blockIdx.x * ALIGN_WARPS + wib;
+    if (gw >= sc.nwarps)
+        return;
+    WarpCtx w;
+    w.sm = &smem[wib];
+    w.peb = sc.peb + (size_t)gw * sc.pcap;
+    w.pcap = sc.pcap;
+    w.pts = sc.pts + (size_t)gw * sc.ptscap;
+    w.ptscap = sc.ptscap;
+    w.st = st;
+    w.lane = lane;
+    w.err = 0;
+    w.cells = 0;
+    MPath* amatch = sc.match + (size_t)gw * 2 * sc.mcap;
+    MPath* bmatch = amatch + sc.mcap;
+    uint16_t* tbuf = sc.tbuf + (size_t)gw * sc.tcap;
+    int* score = sc.bands + (size_t)gw * 3 * sc.nbands - (P.mindiag - 2);
+    int* lastp = score + sc.nbands;
+    int* lasta = lastp + sc.nbands;
+    const int K = P.kmer, BS = P.binshift, TS = P.tspace;
+    const int minhit = (P.hitmin - 1) / K + 1;
+    const unsigned lt = lanemask_lt();
+    unsigned long long nseeds = 0;
+
+    while (true)
+    {
+        unsigned g = 0;
+        if (lane == 0)
+            g = atomicAdd(queue, 1u);
+        g = __shfl_sync(GD_FULL, g, 0);
+        if (g >= ngroups || st->code != 0)
+            break;
+        uint2 grp = groups[order[g]];
+        const int s = (int)grp.x, e = (int)grp.y;
+        w.item = (int)order[g];
+        uint64_t k0 = hkey[s];
+        const int ar = (int)((k0 >> P.hb.pbits) & ((1ull << P.hb.abits) - 1));
+        const int br = (int)(k0 >> (P.hb.pbits + P.hb.abits));
+        const int alen = A.rlen[ar], blen = B.rlen[br];
+        const uint8_t* aseq = A.bases + A.boff[ar];
+        const uint8_t* bseq = B.bases + B.boff[br];
+        const bool doB = P.symmetric && (ar != br || !P.self || !P.comp);
+        PairBuf pb;
+        pb.am = amatch;
+        pb.bm = bmatch;
+        pb.tb = tbuf;
+        pb.ttop = 0;
+        pb.tcap = sc.tcap;
+        pb.err = 0;
+        int novla = 0, novlb = 0;
+        int tlo = INT_MAX, thi = INT_MIN;  // lasta bands touched in this pair
+
+        int nidx = s, amark2 = 0;
+        while (nidx < e && !w.err && !pb.err)
+        {
+            int amark = amark2 + PANEL_SIZE;
+            amark2 = amark - PANEL_OVERLAP;
+            const int lidx = nidx;
+            int q = first_above(hkey, lidx, e, amark, P.hb);
+            const int nend = (q < e) ? q + 1 : e;
+            const int h2 = first_above(hkey, lidx, nend, amark2, P.hb);
+            if (nend - lidx < minhit)
+            {
+                nidx = h2;
+                continue;
+            }
+            // panel band scores (filter.c:1754-1766)
+            for (int base = lidx; base < nend; base += 32)
+            {
+                int i = base + lane;
+                bool valid = i < nend;
+                int ap = 0, dg = 0;
+                if (valid)
+                {
+                    ap = hit_apos(hkey[i], P.hb);
+                    dg = ((int)hdiag[i]) >> BS;
+                }
+                unsigned key = valid ? (unsigned)dg : (0x80000000u | (unsigned)lane);
+                unsigned peers = __match_any_sync(GD_FULL, key);
+                unsigned lower = peers & lt;
+                int src = lower ? 31 - __clz(lower) : lane;
+                int prevap = __shfl_sync(GD_FULL, ap, src);
+                int delta = 0;
+                if (valid)
+                {
+                    int prev = lower ? prevap : lastp[dg];
+                    delta = (ap - prev >= K) ? K : ap - prev;
+                }
+                unsigned todo = __ballot_sync(GD_FULL, valid);
+                while (todo)
+                {
+                    int leader = __ffs(todo) - 1;
+                    unsigned grpm = __shfl_sync(GD_FULL, peers, leader);
+                    int sum = __reduce_add_sync(GD_FULL, ((grpm >> lane) & 1) ? delta : 0);
+                    int last = 31 - __clz(grpm);
+                    int lastap = __shfl_sync(GD_FULL, ap, last);
+                    int gdg = __shfl_sync(GD_FULL, dg, leader);
+                    if (lane == 0)
+                    {
+                        score[gdg] += sum;
+                        lastp[gdg] = lastap;
+                    }
+                    todo &= ~grpm;
+                }
+                __syncwarp();
+            }
+            // seeds in hit order (filter.c:1776-1893)
+            for (int base = lidx; base < nend && !w.err && !pb.err; base += 32)
+            {
+                int i = base + lane;
+                bool valid = i < nend;
+                int ap = 0, d = 0, dg = 0;
+                bool cand = false;
+                if (valid)
+                {
+                    ap = hit_apos(hkey[i], P.hb);
+                    d = (int)hdiag[i];
+                    dg = d >> BS;
+                    int sc0 = score[dg];
+                    cand = (sc0 + score[dg + 1] >= P.hitmin) || (sc0 + score[dg - 1] >= P.hitmin);
+                }
+                unsigned cm = __ballot_sync(GD_FULL, cand);
+                while (cm && !w.err && !pb.err)
+                {
+                    int j = __ffs(cm) - 1;
+                    cm &= cm - 1;
+                    int apj = __shfl_sync(GD_FULL, ap, j);
+                    int dj = __shfl_sync(GD_FULL, d, j);
+                    int dgj = dj >> BS;
+                    if (!(apj > lasta[dgj]))
+                        continue;
+                    nseeds++;
+                    int bpj = apj - dj;
+                    local_alignment(w, P, aseq, bseq, alen, blen, P.comp, dj, apj + bpj);
+                    if (w.err)
+                        break;
+                    const LAPath apth = w.sm->ap;
+                    const LAPath bpth = w.sm->bp;
+                    // Diagonal_Span (filter.c:1568-1599) of the A path, then widen lasta
+                    int lo, hi;
+                    {
+                        const uint16_t* points = w.pts + apth.toff;
+                        int dd = apth.abpos - apth.bbpos, low = dd, hgh = dd;
+                        dd = apth.aepos - apth.bepos;
+                        if (dd < low)
+                            low = dd;
+                        else if (dd > hgh)
+                            hgh = dd;
+                        dd = (apth.abpos / TS) * TS - apth.bbpos;
+                        int tl = apth.tlen - 2;
+                        // prefix sums of (TS - points[2i+1]) in lane chunks
+                        for (int b0 = 1; b0 < tl; b0 += 64)
+                        {
+                            int idx = b0 + 2 * lane;
+                            int v = (idx < tl) ? (TS - (int)points[idx]) : 0;
+                            int x = v;
+#pragma unroll
+                            for (int o = 1; o < 32; o <<= 1)
+                            {
+                                int t = __shfl_up_sync(GD_FULL, x, o);
+                                if (lane >= o)
+                                    x += t;
+                            }
+                            int val = dd + x;
+                            int vlo = (idx < tl) ? val : INT_MAX, vhi = (idx < tl) ? val : INT_MIN;
+                            vlo = __reduce_min_sync(GD_FULL, vlo);
+                            vhi = __reduce_max_sync(GD_FULL, vhi);
+                            low = min(low, vlo);
+                            hgh = max(hgh, vhi);
+                            dd = __shfl_sync(GD_FULL, val, 31);
+                        }
+                        lo = (low >> BS) - 1;
+                        hi = (hgh >> BS) + 1;
+                    }
+                    if (dgj < lo)
+                        lo = dgj;
+                    else if (dgj > hi)
+                        hi = dgj;
+                    // the reference's band arrays end one band past each side (filter.c:2296-2311)
+                    lo = max(lo, P.mindiag - 1);
+                    hi = min(hi, P.maxdiag + 1);
+                    const int ae = apth.aepos;
+                    for (int dd2 = lo + lane; dd2 <= hi; dd2 += 32)
+                        if (ae > lasta[dd2])
+                            lasta[dd2] = ae;
+                    tlo = min(tlo, lo);
+                    thi = max(thi, hi);
+                    __syncwarp();
+                    if ((apth.aepos - apth.abpos) + (apth.bepos - apth.bbpos) >= P.minover)
+                    {
+                        if (novla >= sc.mcap || (doB && novlb >= sc.mcap))
+                        {
+                            if (lane == 0)
+                                gd_fail(st, GD_ERR_MATCHES, w.item, sc.mcap);
+                            w.err = 1;
+                            break;
+                        }
+                        store_path(w, apth, amatch + novla, pb);
+                        novla++;
+                        if (doB)
+                        {
+                            store_path(w, bpth, bmatch + novlb, pb);
+                            novlb++;
+                        }
+                        __syncwarp();
+                        if (pb.err)
+                        {
+                            if (lane == 0)
+                                gd_fail(st, GD_ERR_TRACE, w.item, sc.tcap);
+                            w.err = 1;
+                            break;
+                        }
+                    }
+                }
+            }
+            // reset the panel's band scores (filter.c:1895-1899)
+            for (int i = lidx + lane; i < nend; i += 32)
+            {
+                int dg = ((int)hdiag[i]) >> BS;
+                score[dg] = 0;
+                lastp[dg] = 0;
+            }
+            __syncwarp();
+            nidx = h2;
+        }
+        // reset lasta (filter.c:1902-1920): every band this pair raised
+        if (tlo <= thi)
+            for (int dd2 = tlo + lane; dd2 <= thi; dd2 += 32)
+                lasta[dd2] = 0;
+        if (nidx < e)  // aborted pair: clear score/lastp of all its hits
+            for (int i = s + lane; i < e; i += 32)
+            {
+                int dg = ((int)hdiag[i]) >> BS;
+                score[dg] = 0;
+                lastp[dg] = 0;
+            }
+        __syncwarp();
+        if (w.err)
+            break;
+        // merge redundant paths (filter.c:1922-1938), lane 0
+        if (lane == 0)
+        {
+            if (novla > 1)
+            {
+                if (novlb > 1)
+                    novla = novlb = handle_redundancies(amatch, novla, bmatch, pb, TS, P.comp);
+                else
+                    novla = handle_redundancies(amatch, novla, nullptr, pb, TS, P.comp);
+            }
+            else if (novlb > 1)
+                novlb = handle_redundancies(bmatch, novlb, nullptr, pb, TS, P.comp);
+            if (pb.err)
+                gd_fail(st, GD_ERR_TRACE, w.item, sc.tcap);
+        }
+        novla = __shfl_sync(GD_FULL, novla, 0);
+        novlb = __shfl_sync(GD_FULL, novlb, 0);
+        __syncwarp();
+        emit_paths(w, P, amatch, novla, tbuf, ar + A.ufirst, br + B.ufirst, out);
+        emit_paths(w, P, bmatch, novlb, tbuf, br + B.ufirst, ar + A.ufirst, out);
+        __syncwarp();
+    }
+    if (lane == 0)
+    {
+        atomicAdd(&out.counters[2], (unsigned long long)w.cells);
+        atomicAdd(&out.counters[3], nseeds);
+    }
+}
+
+size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands)
+{
+    size_t per = (size_t)pcap * sizeof(int4) + (size_t)ptscap * 2 + (size_t)2 * mcap * sizeof(MPath) +
+                 (size_t)tcap * 2 + (size_t)3 * nbands * 4 + 4 * 256;
+    return per * nwarps + 4096;
+}
+
+static inline char* align_up(char* p, size_t a)
+{
+    return (char*)(((uintptr_t)p + a - 1) & ~(uintptr_t)(a - 1));
+}
+
+void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands)
+{
+    char* p = align_up((char*)base, 256);
+    s->nwarps = nwarps;
+    s->pcap = pcap;
+    s->peb = (int4*)p;
+    p = align_up(p + (size_t)pcap * sizeof(int4) * nwarps, 256);
+    s->ptscap = ptscap;
+    s->pts = (uint16_t*)p;
+    p = align_up(p + (size_t)ptscap * 2 * nwarps, 256);
+    s->mcap = mcap;
+    s->match = (MPath*)p;
+    p = align_up(p + (size_t)2 * mcap * sizeof(MPath) * nwarps, 256);
+    s->tcap = tcap;
+    s->tbuf = (uint16_t*)p;
+    p = align_up(p + (size_t)tcap * 2 * nwarps, 256);
+    s->nbands = nbands;
+    s->bands = (int*)p;
+}
+
+int align_grid(int* grid_out)
+{
+    int dev = 0, nsm = 0, per = 0;
+    GD_CUDA(cudaGetDevice(&dev));
+    GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_align_pairs, ALIGN_WARPS * 32, 0));
+    if (per < 1)
+        per = 1;
+    *grid_out = nsm * per;
+    return 0;
+}
+
+int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hkey, const uint32_t* hdiag,
+                       const uint2* groups, const uint32_t* order, unsigned ngroups, AlignParams p, AlignScratch sc,
+                       AlignOut out, unsigned* queue, DevStatus* st, int grid, cudaStream_t s)
+{
+    GD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), s));
+    if (ngroups == 0)
+        return 0;
+    k_align_pairs<<<grid, ALIGN_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p, sc, out, queue, st);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// ------------------------------------------------------------------------------------------
+// Local_Alignment batch (tests)
+// ------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(ALIGN_WARPS * 32)
+    k_la_batch(const uint8_t* abase, const int64_t* aoff, const int32_t* alen, const uint8_t* bbase,
+               const int64_t* boff, const int32_t* blen, const int32_t* diag, const int32_t* anti, int nseeds,
+               AlignParams P, AlignScratch sc, int32_t* out12, uint16_t* tr, int trstride, int64_t* cells,
+               DevStatus* st)
+{
+    __shared__ WarpSmem smem[ALIGN_WARPS];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int gw = blockIdx.x * ALIGN_WARPS + wib;
+    if (gw >= sc.nwarps)
+        return;
+    WarpCtx w;
+    w.sm = &smem[wib];
+    w.peb = sc.peb + (size_t)gw * sc.pcap;
+    w.pcap = sc.pcap;
+    w.pts = sc.pts + (size_t)gw * sc.ptscap;
+    w.ptscap = sc.ptscap;
+    w.st = st;
+    w.lane = lane;
+    for (int sd = gw; sd < nseeds; sd += sc.nwarps)
+    {
+        w.err = 0;
+        w.cells = 0;
+        w.item = sd;
+        const uint8_t* aseq = abase + aoff[sd];
+        const uint8_t* bseq = bbase + boff[sd];
+        local_alignment(w, P, aseq, bseq, alen[sd], blen[sd], P.comp, diag[sd], anti[sd]);
+        if (w.err)
+            continue;
+        LAPath a = w.sm->ap, b = w.sm->bp;
+        if (lane == 0)
+        {
+            int32_t* o = out12 + 12 * (size_t)sd;
+            o[0] = a.abpos;
+            o[1] = a.bbpos;
+            o[2] = a.aepos;
+            o[3] = a.bepos;
+            o[4] = a.diffs;
+            o[5] = a.tlen;
+            o[6] = b.abpos;
+            o[7] = b.bbpos;
+            o[8] = b.aepos;
+            o[9] = b.bepos;
+            o[10] = b.diffs;
+            o[11] = b.tlen;
+            cells[sd] = w.cells;
+        }
+        uint16_t* ta = tr + (size_t)sd * trstride;
+        uint16_t* tb = ta + trstride / 2;
+        for (int i = lane; i < a.tlen && i < trstride / 2; i += 32)
+            ta[i] = w.pts[a.toff + i];
+        for (int i = lane; i < b.tlen && i < trstride / 2; i += 32)
+            tb[i] = w.pts[b.toff + i];
+        __syncwarp();
+    }
+}
+
+int launch_la_batch(const uint8_t* aseq_base, const int64_t* aoff, const int32_t* alen, const uint8_t* bseq_base,
+                    const int64_t* boff, const int32_t* blen, const int32_t* diag, const int32_t* anti, int nseeds,
+                    AlignParams p, AlignScratch sc, int32_t* out12, uint16_t* tr, int trstride, int64_t* cells,
+                    DevStatus* st, cudaStream_t s)
+{
+    if (nseeds <= 0)
+        return 0;
+    int grid = gd_cdiv(sc.nwarps, ALIGN_WARPS);
+    k_la_batch<<<grid, ALIGN_WARPS * 32, 0, s>>>(aseq_base, aoff, alen, bseq_base, boff, blen, diag, anti, nseeds, p, sc,
+                                                 out12, tr, trstride, cells, st);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace gd

@@ -1,0 +1,82 @@
+// gd_align.cuh -- warp-per-pair seed scan and adaptive-wave aligner for sm_100a.
+#pragma once
+#include "gd_common.cuh"
+#include "gd_filter.cuh"
+
+namespace gd
+{
+
+constexpr int RING = 256;           // wave-vector ring per warp (diagonal k lives at k & (RING-1))
+constexpr int WAVE_CHUNKS = 4;      // band width up to 32 * WAVE_CHUNKS diagonals per wave
+constexpr int ALIGN_WARPS = 4;      // warps per CTA of the aligner
+constexpr int TRIM_TABLE = 1 << 15; // TRIM_MASK + 1 (dalign/align.c:154)
+
+// One path as Local_Alignment returns it (dalign/align.h:76-83); trace is an offset into
+// the owning buffer.
+struct MPath
+{
+    int32_t toff, tlen, diffs, abpos, bbpos, aepos, bepos, pad;
+};
+
+// One output overlap record (the 40-byte .las record plus where its trace bytes are).
+struct OutRec
+{
+    int32_t tlen, diffs, abpos, bbpos, aepos, bepos;
+    uint32_t flags;
+    int32_t aread, bread, pad;
+    uint64_t toff;
+};
+
+struct AlignParams
+{
+    int tspace, ave_path, kmer, binshift, hitmin, minover;
+    int symmetric, self, comp, trace8, no_trace;
+    int mindiag, maxdiag;  // band range of the block pair: (-maxlen_B >> w) .. (maxlen_A >> w)
+    HitBits hb;
+    const int16_t* table;  // TABLE and SCORE trim tables (set_table, dalign/align.c:196-210)
+    const int16_t* score;
+};
+
+// Per-warp global scratch, carved from one allocation.
+struct AlignScratch
+{
+    int4* peb;         // pebbles {ptr, diag, diff, mark}
+    int pcap;
+    uint16_t* pts;     // Local_Alignment trace points (4 * maxtp + 16 per warp)
+    int ptscap;
+    MPath* match;      // amatch | bmatch, mcap each
+    int mcap;
+    uint16_t* tbuf;    // per-pair trace buffer
+    int tcap;
+    int* bands;        // score | lastp | lasta, each nbands ints
+    int nbands;
+    int nwarps;
+};
+
+struct AlignOut
+{
+    OutRec* rec;
+    uint8_t* trace;
+    unsigned long long* counters;  // [0] records, [1] trace bytes, [2] cells, [3] seeds, [4] LA calls kept
+    uint64_t rcap, tcap;
+};
+
+size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands);
+void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands);
+
+// Persistent seed-scan + alignment over the ordered pair groups.
+int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hkey, const uint32_t* hdiag,
+                       const uint2* groups, const uint32_t* order, unsigned ngroups, AlignParams p, AlignScratch sc,
+                       AlignOut out, unsigned* queue, DevStatus* st, int grid, cudaStream_t s);
+
+// One Local_Alignment per seed (for parity tests of the wave alone).  out12 per seed:
+// A-path {abpos,bbpos,aepos,bepos,diffs,tlen}, B-path the same; traces at
+// tr + seed * trstride (A) and tr + seed * trstride + trstride/2 (B).
+int launch_la_batch(const uint8_t* aseq_base, const int64_t* aoff, const int32_t* alen, const uint8_t* bseq_base,
+                    const int64_t* boff, const int32_t* blen, const int32_t* diag, const int32_t* anti, int nseeds,
+                    AlignParams p, AlignScratch sc, int32_t* out12, uint16_t* tr, int trstride, int64_t* cells,
+                    DevStatus* st, cudaStream_t s);
+
+int align_grid(int* grid_out);
+
+}  // namespace gd

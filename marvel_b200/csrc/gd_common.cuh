@@ -1,0 +1,87 @@
+// gd_common.cuh -- shared device types and helpers of the sm_100a overlap path.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#define GD_WARP 32
+#define GD_FULL 0xffffffffu
+
+#define GD_CUDA(call)                                                                          \
+    do                                                                                         \
+    {                                                                                          \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+        {                                                                                      \
+            gd_set_error("%s:%d: CUDA error %s: %s", __FILE__, __LINE__, cudaGetErrorName(e_), \
+                         cudaGetErrorString(e_));                                              \
+            return -1;                                                                         \
+        }                                                                                      \
+    } while (0)
+
+void gd_set_error(const char* fmt, ...);
+
+// A DB block resident in HBM, laid out like the reference's in-memory block
+// (db/DB.c:1349-1410): one byte per base (0..3), a 4 before read 0 and after every read,
+// read i at bases[boff[i]].  The allocation carries 16 bytes of slack on each side so
+// that 8-byte windows around any base stay in bounds.
+struct DevBlock
+{
+    const uint8_t* bases;
+    const int64_t* boff;
+    const int32_t* rlen;
+    int32_t nreads;
+    int32_t maxlen;
+    int32_t ufirst;
+};
+
+// Device-side error status shared by all kernels of a context.  Kernels never trap:
+// they record the first failure here and skip the remaining work.
+struct DevStatus
+{
+    int32_t code;   // 0 = ok
+    int32_t where;  // pair index or item that failed
+    int32_t info;
+    int32_t pad;
+};
+
+enum
+{
+    GD_ERR_OK = 0,
+    GD_ERR_BAND_WIDTH = 1,   // wave band wider than the register tile
+    GD_ERR_PEBBLES = 2,      // pebble arena exhausted
+    GD_ERR_TRACE = 3,        // trace scratch exhausted
+    GD_ERR_MATCHES = 4,      // per-pair path list exhausted
+    GD_ERR_OUTPUT = 5,       // overlap output buffer exhausted
+    GD_ERR_EMPTY_BAND = 6,   // wave band emptied while the wave continues
+    GD_ERR_RING = 7,         // band left the ring window
+};
+
+__device__ __forceinline__ void gd_fail(DevStatus* st, int code, int where, int info)
+{
+    if (atomicCAS(&st->code, 0, code) == 0)
+    {
+        st->where = where;
+        st->info = info;
+    }
+}
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ int lane_id()
+{
+    int l;
+    asm("mov.u32 %0, %%laneid;" : "=r"(l));
+    return l;
+}
+
+template <typename T>
+__host__ __device__ inline T gd_cdiv(T a, T b)
+{
+    return (a + b - 1) / b;
+}

@@ -1,0 +1,481 @@
+// gd_filter.cu -- k-mer filter kernels for sm_100a.
+//
+// Restates dalign/filter.c's index build (tuple_thread :400-490, Sort_Kmers :698-903) and
+// A x B merge (count_thread :948-1056, merge_thread :1061-1231) as data-parallel passes
+// over HBM-resident arrays: one thread per k-mer slot for extraction, one thread per index
+// entry for the join, with binary searches replacing the reference's merge cursors.
+#include "gd_filter.cuh"
+
+namespace gd
+{
+
+constexpr int FT = 256;
+
+__device__ __forceinline__ int64_t kstart_of(const DevBlock& b, int r, int K)
+{
+    return b.boff[r] - (int64_t)K * r;
+}
+
+// largest r in [0, nreads) with kstart(r) <= s
+__device__ __forceinline__ int read_of_slot(const DevBlock& b, int64_t s, int K)
+{
+    int lo = 0, hi = b.nreads - 1;
+    while (lo < hi)
+    {
+        int mid = (lo + hi + 1) >> 1;
+        if (kstart_of(b, mid, K) <= s)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(FT) k_extract(DevBlock b, const int64_t* __restrict__ mask_anno,
+                                               const int32_t* __restrict__ mask_data, int kmer, K* keys, uint32_t* vals,
+                                               int64_t nslots, uint32_t* nmasked)
+{
+    int64_t s = (int64_t)blockIdx.x * FT + threadIdx.x;
+    bool masked = false;
+    if (s < nslots)
+    {
+        int r = read_of_slot(b, s, kmer);
+        int rpos = (int)(s - kstart_of(b, r, kmer)) + kmer - 1;
+        int p0 = rpos - kmer + 1;
+        if (mask_anno)
+        {
+            // the segment of unmasked bases containing p0 must also contain rpos
+            // (segments [0,b0) [e0,b1) ... [e_last,rlen), tuple_thread's loop :428-457)
+            int64_t f0 = mask_anno[r], f1 = mask_anno[r + 1];
+            int q = b.rlen[r];
+            int p = 0;
+            for (int64_t a = f0; a < f1; a += 2)
+            {
+                int ib = mask_data[a], ie = mask_data[a + 1];
+                if (p0 < ib)
+                {
+                    q = ib;
+                    break;
+                }
+                p = ie;
+                q = b.rlen[r];
+            }
+            masked = !(p0 >= p && rpos < q);
+        }
+        const uint8_t* src = b.bases + b.boff[r] + p0;
+        K c = 0;
+        for (int j = 0; j < kmer; j++)
+            c = (c << 2) | (K)src[j];
+        keys[s] = masked ? (K)~(K)0 : c;
+        vals[s] = (uint32_t)s;
+    }
+    unsigned m = __ballot_sync(GD_FULL, masked);
+    if (m && lane_id() == 0)
+        atomicAdd(nmasked, (unsigned)__popc(m));
+}
+
+template <typename K>
+int launch_extract(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, int kmer, K* keys,
+                   uint32_t* vals, int64_t nslots, uint32_t* nmasked, cudaStream_t s)
+{
+    GD_CUDA(cudaMemsetAsync(nmasked, 0, sizeof(uint32_t), s));
+    if (nslots <= 0)
+        return 0;
+    k_extract<K><<<(unsigned)gd_cdiv<int64_t>(nslots, FT), FT, 0, s>>>(b, mask_anno, mask_data, kmer, keys, vals,
+                                                                        nslots, nmasked);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_decode(DevBlock b, int kmer, const uint32_t* __restrict__ slots, int64_t n,
+                                              int32_t* read, int32_t* rpos)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= n)
+        return;
+    int64_t s = slots[i];
+    int r = read_of_slot(b, s, kmer);
+    read[i] = r;
+    rpos[i] = (int)(s - kstart_of(b, r, kmer)) + kmer - 1;
+}
+
+template <typename K>
+int launch_decode(const DevBlock& b, int kmer, const uint32_t* slots, int64_t n, int32_t* read, int32_t* rpos,
+                  cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_decode<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(b, kmer, slots, n, read, rpos);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename K>
+__device__ __forceinline__ int64_t lower_code(const K* a, int64_t n, K x)
+{
+    int64_t l = 0, r = n;
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] < x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
+template <typename K>
+__device__ __forceinline__ int64_t upper_code(const K* a, int64_t n, K x)
+{
+    int64_t l = 0, r = n;
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] <= x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(FT) k_suppress(const K* __restrict__ code, int64_t n, int t, uint32_t* keep)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= n)
+        return;
+    K c = code[i];
+    int64_t lo = lower_code(code, n, c), hi = upper_code(code, n, c);
+    keep[i] = (hi - lo) < t;
+}
+
+template <typename K>
+int launch_suppress_flags(const K* code, int64_t n, int t, uint32_t* keep, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_suppress<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(code, n, t, keep);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(FT) k_compact_index(const K* code, const int32_t* read, const int32_t* rpos,
+                                                     const uint32_t* keep, const uint32_t* pos, int64_t n, K* code2,
+                                                     int32_t* read2, int32_t* rpos2)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= n || !keep[i])
+        return;
+    uint32_t d = pos[i];
+    code2[d] = code[i];
+    read2[d] = read[i];
+    rpos2[d] = rpos[i];
+}
+
+template <typename K>
+int launch_compact_index(const K* code, const int32_t* read, const int32_t* rpos, const uint32_t* keep,
+                         const uint32_t* pos, int64_t n, K* code2, int32_t* read2, int32_t* rpos2, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_compact_index<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(code, read, rpos, keep, pos, n, code2, read2,
+                                                                         rpos2);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(FT) k_run_flags(const K* __restrict__ code, int64_t n, uint32_t* flags)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i < n)
+        flags[i] = (i == 0 || code[i] != code[i - 1]) ? 1u : 0u;
+}
+
+template <typename K>
+int launch_run_flags(const K* code, int64_t n, uint32_t* flags, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_run_flags<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(code, n, flags);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// For A entry i: the B range with the same code and how many of its entries pair with i.
+template <typename K>
+__global__ void __launch_bounds__(FT) k_pair_count(const K* __restrict__ acode, const int32_t* __restrict__ aread,
+                                                  const int32_t* __restrict__ arpos, const uint32_t* __restrict__ arun_excl,
+                                                  const uint32_t* __restrict__ arun_flag, const K* __restrict__ bcode,
+                                                  const int32_t* __restrict__ bread, const int32_t* __restrict__ brpos,
+                                                  MergeArgs m, uint32_t* jb_out, uint64_t* cnt_out,
+                                                  unsigned long long* ctrun)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    bool act = i < m.na;
+    uint64_t n = 0;
+    uint32_t run = 0;
+    if (act)
+    {
+        K c = acode[i];
+        int64_t jb = lower_code(bcode, m.nb, c);
+        int64_t je = jb;
+        if (jb < m.nb && bcode[jb] == c)
+            je = upper_code(bcode, m.nb, c);
+        int ar = aread[i], ap = arpos[i];
+        int64_t e = je;
+        if (m.self)
+        {
+            // prefix of the B run pairing with this A entry (dalign/filter.c:984-998)
+            int64_t l = jb, r = je;
+            if (m.identity && m.comp)
+            {
+                while (l < r)
+                {
+                    int64_t md = (l + r) >> 1;
+                    if (bread[md] <= ar)
+                        l = md + 1;
+                    else
+                        r = md;
+                }
+            }
+            else if (m.identity)
+            {
+                while (l < r)
+                {
+                    int64_t md = (l + r) >> 1;
+                    int br = bread[md];
+                    if (br < ar || (br == ar && brpos[md] < ap))
+                        l = md + 1;
+                    else
+                        r = md;
+                }
+            }
+            else
+            {
+                while (l < r)
+                {
+                    int64_t md = (l + r) >> 1;
+                    if (bread[md] < ar)
+                        l = md + 1;
+                    else
+                        r = md;
+                }
+            }
+            e = l;
+        }
+        n = (uint64_t)(e - jb);
+        jb_out[i] = (uint32_t)jb;
+        cnt_out[i] = n;
+        run = arun_excl[i] + arun_flag[i] - 1;
+    }
+    // warp-aggregated per-run sums
+    unsigned long long key = act ? (unsigned long long)run : ~0ull;
+    unsigned peers = __match_any_sync(GD_FULL, key);
+    unsigned long long tot = 0;
+    for (unsigned mm = peers; mm; mm &= mm - 1)
+        tot += __shfl_sync(peers, n, __ffs(mm) - 1);
+    if (act && (peers & lanemask_lt()) == 0 && tot)
+        atomicAdd(&ctrun[run], tot);
+}
+
+template <typename K>
+int launch_pair_count(const K* acode, const int32_t* aread, const int32_t* arpos, const uint32_t* arun_excl,
+                      const uint32_t* arun_flag, const K* bcode, const int32_t* bread, const int32_t* brpos,
+                      MergeArgs m, uint32_t* jb, uint64_t* cnt, unsigned long long* ctrun, cudaStream_t s)
+{
+    if (m.na <= 0)
+        return 0;
+    k_pair_count<K><<<(unsigned)gd_cdiv<int64_t>(m.na, FT), FT, 0, s>>>(acode, aread, arpos, arun_excl, arun_flag,
+                                                                         bcode, bread, brpos, m, jb, cnt, ctrun);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_gram(const unsigned long long* ctrun, int64_t nruns, unsigned long long* gram)
+{
+    int64_t r = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (r < nruns)
+    {
+        unsigned long long c = ctrun[r];
+        if (c < (unsigned long long)MAXGRAM)
+            atomicAdd(&gram[c], 1ull);
+    }
+}
+
+int launch_gram(const unsigned long long* ctrun, int64_t nruns, unsigned long long* gram, cudaStream_t s)
+{
+    GD_CUDA(cudaMemsetAsync(gram, 0, sizeof(unsigned long long) * MAXGRAM, s));
+    if (nruns <= 0)
+        return 0;
+    k_gram<<<(unsigned)gd_cdiv<int64_t>(nruns, FT), FT, 0, s>>>(ctrun, nruns, gram);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_cnt_mask(const uint32_t* arun_excl, const uint32_t* arun_flag,
+                                                const unsigned long long* ctrun, int64_t na, int limit, int always,
+                                                uint64_t* cnt)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= na)
+        return;
+    uint32_t run = arun_excl[i] + arun_flag[i] - 1;
+    if (!always && ctrun[run] >= (unsigned long long)limit)
+        cnt[i] = 0;
+}
+
+int launch_cnt_mask(const uint32_t* arun_excl, const uint32_t* arun_flag, const unsigned long long* ctrun, int64_t na,
+                    int limit, int always, uint64_t* cnt, cudaStream_t s)
+{
+    if (na <= 0)
+        return 0;
+    k_cnt_mask<<<(unsigned)gd_cdiv<int64_t>(na, FT), FT, 0, s>>>(arun_excl, arun_flag, ctrun, na, limit, always, cnt);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_emit(const int32_t* __restrict__ aread, const int32_t* __restrict__ arpos,
+                                            const int32_t* __restrict__ bread, const int32_t* __restrict__ brpos,
+                                            const uint32_t* __restrict__ jb, const uint64_t* __restrict__ cnt,
+                                            const uint64_t* __restrict__ hoff, int64_t na, HitBits hb,
+                                            uint64_t* hkey, uint32_t* hdiag)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= na)
+        return;
+    uint64_t n = cnt[i];
+    if (!n)
+        return;
+    uint64_t o = hoff[i];
+    int ar = aread[i], ap = arpos[i];
+    uint64_t akey = ((uint64_t)ar << hb.pbits) | (uint64_t)ap;
+    int sh = hb.pbits + hb.abits;
+    uint32_t b0 = jb[i];
+    for (uint64_t j = 0; j < n; j++)
+    {
+        uint32_t b = b0 + (uint32_t)j;
+        hkey[o + j] = ((uint64_t)bread[b] << sh) | akey;
+        hdiag[o + j] = (uint32_t)(ap - brpos[b]);
+    }
+}
+
+int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread, const int32_t* brpos,
+                const uint32_t* jb, const uint64_t* cnt, const uint64_t* hoff, int64_t na, HitBits hb,
+                uint64_t* hkey, uint32_t* hdiag, cudaStream_t s)
+{
+    if (na <= 0)
+        return 0;
+    k_emit<<<(unsigned)gd_cdiv<int64_t>(na, FT), FT, 0, s>>>(aread, arpos, bread, brpos, jb, cnt, hoff, na, hb, hkey,
+                                                             hdiag);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_pair_flags(const uint64_t* __restrict__ hkey, int64_t n, int pbits,
+                                                  uint32_t* flags)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i < n)
+        flags[i] = (i == 0 || (hkey[i] >> pbits) != (hkey[i - 1] >> pbits)) ? 1u : 0u;
+}
+
+int launch_pair_flags(const uint64_t* hkey, int64_t n, int pbits, uint32_t* flags, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_pair_flags<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(hkey, n, pbits, flags);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_pair_scatter(const uint32_t* flags, const uint32_t* pos, int64_t n,
+                                                    uint32_t* starts)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i < n && flags[i])
+        starts[pos[i]] = (uint32_t)i;
+}
+
+int launch_pair_scatter(const uint32_t* flags, const uint32_t* pos, int64_t n, uint32_t* starts, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_pair_scatter<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(flags, pos, n, starts);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_select_groups(const uint32_t* __restrict__ starts, int64_t nstarts,
+                                                     int64_t nhits, int minhit, const uint64_t* __restrict__ hkey,
+                                                     HitBits hb, const int32_t* __restrict__ arlen,
+                                                     const int32_t* __restrict__ brlen, uint2* groups, uint32_t* cost,
+                                                     uint32_t* idx, unsigned int* ngroups)
+{
+    int64_t g = (int64_t)blockIdx.x * FT + threadIdx.x;
+    bool take = false;
+    uint32_t s = 0, e = 0, c = 0;
+    if (g < nstarts)
+    {
+        s = starts[g];
+        e = (g + 1 < nstarts) ? starts[g + 1] : (uint32_t)nhits;
+        take = (int64_t)(e - s) >= minhit;
+        if (take)
+        {
+            uint64_t k = hkey[s];
+            int ar = (int)((k >> hb.pbits) & ((1ull << hb.abits) - 1));
+            int br = (int)(k >> (hb.pbits + hb.abits));
+            c = (uint32_t)(arlen[ar] + brlen[br]);
+        }
+    }
+    unsigned m = __ballot_sync(GD_FULL, take);
+    unsigned base = 0;
+    if (m)
+    {
+        if (lane_id() == 0)
+            base = atomicAdd(ngroups, (unsigned)__popc(m));
+        base = __shfl_sync(GD_FULL, base, 0);
+    }
+    if (take)
+    {
+        unsigned slot = base + __popc(m & lanemask_lt());
+        groups[slot] = make_uint2(s, e);
+        cost[slot] = ~c;  // ascending sort of ~cost = longest pairs first
+        idx[slot] = slot;
+    }
+}
+
+int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* hkey,
+                         HitBits hb, const int32_t* arlen, const int32_t* brlen, uint2* groups, uint32_t* cost,
+                         uint32_t* idx, unsigned int* ngroups, cudaStream_t s)
+{
+    GD_CUDA(cudaMemsetAsync(ngroups, 0, sizeof(unsigned), s));
+    if (nstarts <= 0)
+        return 0;
+    k_select_groups<<<(unsigned)gd_cdiv<int64_t>(nstarts, FT), FT, 0, s>>>(starts, nstarts, nhits, minhit, hkey, hb,
+                                                                           arlen, brlen, groups, cost, idx, ngroups);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+#define INST(K)                                                                                                  \
+    template int launch_extract<K>(const DevBlock&, const int64_t*, const int32_t*, int, K*, uint32_t*, int64_t, \
+                                   uint32_t*, cudaStream_t);                                                     \
+    template int launch_decode<K>(const DevBlock&, int, const uint32_t*, int64_t, int32_t*, int32_t*,            \
+                                  cudaStream_t);                                                                 \
+    template int launch_suppress_flags<K>(const K*, int64_t, int, uint32_t*, cudaStream_t);                      \
+    template int launch_compact_index<K>(const K*, const int32_t*, const int32_t*, const uint32_t*,              \
+                                         const uint32_t*, int64_t, K*, int32_t*, int32_t*, cudaStream_t);        \
+    template int launch_run_flags<K>(const K*, int64_t, uint32_t*, cudaStream_t);                                \
+    template int launch_pair_count<K>(const K*, const int32_t*, const int32_t*, const uint32_t*, const uint32_t*, \
+                                      const K*, const int32_t*, const int32_t*, MergeArgs, uint32_t*, uint64_t*, \
+                                      unsigned long long*, cudaStream_t);
+INST(uint32_t)
+INST(uint64_t)
+#undef INST
+
+}  // namespace gd

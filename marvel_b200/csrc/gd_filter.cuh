@@ -1,0 +1,65 @@
+// gd_filter.cuh -- device kernels of the k-mer filter (dalign/filter.c restated for sm_100a).
+#pragma once
+#include "gd_common.cuh"
+
+namespace gd
+{
+
+constexpr int MAXGRAM = 10000;  // cap on per-code pair counts (dalign/filter.c:20)
+
+// k-mer slots: read r owns slots [kstart[r], kstart[r+1]) with kstart[r] = boff[r] - K*r,
+// slot s of read r ends at rpos = s - kstart[r] + K - 1 (the tuple_thread layout,
+// dalign/filter.c:410-425).
+template <typename K>
+int launch_extract(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, int kmer, K* keys,
+                   uint32_t* vals, int64_t nslots, uint32_t* nmasked, cudaStream_t s);
+
+template <typename K>
+int launch_decode(const DevBlock& b, int kmer, const uint32_t* slots, int64_t n, int32_t* read, int32_t* rpos,
+                  cudaStream_t s);
+
+// Keep flags for -t suppression: 1 where the entry's code run is shorter than t.
+template <typename K>
+int launch_suppress_flags(const K* code, int64_t n, int t, uint32_t* keep, cudaStream_t s);
+
+template <typename K>
+int launch_compact_index(const K* code, const int32_t* read, const int32_t* rpos, const uint32_t* keep,
+                         const uint32_t* pos, int64_t n, K* code2, int32_t* read2, int32_t* rpos2, cudaStream_t s);
+
+// Merge-join of the A and B indices (count_thread / merge_thread, dalign/filter.c:948-1231).
+struct MergeArgs
+{
+    int64_t na, nb;
+    int self, identity, comp;
+};
+
+template <typename K>
+int launch_run_flags(const K* code, int64_t n, uint32_t* flags, cudaStream_t s);
+
+template <typename K>
+int launch_pair_count(const K* acode, const int32_t* aread, const int32_t* arpos, const uint32_t* arun_excl,
+                      const uint32_t* arun_flag, const K* bcode, const int32_t* bread, const int32_t* brpos,
+                      MergeArgs m, uint32_t* jb, uint64_t* cnt, unsigned long long* ctrun, cudaStream_t s);
+
+int launch_gram(const unsigned long long* ctrun, int64_t nruns, unsigned long long* gram, cudaStream_t s);
+
+int launch_cnt_mask(const uint32_t* arun_excl, const uint32_t* arun_flag, const unsigned long long* ctrun, int64_t na,
+                    int limit, int always, uint64_t* cnt, cudaStream_t s);
+
+struct HitBits
+{
+    int pbits, abits, bbits;
+};
+
+int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread, const int32_t* brpos,
+                const uint32_t* jb, const uint64_t* cnt, const uint64_t* hoff, int64_t na, HitBits hb,
+                uint64_t* hkey, uint32_t* hdiag, cudaStream_t s);
+
+// Pair groups of the sorted hits: start flags, then (start, end) of groups with >= minhit hits.
+int launch_pair_flags(const uint64_t* hkey, int64_t n, int pbits, uint32_t* flags, cudaStream_t s);
+int launch_pair_scatter(const uint32_t* flags, const uint32_t* pos, int64_t n, uint32_t* starts, cudaStream_t s);
+int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* hkey,
+                         HitBits hb, const int32_t* arlen, const int32_t* brlen, uint2* groups, uint32_t* cost,
+                         uint32_t* idx, unsigned int* ngroups, cudaStream_t s);
+
+}  // namespace gd

@@ -1,0 +1,1009 @@
+// gd_pipeline.cu -- host orchestration of the overlap path and its C ABI (include/gpudalign.h).
+//
+// Per Match_Filter call the device runs: run flags + scan over the A index, per-entry pair
+// counts against the B index, the count histogram (the host derives the pair cap from it
+// exactly as dalign/filter.c:2107-2174 does), per-entry hit counts + scan, hit emission,
+// the stable radix sort of hits by (bread, aread, apos), pair-group detection, groups
+// ordered longest-first, and the persistent seed-scan/alignment kernel.  The overlaps it
+// writes come back to host memory, where Write_Overlap_Buffer's sort and file layout are
+// applied.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gpudalign.h"
+#include "gd_align.cuh"
+#include "gd_filter.cuh"
+#include "gd_prims.cuh"
+
+static thread_local char g_err[1024] = "";
+
+void gd_set_error(const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+namespace
+{
+
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t n = 0;
+};
+
+int ensure(DevBuf& b, size_t bytes)
+{
+    if (bytes == 0)
+        bytes = 16;
+    if (bytes <= b.n)
+        return 0;
+    if (b.p)
+        cudaFree(b.p);
+    b.p = nullptr;
+    b.n = 0;
+    size_t want = bytes + bytes / 8;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess)
+    {
+        b.p = nullptr;
+        gd_set_error("cudaMalloc of %zu bytes failed: %s", want, cudaGetErrorString(e));
+        return -1;
+    }
+    b.n = want;
+    return 0;
+}
+
+void release(DevBuf& b)
+{
+    if (b.p)
+        cudaFree(b.p);
+    b.p = nullptr;
+    b.n = 0;
+}
+
+template <typename T>
+T* P(DevBuf& b)
+{
+    return (T*)b.p;
+}
+
+struct Slot
+{
+    DevBuf bases, boff, rlen, manno, mdata;
+    DevBlock blk{};
+    int64_t totlen = 0, nslots = 0;
+    int has_mask = 0, loaded = 0;
+    DevBuf code, read, rpos;
+    int64_t nk = -1;
+    std::vector<int32_t> hrlen;
+};
+
+int bits_for(int64_t maxval)
+{
+    int b = 1;
+    while (b < 63 && (1ll << b) <= maxval)
+        b++;
+    return b;
+}
+
+}  // namespace
+
+struct gd_context
+{
+    cudaStream_t s = nullptr;
+    int kmer = 14, binshift = 6, suppress = 0, hitmin = 35;
+    double ave_corr = .70;
+    int tspace = 100;
+    float freq[4] = {.25f, .25f, .25f, .25f};
+    int symmetric = 1, only_identity = 0, no_trace = 0;
+    int minover = 2000, identity = 0;
+    uint64_t mem_limit = 0;
+    int ave_path = 0;
+    int spec_set = 0;
+    DevBuf tables;
+    Slot slot[3];
+    DevBuf k0, v0, k1, v1, scratch, flags, excl, jb, cnt, hoff, ctrun, gram, misc;
+    DevBuf hk0, hd0, hk1, hd1, starts, groups, gcost, gidx, gcost2, gidx2;
+    uint64_t* hkey = nullptr;
+    uint32_t* hdiag = nullptr;
+    int64_t nhits = 0;
+    gd::HitBits hb{};
+    DevBuf ascr, outrec, outtr, counters, status, queue;
+    int agrid = 0;
+    int pcap = 32768, mcap = 1024, tcap = 1 << 17;
+    uint64_t rcap = 1 << 20, tbcap = 64ull << 20;
+    std::vector<gd_overlap> recs;
+    std::vector<uint8_t> trace;
+    gd_stats stats;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+// ----------------------------------------------------------------------------------------
+// align spec: trim tables (set_table / New_Align_Spec, dalign/align.c:196-279)
+// ----------------------------------------------------------------------------------------
+
+static const double kBias[10] = {.690, .690, .690, .690, .780, .850, .900, .933, .966, 1.000};
+
+static void set_table(int bit, int prefix, int score, int max, int mscore, int dscore, int16_t* table, int16_t* sc)
+{
+    if (bit >= 15)
+    {
+        table[prefix] = (int16_t)(score - max);
+        sc[prefix] = (int16_t)score;
+    }
+    else
+    {
+        if (score > max)
+            max = score;
+        set_table(bit + 1, prefix << 1, score - dscore, max, mscore, dscore, table, sc);
+        set_table(bit + 1, (prefix << 1) | 1, score + mscore, max, mscore, dscore, table, sc);
+    }
+}
+
+static int upload_spec(gd_context* c)
+{
+    double match = c->freq[0] + c->freq[3];
+    if (match > .5)
+        match = 1. - match;
+    int bias = (int)((match + .025) * 20. - 1.);
+    if (match < .2)
+    {
+        fprintf(stderr, "Warning: Base bias worse than 80/20%% ! (New_Align_Spec)\n");
+        fprintf(stderr, "         Capping bias at this ratio.\n");
+        bias = 3;
+    }
+    c->ave_path = (int)(60 * (1. - kBias[bias] * (1. - c->ave_corr)));
+    int mscore = (int)(1000 * kBias[bias] * (1. - c->ave_corr));
+    int dscore = 1000 - mscore;
+    std::vector<int16_t> t(2 * gd::TRIM_TABLE);
+    set_table(0, 0, 0, 0, mscore, dscore, t.data(), t.data() + gd::TRIM_TABLE);
+    if (ensure(c->tables, t.size() * 2))
+        return -1;
+    GD_CUDA(cudaMemcpy(c->tables.p, t.data(), t.size() * 2, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// ----------------------------------------------------------------------------------------
+// k-mer index (Sort_Kmers)
+// ----------------------------------------------------------------------------------------
+
+template <typename K>
+static int64_t index_slot_t(gd_context* c, Slot& sl)
+{
+    using namespace gd;
+    const int Kmer = c->kmer;
+    int64_t nslots = sl.nslots;
+    cudaStream_t s = c->s;
+    sl.nk = 0;
+    if (nslots <= 0)
+        return 0;
+    if (ensure(c->k0, nslots * sizeof(K)) || ensure(c->k1, nslots * 8) || ensure(c->v0, nslots * 4) ||
+        ensure(c->v1, nslots * 4) || ensure(c->scratch, radix_scratch_bytes(nslots)) || ensure(c->misc, 64))
+        return -1;
+    uint32_t* nmasked = P<uint32_t>(c->misc);
+    if (launch_extract<K>(sl.blk, sl.has_mask ? P<int64_t>(sl.manno) : nullptr,
+                          sl.has_mask ? P<int32_t>(sl.mdata) : nullptr, Kmer, P<K>(c->k0), P<uint32_t>(c->v0), nslots,
+                          nmasked, s))
+        return -1;
+    int sort_bits = 8 * ((2 * Kmer + 7) / 8);  // mersort bytes (filter.c:713-716)
+    if (sort_bits > (int)(8 * sizeof(K)))
+        sort_bits = 8 * sizeof(K);
+    int which = radix_sort_pairs<K>(P<K>(c->k0), P<uint32_t>(c->v0), P<K>(c->k1), P<uint32_t>(c->v1), nslots, 0,
+                                    sort_bits, c->scratch.p, s);
+    if (which < 0)
+        return -1;
+    K* skeys = which ? P<K>(c->k1) : P<K>(c->k0);
+    uint32_t* svals = which ? P<uint32_t>(c->v1) : P<uint32_t>(c->v0);
+    uint32_t hmask = 0;
+    GD_CUDA(cudaMemcpyAsync(&hmask, nmasked, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    int64_t n = nslots - hmask;
+    if (ensure(sl.code, (n + 1) * sizeof(K)) || ensure(sl.read, (n + 1) * 4) || ensure(sl.rpos, (n + 1) * 4))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(sl.code.p, skeys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+    if (launch_decode<K>(sl.blk, Kmer, svals, n, P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
+        return -1;
+    if (c->suppress > 0 && n > 0)
+    {
+        // -t: drop codes occurring >= t times (compsize/compress_thread, filter.c:645-696)
+        uint32_t* keep = P<uint32_t>(c->v0);
+        uint32_t* pos = P<uint32_t>(c->v1);
+        if (ensure(c->misc, 64))
+            return -1;
+        uint32_t* tot = P<uint32_t>(c->misc) + 4;
+        if (launch_suppress_flags<K>(P<K>(sl.code), n, c->suppress, keep, s) ||
+            exclusive_scan<uint32_t>(keep, pos, n, tot, c->scratch.p, s))
+            return -1;
+        uint32_t kept = 0;
+        GD_CUDA(cudaMemcpyAsync(&kept, tot, 4, cudaMemcpyDeviceToHost, s));
+        // compact into k0 / v-buffers then copy back
+        K* code2 = P<K>(c->k0);
+        int32_t* read2 = (int32_t*)P<K>(c->k1);
+        int32_t* rpos2 = read2 + n;
+        if (launch_compact_index<K>(P<K>(sl.code), P<int32_t>(sl.read), P<int32_t>(sl.rpos), keep, pos, n, code2,
+                                    read2, rpos2, s))
+            return -1;
+        GD_CUDA(cudaStreamSynchronize(s));
+        GD_CUDA(cudaMemcpyAsync(sl.code.p, code2, kept * sizeof(K), cudaMemcpyDeviceToDevice, s));
+        GD_CUDA(cudaMemcpyAsync(sl.read.p, read2, kept * 4ull, cudaMemcpyDeviceToDevice, s));
+        GD_CUDA(cudaMemcpyAsync(sl.rpos.p, rpos2, kept * 4ull, cudaMemcpyDeviceToDevice, s));
+        n = kept;
+    }
+    GD_CUDA(cudaStreamSynchronize(s));
+    sl.nk = n;
+    return n;
+}
+
+// ----------------------------------------------------------------------------------------
+// Match_Filter
+// ----------------------------------------------------------------------------------------
+
+template <typename K>
+static int match_filter_t(gd_context* c, int bslot, int comp, int self)
+{
+    using namespace gd;
+    cudaStream_t s = c->s;
+    Slot& A = c->slot[0];
+    Slot& B = c->slot[bslot];
+    int oi = comp ? 1 : 0;
+    c->stats.hits[oi] = c->stats.groups[oi] = c->stats.seeds[oi] = c->stats.cells[oi] = 0;
+    c->stats.ms_merge[oi] = c->stats.ms_align[oi] = 0;
+    c->nhits = 0;
+    int64_t na = A.nk, nb = B.nk;
+    if (na <= 0 || nb <= 0)
+        return 0;
+    GD_CUDA(cudaEventRecord(c->ev0, s));
+    // run ids of the A index
+    if (ensure(c->flags, na * 4) || ensure(c->excl, na * 4) || ensure(c->jb, na * 4) || ensure(c->cnt, na * 8) ||
+        ensure(c->hoff, na * 8) || ensure(c->scratch, std::max(scan_scratch_bytes<uint64_t>(na), (size_t)4096)) ||
+        ensure(c->misc, 256) || ensure(c->gram, MAXGRAM * 8))
+        return -1;
+    uint32_t* d_nruns = P<uint32_t>(c->misc) + 8;
+    if (launch_run_flags<K>(P<K>(A.code), na, P<uint32_t>(c->flags), s) ||
+        exclusive_scan<uint32_t>(P<uint32_t>(c->flags), P<uint32_t>(c->excl), na, d_nruns, c->scratch.p, s))
+        return -1;
+    uint32_t nruns = 0;
+    GD_CUDA(cudaMemcpyAsync(&nruns, d_nruns, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    if (ensure(c->ctrun, (size_t)nruns * 8 + 8))
+        return -1;
+    GD_CUDA(cudaMemsetAsync(c->ctrun.p, 0, (size_t)nruns * 8, s));
+    MergeArgs m{na, nb, self, c->identity, comp};
+    if (launch_pair_count<K>(P<K>(A.code), P<int32_t>(A.read), P<int32_t>(A.rpos), P<uint32_t>(c->excl),
+                             P<uint32_t>(c->flags), P<K>(B.code), P<int32_t>(B.read), P<int32_t>(B.rpos), m,
+                             P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<unsigned long long>(c->ctrun), s) ||
+        launch_gram(P<unsigned long long>(c->ctrun), nruns, P<unsigned long long>(c->gram), s))
+        return -1;
+    std::vector<unsigned long long> gram(MAXGRAM);
+    GD_CUDA(cudaMemcpyAsync(gram.data(), c->gram.p, MAXGRAM * 8, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    // the pair cap from the memory limit (filter.c:2107-2174)
+    int limit = INT32_MAX;
+    if (c->mem_limit > 0)
+    {
+        int64_t avail;
+        int same_index = self && !comp;  // asort == bsort only for the self N call
+        uint64_t dsz = c->mem_limit / 16;
+        if (same_index || (int64_t)dsz > na + 2 * nb)
+            avail = ((int64_t)dsz - na) / 2;
+        else
+            avail = (int64_t)dsz - (na + nb);
+        avail = (int64_t)(avail * .98);
+        int64_t tom = 0;
+        int j;
+        for (j = 0; j < MAXGRAM; j++)
+        {
+            tom += (int64_t)j * (int64_t)gram[j];
+            if (tom > avail)
+                break;
+        }
+        limit = j;
+        if (limit == 1)
+        {
+            gd_set_error("Insufficient memory allocation (%.1fGb), reduce block size or increase allocation",
+                         (1. * c->mem_limit) / 0x40000000ll);
+            return -1;
+        }
+        if (limit < 10)
+            fprintf(stderr, "\nWarning: Sensitivity hampered by low memory allocation (%.1fGb)\n",
+                    (1. * c->mem_limit) / 0x40000000ll);
+    }
+    c->stats.limit[oi] = limit;
+    uint64_t* d_nhits = (uint64_t*)(P<uint32_t>(c->misc) + 16);
+    if (launch_cnt_mask(P<uint32_t>(c->excl), P<uint32_t>(c->flags), P<unsigned long long>(c->ctrun), na, limit,
+                        self && c->identity && comp, P<uint64_t>(c->cnt), s) ||
+        exclusive_scan<uint64_t>(P<uint64_t>(c->cnt), P<uint64_t>(c->hoff), na, d_nhits, c->scratch.p, s))
+        return -1;
+    uint64_t nhits = 0;
+    GD_CUDA(cudaMemcpyAsync(&nhits, d_nhits, 8, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    c->stats.hits[oi] = (int64_t)nhits;
+    if (nhits == 0)
+        return 0;
+    if (nhits > 0xffffffffull)
+    {
+        gd_set_error("%llu hits exceed the 32-bit hit index of this build", (unsigned long long)nhits);
+        return -1;
+    }
+    HitBits hb;
+    hb.pbits = bits_for(std::max(A.blk.maxlen - 1, 1));
+    hb.abits = bits_for(std::max(A.blk.nreads - 1, 1));
+    hb.bbits = bits_for(std::max(B.blk.nreads - 1, 1));
+    int hbits = hb.pbits + hb.abits + hb.bbits;
+    if (hbits > 64)
+    {
+        gd_set_error("hit key needs %d bits (> 64): block too large for this build", hbits);
+        return -1;
+    }
+    if (ensure(c->hk0, nhits * 8) || ensure(c->hk1, nhits * 8) || ensure(c->hd0, nhits * 4) ||
+        ensure(c->hd1, nhits * 4) || ensure(c->scratch, radix_scratch_bytes(nhits)))
+        return -1;
+    if (launch_emit(P<int32_t>(A.read), P<int32_t>(A.rpos), P<int32_t>(B.read), P<int32_t>(B.rpos),
+                    P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<uint64_t>(c->hoff), na, hb, P<uint64_t>(c->hk0),
+                    P<uint32_t>(c->hd0), s))
+        return -1;
+    // hit sort by (bread, aread, apos), stable (pairsort, filter.c:2030-2054, 2239-2252)
+    int which = radix_sort_pairs<uint64_t>(P<uint64_t>(c->hk0), P<uint32_t>(c->hd0), P<uint64_t>(c->hk1),
+                                           P<uint32_t>(c->hd1), nhits, 0, hbits, c->scratch.p, s);
+    if (which < 0)
+        return -1;
+    uint64_t* hkey = which ? P<uint64_t>(c->hk1) : P<uint64_t>(c->hk0);
+    uint32_t* hdiag = which ? P<uint32_t>(c->hd1) : P<uint32_t>(c->hd0);
+    c->hkey = hkey;
+    c->hdiag = hdiag;
+    c->nhits = (int64_t)nhits;
+    c->hb = hb;
+    // pair groups with >= ceil(h/k) hits (report_thread's minhit test, filter.c:1699-1709)
+    uint32_t* pflags = which ? P<uint32_t>(c->hd0) : P<uint32_t>(c->hd1);  // free ping-pong half
+    uint32_t* ppos = (uint32_t*)(which ? P<uint64_t>(c->hk0) : P<uint64_t>(c->hk1));
+    uint32_t* d_nst = P<uint32_t>(c->misc) + 24;
+    if (launch_pair_flags(hkey, nhits, hb.pbits, pflags, s) ||
+        exclusive_scan<uint32_t>(pflags, ppos, nhits, d_nst, c->scratch.p, s))
+        return -1;
+    uint32_t nst = 0;
+    GD_CUDA(cudaMemcpyAsync(&nst, d_nst, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    if (ensure(c->starts, (size_t)nst * 4 + 8) || ensure(c->groups, (size_t)nst * 8 + 8) ||
+        ensure(c->gcost, (size_t)nst * 4 + 8) || ensure(c->gidx, (size_t)nst * 4 + 8) ||
+        ensure(c->gcost2, (size_t)nst * 4 + 8) || ensure(c->gidx2, (size_t)nst * 4 + 8))
+        return -1;
+    unsigned* d_ng = P<unsigned>(c->misc) + 28;
+    if (launch_pair_scatter(pflags, ppos, nhits, P<uint32_t>(c->starts), s) ||
+        launch_select_groups(P<uint32_t>(c->starts), nst, nhits, (c->hitmin - 1) / c->kmer + 1, hkey, hb,
+                             P<int32_t>(A.rlen), P<int32_t>(B.rlen), P<uint2>(c->groups), P<uint32_t>(c->gcost),
+                             P<uint32_t>(c->gidx), d_ng, s))
+        return -1;
+    unsigned ng = 0;
+    GD_CUDA(cudaMemcpyAsync(&ng, d_ng, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    c->stats.groups[oi] = ng;
+    if (ensure(c->scratch, std::max(c->scratch.n, radix_scratch_bytes(ng) + 4096)))
+        return -1;
+    int gw = radix_sort_pairs<uint32_t>(P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), P<uint32_t>(c->gcost2),
+                                        P<uint32_t>(c->gidx2), ng, 0, 32, c->scratch.p, s);
+    if (gw < 0)
+        return -1;
+    uint32_t* order = gw ? P<uint32_t>(c->gidx2) : P<uint32_t>(c->gidx);
+    GD_CUDA(cudaEventRecord(c->ev1, s));
+    GD_CUDA(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->stats.ms_merge[oi] = ms;
+    if (ng == 0)
+        return 0;
+
+    // seed scan + alignment
+    AlignParams ap{};
+    ap.tspace = c->tspace;
+    ap.ave_path = c->ave_path;
+    ap.kmer = c->kmer;
+    ap.binshift = c->binshift;
+    ap.hitmin = c->hitmin;
+    ap.minover = c->minover;
+    ap.symmetric = c->symmetric;
+    ap.self = self;
+    ap.comp = comp;
+    ap.trace8 = c->tspace <= 125;
+    ap.no_trace = c->no_trace;
+    ap.maxdiag = A.blk.maxlen >> c->binshift;
+    ap.mindiag = (-B.blk.maxlen) >> c->binshift;
+    ap.hb = hb;
+    ap.table = P<int16_t>(c->tables);
+    ap.score = P<int16_t>(c->tables) + TRIM_TABLE;
+    if (!c->agrid && align_grid(&c->agrid))
+        return -1;
+    int nwarps = c->agrid * ALIGN_WARPS;
+    int maxlen = std::max(A.blk.maxlen, B.blk.maxlen);
+    int ptscap = 4 * (2 * (maxlen / c->tspace + 2)) + 32;
+    int nbands = ap.maxdiag - ap.mindiag + 8;
+    for (int attempt = 0; attempt < 6; attempt++)
+    {
+        AlignScratch sc{};
+        size_t need = align_scratch_bytes(nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+        bool fresh = need > c->ascr.n;
+        if (ensure(c->ascr, need))
+            return -1;
+        align_scratch_carve(&sc, c->ascr.p, nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+        if (fresh || attempt > 0)
+            GD_CUDA(cudaMemsetAsync(sc.bands, 0, (size_t)nwarps * 3 * nbands * 4, s));
+        if (ensure(c->outrec, c->rcap * sizeof(OutRec)) || ensure(c->outtr, c->tbcap) ||
+            ensure(c->counters, 8 * 8) || ensure(c->status, sizeof(DevStatus)) || ensure(c->queue, 16))
+            return -1;
+        GD_CUDA(cudaMemsetAsync(c->counters.p, 0, 64, s));
+        GD_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), s));
+        AlignOut out{P<OutRec>(c->outrec), P<uint8_t>(c->outtr), P<unsigned long long>(c->counters), c->rcap,
+                     c->tbcap};
+        GD_CUDA(cudaEventRecord(c->ev0, s));
+        if (launch_align_pairs(A.blk, B.blk, hkey, hdiag, P<uint2>(c->groups), order, ng, ap, sc, out,
+                               P<unsigned>(c->queue), P<DevStatus>(c->status), c->agrid, s))
+            return -1;
+        GD_CUDA(cudaEventRecord(c->ev1, s));
+        GD_CUDA(cudaEventSynchronize(c->ev1));
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        c->stats.ms_align[oi] = ms;
+        DevStatus st;
+        unsigned long long cnt[8];
+        GD_CUDA(cudaMemcpy(&st, c->status.p, sizeof(st), cudaMemcpyDeviceToHost));
+        GD_CUDA(cudaMemcpy(cnt, c->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost));
+        if (st.code != 0)
+        {
+            if (st.code == GD_ERR_PEBBLES)
+                c->pcap *= 2;
+            else if (st.code == GD_ERR_TRACE)
+                c->tcap *= 2;
+            else if (st.code == GD_ERR_MATCHES)
+                c->mcap *= 2;
+            else
+            {
+                gd_set_error("aligner failed on pair group %d: code %d info %d", st.where, st.code, st.info);
+                return -1;
+            }
+            continue;
+        }
+        if (cnt[0] > c->rcap || cnt[1] > c->tbcap)
+        {
+            c->rcap = std::max(c->rcap, (uint64_t)(cnt[0] * 5 / 4 + 1024));
+            c->tbcap = std::max(c->tbcap, (uint64_t)(cnt[1] * 5 / 4 + 65536));
+            continue;
+        }
+        c->stats.cells[oi] = (int64_t)cnt[2];
+        c->stats.seeds[oi] = (int64_t)cnt[3];
+        // bring the overlaps home
+        size_t r0 = c->recs.size();
+        size_t t0 = c->trace.size();
+        std::vector<OutRec> tmp(cnt[0]);
+        c->trace.resize(t0 + cnt[1]);
+        if (cnt[0])
+            GD_CUDA(cudaMemcpy(tmp.data(), c->outrec.p, cnt[0] * sizeof(OutRec), cudaMemcpyDeviceToHost));
+        if (cnt[1])
+            GD_CUDA(cudaMemcpy(c->trace.data() + t0, c->outtr.p, cnt[1], cudaMemcpyDeviceToHost));
+        c->recs.resize(r0 + cnt[0]);
+        for (size_t i = 0; i < cnt[0]; i++)
+        {
+            gd_overlap& o = c->recs[r0 + i];
+            const OutRec& x = tmp[i];
+            o.tlen = x.tlen;
+            o.diffs = x.diffs;
+            o.abpos = x.abpos;
+            o.bbpos = x.bbpos;
+            o.aepos = x.aepos;
+            o.bepos = x.bepos;
+            o.flags = x.flags;
+            o.aread = x.aread;
+            o.bread = x.bread;
+            o.pad = 0;
+            o.toff = x.toff + t0;
+        }
+        return 0;
+    }
+    gd_set_error("aligner scratch could not be grown enough");
+    return -1;
+}
+
+// ----------------------------------------------------------------------------------------
+// overlap sort + .las writing (Write_Overlap_Buffer, dalign/align.c:5786-6043)
+// ----------------------------------------------------------------------------------------
+
+static bool ovl_less(const gd_overlap& l, const gd_overlap& r)
+{
+    if (l.aread != r.aread)
+        return l.aread < r.aread;
+    if (l.bread != r.bread)
+        return l.bread < r.bread;
+    if ((l.flags & 1) != (r.flags & 1))
+        return (l.flags & 1) < (r.flags & 1);
+    if (l.abpos != r.abpos)
+        return l.abpos < r.abpos;
+    // keys tie: the reference's qsort leaves these unordered; fix an order
+    if (l.aepos != r.aepos)
+        return l.aepos < r.aepos;
+    if (l.bbpos != r.bbpos)
+        return l.bbpos < r.bbpos;
+    return l.toff < r.toff;
+}
+
+static std::vector<size_t> sorted_order(gd_context* c)
+{
+    std::vector<size_t> idx;
+    idx.reserve(c->recs.size());
+    for (size_t i = 0; i < c->recs.size(); i++)
+        if (!c->only_identity || c->recs[i].aread == c->recs[i].bread)
+            idx.push_back(i);
+    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return ovl_less(c->recs[a], c->recs[b]); });
+    return idx;
+}
+
+static int write_las(gd_context* c, const char* path, const std::vector<size_t>& idx, size_t from, size_t to)
+{
+    FILE* f = fopen(path, "w");
+    if (!f)
+    {
+        gd_set_error("Cannot open file %s for writing", path);
+        return -1;
+    }
+    int tbytes = c->tspace <= 125 ? 1 : 2;
+    int64_t n = (int64_t)(to - from);
+    int32_t ts = c->tspace;
+    fwrite(&n, 8, 1, f);
+    fwrite(&ts, 4, 1, f);
+    std::vector<uint8_t> buf;
+    buf.reserve(1 << 20);
+    for (size_t i = from; i < to; i++)
+    {
+        const gd_overlap& o = c->recs[idx[i]];
+        int32_t r[10] = {o.tlen, o.diffs, o.abpos, o.bbpos, o.aepos, o.bepos, (int32_t)o.flags, o.aread, o.bread, 0};
+        const uint8_t* rb = (const uint8_t*)r;
+        buf.insert(buf.end(), rb, rb + 40);
+        if (o.tlen > 0)
+            buf.insert(buf.end(), c->trace.data() + o.toff, c->trace.data() + o.toff + (size_t)o.tlen * tbytes);
+        if (buf.size() > (1 << 20))
+        {
+            fwrite(buf.data(), 1, buf.size(), f);
+            buf.clear();
+        }
+    }
+    fwrite(buf.data(), 1, buf.size(), f);
+    if (fclose(f))
+    {
+        gd_set_error("write to %s failed", path);
+        return -1;
+    }
+    return 0;
+}
+
+static std::string dirname_of(int run_id, int block)
+{
+    // getDir (db/DB.c:1661-1675)
+    if (block == 0)
+        return ".";
+    char b[64];
+    snprintf(b, sizeof b, "%03d_%05d", run_id, block);
+    return b;
+}
+
+// ----------------------------------------------------------------------------------------
+// C ABI
+// ----------------------------------------------------------------------------------------
+
+extern "C" {
+
+const char* gd_last_error(void)
+{
+    return g_err;
+}
+
+gd_context* gd_create(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    {
+        gd_set_error("no CUDA device: the overlap path runs on the GPU only");
+        return nullptr;
+    }
+    gd_context* c = new gd_context();
+    memset(&c->stats, 0, sizeof(c->stats));
+    if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+    {
+        gd_set_error("stream/event creation failed");
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void gd_destroy(gd_context* c)
+{
+    if (!c)
+        return;
+    cudaStreamSynchronize(c->s);
+    DevBuf* bufs[] = {&c->tables, &c->k0,     &c->v0,    &c->k1,     &c->v1,     &c->scratch, &c->flags,
+                      &c->excl,   &c->jb,     &c->cnt,   &c->hoff,   &c->ctrun,  &c->gram,    &c->misc,
+                      &c->hk0,    &c->hd0,    &c->hk1,   &c->hd1,    &c->starts, &c->groups,  &c->gcost,
+                      &c->gidx,   &c->gcost2, &c->gidx2, &c->ascr,   &c->outrec, &c->outtr,   &c->counters,
+                      &c->status, &c->queue};
+    for (DevBuf* b : bufs)
+        release(*b);
+    for (Slot& s : c->slot)
+    {
+        DevBuf* sb[] = {&s.bases, &s.boff, &s.rlen, &s.manno, &s.mdata, &s.code, &s.read, &s.rpos};
+        for (DevBuf* b : sb)
+            release(*b);
+    }
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    cudaStreamDestroy(c->s);
+    delete c;
+}
+
+int gd_set_filter_params(gd_context* c, int kmer, int binshift, int suppress, int hitmin)
+{
+    if (kmer <= 1)
+    {
+        gd_set_error("Illegal combination of filter parameters");
+        return -1;
+    }
+    if (kmer > 32)
+    {
+        gd_set_error("k-mer length %d exceeds 32", kmer);
+        return -1;
+    }
+    c->kmer = kmer;
+    c->binshift = binshift;
+    c->suppress = suppress;
+    c->hitmin = hitmin;
+    for (Slot& s : c->slot)
+        s.nk = -1;
+    return 0;
+}
+
+int gd_new_align_spec(gd_context* c, double ave_corr, int trace_space, const float freq[4], int symmetric,
+                      int only_identity, int no_trace_points)
+{
+    if (trace_space <= 0)
+    {
+        gd_set_error("invalid trace spacing of (%d)", trace_space);
+        return -1;
+    }
+    c->ave_corr = ave_corr;
+    c->tspace = trace_space;
+    for (int i = 0; i < 4; i++)
+        c->freq[i] = freq[i];
+    c->symmetric = symmetric;
+    c->only_identity = only_identity;
+    c->no_trace = no_trace_points;
+    c->spec_set = 1;
+    return upload_spec(c);
+}
+
+int gd_set_globals(gd_context* c, int minover, int identity, uint64_t mem_limit)
+{
+    c->minover = minover;
+    c->identity = identity;
+    c->mem_limit = mem_limit;
+    return 0;
+}
+
+int gd_load_block(gd_context* c, int slot, const gd_block* b)
+{
+    if (slot < 0 || slot > 2)
+    {
+        gd_set_error("slot %d out of range", slot);
+        return -1;
+    }
+    Slot& s = c->slot[slot];
+    int64_t nb = b->boff[b->nreads];  // bytes after bases[-1], through the last 4
+    for (int i = 0; i < b->nreads; i++)
+        if (b->rlen[i] < c->kmer)
+        {
+            gd_set_error("Block contains reads < %dbp long !  Run DBsplit.", c->kmer);
+            return -1;
+        }
+    if (ensure(s.bases, nb + 1 + 64) || ensure(s.boff, (b->nreads + 1) * 8) || ensure(s.rlen, b->nreads * 4 + 4))
+        return -1;
+    GD_CUDA(cudaMemsetAsync(s.bases.p, 4, nb + 1 + 64, c->s));
+    GD_CUDA(cudaMemcpyAsync((uint8_t*)s.bases.p + 32, b->bases - 1, nb + 1, cudaMemcpyHostToDevice, c->s));
+    GD_CUDA(cudaMemcpyAsync(s.boff.p, b->boff, (b->nreads + 1) * 8, cudaMemcpyHostToDevice, c->s));
+    GD_CUDA(cudaMemcpyAsync(s.rlen.p, b->rlen, b->nreads * 4, cudaMemcpyHostToDevice, c->s));
+    s.has_mask = b->mask_anno != nullptr;
+    if (s.has_mask)
+    {
+        int64_t nd = b->mask_anno[b->nreads];
+        if (ensure(s.manno, (b->nreads + 1) * 8) || ensure(s.mdata, nd * 4 + 8))
+            return -1;
+        GD_CUDA(cudaMemcpyAsync(s.manno.p, b->mask_anno, (b->nreads + 1) * 8, cudaMemcpyHostToDevice, c->s));
+        if (nd)
+            GD_CUDA(cudaMemcpyAsync(s.mdata.p, b->mask_data, nd * 4, cudaMemcpyHostToDevice, c->s));
+    }
+    s.blk.bases = (const uint8_t*)s.bases.p + 33;
+    s.blk.boff = P<int64_t>(s.boff);
+    s.blk.rlen = P<int32_t>(s.rlen);
+    s.blk.nreads = b->nreads;
+    s.blk.maxlen = b->maxlen;
+    s.blk.ufirst = b->ufirst;
+    s.totlen = b->totlen;
+    s.nslots = nb - (int64_t)c->kmer * b->nreads;
+    s.hrlen.assign(b->rlen, b->rlen + b->nreads);
+    s.loaded = 1;
+    s.nk = -1;
+    GD_CUDA(cudaStreamSynchronize(c->s));
+    return 0;
+}
+
+int64_t gd_sort_kmers(gd_context* c, int slot)
+{
+    if (slot < 0 || slot > 2 || !c->slot[slot].loaded)
+    {
+        gd_set_error("slot %d not loaded", slot);
+        return -1;
+    }
+    GD_CUDA(cudaEventRecord(c->ev0, c->s));
+    int64_t n = c->kmer <= 15 ? index_slot_t<uint32_t>(c, c->slot[slot]) : index_slot_t<uint64_t>(c, c->slot[slot]);
+    GD_CUDA(cudaEventRecord(c->ev1, c->s));
+    GD_CUDA(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->stats.ms_index[slot] = ms;
+    c->stats.kmers[slot] = n;
+    return n;
+}
+
+int64_t gd_get_kmers(gd_context* c, int slot, uint64_t* code, int32_t* read, int32_t* rpos, int64_t cap)
+{
+    Slot& s = c->slot[slot];
+    if (s.nk < 0)
+    {
+        gd_set_error("slot %d has no index", slot);
+        return -1;
+    }
+    int64_t n = std::min(s.nk, cap);
+    if (c->kmer <= 15)
+    {
+        std::vector<uint32_t> t(n);
+        GD_CUDA(cudaMemcpy(t.data(), s.code.p, n * 4, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < n; i++)
+            code[i] = t[i];
+    }
+    else
+        GD_CUDA(cudaMemcpy(code, s.code.p, n * 8, cudaMemcpyDeviceToHost));
+    GD_CUDA(cudaMemcpy(read, s.read.p, n * 4, cudaMemcpyDeviceToHost));
+    GD_CUDA(cudaMemcpy(rpos, s.rpos.p, n * 4, cudaMemcpyDeviceToHost));
+    return s.nk;
+}
+
+int gd_match_filter(gd_context* c, int bslot, int comp, int self)
+{
+    if (!c->spec_set)
+    {
+        gd_set_error("gd_new_align_spec has not been called");
+        return -1;
+    }
+    if (c->slot[0].nk < 0 || bslot < 0 || bslot > 2 || c->slot[bslot].nk < 0)
+    {
+        gd_set_error("both indices must be built before Match_Filter");
+        return -1;
+    }
+    return c->kmer <= 15 ? match_filter_t<uint32_t>(c, bslot, comp, self)
+                         : match_filter_t<uint64_t>(c, bslot, comp, self);
+}
+
+int64_t gd_get_hits(gd_context* c, int32_t* rows4, int64_t cap)
+{
+    int64_t n = std::min(c->nhits, cap);
+    if (n <= 0)
+        return c->nhits;
+    std::vector<uint64_t> k(n);
+    std::vector<uint32_t> d(n);
+    GD_CUDA(cudaMemcpy(k.data(), c->hkey, n * 8, cudaMemcpyDeviceToHost));
+    GD_CUDA(cudaMemcpy(d.data(), c->hdiag, n * 4, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < n; i++)
+    {
+        rows4[4 * i + 0] = (int32_t)d[i];
+        rows4[4 * i + 1] = (int32_t)(k[i] & ((1ull << c->hb.pbits) - 1));
+        rows4[4 * i + 2] = (int32_t)((k[i] >> c->hb.pbits) & ((1ull << c->hb.abits) - 1));
+        rows4[4 * i + 3] = (int32_t)(k[i] >> (c->hb.pbits + c->hb.abits));
+    }
+    return c->nhits;
+}
+
+int64_t gd_num_overlaps(gd_context* c, int64_t* trace_bytes)
+{
+    if (trace_bytes)
+        *trace_bytes = (int64_t)c->trace.size();
+    return (int64_t)c->recs.size();
+}
+
+int64_t gd_get_overlaps(gd_context* c, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap)
+{
+    std::vector<size_t> idx = sorted_order(c);
+    int tbytes = c->tspace <= 125 ? 1 : 2;
+    uint64_t t = 0;
+    int64_t n = 0;
+    for (size_t i = 0; i < idx.size() && n < rcap; i++, n++)
+    {
+        gd_overlap o = c->recs[idx[i]];
+        size_t len = (size_t)o.tlen * tbytes;
+        if ((int64_t)(t + len) > tcap)
+            break;
+        memcpy(trace + t, c->trace.data() + o.toff, len);
+        o.toff = t;
+        recs[n] = o;
+        t += len;
+    }
+    return n;
+}
+
+int gd_write_overlap_buffer(gd_context* c, int run_id, const char* ablock, const char* bblock, int last_read)
+{
+    std::vector<size_t> idx = sorted_order(c);
+    // block ids and roots from the names (dalign/align.c:5858-5877)
+    auto split = [](const char* name, std::string& root, int& id) {
+        const char* dot = strrchr(name, '.');
+        id = 0;
+        root = name;
+        if (dot)
+        {
+            id = atoi(dot + 1);
+            root = std::string(name, dot - name);
+        }
+    };
+    std::string aroot, broot;
+    int aid, bid;
+    split(ablock, aroot, aid);
+    split(bblock, broot, bid);
+    char path1[4096], path2[4096];
+    if (strcmp(ablock, bblock) == 0 || c->symmetric == 0)
+    {
+        std::string dir = dirname_of(run_id, aid);
+        if (aid > 0 && bid > 0)
+            snprintf(path1, sizeof path1, "%s/%s.%d.%s.%d.las", dir.c_str(), aroot.c_str(), aid, broot.c_str(), bid);
+        else if (aid > 0)
+            snprintf(path1, sizeof path1, "%s/%s.%d.%s.las", dir.c_str(), aroot.c_str(), aid, broot.c_str());
+        else if (bid > 0)
+            snprintf(path1, sizeof path1, "%s.%s.%d.las", aroot.c_str(), broot.c_str(), bid);
+        else
+            snprintf(path1, sizeof path1, "%s.%s.las", aroot.c_str(), broot.c_str());
+        return write_las(c, path1, idx, 0, idx.size());
+    }
+    std::string d1 = dirname_of(run_id, aid), d2 = dirname_of(run_id, bid);
+    if (aid > 0)
+    {
+        if (bid > 0)
+        {
+            snprintf(path1, sizeof path1, "%s/%s.%d.%s.%d.las", d1.c_str(), aroot.c_str(), aid, broot.c_str(), bid);
+            snprintf(path2, sizeof path2, "%s/%s.%d.%s.%d.las", d2.c_str(), broot.c_str(), bid, aroot.c_str(), aid);
+        }
+        else
+        {
+            snprintf(path1, sizeof path1, "%s/%s.%d.%s.las", d1.c_str(), aroot.c_str(), aid, broot.c_str());
+            snprintf(path2, sizeof path2, "%s.%s.%d.las", broot.c_str(), aroot.c_str(), aid);
+        }
+    }
+    else
+    {
+        if (bid > 0)
+        {
+            snprintf(path1, sizeof path1, "%s.%s.%d.las", aroot.c_str(), broot.c_str(), bid);
+            snprintf(path2, sizeof path2, "%s/%s.%d.%s.las", d2.c_str(), broot.c_str(), bid, aroot.c_str());
+        }
+        else
+        {
+            snprintf(path1, sizeof path1, "%s.%s.las", aroot.c_str(), broot.c_str());
+            snprintf(path2, sizeof path2, "%s.%s.las", broot.c_str(), aroot.c_str());
+        }
+    }
+    const char* p1 = path1;
+    const char* p2 = path2;
+    if (bid < aid)
+        std::swap(p1, p2);
+    size_t j = 0;
+    while (j < idx.size() && c->recs[idx[j]].aread <= last_read)
+        j++;
+    if (write_las(c, p1, idx, 0, j))
+        return -1;
+    return write_las(c, p2, idx, j, idx.size());
+}
+
+int gd_reset_overlap_buffer(gd_context* c)
+{
+    c->recs.clear();
+    c->trace.clear();
+    return 0;
+}
+
+int gd_get_stats(gd_context* c, gd_stats* st)
+{
+    c->stats.records = (int64_t)c->recs.size();
+    *st = c->stats;
+    return 0;
+}
+
+int gd_local_alignment_batch(gd_context* c, const uint8_t* abases, int64_t alen_total, const uint8_t* bbases,
+                             int64_t blen_total, const int64_t* aoff, const int32_t* alen, const int64_t* boff,
+                             const int32_t* blen, const int32_t* diag, const int32_t* anti, int nseeds, int comp,
+                             int32_t* out12, uint16_t* trace, int trstride, int64_t* cells)
+{
+    using namespace gd;
+    if (!c->spec_set)
+    {
+        gd_set_error("gd_new_align_spec has not been called");
+        return -1;
+    }
+    if (nseeds <= 0)
+        return 0;
+    DevBuf da, db, dao, dal, dbo, dbl, dd, dn, dout, dtr, dc, dst;
+    int rc = -1;
+    int maxlen = 0;
+    for (int i = 0; i < nseeds; i++)
+        maxlen = std::max(maxlen, std::max(alen[i], blen[i]));
+    AlignParams ap{};
+    ap.tspace = c->tspace;
+    ap.ave_path = c->ave_path;
+    ap.comp = comp;
+    ap.trace8 = c->tspace <= 125;
+    ap.table = P<int16_t>(c->tables);
+    ap.score = P<int16_t>(c->tables) + TRIM_TABLE;
+    int grid = 0;
+    if (align_grid(&grid))
+        return -1;
+    int nwarps = std::min(grid * ALIGN_WARPS, ((nseeds + ALIGN_WARPS - 1) / ALIGN_WARPS) * ALIGN_WARPS);
+    int ptscap = 4 * (2 * (maxlen / c->tspace + 2)) + 32;
+    AlignScratch sc{};
+    DevBuf scr;
+    do
+    {
+        if (ensure(da, alen_total + 128) || ensure(db, blen_total + 128) || ensure(dao, nseeds * 8) ||
+            ensure(dal, nseeds * 4) || ensure(dbo, nseeds * 8) || ensure(dbl, nseeds * 4) ||
+            ensure(dd, nseeds * 4) || ensure(dn, nseeds * 4) || ensure(dout, (size_t)nseeds * 48) ||
+            ensure(dtr, (size_t)nseeds * trstride * 2) || ensure(dc, nseeds * 8) || ensure(dst, sizeof(DevStatus)) ||
+            ensure(scr, align_scratch_bytes(nwarps, c->pcap, ptscap, 4, 4, 4)))
+            break;
+        align_scratch_carve(&sc, scr.p, nwarps, c->pcap, ptscap, 4, 4, 4);
+        // sequences: caller buffers hold [4, read, 4, read, ...] with offsets relative to index 0
+        if (cudaMemset(da.p, 4, alen_total + 128) != cudaSuccess || cudaMemset(db.p, 4, blen_total + 128) != cudaSuccess)
+            break;
+        cudaMemcpy((uint8_t*)da.p + 64, abases, alen_total, cudaMemcpyHostToDevice);
+        cudaMemcpy((uint8_t*)db.p + 64, bbases, blen_total, cudaMemcpyHostToDevice);
+        cudaMemcpy(dao.p, aoff, nseeds * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(dal.p, alen, nseeds * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(dbo.p, boff, nseeds * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(dbl.p, blen, nseeds * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(dd.p, diag, nseeds * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(dn.p, anti, nseeds * 4, cudaMemcpyHostToDevice);
+        cudaMemset(dst.p, 0, sizeof(DevStatus));
+        cudaMemset(dout.p, 0, (size_t)nseeds * 48);
+        if (launch_la_batch((const uint8_t*)da.p + 64, P<int64_t>(dao), P<int32_t>(dal), (const uint8_t*)db.p + 64,
+                            P<int64_t>(dbo), P<int32_t>(dbl), P<int32_t>(dd), P<int32_t>(dn), nseeds, ap, sc,
+                            P<int32_t>(dout), P<uint16_t>(dtr), trstride, P<int64_t>(dc), P<DevStatus>(dst), 0))
+            break;
+        if (cudaDeviceSynchronize() != cudaSuccess)
+        {
+            gd_set_error("Local_Alignment batch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        DevStatus st;
+        cudaMemcpy(&st, dst.p, sizeof st, cudaMemcpyDeviceToHost);
+        if (st.code)
+        {
+            gd_set_error("Local_Alignment batch: seed %d failed with code %d (info %d)", st.where, st.code, st.info);
+            break;
+        }
+        cudaMemcpy(out12, dout.p, (size_t)nseeds * 48, cudaMemcpyDeviceToHost);
+        cudaMemcpy(trace, dtr.p, (size_t)nseeds * trstride * 2, cudaMemcpyDeviceToHost);
+        cudaMemcpy(cells, dc.p, nseeds * 8, cudaMemcpyDeviceToHost);
+        rc = 0;
+    } while (0);
+    DevBuf* all[] = {&da, &db, &dao, &dal, &dbo, &dbl, &dd, &dn, &dout, &dtr, &dc, &dst, &scr};
+    for (DevBuf* b : all)
+        release(*b);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,285 @@
+// gd_prims.cu -- exclusive scan and stable LSD radix sort (see gd_prims.cuh).
+#include "gd_prims.cuh"
+
+namespace gd
+{
+
+template <typename T>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const T* __restrict__ in, int64_t n, T* partial)
+{
+    __shared__ T red[SCAN_THREADS / 32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+    T acc = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+    {
+        int64_t idx = base + i * SCAN_THREADS + threadIdx.x;
+        if (idx < n)
+            acc += in[idx];
+    }
+    for (int o = 16; o; o >>= 1)
+        acc += __shfl_xor_sync(GD_FULL, acc, o);
+    if ((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        T t = 0;
+        for (int w = 0; w < SCAN_THREADS / 32; w++)
+            t += red[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// Single-CTA exclusive scan of the tile partials (in place); writes the grand total.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_scan_partials(T* partial, int64_t m, T* total)
+{
+    __shared__ T warp_tot[32];
+    __shared__ T carry_s;
+    if (threadIdx.x == 0)
+        carry_s = 0;
+    __syncthreads();
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t base = 0; base < m; base += 1024)
+    {
+        int64_t idx = base + threadIdx.x;
+        T v = idx < m ? partial[idx] : 0;
+        T x = v;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            T y = __shfl_up_sync(GD_FULL, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_tot[wid] = x;
+        __syncthreads();
+        if (wid == 0)
+        {
+            T w = warp_tot[lane];
+            T z = w;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                T y = __shfl_up_sync(GD_FULL, z, o);
+                if (lane >= o)
+                    z += y;
+            }
+            warp_tot[lane] = z - w;  // exclusive over warps
+        }
+        __syncthreads();
+        T carry = carry_s;
+        T excl = carry + warp_tot[wid] + x - v;
+        if (idx < m)
+            partial[idx] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023)
+            carry_s = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total)
+        *total = carry_s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const T* in, T* out, int64_t n, const T* partial)
+{
+    __shared__ T tile[SCAN_TILE];
+    __shared__ T warp_tot[SCAN_THREADS / 32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+    {
+        int64_t idx = base + i * SCAN_THREADS + threadIdx.x;
+        tile[i * SCAN_THREADS + threadIdx.x] = idx < n ? in[idx] : 0;
+    }
+    __syncthreads();
+    T loc[SCAN_ITEMS];
+    T sum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+    {
+        loc[i] = sum;
+        sum += tile[threadIdx.x * SCAN_ITEMS + i];
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    T x = sum;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        T y = __shfl_up_sync(GD_FULL, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        warp_tot[wid] = x;
+    __syncthreads();
+    T wpre = 0;
+    for (int w = 0; w < wid; w++)
+        wpre += warp_tot[w];
+    T pre = partial[blockIdx.x] + wpre + x - sum;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+        tile[threadIdx.x * SCAN_ITEMS + i] = pre + loc[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+    {
+        int64_t idx = base + i * SCAN_THREADS + threadIdx.x;
+        if (idx < n)
+            out[idx] = tile[i * SCAN_THREADS + threadIdx.x];
+    }
+}
+
+template <typename T>
+int exclusive_scan(const T* in, T* out, int64_t n, T* total, void* scratch, cudaStream_t s)
+{
+    int64_t tiles = gd_cdiv<int64_t>(n, SCAN_TILE);
+    T* partial = (T*)scratch;
+    if (n <= 0)
+    {
+        if (total)
+            GD_CUDA(cudaMemsetAsync(total, 0, sizeof(T), s));
+        return 0;
+    }
+    k_scan_reduce<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, partial);
+    k_scan_partials<T><<<1, 1024, 0, s>>>(partial, tiles, total);
+    k_scan_down<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, out, n, partial);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template int exclusive_scan<uint32_t>(const uint32_t*, uint32_t*, int64_t, uint32_t*, void*, cudaStream_t);
+template int exclusive_scan<uint64_t>(const uint64_t*, uint64_t*, int64_t, uint64_t*, void*, cudaStream_t);
+
+// ---------------------------------------------------------------------------------------
+// radix sort
+// ---------------------------------------------------------------------------------------
+
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ keys, int64_t n, int shift,
+                                                       uint32_t* counts, int ntiles)
+{
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    int64_t base = (int64_t)blockIdx.x * RS_TILE;
+#pragma unroll 4
+    for (int i = 0; i < RS_ROUNDS; i++)
+    {
+        int64_t idx = base + i * RS_THREADS + threadIdx.x;
+        if (idx < n)
+        {
+            unsigned d = (unsigned)(keys[idx] >> shift) & 255u;
+            unsigned peers = __match_any_sync(__activemask(), d);
+            if ((peers & lanemask_lt()) == 0)
+                atomicAdd(&h[d], (unsigned)__popc(peers));
+        }
+    }
+    __syncthreads();
+    counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                          K* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
+                                                          int shift, const uint32_t* __restrict__ offs, int ntiles)
+{
+    __shared__ uint32_t wcnt[RS_WARPS][256];
+    __shared__ uint32_t toff[256];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < RS_WARPS; i++)
+        wcnt[i][threadIdx.x] = 0;
+    toff[threadIdx.x] = offs[(int64_t)threadIdx.x * ntiles + blockIdx.x];
+    __syncthreads();
+
+    int64_t base = (int64_t)blockIdx.x * RS_TILE + (int64_t)w * (RS_ROUNDS * 32);
+    K key[RS_ROUNDS];
+    uint32_t val[RS_ROUNDS];
+    uint32_t rank[RS_ROUNDS];
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; r++)
+    {
+        int64_t idx = base + r * 32 + lane;
+        bool valid = idx < n;
+        unsigned d = 256;
+        if (valid)
+        {
+            key[r] = kin[idx];
+            val[r] = vin[idx];
+            d = (unsigned)(key[r] >> shift) & 255u;
+        }
+        unsigned peers = __match_any_sync(GD_FULL, d);
+        unsigned c = valid ? wcnt[w][d] : 0;
+        rank[r] = c + __popc(peers & lt);
+        __syncwarp();
+        if (valid && (peers & lt) == 0)
+            wcnt[w][d] = c + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        uint32_t run = 0;
+#pragma unroll
+        for (int i = 0; i < RS_WARPS; i++)
+        {
+            uint32_t t = wcnt[i][threadIdx.x];
+            wcnt[i][threadIdx.x] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; r++)
+    {
+        int64_t idx = base + r * 32 + lane;
+        if (idx < n)
+        {
+            unsigned d = (unsigned)(key[r] >> shift) & 255u;
+            uint32_t dest = toff[d] + wcnt[w][d] + rank[r];
+            kout[dest] = key[r];
+            vout[dest] = val[r];
+        }
+    }
+}
+
+template <typename K>
+int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int begin_bit, int end_bit, void* scratch,
+                     cudaStream_t s)
+{
+    if (n <= 1 || end_bit <= begin_bit)
+        return 0;
+    int64_t tiles64 = gd_cdiv<int64_t>(n, RS_TILE);
+    if (tiles64 > (1 << 30) || n > 0xffffffffll)
+    {
+        gd_set_error("radix sort of %lld items exceeds 32-bit offsets", (long long)n);
+        return -1;
+    }
+    int ntiles = (int)tiles64;
+    int64_t ncnt = (int64_t)ntiles * 256;
+    uint32_t* counts = (uint32_t*)scratch;
+    void* sscr = (void*)(((uintptr_t)(counts + ncnt) + 255) & ~(uintptr_t)255);
+    int cur = 0;
+    for (int b = begin_bit; b < end_bit; b += 8)
+    {
+        K* kin = cur ? k1 : k0;
+        uint32_t* vin = cur ? v1 : v0;
+        K* kout = cur ? k0 : k1;
+        uint32_t* vout = cur ? v0 : v1;
+        k_rs_hist<K><<<ntiles, RS_THREADS, 0, s>>>(kin, n, b, counts, ntiles);
+        if (exclusive_scan<uint32_t>(counts, counts, ncnt, (uint32_t*)nullptr, sscr, s))
+            return -1;
+        k_rs_scatter<K><<<ntiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, b, counts, ntiles);
+        cur ^= 1;
+    }
+    GD_CUDA(cudaGetLastError());
+    return cur;
+}
+
+template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, int64_t, int, int, void*,
+                                        cudaStream_t);
+template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, int64_t, int, int, void*,
+                                        cudaStream_t);
+
+}  // namespace gd

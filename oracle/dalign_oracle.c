@@ -466,6 +466,7 @@ typedef struct
     uint16_t* pts; /* trace point buffer: [maxtp | A (2 maxtp) | B ...] */
     int64_t ptsmax;
     int64_t cells_count; /* sum of wave widths (WAVE_STATS TOT, align.c:957-963) */
+    int64_t max_width, max_cells, waves, snakes;
 } Work;
 
 typedef struct
@@ -731,7 +732,7 @@ static void fwd_wave(Work* w, const Spec* sp, const uint8_t* aseq, const uint8_t
                     break;
                 }
                 y += 1;
-                w->cells_count += 0;
+                w->snakes++;
                 if ((b & PATH_TOP) == 0)
                     m += 1;
                 b = (b << 1) | 1;
@@ -821,6 +822,9 @@ static void fwd_wave(Work* w, const Spec* sp, const uint8_t* aseq, const uint8_t
                 break;
             }
         w->cells_count += (hgh - low) + 1;
+        w->waves++;
+        if (hgh - low + 1 > w->max_width) w->max_width = hgh - low + 1;
+        if (w->ncell > w->max_cells) w->max_cells = w->ncell;
     }
 
     {
@@ -1225,6 +1229,9 @@ static void rev_wave(Work* w, const Spec* sp, const uint8_t* aseq0, const uint8_
                 break;
             }
         w->cells_count += (hgh - low) + 1;
+        w->waves++;
+        if (hgh - low + 1 > w->max_width) w->max_width = hgh - low + 1;
+        if (w->ncell > w->max_cells) w->max_cells = w->ncell;
     }
 
     {
@@ -2029,6 +2036,8 @@ int or_daligner(const or_block* a, const or_block* b, const or_block* bc, const 
     res->tbytes_total = ob.ttop;
     res->tbytes = ob.tbytes;
     res->cells = w.cells_count;
+    res->snake_steps = w.snakes;
+    fprintf(stderr, "oracle stats: max_width %lld max_cells %lld waves %lld snakes %lld\n", (long long)w.max_width, (long long)w.max_cells, (long long)w.waves, (long long)w.snakes);
     free(w.mem);
     free(w.cells);
     free(w.pts);
