@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""bench.py -- overlaps/s of daligner's overlap path on B200.
+
+A step is one daligner block comparison: one DB block against itself in both
+orientations (Sort_Kmers(A), Match_Filter(A,A), complement_DB, Sort_Kmers(cA),
+Match_Filter(A,cA), dalign/daligner.c:957-1012), on the bacterial-scale workload with
+repeats (4.6 Mbp genome + 40 x 5 kbp repeats at 1.5% + 3 x 6 kbp at 0.2%, 25x PacBio-like
+reads, mean 10 kbp; k14 w6 h35 e.70 l1000 s100 M32), generated from a seed.
+
+  value  overlaps/s with the block resident in HBM (all device stages, overlaps brought
+         to host memory, device-timed with CUDA events on the library's stream)
+  e2e    the same through the C ABI from pinned host buffers: block H2D + pipeline +
+         sorted overlap buffer D2H, device-timed
+
+Multi-GPU: each rank compares its own block (seed + rank): weak scaling, no collective on
+the data path; the job value is all ranks' overlaps over the slowest rank's time.
+
+--impl reference runs the reference daligner (built from source into oracle/_ref) on
+the host cores with a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from marvel_b200 import dazzdb, synth  # noqa: E402
+
+PARAMS = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=32)
+CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
+CPU_SAMPLE_SCALE = 0.2   # CPU baseline: the same genome/read model on a 1/5-size genome
+
+
+def make_db(workload, seed_offset=0, scale=1.0):
+    """Generates (or reuses) the DB of a workload; returns the path of block 1."""
+    w = synth.WORKLOADS[workload]
+    import dataclasses
+    w = dataclasses.replace(w, seed=w.seed + 1000 * seed_offset)
+    if scale != 1.0:
+        g = w.genome
+        reps = tuple((max(1, int(round(c * scale))), u, d) for c, u, d in g.repeats)
+        w = dataclasses.replace(w, genome=dataclasses.replace(g, length=int(g.length * scale), repeats=reps))
+    d = os.path.join(CACHE, f"{workload}_s{w.seed}_x{scale}")
+    root = os.path.join(d, "W")
+    if not os.path.exists(root + ".db"):
+        reads, _ = synth.generate(w)
+        tmp = d + f".tmp{os.getpid()}"
+        os.makedirs(tmp, exist_ok=True)
+        dazzdb.write_db(os.path.join(tmp, "W"), reads, 100000)   # a single block
+        try:
+            os.rename(tmp, d)
+        except OSError:   # another process finished first
+            pass
+    return root + ".1"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_gpu(args):
+    import torch
+    import marvel_b200 as mb
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.synchronize()
+
+    path = make_db(args.workload, seed_offset=rank)
+    A = dazzdb.open_block(path)
+    ctx = mb.Context()
+    p = PARAMS
+    ctx.set_filter_params(p["k"], p["w"], p["t"], p["h"])
+    ctx.new_align_spec(p["e"], p["s"], A.freq)
+    ctx.set_globals(2 * p["l"], False, p["M"] * 0x40000000)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def reduce(vals, op):
+        if ws == 1:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=op)
+        return t.tolist()
+
+    # ---- device-resident timing
+    ctx.load_block(0, A)
+    for _ in range(args.warmup):
+        ctx.reset_overlap_buffer()
+        mb.run_loaded(ctx, True)
+    barrier()
+    l0 = mb.kernel_launches()
+    times, recs = [], 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            ctx.reset_overlap_buffer()
+            ctx.timer_mark(0)
+            mb.run_loaded(ctx, True)
+            ctx.timer_mark(1)
+            times.append(ctx.timer_elapsed_ms())
+            recs += ctx.stats()["records"]
+    barrier()
+    launches = mb.kernel_launches() - l0
+    st = ctx.stats()
+    tot_ms = sum(times)
+    tot_ms_max, = reduce([tot_ms], torch.distributed.ReduceOp.MAX if ws > 1 else None)
+    recs_all, = reduce([float(recs)], torch.distributed.ReduceOp.SUM if ws > 1 else None)
+    value = recs_all / (tot_ms_max / 1e3)
+
+    # ---- end to end through the C ABI from pinned host buffers
+    pin_bases = torch.empty(A.bases.size, dtype=torch.uint8, pin_memory=True)
+    pin_bases.numpy()[:] = A.bases
+    Ap = dazzdb.Block(pin_bases.numpy(), A.boff, A.rlen, A.ufirst, A.part, A.freq, A.maxlen, A.totlen)
+    h2d = A.bases.size + A.boff.nbytes + A.rlen.nbytes
+    etimes, erecs, d2h = [], 0, 0
+    for i in range(args.warmup + args.steps):
+        ctx.reset_overlap_buffer()
+        ctx.timer_mark(0)
+        ctx.load_block(0, Ap)
+        mb.run_loaded(ctx, True)
+        r, tr = ctx.overlaps()
+        ctx.timer_mark(1)
+        if i >= args.warmup:
+            etimes.append(ctx.timer_elapsed_ms())
+            erecs += r.size
+            d2h = r.size * mb.OVL_DTYPE.itemsize + tr.size
+    barrier()
+    e_ms_max, = reduce([sum(etimes)], torch.distributed.ReduceOp.MAX if ws > 1 else None)
+    erecs_all, = reduce([float(erecs)], torch.distributed.ReduceOp.SUM if ws > 1 else None)
+    e2e = erecs_all / (e_ms_max / 1e3)
+
+    out = None
+    if rank == 0:
+        ms_step = tot_ms_max / args.steps
+        cells = sum(st["cells"])
+        align_ms = sum(st["ms_align"])
+        gcups = cells / (align_ms / 1e3) / 1e9 if align_ms > 0 else None
+        peaks = load_peaks()
+        clocks = clk.summary()
+        # roofline of the dominant stage: the seed-scan/alignment kernel is integer-issue bound;
+        # its algorithmic work is 16 integer lane-ops per wave cell (the reference's per-cell
+        # body, dalign/align.c:748-910).  Peak = 148 SMs x 4 schedulers x 32 lanes x SM clock.
+        sm_hz = (clocks["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)) * 1e6
+        issue_peak = 148 * 128 * sm_hz / 1e12  # T lane-ops/s
+        achieved = cells * 16 / (align_ms / 1e3) / 1e12 if align_ms > 0 else None
+        kmers = sum(st["kmers"][0:3:2])
+        idx_ms = st["ms_index"][0] + st["ms_index"][2]
+        # k-mer index: extraction writes 8 B per k-mer and reads 1 B/base; 4 LSD passes move
+        # 16 B per k-mer each (read+write key and value), as the reference's pass count
+        idx_bytes = kmers * (8 + 1 + 4 * 16 + 12)
+        out = {
+            "metric": "overlaps/s (plain daligner path, one block vs itself)",
+            "value": round(value, 1),
+            "unit": "overlaps/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_step, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u8/int32",
+            "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": f"{args.workload}: " + WORKLOAD_DESC.get(args.workload, args.workload),
+                       "flags": "-k14 -w6 -h35 -e.70 -l1000 -s100 -M32", "block_reads": A.nreads,
+                       "block_bases": int(A.totlen), "parallelism": f"dp{ws} (one block per GPU)",
+                       "l2": "inputs larger than L2 (k-mer index > 1 GB)"},
+            "records_per_step": recs // args.steps,
+            "stages_ms": {"index": round(idx_ms, 3), "merge_hitsort": round(sum(st["ms_merge"]), 3),
+                          "seed_scan_align": round(align_ms, 3)},
+            "gcups": round(gcups, 2) if gcups else None,
+            "roofline": {"bound": "issue", "kernel": "k_align_pairs", "achieved": round(achieved, 3),
+                         "peak": round(issue_peak, 2), "unit": "T int lane-ops/s",
+                         "frac": round(achieved / issue_peak, 4), "traffic": None,
+                         "peak_source": "derived: 148 SM x 128 lanes/clk x median SM clock under load"},
+            "roofline_filter": {"bound": "hbm", "kernel": "k-mer index (extract + 4 LSD passes)",
+                                "achieved": round(idx_bytes / (idx_ms / 1e3) / 1e9, 1),
+                                "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                                "frac": round(idx_bytes / (idx_ms / 1e3) / 1e9 / peaks.get("hbm_gbs", 6650.0), 4),
+                                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+            "e2e": {"value": round(e2e, 1), "unit": "overlaps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        if args.cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return out
+
+
+WORKLOAD_DESC = {
+    "cfg2": "4.6 Mbp random genome + 40x5 kbp repeats @1.5% + 3x6 kbp @0.2%, 25x reads, log-normal mean 10 kbp "
+            "sd 5 kbp, 9/4.5/1.5% ins/del/sub; one block (~115 Mbp) vs itself",
+    "cfg1": "1 Mbp genome, 20x, mean 8 kbp sd 4 kbp, 9/4.5/1.5% ins/del/sub; one block vs itself",
+    "cfg3": "10 Mbp genome, 30x, mean 20 kbp sd 15 kbp (1-150 kbp), 3/5/2% ins/del/sub; one block vs itself",
+}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def ref_binary():
+    b = os.path.join(ROOT, "oracle", "_ref", "daligner")
+    return b if os.path.exists(b) and os.access(b, os.X_OK) else None
+
+
+def ref_threads():
+    n = os.cpu_count() or 1
+    j = 1
+    while j * 2 <= n:
+        j *= 2
+    return j
+
+
+def run_reference_once(path, threads):
+    """The reference daligner on a block against itself; returns (records, seconds)."""
+    b = ref_binary()
+    d = os.path.dirname(path)
+    name = os.path.basename(path)
+    cmd = [b, f"-j{threads}", "-M32", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100", name, name]
+    t = time.perf_counter()
+    subprocess.run(cmd, cwd=d, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    dt = time.perf_counter() - t
+    las = os.path.join(d, "001_00001", "W.1.W.1.las")
+    with open(las, "rb") as f:
+        n = int(np.frombuffer(f.read(8), "<i8")[0])
+    return n, dt
+
+
+def cpu_baseline(args):
+    path = make_db(args.workload, scale=CPU_SAMPLE_SCALE)
+    if ref_binary():
+        j = ref_threads()
+        n, dt = run_reference_once(path, j)
+        return {"value": round(n / dt, 1), "unit": "overlaps/s", "cores": j, "kind": "reference",
+                "sample": f"reference daligner -j{j} on the {args.workload} model with a {CPU_SAMPLE_SCALE}x genome "
+                          f"({n} overlaps, {dt:.1f} s wall)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    A = dazzdb.open_block(path)
+    p = oracle.make_params(A.freq)
+    t = time.perf_counter()
+    recs, _, _ = oracle.daligner(A, A, dazzdb.complement_block(A), p, True)
+    dt = time.perf_counter() - t
+    return {"value": round(len(recs) / dt, 1), "unit": "overlaps/s", "cores": 1, "kind": "port",
+            "sample": f"C restatement, 1 thread, {args.workload} model with a {CPU_SAMPLE_SCALE}x genome"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return None
+    if not ref_binary():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/daligner was not built "
+                          "(make -C oracle ref needs the reference sources)"}))
+        return None
+    path = make_db(args.workload, scale=CPU_SAMPLE_SCALE)
+    j = ref_threads()
+    for _ in range(args.warmup):
+        run_reference_once(path, j)
+    n_tot, t_tot = 0, 0.0
+    for _ in range(args.steps):
+        n, dt = run_reference_once(path, j)
+        n_tot += n
+        t_tot += dt
+    v = n_tot / t_tot
+    sample = (f"reference daligner -j{j} (host cores) on the {args.workload} model with a {CPU_SAMPLE_SCALE}x genome, "
+              f"{n_tot // args.steps} overlaps per step")
+    out = {"impl": "reference", "metric": "overlaps/s (plain daligner path, one block vs itself)",
+           "value": round(v, 1), "unit": "overlaps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(1e3 * t_tot / args.steps, 1), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded generator, no dataset)",
+           "config": {"workload": f"{args.workload}: " + WORKLOAD_DESC.get(args.workload, args.workload),
+                      "flags": "-k14 -w6 -h35 -e.70 -l1000 -s100 -M32", "cpu_sample_scale": CPU_SAMPLE_SCALE},
+           "cpu_baseline": {"value": round(v, 1), "unit": "overlaps/s", "cores": j, "kind": "reference",
+                            "sample": sample},
+           "e2e": {"value": round(v, 1), "unit": "overlaps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(synth.WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -80,6 +80,10 @@ int gd_set_globals(gd_context* ctx, int minover, int identity, uint64_t mem_limi
 /* Copy a block to the device into slot 0 (A), 1 (B) or 2 (complemented B). */
 int gd_load_block(gd_context* ctx, int slot, const gd_block* block);
 
+/* complement_DB (dalign/daligner.c:474-573) on the device: slot dst becomes the
+ * reverse complement of slot src (reads, and mask intervals mirrored). */
+int gd_complement_block(gd_context* ctx, int src, int dst);
+
 /* Sort_Kmers (dalign/filter.c:698-903): builds the sorted k-mer index of a loaded slot on
  * the device; returns its length. */
 int64_t gd_sort_kmers(gd_context* ctx, int slot);
@@ -103,6 +107,13 @@ int gd_write_overlap_buffer(gd_context* ctx, int run_id, const char* ablock, con
 int gd_reset_overlap_buffer(gd_context* ctx);
 
 int gd_get_stats(gd_context* ctx, gd_stats* st);
+
+/* Device timer on the context's stream: mark 0 = start, mark 1 = stop; elapsed in ms. */
+int gd_timer_mark(gd_context* ctx, int which);
+double gd_timer_elapsed_ms(gd_context* ctx);
+
+/* Kernels this library has launched since it was loaded (launch accounting). */
+unsigned long long gd_kernel_launches(void);
 
 /* Local_Alignment (dalign/align.c:1922-2060) for a batch of seeds on the device.
  * Sequences are host buffers in gd_block layout; per seed: read offsets into abases /

@@ -57,7 +57,8 @@ class GdStats(C.Structure):
 SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "gd_new_align_spec",
            "gd_set_globals", "gd_load_block", "gd_sort_kmers", "gd_get_kmers", "gd_match_filter", "gd_get_hits",
            "gd_num_overlaps", "gd_get_overlaps", "gd_write_overlap_buffer", "gd_reset_overlap_buffer",
-           "gd_get_stats", "gd_local_alignment_batch"]
+           "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
+           "gd_timer_elapsed_ms", "gd_kernel_launches"]
 
 
 def lib():
@@ -92,8 +93,18 @@ def lib():
     L.gd_local_alignment_batch.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                            C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    L.gd_complement_block.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.gd_timer_mark.argtypes = [C.c_void_p, C.c_int]
+    L.gd_timer_elapsed_ms.argtypes = [C.c_void_p]
+    L.gd_timer_elapsed_ms.restype = C.c_double
+    L.gd_kernel_launches.restype = C.c_ulonglong
     _lib = L
     return L
+
+
+def kernel_launches():
+    """Kernels libgpudalign.so has launched since it was loaded."""
+    return int(lib().gd_kernel_launches())
 
 
 class GpuError(RuntimeError):
@@ -170,6 +181,18 @@ class Context:
         r = _BlockRef(blk)
         _check(lib().gd_load_block(self.h, slot, C.byref(r.s)))
 
+    def complement_block(self, src, dst):
+        _check(lib().gd_complement_block(self.h, src, dst))
+
+    def timer_mark(self, which):
+        _check(lib().gd_timer_mark(self.h, which))
+
+    def timer_elapsed_ms(self):
+        ms = lib().gd_timer_elapsed_ms(self.h)
+        if ms < 0:
+            raise GpuError(lib().gd_last_error().decode())
+        return ms
+
     def sort_kmers(self, slot):
         return _check(lib().gd_sort_kmers(self.h, slot))
 
@@ -237,19 +260,26 @@ def daligner_block(ctx: Context, A: dazzdb.Block, B: dazzdb.Block | None = None,
     ctx.set_globals(2 * l, identity or only_identity, int(M) * 0x40000000)
     ctx.reset_overlap_buffer()
     ctx.load_block(0, A)
+    if not self_cmp:
+        ctx.load_block(1, B)
+    run_loaded(ctx, self_cmp)
+    return ctx.overlaps()
+
+
+def run_loaded(ctx: Context, self_cmp: bool):
+    """The per-block device pipeline once the blocks are resident: Sort_Kmers(A),
+    Match_Filter(A, B), complement_DB(B), Sort_Kmers(cB), Match_Filter(A, cB)
+    (dalign/daligner.c:957-1012)."""
     ctx.sort_kmers(0)
     if self_cmp:
         ctx.match_filter(0, 0, 1)
-        Bc = dazzdb.complement_block(A)
+        ctx.complement_block(0, 2)
     else:
-        ctx.load_block(1, B)
         ctx.sort_kmers(1)
         ctx.match_filter(1, 0, 0)
-        Bc = dazzdb.complement_block(B)
-    ctx.load_block(2, Bc)
+        ctx.complement_block(1, 2)
     ctx.sort_kmers(2)
     ctx.match_filter(2, 1, int(self_cmp))
-    return ctx.overlaps()
 
 
 def write_las(path, recs, trace, tspace):

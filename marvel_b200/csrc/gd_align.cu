@@ -1531,6 +1531,7 @@ int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hke
     if (ngroups == 0)
         return 0;
     k_align_pairs<<<grid, ALIGN_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p, sc, out, queue, st);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -1607,6 +1608,7 @@ int launch_la_batch(const uint8_t* aseq_base, const int64_t* aoff, const int32_t
     int grid = gd_cdiv(sc.nwarps, ALIGN_WARPS);
     k_la_batch<<<grid, ALIGN_WARPS * 32, 0, s>>>(aseq_base, aoff, alen, bseq_base, boff, blen, diag, anti, nseeds, p, sc,
                                                  out12, tr, trstride, cells, st);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }

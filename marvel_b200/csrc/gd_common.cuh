@@ -21,6 +21,10 @@
 
 void gd_set_error(const char* fmt, ...);
 
+// Number of kernels this library has launched (all contexts), for launch accounting.
+extern unsigned long long g_gd_launches;
+#define GD_LAUNCHED(n) (g_gd_launches += (n))
+
 // A DB block resident in HBM, laid out like the reference's in-memory block
 // (db/DB.c:1349-1410): one byte per base (0..3), a 4 before read 0 and after every read,
 // read i at bases[boff[i]].  The allocation carries 16 bytes of slack on each side so

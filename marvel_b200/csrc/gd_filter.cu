@@ -84,6 +84,7 @@ int launch_extract(const DevBlock& b, const int64_t* mask_anno, const int32_t* m
         return 0;
     k_extract<K><<<(unsigned)gd_cdiv<int64_t>(nslots, FT), FT, 0, s>>>(b, mask_anno, mask_data, kmer, keys, vals,
                                                                         nslots, nmasked);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -107,6 +108,7 @@ int launch_decode(const DevBlock& b, int kmer, const uint32_t* slots, int64_t n,
     if (n <= 0)
         return 0;
     k_decode<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(b, kmer, slots, n, read, rpos);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -158,6 +160,7 @@ int launch_suppress_flags(const K* code, int64_t n, int t, uint32_t* keep, cudaS
     if (n <= 0)
         return 0;
     k_suppress<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(code, n, t, keep);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -184,6 +187,7 @@ int launch_compact_index(const K* code, const int32_t* read, const int32_t* rpos
         return 0;
     k_compact_index<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(code, read, rpos, keep, pos, n, code2, read2,
                                                                          rpos2);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -202,6 +206,7 @@ int launch_run_flags(const K* code, int64_t n, uint32_t* flags, cudaStream_t s)
     if (n <= 0)
         return 0;
     k_run_flags<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(code, n, flags);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -292,6 +297,7 @@ int launch_pair_count(const K* acode, const int32_t* aread, const int32_t* arpos
         return 0;
     k_pair_count<K><<<(unsigned)gd_cdiv<int64_t>(m.na, FT), FT, 0, s>>>(acode, aread, arpos, arun_excl, arun_flag,
                                                                          bcode, bread, brpos, m, jb, cnt, ctrun);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -313,6 +319,7 @@ int launch_gram(const unsigned long long* ctrun, int64_t nruns, unsigned long lo
     if (nruns <= 0)
         return 0;
     k_gram<<<(unsigned)gd_cdiv<int64_t>(nruns, FT), FT, 0, s>>>(ctrun, nruns, gram);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -335,6 +342,7 @@ int launch_cnt_mask(const uint32_t* arun_excl, const uint32_t* arun_flag, const 
     if (na <= 0)
         return 0;
     k_cnt_mask<<<(unsigned)gd_cdiv<int64_t>(na, FT), FT, 0, s>>>(arun_excl, arun_flag, ctrun, na, limit, always, cnt);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -372,6 +380,7 @@ int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread
         return 0;
     k_emit<<<(unsigned)gd_cdiv<int64_t>(na, FT), FT, 0, s>>>(aread, arpos, bread, brpos, jb, cnt, hoff, na, hb, hkey,
                                                              hdiag);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -389,6 +398,7 @@ int launch_pair_flags(const uint64_t* hkey, int64_t n, int pbits, uint32_t* flag
     if (n <= 0)
         return 0;
     k_pair_flags<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(hkey, n, pbits, flags);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -406,6 +416,7 @@ int launch_pair_scatter(const uint32_t* flags, const uint32_t* pos, int64_t n, u
     if (n <= 0)
         return 0;
     k_pair_scatter<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(flags, pos, n, starts);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -458,6 +469,50 @@ int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits,
         return 0;
     k_select_groups<<<(unsigned)gd_cdiv<int64_t>(nstarts, FT), FT, 0, s>>>(starts, nstarts, nhits, minhit, hkey, hb,
                                                                            arlen, brlen, groups, cost, idx, ngroups);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_complement(DevBlock b, uint8_t* dst)
+{
+    int r = blockIdx.x;
+    int len = b.rlen[r];
+    const uint8_t* s = b.bases + b.boff[r];
+    uint8_t* d = dst + b.boff[r];
+    for (int p = threadIdx.x; p < len; p += FT)
+        d[p] = (uint8_t)(3 - s[len - 1 - p]);
+}
+
+__global__ void __launch_bounds__(FT) k_complement_mask(DevBlock b, const int64_t* anno, const int32_t* src,
+                                                       int32_t* dst)
+{
+    int r = blockIdx.x * FT + threadIdx.x;
+    if (r >= b.nreads)
+        return;
+    int64_t a0 = anno[r], a1 = anno[r + 1];
+    int len = b.rlen[r];
+    int64_t npair = (a1 - a0) / 2;
+    for (int64_t j = 0; j < npair; j++)
+    {
+        int64_t q = a0 + 2 * (npair - 1 - j);
+        dst[a0 + 2 * j] = len - src[q + 1];
+        dst[a0 + 2 * j + 1] = len - src[q];
+    }
+}
+
+int launch_complement(const DevBlock& src, uint8_t* dst_bases, const int64_t* anno, const int32_t* mdata,
+                      int32_t* mdata_dst, cudaStream_t s)
+{
+    if (src.nreads <= 0)
+        return 0;
+    k_complement<<<src.nreads, FT, 0, s>>>(src, dst_bases);
+    GD_LAUNCHED(1);
+    if (anno)
+    {
+        k_complement_mask<<<(unsigned)gd_cdiv(src.nreads, FT), FT, 0, s>>>(src, anno, mdata, mdata_dst);
+        GD_LAUNCHED(1);
+    }
     GD_CUDA(cudaGetLastError());
     return 0;
 }

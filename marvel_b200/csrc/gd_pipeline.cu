@@ -20,6 +20,7 @@
 #include "gd_prims.cuh"
 
 static thread_local char g_err[1024] = "";
+unsigned long long g_gd_launches = 0;
 
 void gd_set_error(const char* fmt, ...)
 {
@@ -122,7 +123,7 @@ struct gd_context
     std::vector<gd_overlap> recs;
     std::vector<uint8_t> trace;
     gd_stats stats;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
 };
 
 // ----------------------------------------------------------------------------------------
@@ -610,7 +611,8 @@ gd_context* gd_create(void)
     gd_context* c = new gd_context();
     memset(&c->stats, 0, sizeof(c->stats));
     if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->tev0) != cudaSuccess || cudaEventCreate(&c->tev1) != cudaSuccess)
     {
         gd_set_error("stream/event creation failed");
         delete c;
@@ -639,6 +641,8 @@ void gd_destroy(gd_context* c)
     }
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
+    cudaEventDestroy(c->tev0);
+    cudaEventDestroy(c->tev1);
     cudaStreamDestroy(c->s);
     delete c;
 }
@@ -735,6 +739,76 @@ int gd_load_block(gd_context* c, int slot, const gd_block* b)
     s.nk = -1;
     GD_CUDA(cudaStreamSynchronize(c->s));
     return 0;
+}
+
+int gd_complement_block(gd_context* c, int src, int dst)
+{
+    if (src < 0 || src > 2 || dst < 0 || dst > 2 || src == dst || !c->slot[src].loaded)
+    {
+        gd_set_error("bad complement slots %d -> %d", src, dst);
+        return -1;
+    }
+    Slot& S = c->slot[src];
+    Slot& D = c->slot[dst];
+    int64_t nb = S.blk.boff ? 0 : 0;
+    int n = S.blk.nreads;
+    std::vector<int64_t> boff_last(1);
+    GD_CUDA(cudaMemcpy(boff_last.data(), S.blk.boff + n, 8, cudaMemcpyDeviceToHost));
+    nb = boff_last[0];
+    if (ensure(D.bases, nb + 1 + 64) || ensure(D.boff, (n + 1) * 8) || ensure(D.rlen, n * 4 + 4))
+        return -1;
+    GD_CUDA(cudaMemsetAsync(D.bases.p, 4, nb + 1 + 64, c->s));
+    GD_CUDA(cudaMemcpyAsync(D.boff.p, S.boff.p, (n + 1) * 8, cudaMemcpyDeviceToDevice, c->s));
+    GD_CUDA(cudaMemcpyAsync(D.rlen.p, S.rlen.p, n * 4, cudaMemcpyDeviceToDevice, c->s));
+    D.has_mask = S.has_mask;
+    int32_t* mdst = nullptr;
+    if (S.has_mask)
+    {
+        int64_t nd = 0;
+        GD_CUDA(cudaMemcpy(&nd, P<int64_t>(S.manno) + n, 8, cudaMemcpyDeviceToHost));
+        if (ensure(D.manno, (n + 1) * 8) || ensure(D.mdata, nd * 4 + 8))
+            return -1;
+        GD_CUDA(cudaMemcpyAsync(D.manno.p, S.manno.p, (n + 1) * 8, cudaMemcpyDeviceToDevice, c->s));
+        mdst = P<int32_t>(D.mdata);
+    }
+    D.blk = S.blk;
+    D.blk.bases = (const uint8_t*)D.bases.p + 33;
+    D.blk.boff = P<int64_t>(D.boff);
+    D.blk.rlen = P<int32_t>(D.rlen);
+    if (gd::launch_complement(S.blk, (uint8_t*)D.bases.p + 33, S.has_mask ? P<int64_t>(S.manno) : nullptr,
+                              S.has_mask ? P<int32_t>(S.mdata) : nullptr, mdst, c->s))
+        return -1;
+    D.totlen = S.totlen;
+    D.nslots = S.nslots;
+    D.hrlen = S.hrlen;
+    D.loaded = 1;
+    D.nk = -1;
+    GD_CUDA(cudaStreamSynchronize(c->s));
+    return 0;
+}
+
+int gd_timer_mark(gd_context* c, int which)
+{
+    if (which < 0 || which > 1)
+        return -1;
+    GD_CUDA(cudaEventRecord(which ? c->tev1 : c->tev0, c->s));
+    return 0;
+}
+
+double gd_timer_elapsed_ms(gd_context* c)
+{
+    float ms = -1.f;
+    if (cudaEventSynchronize(c->tev1) != cudaSuccess || cudaEventElapsedTime(&ms, c->tev0, c->tev1) != cudaSuccess)
+    {
+        gd_set_error("timer events not recorded");
+        return -1.0;
+    }
+    return ms;
+}
+
+unsigned long long gd_kernel_launches(void)
+{
+    return g_gd_launches;
 }
 
 int64_t gd_sort_kmers(gd_context* c, int slot)

@@ -142,8 +142,11 @@ int exclusive_scan(const T* in, T* out, int64_t n, T* total, void* scratch, cuda
         return 0;
     }
     k_scan_reduce<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, partial);
+    GD_LAUNCHED(1);
     k_scan_partials<T><<<1, 1024, 0, s>>>(partial, tiles, total);
+    GD_LAUNCHED(1);
     k_scan_down<T><<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, out, n, partial);
+    GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -268,9 +271,11 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
         K* kout = cur ? k0 : k1;
         uint32_t* vout = cur ? v0 : v1;
         k_rs_hist<K><<<ntiles, RS_THREADS, 0, s>>>(kin, n, b, counts, ntiles);
+        GD_LAUNCHED(1);
         if (exclusive_scan<uint32_t>(counts, counts, ncnt, (uint32_t*)nullptr, sscr, s))
             return -1;
         k_rs_scatter<K><<<ntiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, b, counts, ntiles);
+        GD_LAUNCHED(1);
         cur ^= 1;
     }
     GD_CUDA(cudaGetLastError());

@@ -175,7 +175,7 @@ def write_db(path_root, reads, block_mbp=200, ufirst_split=True):
         f.write(bytes(hdr))
         f.write(recs.tobytes())
     # block boundaries exactly as DBsplit -s computes them
-    size = block_mbp * 1000000
+    size = int(block_mbp * 1000000)
     bounds = [0]
     tot = 0
     for i in range(n):

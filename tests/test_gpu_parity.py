@@ -1,0 +1,182 @@
+"""GPU parity: the sm_100a path against the reference's golden .las files and the oracle.
+
+Bit-exact for everything (integer work): .las records and every trace byte, the k-mer
+index, the sorted hit list, and single Local_Alignment calls."""
+import os
+
+import numpy as np
+import pytest
+
+import daligner_run
+from golden_cases import cases, load
+from marvel_b200 import dazzdb, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mb():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import marvel_b200
+    return marvel_b200
+
+
+@pytest.mark.parametrize("name", cases())
+def test_gpu_matches_reference_golden(mb, name, tmp_path):
+    d, meta = load(name)
+    names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "gpu")
+    assert sorted(names) == sorted(meta["las"])
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
+        assert ok, f"{name} {n}: {msg}"
+
+
+def _ctx(mb, A, k=14, w=6, t=0, h=35):
+    ctx = mb.Context()
+    ctx.set_filter_params(k, w, t, h)
+    ctx.new_align_spec(0.70, 100, A.freq)
+    ctx.set_globals(2000, False, 32 << 30)
+    return ctx
+
+
+@pytest.mark.parametrize("name,k", [("self_default", 14), ("self_k16_w5", 16)])
+def test_kmer_index_and_hits_match_oracle(mb, name, k):
+    import oracle
+    d, _ = load(name)
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    p = oracle.make_params(A.freq, k=k)
+    ctx = _ctx(mb, A, k=k)
+    ctx.load_block(0, A)
+    n = ctx.sort_kmers(0)
+    gc, gr, gp = ctx.get_kmers(0, n)
+    oc, orr, op = oracle.sort_kmers(A, p)
+    assert n == oc.size
+    assert (gc == oc).all() and (gr == orr).all() and (gp == op).all()
+    ctx.match_filter(0, 0, 1)
+    gh = ctx.get_hits()
+    oh, limit = oracle.match_hits(A, A, p, True)
+    assert gh.shape == oh.shape and (gh == oh).all()
+    assert ctx.stats()["limit"][0] == limit
+    ctx.close()
+
+
+def test_masked_index_matches_oracle(mb):
+    """-m track masking in tuple extraction (dalign/filter.c:428-470), masks mirrored for cB."""
+    import oracle
+    d, _ = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    rng = np.random.default_rng(3)
+    mask = []
+    for i in range(A.nreads):
+        L = int(A.rlen[i])
+        cuts = np.sort(rng.choice(L, size=2 * int(rng.integers(0, 4)), replace=False)).tolist()
+        iv = [(cuts[j], cuts[j + 1]) for j in range(0, len(cuts), 2)]
+        if i % 7 == 0:
+            iv = [(0, 30)] + [x for x in iv if x[0] > 30]
+        mask.append(iv)
+    A.mask = mask
+    p = oracle.make_params(A.freq)
+    ctx = _ctx(mb, A)
+    ctx.load_block(0, A)
+    n = ctx.sort_kmers(0)
+    gc, gr, gp = ctx.get_kmers(0, n)
+    oc, orr, op = oracle.sort_kmers(A, p)
+    assert n == oc.size and (gc == oc).all() and (gr == orr).all() and (gp == op).all()
+    # the device complement mirrors the intervals like complement_DB
+    ctx.complement_block(0, 2)
+    n2 = ctx.sort_kmers(2)
+    c2, r2, p2 = ctx.get_kmers(2, n2)
+    oc2, or2, op2 = oracle.sort_kmers(dazzdb.complement_block(A), p)
+    assert n2 == oc2.size and (c2 == oc2).all() and (r2 == or2).all() and (p2 == op2).all()
+    # and the full masked comparison equals the oracle's
+    import oracle as O
+    recs, traces, _ = O.daligner(A, A, dazzdb.complement_block(A), p, True)
+    ctx.reset_overlap_buffer()
+    ctx.match_filter(0, 0, 1)
+    ctx.match_filter(2, 1, 1)
+    r, tr = ctx.overlaps()
+    assert r.size == len(recs)
+    for x, y, t in zip(r, recs, traces):
+        for f in ("aread", "bread", "flags", "abpos", "aepos", "bbpos", "bepos", "diffs", "tlen"):
+            assert int(x[f]) == int(y[f]), f
+        assert (tr[int(x["toff"]):int(x["toff"]) + int(x["tlen"])] == t).all()
+    ctx.close()
+
+
+@pytest.mark.parametrize("comp", [0, 1])
+def test_local_alignment_batch_matches_oracle(mb, comp):
+    """Single Local_Alignment calls from seeds on real hits (and, for comp=1, from the same
+    points on the complemented read: mostly dead starts that exercise the boundary logic)."""
+    import oracle
+    d, _ = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    B = dazzdb.complement_block(A) if comp else A
+    p = oracle.make_params(A.freq)
+    h, _ = oracle.match_hits(A, A, p, True)
+    rng = np.random.default_rng(11 + comp)
+    rows = h[rng.choice(len(h), size=600, replace=False)]
+    diag, apos, ar, br = rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3]
+    anti = 2 * apos - diag
+    aoff, boff = A.boff[ar] + 1, B.boff[br] + 1
+    alen, blen = A.rlen[ar], B.rlen[br]
+    ctx = _ctx(mb, A)
+    out, tr, cells = ctx.local_alignment_batch(A.bases, aoff, alen, B.bases, boff, blen, diag, anti, comp)
+    half = tr.shape[1] // 2
+    for i in range(len(diag)):
+        a = A.bases[aoff[i] - 1:aoff[i] + alen[i] + 1]
+        b = B.bases[boff[i] - 1:boff[i] + blen[i] + 1]
+        o, at, bt, oc = oracle.local_alignment(a, b, comp, int(diag[i]), int(anti[i]), p)
+        assert (out[i] == o).all(), (i, out[i], o)
+        assert (tr[i, :o[5]] == at).all() and (tr[i, half:half + o[11]] == bt).all()
+        assert cells[i] == oc
+    ctx.close()
+
+
+def test_full_block_cfg1_matches_oracle_and_is_deterministic(mb, tmp_path):
+    """The 1 Mbp / 20x workload (2.5k reads, 21 Mbp) end to end against the oracle."""
+    import oracle
+    reads, _ = synth.generate("cfg1")
+    dazzdb.write_db(str(tmp_path / "C"), reads, 200)
+    A = dazzdb.open_block(str(tmp_path / "C.1"))
+    ctx = mb.Context()
+    r1, t1 = mb.daligner_block(ctx, A)
+    r2, t2 = mb.daligner_block(ctx, A)
+    assert (r1 == r2).all() and (t1 == t2).all()
+    st = ctx.stats()
+    ctx.close()
+    recs, traces, ost = oracle.daligner(A, A, dazzdb.complement_block(A), oracle.make_params(A.freq), True)
+    assert r1.size == len(recs)
+    assert st["seeds"] == [ost["seeds_n"], ost["seeds_c"]]
+    assert sum(st["cells"]) == ost["cells"]
+    mb.write_las(str(tmp_path / "g.las"), r1, t1, 100)
+    oracle.write_las(str(tmp_path / "o.las"), recs, traces, 100)
+    ok, msg = dazzdb.las_equal(str(tmp_path / "g.las"), str(tmp_path / "o.las"))
+    assert ok, msg
+
+
+def test_size_independent_properties_cfg2(mb, tmp_path):
+    """The bacterial workload at full size (~115 Mbp block): the output is sorted by
+    (aread, bread, comp, abpos), every A-path has its B-path mirror, traces are consistent
+    (Check_Trace_Points, dalign/align.c:3419-3449), and two runs are identical."""
+    import bench
+    A = dazzdb.open_block(bench.make_db("cfg2"))
+    ctx = mb.Context()
+    r, t = mb.daligner_block(ctx, A)
+    r2, t2 = mb.daligner_block(ctx, A)
+    ctx.close()
+    assert (r == r2).all() and (t == t2).all()
+    key = np.stack([r["aread"], r["bread"], r["flags"] & 1, r["abpos"]], 1)
+    srt = key[np.lexsort(key.T[::-1])]
+    assert (key == srt).all()
+    # symmetric: an A-path (ar, br) record has a B-path (br, ar) record of the same orientation
+    fwd = set(zip(r["aread"].tolist(), r["bread"].tolist(), (r["flags"] & 1).tolist()))
+    assert all((b, a, c) in fwd for (a, b, c) in fwd)
+    # trace points: pairs, sum of b deltas = b span, one pair per trace interval of a
+    for i in range(0, r.size, 97):
+        x = r[i]
+        tr = t[int(x["toff"]):int(x["toff"]) + int(x["tlen"])]
+        assert int(x["tlen"]) % 2 == 0
+        assert int(tr[1::2].sum()) == int(x["bepos"] - x["bbpos"])
+        npts = (int(x["aepos"]) - 1) // 100 - int(x["abpos"]) // 100 + 1
+        assert int(x["tlen"]) == 2 * npts

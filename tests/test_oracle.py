@@ -1,0 +1,47 @@
+"""The CPU restatement (oracle) reproduces the reference daligner's golden .las files."""
+import os
+
+import pytest
+
+import daligner_run
+from golden_cases import cases, load
+from marvel_b200 import dazzdb
+
+
+@pytest.mark.parametrize("name", cases())
+def test_oracle_matches_reference_golden(name, tmp_path):
+    d, meta = load(name)
+    names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "oracle")
+    assert sorted(names) == sorted(meta["las"])
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
+        assert ok, f"{name} {n}: {msg}"
+
+
+def test_oracle_kmer_index_is_sorted_and_complete():
+    import oracle
+    d, _ = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    p = oracle.make_params(A.freq)
+    code, read, rpos = oracle.sort_kmers(A, p)
+    assert code.size == A.totlen - A.nreads * (14 - 1)
+    key = (code.astype(object) << 64) | (read.astype(object) << 32) | rpos.astype(object)
+    assert all(key[i] < key[i + 1] for i in range(0, code.size - 1, 997))
+    # spot-check codes against the bases
+    for i in range(0, code.size, 50021):
+        s = A.read(int(read[i]))[int(rpos[i]) - 13:int(rpos[i]) + 1]
+        c = 0
+        for x in s:
+            c = (c << 2) | int(x)
+        assert c == int(code[i])
+
+
+def test_oracle_hits_sorted_by_bread_aread_apos():
+    import oracle
+    d, _ = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    h, limit = oracle.match_hits(A, A, oracle.make_params(A.freq), True)
+    assert limit == 10000
+    k = list(zip(h[:, 3], h[:, 2], h[:, 1], -h[:, 0]))
+    assert k == sorted(k)
+    assert (h[:, 3] < h[:, 2]).all()   # within a block only b-read < a-read pairs
