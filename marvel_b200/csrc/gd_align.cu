@@ -86,6 +86,16 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
 {
     if (FWD)
     {
+        {
+            int cb = __ldg(bseq + y), ca = __ldg(aseq + y + k);
+            if (cb != ca || cb == 4)
+            {
+                bend = (cb == 4);
+                aend = !bend && (ca == 4);
+                return y;
+            }
+            y += 1;
+        }
         // the 4 after every read stops the extension; the cap only guards against a bad pointer
         for (int guard = (lim >> 3) + 2; guard > 0; guard--)
         {
@@ -93,31 +103,47 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
             uint64_t stop = (wa ^ wb) | (wb & SENT4);
             if (stop)
             {
-                y += (__ffsll((long long)stop) - 1) >> 3;
-                break;
+                int i = (__ffsll((long long)stop) - 1) >> 3;
+                y += i;
+                // the stop bases come from the compare windows themselves
+                int cb = (int)(wb >> (8 * i)) & 0xff;
+                bend = (cb == 4);
+                aend = !bend && (((int)(wa >> (8 * i)) & 0xff) == 4);
+                return y;
             }
             y += 8;
         }
-        int cb = __ldg(bseq + y);
-        bend = (cb == 4);
-        aend = !bend && (__ldg(aseq + y + k) == 4);
+        bend = aend = true;  // unreachable with well-formed blocks (every read ends with a 4)
     }
     else
     {
+        {
+            int cb = __ldg(bseq + y - 1), ca = __ldg(aseq + y + k - 1);
+            if (cb != ca || cb == 4)
+            {
+                bend = (cb == 4);
+                aend = !bend && (ca == 4);
+                return y;
+            }
+            y -= 1;
+        }
         for (int guard = (lim >> 3) + 2; guard > 0; guard--)
         {
             uint64_t wb = ld8u(bseq + y - 8), wa = ld8u(aseq + y + k - 8);
             uint64_t stop = (wa ^ wb) | (wb & SENT4);
             if (stop)
             {
-                y -= __clzll((long long)stop) >> 3;
-                break;
+                int i = __clzll((long long)stop) >> 3;
+                y -= i;
+                int sh = 8 * (7 - i);
+                int cb = (int)(wb >> sh) & 0xff;
+                bend = (cb == 4);
+                aend = !bend && (((int)(wa >> sh) & 0xff) == 4);
+                return y;
             }
             y -= 8;
         }
-        int cb = __ldg(bseq + y - 1);
-        bend = (cb == 4);
-        aend = !bend && (__ldg(aseq + y + k - 1) == 4);
+        bend = aend = true;
     }
     return y;
 }
@@ -365,6 +391,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             return;
         }
         const int nch = (width + 31) >> 5;
+        const int hgh0 = hgh, low0 = low;
         int rc[WAVE_CHUNKS], rha[WAVE_CHUNKS], rhb[WAVE_CHUNKS], rna[WAVE_CHUNKS], rnb[WAVE_CHUNKS];
         unsigned long long rb[WAVE_CHUNKS];
 #pragma unroll
@@ -505,26 +532,47 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 more = 0;
             }
 
-            // best point: every new maximum in scan order is a record (align.c:880-897)
+            // best point: every new maximum in scan order is a record (align.c:880-897).  The
+            // last record is the first lane holding the chunk maximum; when it also passes the
+            // PATH_AVE and trim-table tests it decides besta, lasta and trim at once, otherwise
+            // the records are enumerated with a prefix-max scan.
             int wv = valid ? (FWD ? c : -c) : INT_MIN;
-            int incl = warp_max_incl(wv, lane);
-            int excl = __shfl_up_sync(GD_FULL, incl, 1);
-            if (lane == 0)
-                excl = INT_MIN;
             int wbest = FWD ? besta : -besta;
-            bool rec = valid && wv > max(wbest, excl);
-            unsigned recm = __ballot_sync(GD_FULL, rec);
-            if (recm)
+            int wmax = __reduce_max_sync(GD_FULL, wv);
+            if (wmax > wbest)
             {
-                int j = 31 - __clz(recm);
-                besta = __shfl_sync(GD_FULL, c, j);
-                besty = __shfl_sync(GD_FULL, y, j);
-                bool p1 = rec && (__popcll(b & MASK61) >= PATH_AVE);
-                unsigned m1 = __ballot_sync(GD_FULL, p1);
-                if (m1)
+                int jm = __ffs(__ballot_sync(GD_FULL, wv == wmax)) - 1;
+                besta = __shfl_sync(GD_FULL, c, jm);
+                besty = __shfl_sync(GD_FULL, y, jm);
+                unsigned long long bj = __shfl_sync(GD_FULL, b, jm);
+                bool p1j = __popcll(bj & MASK61) >= PATH_AVE;
+                bool p2j = false;
+                if (p1j)
                 {
-                    int j1 = 31 - __clz(m1);
-                    lasta = __shfl_sync(GD_FULL, c, j1);
+                    int lo15 = (int)(bj & TRIM_MASK), hi15 = (int)((bj >> TRIM_LEN) & TRIM_MASK);
+                    p2j = (__ldg(P.table + lo15) >= 0) && (__ldg(P.table + hi15) + __ldg(P.score + lo15) >= 0);
+                }
+                if (p1j)
+                    lasta = besta;
+                if (p2j)
+                {
+                    trima = besta;
+                    trimy = besty;
+                    trimd = dif;
+                    trimha = __shfl_sync(GD_FULL, ha, jm);
+                    trimhb = __shfl_sync(GD_FULL, hb, jm);
+                }
+                else
+                {
+                    int incl = warp_max_incl(wv, lane);
+                    int excl = __shfl_up_sync(GD_FULL, incl, 1);
+                    if (lane == 0)
+                        excl = INT_MIN;
+                    bool rec = valid && wv > max(wbest, excl) && lane < jm;
+                    bool p1 = rec && (__popcll(b & MASK61) >= PATH_AVE);
+                    unsigned m1 = __ballot_sync(GD_FULL, p1);
+                    if (m1 && !p1j)
+                        lasta = __shfl_sync(GD_FULL, c, 31 - __clz(m1));
                     bool p2 = false;
                     if (p1)
                     {
@@ -565,20 +613,27 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
         __syncwarp();
         clip_block();
 
-        // drop diagonals more than WAVE_LAG behind the best (align.c:946-955)
+        // drop diagonals more than WAVE_LAG behind the best (align.c:946-955), from the
+        // new values still in registers; k runs monotonically with the lane position
         {
-            int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
-            int w2 = hgh - low + 1;
+            const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
+            const int hw = FWD ? hgh0 : low0;  // wave origin before clipping
             int nl = INT_MAX, nh = INT_MIN;
-            for (int base = 0; base < w2; base += 32)
+#pragma unroll
+            for (int ch = 0; ch < WAVE_CHUNKS; ch++)
             {
-                int k = low + base + lane;
-                bool good = (base + lane < w2) && (FWD ? (R.V[k & RM] >= n) : (R.V[k & RM] <= n));
+                if (ch >= nch)
+                    break;
+                int p = ch * 32 + lane;
+                int k = FWD ? hw - p : hw + p;
+                bool good = p < width && k >= low && k <= hgh && (FWD ? (rc[ch] >= n) : (rc[ch] <= n));
                 unsigned gm = __ballot_sync(GD_FULL, good);
                 if (gm)
                 {
-                    nl = min(nl, low + base + __ffs(gm) - 1);
-                    nh = max(nh, low + base + 31 - __clz(gm));
+                    int pf = ch * 32 + __ffs(gm) - 1, pl = ch * 32 + 31 - __clz(gm);
+                    int k1 = FWD ? hw - pf : hw + pf, k2 = FWD ? hw - pl : hw + pl;
+                    nl = min(nl, min(k1, k2));
+                    nh = max(nh, max(k1, k2));
                 }
             }
             if (nh != INT_MIN)
@@ -1203,7 +1258,7 @@ __device__ void emit_paths(WarpCtx& w, const AlignParams& P, const MPath* m, int
     }
 }
 
-__global__ void __launch_bounds__(ALIGN_WARPS * 32)
+__global__ void __launch_bounds__(ALIGN_WARPS * 32, 4)
     k_align_pairs(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
                   AlignScratch sc, AlignOut out, unsigned* queue, DevStatus* st)

@@ -302,15 +302,32 @@ int launch_pair_count(const K* acode, const int32_t* aread, const int32_t* arpos
     return 0;
 }
 
-__global__ void __launch_bounds__(FT) k_gram(const unsigned long long* ctrun, int64_t nruns, unsigned long long* gram)
+// Histogram of per-code pair counts (< MAXGRAM): block-local shared bins, match-any
+// aggregation of equal counts inside a warp, one global add per non-empty bin per block.
+__global__ void __launch_bounds__(FT) k_gram(const unsigned long long* __restrict__ ctrun, int64_t nruns,
+                                            unsigned long long* gram)
 {
-    int64_t r = (int64_t)blockIdx.x * FT + threadIdx.x;
-    if (r < nruns)
+    __shared__ unsigned int h[MAXGRAM];
+    for (int i = threadIdx.x; i < MAXGRAM; i += FT)
+        h[i] = 0;
+    __syncthreads();
+    for (int64_t base = (int64_t)blockIdx.x * FT; base < nruns; base += (int64_t)gridDim.x * FT)
     {
-        unsigned long long c = ctrun[r];
-        if (c < (unsigned long long)MAXGRAM)
-            atomicAdd(&gram[c], 1ull);
+        int64_t r = base + threadIdx.x;
+        unsigned c = MAXGRAM;
+        if (r < nruns)
+        {
+            unsigned long long x = ctrun[r];
+            c = x < (unsigned long long)MAXGRAM ? (unsigned)x : MAXGRAM;
+        }
+        unsigned peers = __match_any_sync(GD_FULL, c);
+        if (c < MAXGRAM && (peers & lanemask_lt()) == 0)
+            atomicAdd(&h[c], (unsigned)__popc(peers));
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < MAXGRAM; i += FT)
+        if (h[i])
+            atomicAdd(&gram[i], (unsigned long long)h[i]);
 }
 
 int launch_gram(const unsigned long long* ctrun, int64_t nruns, unsigned long long* gram, cudaStream_t s)
@@ -318,7 +335,12 @@ int launch_gram(const unsigned long long* ctrun, int64_t nruns, unsigned long lo
     GD_CUDA(cudaMemsetAsync(gram, 0, sizeof(unsigned long long) * MAXGRAM, s));
     if (nruns <= 0)
         return 0;
-    k_gram<<<(unsigned)gd_cdiv<int64_t>(nruns, FT), FT, 0, s>>>(ctrun, nruns, gram);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int64_t want = gd_cdiv<int64_t>(nruns, FT);
+    int grid = (int)(want < 4 * nsm ? want : 4 * nsm);
+    k_gram<<<grid, FT, 0, s>>>(ctrun, nruns, gram);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;

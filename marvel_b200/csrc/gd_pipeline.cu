@@ -119,7 +119,7 @@ struct gd_context
     DevBuf ascr, outrec, outtr, counters, status, queue;
     int agrid = 0;
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
-    uint64_t rcap = 1 << 20, tbcap = 64ull << 20;
+    uint64_t rcap = 1 << 22, tbcap = 512ull << 20;
     std::vector<gd_overlap> recs;
     std::vector<uint8_t> trace;
     gd_stats stats;
