@@ -125,6 +125,28 @@ int gd_local_alignment_batch(gd_context* ctx, const uint8_t* abases, int64_t ale
                              const int32_t* blen, const int32_t* diag, const int32_t* anti, int nseeds, int comp,
                              int32_t* out12, uint16_t* trace, int trstride, int64_t* cells);
 
+/* Local_Alignment batch that allocates nothing, for callers that may not call cudaMalloc
+ * once they run (an application that gives all HBM to its own pool, or a latency-critical
+ * loop where an allocation's implicit device synchronization is not allowed).  It has no
+ * counterpart in the reference.  All array arguments are DEVICE pointers owned by the
+ * caller, in the layout of gd_local_alignment_batch (sequence buffers need 16 readable
+ * bytes before the first base and after the last 4); maxlen is the longest read among the
+ * seeds; stream is a cudaStream_t (NULL = legacy default stream).  ctx must have had
+ * gd_new_align_spec called (that call may allocate; do it during set-up).
+ * Working memory is one file-scope device array of 2,359,552 bytes (16 warps, 8192
+ * pebbles and 8192 trace-point slots per warp) that every GPU loading the library keeps
+ * until exit; maxlen / tspace may be at most 1020 (reads up to 102,099 bp at trace
+ * spacing 100), larger batches are rejected with an error.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current, so make the first call before any
+ * stream capture.  Calls share the array: two calls that overlap on the GPU (different
+ * streams or threads) race and must be serialised by the caller.  The call synchronizes
+ * its stream to read the status word. */
+int gd_local_alignment_batch_noalloc(gd_context* ctx, const uint8_t* d_abases, const uint8_t* d_bbases,
+                                     const int64_t* d_aoff, const int32_t* d_alen, const int64_t* d_boff,
+                                     const int32_t* d_blen, const int32_t* d_diag, const int32_t* d_anti, int nseeds,
+                                     int maxlen, int comp, int32_t* d_out12, uint16_t* d_trace, int trstride,
+                                     int64_t* d_cells, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,7 +58,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_set_globals", "gd_load_block", "gd_sort_kmers", "gd_get_kmers", "gd_match_filter", "gd_get_hits",
            "gd_num_overlaps", "gd_get_overlaps", "gd_write_overlap_buffer", "gd_reset_overlap_buffer",
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
-           "gd_timer_elapsed_ms", "gd_kernel_launches"]
+           "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc"]
 
 
 def lib():
@@ -98,6 +98,8 @@ def lib():
     L.gd_timer_elapsed_ms.argtypes = [C.c_void_p]
     L.gd_timer_elapsed_ms.restype = C.c_double
     L.gd_kernel_launches.restype = C.c_ulonglong
+    L.gd_local_alignment_batch_noalloc.argtypes = [C.c_void_p] + [C.c_void_p] * 8 + [C.c_int] * 3 + \
+        [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 

@@ -3,6 +3,12 @@
 #include "gd_common.cuh"
 #include "gd_filter.cuh"
 
+struct gd_context;
+
+// The alignment spec of a context (trim tables, trace spacing, PATH_AVE) for entry points
+// outside gd_pipeline.cu; null until gd_new_align_spec has been called.
+const int16_t* gd_context_align_tables(gd_context* ctx, int* tspace, int* ave_path);
+
 namespace gd
 {
 

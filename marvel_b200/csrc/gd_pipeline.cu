@@ -589,6 +589,15 @@ static std::string dirname_of(int run_id, int block)
     return b;
 }
 
+const int16_t* gd_context_align_tables(gd_context* c, int* tspace, int* ave_path)
+{
+    if (!c || !c->spec_set)
+        return nullptr;
+    *tspace = c->tspace;
+    *ave_path = c->ave_path;
+    return P<int16_t>(c->tables);
+}
+
 // ----------------------------------------------------------------------------------------
 // C ABI
 // ----------------------------------------------------------------------------------------
