@@ -42,7 +42,7 @@ def build(verbose=False, force=False):
     cli_src = os.path.join(CSRC, "host", "daligner_main.c")
     if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB, os.path.join(CSRC, "host", "dazz_db.c")])):
         cmd = ["gcc", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), "-o", CLI, cli_src,
-               os.path.join(CSRC, "host", "dazz_db.c"), "-L" + HERE, "-lgpudalign", "-Wl,-rpath,$ORIGIN", "-lz"]
+               os.path.join(CSRC, "host", "dazz_db.c"), "-L" + HERE, "-lgpudalign", "-Wl,-rpath,$ORIGIN"]
         subprocess.run(cmd, check=True)
     return LIB
 

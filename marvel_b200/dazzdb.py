@@ -126,6 +126,50 @@ def _unpack(raw, foff, rlen):
     return out, boff
 
 
+def load_track(b: Block, name: str):
+    """Adds interval track `name` as b.mask (the .anno/.data layout Load_Track reads,
+    db/DB.c:967-1120; a per-block ".X.n.track" file wins over the whole-DB one).  A second
+    track is united with the masks already there."""
+    d, root = os.path.split(b.root)
+    cands = []
+    if b.part > 0:
+        cands.append((os.path.join(d, f".{root}.{b.part}.{name}"), True))
+    cands.append((os.path.join(d, f".{root}.{name}"), False))
+    for base, ispart in cands:
+        if os.path.exists(base + ".anno"):
+            break
+    else:
+        raise FileNotFoundError(f"track {name} not found for {b.root}")
+    raw = open(base + ".anno", "rb").read()
+    tracklen, size = np.frombuffer(raw[:8], "<i4")
+    anno = np.frombuffer(raw[8:], "<i8" if size == 8 else "<i4").astype(np.int64)
+    first = 0 if ispart else b.ufirst
+    anno = anno[first:first + b.nreads + 1]
+    data = np.fromfile(base + ".data", dtype="<i4")
+    off = int(anno[0]) // 4
+    iv = []
+    for i in range(b.nreads):
+        s, e = int(anno[i]) // 4, int(anno[i + 1]) // 4
+        x = data[s:e]
+        iv.append([(int(x[j]), int(x[j + 1])) for j in range(0, len(x), 2)])
+    del off
+    if b.mask is None:
+        b.mask = iv
+    else:
+        merged = []
+        for a, c in zip(b.mask, iv):
+            allv = sorted(a + c)
+            out = []
+            for s, e in allv:
+                if out and s <= out[-1][1]:
+                    out[-1] = (out[-1][0], max(out[-1][1], e))
+                else:
+                    out.append((s, e))
+            merged.append(out)
+        b.mask = merged
+    return b
+
+
 def complement_block(b: Block) -> Block:
     """Reverse-complement every read in place of a copy (dalign/daligner.c:474-573)."""
     bases = b.bases.copy()

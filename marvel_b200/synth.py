@@ -28,6 +28,7 @@ class GenomeModel:
     interspersed_len: tuple = (1000, 10000)
     interspersed_div: tuple = (0.05, 0.15)
     tandem_frac: float = 0.0
+    tandem_period: tuple = (2, 201)
     diploid_snp: float = 0.0
     diploid_indel: float = 0.0
 
@@ -115,7 +116,7 @@ def make_genome(model: GenomeModel, rng: np.random.Generator):
         target = int(model.tandem_frac * n)
         covered = 0
         while covered < target:
-            period = int(rng.integers(2, 201))
+            period = int(rng.integers(*model.tandem_period))
             unit = rng.integers(0, 4, period, dtype=np.uint8)
             span = int(rng.integers(500, 5000))
             arr = np.tile(unit, span // period + 1)[:span]
@@ -205,6 +206,8 @@ WORKLOADS = {
     # small cases for tests
     "tiny": Workload("tiny", GenomeModel(60_000),
                      ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=11),
+    "tiny_tandem": Workload("tiny_tandem", GenomeModel(80_000, tandem_frac=0.10, tandem_period=(2, 7)),
+                            ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=13),
     "small": Workload("small", GenomeModel(200_000, repeats=((6, 3000, 0.015),)),
                       ReadModel(15, 6000, 3000, 1000, 20000, **PACBIO), seed=12),
 }

@@ -11,7 +11,7 @@ from marvel_b200 import dazzdb
 
 
 def parse_flags(flags):
-    o = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=None, A=False, I=False, O=False, T=False, r=1)
+    o = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=None, A=False, I=False, O=False, T=False, r=1, m=[])
     for f in flags:
         c, v = f[1], f[2:]
         if c in "kwhtlsHr":
@@ -21,6 +21,8 @@ def parse_flags(flags):
             o["M"] = int(v)
         elif c == "e":
             o["e"] = float(v)
+        elif c == "m":
+            o["m"].append(v)
         elif c in "AIOT":
             o[c] = True
         elif c == "j":
@@ -66,6 +68,10 @@ def run(dbdir, flags, blocks, outdir, impl):
     A = dazzdb.open_block(os.path.join(dbdir, aname))
     self_cmp = aname == bname
     B = A if self_cmp else dazzdb.open_block(os.path.join(dbdir, bname))
+    for t in o["m"]:
+        dazzdb.load_track(A, t)
+        if not self_cmp:
+            dazzdb.load_track(B, t)
     symmetric = not o["A"]
     mem = 0 if o["M"] is None else o["M"] * 0x40000000
     if self_cmp:

@@ -30,7 +30,11 @@ CASES = {
     "self_identity": ("tiny", 0.5, 200, ["-I", "-k12", "-w6", "-h30", "-e.70", "-l500", "-s100"], ["G.1", "G.1"]),
     "self_asym_lowmem": ("tiny", 0.7, 200, ["-A", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100", "-M0"],
                          ["G.1", "G.1"]),
+    # tandem repeats masked by the reference DBdust track (-mdust), blocks of ~0.4 Mbp
+    "pair_dust": ("tiny_tandem", 1.0, 0.4, ["-mdust", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100"],
+                  ["G.1", "G.2"]),
 }
+DUST = os.path.join(ROOT, "oracle", "_ref", "DBdust")
 
 
 def make_case(name):
@@ -41,6 +45,8 @@ def make_case(name):
     os.makedirs(d)
     reads, _ = synth.generate(wl, scale)
     dazzdb.write_db(os.path.join(d, "G"), reads, bsize)
+    if any(f.startswith("-m") for f in flags):
+        subprocess.run([DUST, "G"], cwd=d, check=True, stdout=subprocess.DEVNULL)
     cmd = [REF, "-j4", "-M32"] + flags + blocks
     subprocess.run(cmd, cwd=d, check=True, stdout=subprocess.DEVNULL)
     las = []
