@@ -86,16 +86,6 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
 {
     if (FWD)
     {
-        {
-            int cb = __ldg(bseq + y), ca = __ldg(aseq + y + k);
-            if (cb != ca || cb == 4)
-            {
-                bend = (cb == 4);
-                aend = !bend && (ca == 4);
-                return y;
-            }
-            y += 1;
-        }
         // the 4 after every read stops the extension; the cap only guards against a bad pointer
         for (int guard = (lim >> 3) + 2; guard > 0; guard--)
         {
@@ -117,16 +107,6 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
     }
     else
     {
-        {
-            int cb = __ldg(bseq + y - 1), ca = __ldg(aseq + y + k - 1);
-            if (cb != ca || cb == 4)
-            {
-                bend = (cb == 4);
-                aend = !bend && (ca == 4);
-                return y;
-            }
-            y -= 1;
-        }
         for (int guard = (lim >> 3) + 2; guard > 0; guard--)
         {
             uint64_t wb = ld8u(bseq + y - 8), wa = ld8u(aseq + y + k - 8);
@@ -146,6 +126,14 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
         bend = aend = true;
     }
     return y;
+}
+
+// The trim test of forward_wave/reverse_wave (align.c:884-896): the newest 15 columns are
+// suffix-positive and so are the newest 30 (TABLE / SCORE built by set_table, align.c:196-210).
+__device__ __forceinline__ bool trim_ok(unsigned long long b, const int16_t* table, const int16_t* score)
+{
+    int lo15 = (int)(b & TRIM_MASK), hi15 = (int)((b >> TRIM_LEN) & TRIM_MASK);
+    return (__ldg(table + lo15) >= 0) && (__ldg(table + hi15) + __ldg(score + lo15) >= 0);
 }
 
 __device__ __forceinline__ int warp_max_incl(int v, int lane)
@@ -345,28 +333,22 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
     // ---- successive waves
     while (more && (FWD ? (lasta >= besta - TRIM_MLAG) : (lasta <= besta + TRIM_MLAG)))
     {
+        // widen the band by one each side (align.c:636-745).  Diagonals outside the previous
+        // band read as VNONE and new end diagonals take their inner neighbour's NA/NB: the
+        // reference writes those values into its vectors first, here they are read that way.
+        const int olow = low, ohgh = hgh;
+        if (olow > ohgh)  // every diagonal fell WAVE_LAG behind: the reference would read stale vectors
+        {
+            if (lane == 0)
+                gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
+            w.err = 1;
+            return;
+        }
         low -= 1;
         hgh += 1;
-        bool newlow = low >= minp;
-        if (!newlow)
+        if (low < minp)
             low += 1;
-        bool newhgh = hgh <= maxp;
-        if (lane == 0)
-        {
-            if (newlow)
-            {
-                R.NA[low & RM] = R.NA[(low + 1) & RM];
-                R.NB[low & RM] = R.NB[(low + 1) & RM];
-                R.V[low & RM] = VNONE;
-            }
-            if (newhgh)
-            {
-                R.NA[hgh & RM] = R.NA[(hgh - 1) & RM];
-                R.NB[hgh & RM] = R.NB[(hgh - 1) & RM];
-                R.V[hgh & RM] = VNONE;
-            }
-        }
-        if (!newhgh)
+        if (hgh > maxp)
             hgh -= 1;
         dif += 1;
         if (dif > alen + blen + 2)  // the edit distance cannot exceed alen + blen
@@ -376,12 +358,6 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             w.err = 1;
             return;
         }
-        if (lane == 0)
-        {
-            R.V[(hgh + 1) & RM] = VNONE;
-            R.V[(low - 1) & RM] = VNONE;
-        }
-        __syncwarp();
         const int width = hgh - low + 1;
         if (width <= 0 || width > 32 * WAVE_CHUNKS)
         {
@@ -408,7 +384,10 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             if (valid)
             {
                 // choose the furthest of the three predecessors (align.c:748-797)
-                int vP = R.V[(k + S) & RM], vC = R.V[k & RM], vN = R.V[(k - S) & RM];
+                const int kP = k + S, kN = k - S;
+                int vP = (kP >= olow && kP <= ohgh) ? R.V[kP & RM] : VNONE;
+                int vC = (k >= olow && k <= ohgh) ? R.V[k & RM] : VNONE;
+                int vN = (kN >= olow && kN <= ohgh) ? R.V[kN & RM] : VNONE;
                 int wP = FWD ? vP : -vP, wC = FWD ? vC : -vC, wN = FWD ? vN : -vN;
                 int ks, vs, step;
                 if (wC < wN)
@@ -447,21 +426,24 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 int L = FWD ? (y - y0) : (y0 - y);
                 b = (L >= 61) ? ~0ull : ((b << L) | ((1ull << L) - 1ull));
                 c = (y << 1) + k;
-                na = R.NA[k & RM];
-                nb = R.NB[k & RM];
+                const int kn = k < olow ? olow : (k > ohgh ? ohgh : k);
+                na = R.NA[kn & RM];
+                nb = R.NB[kn & RM];
             }
-            // A trace points (align.c:826-852)
+            // trace points of A and B crossed by this extension (align.c:826-878)
             while (true)
             {
-                bool need = valid && (FWD ? (y + k >= na) : (y + k <= na));
-                if (!__any_sync(GD_FULL, need))
+                bool needA = valid && (FWD ? (y + k >= na) : (y + k <= na));
+                bool needB = valid && (FWD ? (y >= nb) : (y <= nb));
+                if (!__any_sync(GD_FULL, needA || needB))
                     break;
-                bool create = need && (FWD ? (w.peb[ha].w < na) : (w.peb[ha].w > na));
-                unsigned cm = __ballot_sync(GD_FULL, create);
-                if (cm)
+                bool cA = needA && (FWD ? (w.peb[ha].w < na) : (w.peb[ha].w > na));
+                bool cB = needB && (FWD ? (w.peb[hb].w < nb) : (w.peb[hb].w > nb));
+                unsigned ma = __ballot_sync(GD_FULL, cA), mbb = __ballot_sync(GD_FULL, cB);
+                if (ma | mbb)
                 {
                     int base = npeb;
-                    npeb += __popc(cm);
+                    npeb += __popc(ma) + __popc(mbb);
                     if (npeb > w.pcap)
                     {
                         if (lane == 0)
@@ -469,43 +451,22 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                         w.err = 1;
                         return;
                     }
-                    if (create)
+                    if (cA)
                     {
-                        int idx = base + __popc(cm & lt);
+                        int idx = base + __popc(ma & lt);
                         w.peb[idx] = make_int4(ha, k, dif, na);
                         ha = idx;
                     }
-                }
-                if (need)
-                    na += FWD ? TS : -TS;
-            }
-            // B trace points (align.c:854-878)
-            while (true)
-            {
-                bool need = valid && (FWD ? (y >= nb) : (y <= nb));
-                if (!__any_sync(GD_FULL, need))
-                    break;
-                bool create = need && (FWD ? (w.peb[hb].w < nb) : (w.peb[hb].w > nb));
-                unsigned cm = __ballot_sync(GD_FULL, create);
-                if (cm)
-                {
-                    int base = npeb;
-                    npeb += __popc(cm);
-                    if (npeb > w.pcap)
+                    if (cB)
                     {
-                        if (lane == 0)
-                            gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
-                        w.err = 1;
-                        return;
-                    }
-                    if (create)
-                    {
-                        int idx = base + __popc(cm & lt);
+                        int idx = base + __popc(ma) + __popc(mbb & lt);
                         w.peb[idx] = make_int4(hb, k, dif, nb);
                         hb = idx;
                     }
                 }
-                if (need)
+                if (needA)
+                    na += FWD ? TS : -TS;
+                if (needB)
                     nb += FWD ? TS : -TS;
             }
             rc[ch] = c;
@@ -546,12 +507,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 besty = __shfl_sync(GD_FULL, y, jm);
                 unsigned long long bj = __shfl_sync(GD_FULL, b, jm);
                 bool p1j = __popcll(bj & MASK61) >= PATH_AVE;
-                bool p2j = false;
-                if (p1j)
-                {
-                    int lo15 = (int)(bj & TRIM_MASK), hi15 = (int)((bj >> TRIM_LEN) & TRIM_MASK);
-                    p2j = (__ldg(P.table + lo15) >= 0) && (__ldg(P.table + hi15) + __ldg(P.score + lo15) >= 0);
-                }
+                bool p2j = p1j && trim_ok(bj, P.table, P.score);
                 if (p1j)
                     lasta = besta;
                 if (p2j)
@@ -573,12 +529,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                     unsigned m1 = __ballot_sync(GD_FULL, p1);
                     if (m1 && !p1j)
                         lasta = __shfl_sync(GD_FULL, c, 31 - __clz(m1));
-                    bool p2 = false;
-                    if (p1)
-                    {
-                        int lo15 = (int)(b & TRIM_MASK), hi15 = (int)((b >> TRIM_LEN) & TRIM_MASK);
-                        p2 = (__ldg(P.table + lo15) >= 0) && (__ldg(P.table + hi15) + __ldg(P.score + lo15) >= 0);
-                    }
+                    bool p2 = p1 && trim_ok(b, P.table, P.score);
                     unsigned m2 = __ballot_sync(GD_FULL, p2);
                     if (m2)
                     {

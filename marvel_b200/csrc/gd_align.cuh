@@ -7,7 +7,7 @@ struct gd_context;
 
 // The alignment spec of a context (trim tables, trace spacing, PATH_AVE) for entry points
 // outside gd_pipeline.cu; null until gd_new_align_spec has been called.
-const int16_t* gd_context_align_tables(gd_context* ctx, int* tspace, int* ave_path);
+const int16_t* gd_context_align_tables(gd_context* ctx, int* tspace, int* ave_path, int* mscore, int* dscore);
 
 namespace gd
 {
@@ -41,6 +41,7 @@ struct AlignParams
     HitBits hb;
     const int16_t* table;  // TABLE and SCORE trim tables (set_table, dalign/align.c:196-210)
     const int16_t* score;
+    int mscore, dscore;    // match / edit weights the tables are built from (align.c:238-240)
 };
 
 // Per-warp global scratch, carved from one allocation.

@@ -46,8 +46,8 @@ extern "C" int gd_local_alignment_batch_noalloc(gd_context* ctx, const uint8_t* 
         gd_set_error("gd_local_alignment_batch_noalloc: null context");
         return -1;
     }
-    int tspace = 0, ave_path = 0;
-    const int16_t* tables = gd_context_align_tables(ctx, &tspace, &ave_path);
+    int tspace = 0, ave_path = 0, mscore = 0, dscore = 0;
+    const int16_t* tables = gd_context_align_tables(ctx, &tspace, &ave_path, &mscore, &dscore);
     if (!tables)
     {
         gd_set_error("gd_local_alignment_batch_noalloc: gd_new_align_spec has not been called on this context");
@@ -117,6 +117,8 @@ extern "C" int gd_local_alignment_batch_noalloc(gd_context* ctx, const uint8_t* 
     ap.trace8 = tspace <= 125;
     ap.table = tables;
     ap.score = tables + gd::TRIM_TABLE;
+    ap.mscore = mscore;
+    ap.dscore = dscore;
     if (gd::launch_la_batch(d_abases, d_aoff, d_alen, d_bbases, d_boff, d_blen, d_diag, d_anti, nseeds, ap, sc, d_out12,
                             d_trace, trstride, d_cells, st, s))
         return -1;

@@ -106,7 +106,7 @@ struct gd_context
     int symmetric = 1, only_identity = 0, no_trace = 0;
     int minover = 2000, identity = 0;
     uint64_t mem_limit = 0;
-    int ave_path = 0;
+    int ave_path = 0, mscore = 0, dscore = 0;
     int spec_set = 0;
     DevBuf tables;
     Slot slot[3];
@@ -163,6 +163,8 @@ static int upload_spec(gd_context* c)
     c->ave_path = (int)(60 * (1. - kBias[bias] * (1. - c->ave_corr)));
     int mscore = (int)(1000 * kBias[bias] * (1. - c->ave_corr));
     int dscore = 1000 - mscore;
+    c->mscore = mscore;
+    c->dscore = dscore;
     std::vector<int16_t> t(2 * gd::TRIM_TABLE);
     set_table(0, 0, 0, 0, mscore, dscore, t.data(), t.data() + gd::TRIM_TABLE);
     if (ensure(c->tables, t.size() * 2))
@@ -418,6 +420,8 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     ap.hb = hb;
     ap.table = P<int16_t>(c->tables);
     ap.score = P<int16_t>(c->tables) + TRIM_TABLE;
+    ap.mscore = c->mscore;
+    ap.dscore = c->dscore;
     if (!c->agrid && align_grid(&c->agrid))
         return -1;
     int nwarps = c->agrid * ALIGN_WARPS;
@@ -589,12 +593,14 @@ static std::string dirname_of(int run_id, int block)
     return b;
 }
 
-const int16_t* gd_context_align_tables(gd_context* c, int* tspace, int* ave_path)
+const int16_t* gd_context_align_tables(gd_context* c, int* tspace, int* ave_path, int* mscore, int* dscore)
 {
     if (!c || !c->spec_set)
         return nullptr;
     *tspace = c->tspace;
     *ave_path = c->ave_path;
+    *mscore = c->mscore;
+    *dscore = c->dscore;
     return P<int16_t>(c->tables);
 }
 
@@ -1033,6 +1039,8 @@ int gd_local_alignment_batch(gd_context* c, const uint8_t* abases, int64_t alen_
     ap.trace8 = c->tspace <= 125;
     ap.table = P<int16_t>(c->tables);
     ap.score = P<int16_t>(c->tables) + TRIM_TABLE;
+    ap.mscore = c->mscore;
+    ap.dscore = c->dscore;
     int grid = 0;
     if (align_grid(&grid))
         return -1;
