@@ -108,6 +108,15 @@ int gd_reset_overlap_buffer(gd_context* ctx);
 
 int gd_get_stats(gd_context* ctx, gd_stats* st);
 
+/* Compute_Trace_PTS (dalign/align.c:5286-5397) over n .las records: the exact number of
+ * differences of each record, aligning every trace-point interval with iter_np's O(np)
+ * waves (dalign/align.c:4556-4917) -- the check LAcheck -a makes (utils/LAcheck.c:236-252).
+ * Records and trace bytes as gd_get_overlaps returns them; A reads come from aslot, B reads
+ * from bslot, or from cslot (the complemented B block) for records with the COMP flag.
+ * diffs_out[i] receives record i's exact diffs. */
+int gd_compute_trace_pts(gd_context* ctx, int aslot, int bslot, int cslot, const gd_overlap* recs,
+                         const uint8_t* trace, int64_t n, int32_t* diffs_out);
+
 /* Device timer on the context's stream: mark 0 = start, mark 1 = stop; elapsed in ms. */
 int gd_timer_mark(gd_context* ctx, int which);
 double gd_timer_elapsed_ms(gd_context* ctx);

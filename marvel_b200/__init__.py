@@ -58,7 +58,8 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_set_globals", "gd_load_block", "gd_sort_kmers", "gd_get_kmers", "gd_match_filter", "gd_get_hits",
            "gd_num_overlaps", "gd_get_overlaps", "gd_write_overlap_buffer", "gd_reset_overlap_buffer",
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
-           "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc"]
+           "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
+           "gd_compute_trace_pts"]
 
 
 def lib():
@@ -98,6 +99,8 @@ def lib():
     L.gd_timer_elapsed_ms.argtypes = [C.c_void_p]
     L.gd_timer_elapsed_ms.restype = C.c_double
     L.gd_kernel_launches.restype = C.c_ulonglong
+    L.gd_compute_trace_pts.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int64,
+                                       C.c_void_p]
     L.gd_local_alignment_batch_noalloc.argtypes = [C.c_void_p] + [C.c_void_p] * 8 + [C.c_int] * 3 + \
         [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     _lib = L
@@ -224,6 +227,15 @@ class Context:
 
     def write_overlap_buffer(self, run_id, ablock, bblock, last_read):
         _check(lib().gd_write_overlap_buffer(self.h, run_id, ablock.encode(), bblock.encode(), last_read))
+
+    def compute_trace_pts(self, recs, trace, aslot=0, bslot=0, cslot=2):
+        """Exact diffs of each record (Compute_Trace_PTS) from the loaded blocks."""
+        recs = np.ascontiguousarray(recs, dtype=OVL_DTYPE)
+        trace = np.ascontiguousarray(trace, dtype=np.uint8)
+        out = np.zeros(max(recs.size, 1), np.int32)
+        _check(lib().gd_compute_trace_pts(self.h, aslot, bslot, cslot, recs.ctypes.data, trace.ctypes.data, recs.size,
+                                          out.ctypes.data))
+        return out[:recs.size]
 
     def reset_overlap_buffer(self):
         _check(lib().gd_reset_overlap_buffer(self.h))

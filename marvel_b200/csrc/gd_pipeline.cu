@@ -18,6 +18,7 @@
 #include "gd_align.cuh"
 #include "gd_filter.cuh"
 #include "gd_prims.cuh"
+#include "gd_verify.cuh"
 
 static thread_local char g_err[1024] = "";
 unsigned long long g_gd_launches = 0;
@@ -998,6 +999,104 @@ int gd_write_overlap_buffer(gd_context* c, int run_id, const char* ablock, const
     if (write_las(c, p1, idx, 0, j))
         return -1;
     return write_las(c, p2, idx, j, idx.size());
+}
+
+int gd_compute_trace_pts(gd_context* c, int aslot, int bslot, int cslot, const gd_overlap* recs, const uint8_t* trace,
+                         int64_t n, int32_t* diffs_out)
+{
+    using namespace gd;
+    if (aslot < 0 || aslot > 2 || bslot < 0 || bslot > 2 || cslot < 0 || cslot > 2 || !c->slot[aslot].loaded ||
+        !c->slot[bslot].loaded)
+    {
+        gd_set_error("gd_compute_trace_pts: bad or unloaded slots");
+        return -1;
+    }
+    if (n <= 0)
+        return 0;
+    Slot& A = c->slot[aslot];
+    Slot& B = c->slot[bslot];
+    Slot& Cc = c->slot[cslot];
+    const int TS = c->tspace;
+    const int tbytes = TS <= 125 ? 1 : 2;
+    bool any_comp = false;
+    std::vector<Segment> seg;
+    int R = 8;
+    for (int64_t r = 0; r < n; r++)
+    {
+        const gd_overlap& o = recs[r];
+        int ar = o.aread - A.blk.ufirst, br = o.bread - B.blk.ufirst;
+        if (ar < 0 || ar >= A.blk.nreads || br < 0 || br >= B.blk.nreads)
+        {
+            gd_set_error("gd_compute_trace_pts: record %lld names reads outside the loaded blocks", (long long)r);
+            return -1;
+        }
+        if (o.aepos > A.hrlen[ar] || o.bepos > B.hrlen[br] || o.abpos < 0 || o.bbpos < 0 || o.abpos > o.aepos ||
+            o.bbpos > o.bepos)
+        {
+            gd_set_error("gd_compute_trace_pts: record %lld has positions outside its reads", (long long)r);
+            return -1;
+        }
+        int comp = o.flags & 1;
+        any_comp |= comp != 0;
+        const uint8_t* t = trace + o.toff;
+        auto pt = [&](int i) { return tbytes == 1 ? (int)t[i] : (int)(t[2 * i] | (t[2 * i + 1] << 8)); };
+        // segments between consecutive trace points (align.c:5355-5389)
+        int ab = o.abpos, ae = (o.abpos / TS) * TS, bb = o.bbpos, be;
+        for (int i = 1; i < o.tlen - 2; i += 2)
+        {
+            ae += TS;
+            be = bb + pt(i);
+            seg.push_back(Segment{ar, br, ab, ae, bb, be, (int32_t)r, comp});
+            R = std::max(R, (ae - ab) + (be - bb) + 8);
+            ab = ae;
+            bb = be;
+        }
+        seg.push_back(Segment{ar, br, ab, o.aepos, bb, o.bepos, (int32_t)r, comp});
+        R = std::max(R, (o.aepos - ab) + (o.bepos - bb) + 8);
+    }
+    if (any_comp && !Cc.loaded)
+    {
+        gd_set_error("gd_compute_trace_pts: complemented records need the complemented block in slot %d", cslot);
+        return -1;
+    }
+    int64_t nseg = (int64_t)seg.size();
+    int64_t nthreads = std::min<int64_t>(nseg, 148 * 512);
+    nthreads = (nthreads + 127) / 128 * 128;
+    DevBuf dseg, dscr, ddiff, dst;
+    int rc = -1;
+    do
+    {
+        if (ensure(dseg, nseg * sizeof(Segment)) || ensure(dscr, (size_t)nthreads * 3 * (2 * R + 1) * 4) ||
+            ensure(ddiff, n * 4) || ensure(dst, sizeof(DevStatus)))
+            break;
+        if (cudaMemcpy(dseg.p, seg.data(), nseg * sizeof(Segment), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(ddiff.p, 0, n * 4) != cudaSuccess || cudaMemset(dst.p, 0, sizeof(DevStatus)) != cudaSuccess)
+        {
+            gd_set_error("gd_compute_trace_pts: copies failed");
+            break;
+        }
+        if (launch_trace_pts(A.blk, B.blk, Cc.loaded ? Cc.blk : B.blk, P<Segment>(dseg), nseg, P<int>(dscr), R,
+                             (int)nthreads, P<int>(ddiff), P<DevStatus>(dst), c->s))
+            break;
+        DevStatus st;
+        if (cudaStreamSynchronize(c->s) != cudaSuccess ||
+            cudaMemcpy(&st, dst.p, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(diffs_out, ddiff.p, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        {
+            gd_set_error("gd_compute_trace_pts: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if (st.code)
+        {
+            gd_set_error("gd_compute_trace_pts: record %d failed (code %d)", st.where, st.code);
+            break;
+        }
+        rc = 0;
+    } while (0);
+    DevBuf* all[] = {&dseg, &dscr, &ddiff, &dst};
+    for (DevBuf* b : all)
+        release(*b);
+    return rc;
 }
 
 int gd_reset_overlap_buffer(gd_context* c)

@@ -2044,13 +2044,119 @@ int or_daligner(const or_block* a, const or_block* b, const or_block* bc, const 
     return 0;
 }
 
+/* iter_np (align.c:4556-4917), the distance part: the O(np) waves between A[0..M) and
+ * B[0..N) with substitutions.  F0/F1/F2 are waves D, D-1, D-2 indexed by diagonal (the
+ * reference keeps every wave for its traceback; the distance needs three).  A and B are
+ * separate buffers here, as LAcheck and LAshow load them, so no self-comparison borders.
+ * Each of the three buffers holds 2*R+1 diagonals centred on 0, R >= M + N + 4. */
+static int iter_np_dist(const uint8_t* A, int M, const uint8_t* B, int N, int* b0, int* b1, int* b2)
+{
+    int del = M - N, low, hgh, D, k, j, i, am, ac, ap;
+    int *F0, *F1, *F2, *nf;
+    if (del >= 0)
+    {
+        low = 0;
+        hgh = del;
+    }
+    else
+    {
+        low = del;
+        hgh = 0;
+    }
+    F1 = b1;
+    F0 = b2;
+    nf = b0;
+    for (k = low - 1; k <= hgh + 1; k++)
+        F1[k] = F0[k] = -2;
+    F0[0] = -1;
+    low += 1;
+    hgh -= 1;
+    for (D = 0;; D++)
+    {
+        int* t = nf;
+        F2 = F1;
+        F1 = F0;
+        F0 = t;
+        nf = F2;
+        if ((D & 1) == 0)
+        {
+            low -= 1;
+            hgh += 1;
+        }
+        F0[hgh + 1] = F0[low - 1] = -2;
+#define FS(AP, AM)                                    \
+    ap = (AP);                                        \
+    am = (AM);                                        \
+    ac = F1[k] + 1;                                   \
+    if (ac < am)                                      \
+        j = (ap < am) ? am : ap;                      \
+    else if (ap < ac)                                 \
+        j = ac;                                       \
+    else                                              \
+        j = ap;                                       \
+    i = M - k;                                        \
+    {                                                 \
+        int lim = (N < i) ? N : i;                    \
+        while (j < lim && B[j] == A[j + k])           \
+            j += 1;                                   \
+    }                                                 \
+    F0[k] = j;
+        j = -2;
+        for (k = hgh; k > del; k--)
+        {
+            FS(j + 1, F2[k - 1])
+        }
+        j = -2;
+        for (k = low; k < del; k++)
+        {
+            FS(F2[k + 1] + 1, j)
+        }
+        k = del;
+        FS(F0[del + 1] + 1, j)
+#undef FS
+        if (F0[del] >= N)
+            break;
+    }
+    return D + abs(del);
+}
+
+/* Compute_Trace_PTS (align.c:5286-5397): exact differences of a .las record, segment by
+ * segment between its trace points.  aseq/bseq point at the reads' first bases (bseq
+ * already complemented for a COMP record). */
 int or_trace_pts_diffs(const uint8_t* aseq, const uint8_t* bseq, int alen, int blen, int abpos, int bbpos, int aepos,
                        int bepos, const uint8_t* trace8, const uint16_t* trace16, int tlen, int tspace,
                        int32_t* diffs_out)
 {
-    (void)aseq; (void)bseq; (void)alen; (void)blen; (void)abpos; (void)bbpos; (void)aepos; (void)bepos;
-    (void)trace8; (void)trace16; (void)tlen; (void)tspace; (void)diffs_out;
-    return -1;
+    (void)alen;
+    (void)blen;
+    int nmax = 0, dmax = 0;
+    for (int d = 1; d < tlen; d += 2)
+    {
+        int dv = trace8 ? trace8[d - 1] : trace16[d - 1];
+        int nv = trace8 ? trace8[d] : trace16[d];
+        if (dv > dmax)
+            dmax = dv;
+        if (nv > nmax)
+            nmax = nv;
+    }
+    if (tlen <= 1)
+        nmax = bepos - bbpos;
+    int R = tspace + nmax + (aepos - abpos) + (bepos - bbpos) + 16;
+    int* mem = (int*)malloc(sizeof(int) * 3 * (2 * R + 1));
+    int *b0 = mem + R, *b1 = mem + (2 * R + 1) + R, *b2 = mem + 2 * (2 * R + 1) + R;
+    int diffs = 0, ab = abpos, ae = (abpos / tspace) * tspace, bb = bbpos, be;
+    for (int i = 1; i < tlen - 2; i += 2)
+    {
+        ae = ae + tspace;
+        be = bb + (trace8 ? trace8[i] : trace16[i]);
+        diffs += iter_np_dist(aseq + ab, ae - ab, bseq + bb, be - bb, b0, b1, b2);
+        ab = ae;
+        bb = be;
+    }
+    diffs += iter_np_dist(aseq + ab, aepos - ab, bseq + bb, bepos - bb, b0, b1, b2);
+    free(mem);
+    *diffs_out = diffs;
+    return 0;
 }
 
 void or_free(void* p)

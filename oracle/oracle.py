@@ -56,6 +56,8 @@ def lib():
                                             C.POINTER(or_params), C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.POINTER(C.c_int64)]
         _lib.or_free.argtypes = [C.c_void_p]
+        _lib.or_trace_pts_diffs.argtypes = [C.c_void_p] * 2 + [C.c_int] * 6 + [C.c_void_p, C.c_void_p, C.c_int,
+                                                                                C.c_int, C.POINTER(C.c_int32)]
     return _lib
 
 
@@ -186,3 +188,18 @@ def local_alignment(aseq, bseq, comp, diag, anti, params):
     L.or_local_alignment(aseq.ctypes.data + 1, bseq.ctypes.data + 1, alen, blen, comp, diag, anti, C.byref(params),
                          out.ctypes.data, at.ctypes.data, bt.ctypes.data, C.byref(cells))
     return out, at[:out[5]].copy(), bt[:out[11]].copy(), cells.value
+
+
+def trace_pts_diffs(aread_seq, bread_seq, rec, trace, tspace):
+    """Compute_Trace_PTS diffs of one record; sequences are the reads' bases (B complemented
+    for a COMP record), trace the record's trace values."""
+    L = lib()
+    a = np.ascontiguousarray(aread_seq, np.uint8)
+    b = np.ascontiguousarray(bread_seq, np.uint8)
+    out = C.c_int32()
+    t8 = np.ascontiguousarray(trace, np.uint8) if tspace <= 125 else None
+    t16 = None if tspace <= 125 else np.ascontiguousarray(trace, np.uint16)
+    L.or_trace_pts_diffs(a.ctypes.data, b.ctypes.data, a.size, b.size, int(rec["abpos"]), int(rec["bbpos"]),
+                         int(rec["aepos"]), int(rec["bepos"]), None if t8 is None else t8.ctypes.data,
+                         None if t16 is None else t16.ctypes.data, int(rec["tlen"]), tspace, C.byref(out))
+    return out.value

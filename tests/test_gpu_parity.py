@@ -180,3 +180,35 @@ def test_size_independent_properties_cfg2(mb, tmp_path):
         assert int(tr[1::2].sum()) == int(x["bepos"] - x["bbpos"])
         npts = (int(x["aepos"]) - 1) // 100 - int(x["abpos"]) // 100 + 1
         assert int(x["tlen"]) == 2 * npts
+
+
+@pytest.mark.parametrize("name", ["self_default", "pair_blocks", "self_s200_t20"])
+def test_compute_trace_pts_matches_oracle(mb, name):
+    """Compute_Trace_PTS (dalign/align.c:5286-5397) on the device: exact diffs of every
+    record of a reference .las file, against the oracle's restatement of iter_np."""
+    import oracle
+    d, meta = load(name)
+    aname, bname = meta["blocks"]
+    A = dazzdb.open_block(os.path.join(d, aname))
+    B = dazzdb.open_block(os.path.join(d, bname))
+    Bc = dazzdb.complement_block(B)
+    ts, recs, traces = dazzdb.read_las(os.path.join(d, meta["las"][0]))
+    tb = 1 if ts <= 125 else 2
+    rec = np.zeros(recs.size, mb.OVL_DTYPE)
+    for f in ("tlen", "diffs", "abpos", "bbpos", "aepos", "bepos", "flags", "aread", "bread"):
+        rec[f] = recs[f]
+    offs = np.cumsum([0] + [t.size * tb for t in traces])
+    rec["toff"] = offs[:-1]
+    tr = np.concatenate([t.view(np.uint8) if tb == 2 else t for t in traces]) if traces else np.zeros(1, np.uint8)
+    ctx = mb.Context()
+    ctx.new_align_spec(0.70, ts, A.freq)
+    ctx.load_block(0, A)
+    ctx.load_block(1, B)
+    ctx.complement_block(1, 2)
+    g = ctx.compute_trace_pts(rec, tr, 0, 1, 2)
+    ctx.close()
+    for i in range(recs.size):
+        r = recs[i]
+        bb = (Bc if r["flags"] & 1 else B).read(int(r["bread"]) - B.ufirst)
+        o = oracle.trace_pts_diffs(A.read(int(r["aread"]) - A.ufirst), bb, r, traces[i], ts)
+        assert int(g[i]) == o, (i, int(g[i]), o)
