@@ -59,6 +59,7 @@ typedef struct
     double ms_index[3];   /* device time of Sort_Kmers per slot */
     double ms_merge[2];   /* device time of merge + hit sort */
     double ms_align[2];   /* device time of seed scan + alignment */
+    int64_t skipped[2];   /* pair groups the learned triage skipped (0 with no model set) */
 } gd_stats;
 
 /* Context on the current CUDA device. */
@@ -155,6 +156,51 @@ int gd_local_alignment_batch_noalloc(gd_context* ctx, const uint8_t* d_abases, c
                                      const int32_t* d_blen, const int32_t* d_diag, const int32_t* d_anti, int nseeds,
                                      int maxlen, int comp, int32_t* d_out12, uint16_t* d_trace, int trstride,
                                      int64_t* d_cells, void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * Learned triage of pair groups.  No counterpart in the reference: an addition in front of
+ * the aligner (report_thread, dalign/filter.c:1656-1995, aligns every pair group that has
+ * >= ceil(h/k) hits).  Each pair group is described by 12 features of its hits (TRI_NF);
+ * a 12-64-64-1 MLP (BF16 tensor-core kernels, FP32 accumulate, FP32 Adam state) predicts
+ * whether the group yields an overlap.  A group is skipped or aligned as a whole, so every
+ * record of the triaged path is a record of the plain path.
+ * Parameter vector (GD_TRI_NPARAM floats): mean[12], scale[12] (features are standardised
+ * as (f - mean) / scale), W1[64][12], b1[64], W2[64][64], b2[64], W3[64], b3.
+ * ------------------------------------------------------------------------------------ */
+#define GD_TRI_NF 12
+#define GD_TRI_NPARAM 5081
+
+/* Collect, per pair group of every following gd_match_filter, its features and the plain
+ * path's outcome (records emitted, wave cells); on != 0 turns collection on. */
+int gd_triage_collect(gd_context* ctx, int on);
+
+/* Copies up to cap collected rows (feat: cap x 12 floats, records, cells; any may be NULL);
+ * returns the number of rows collected. */
+int64_t gd_triage_get_groups(gd_context* ctx, float* feat, uint32_t* records, uint32_t* cells, int64_t cap);
+
+int gd_triage_reset(gd_context* ctx);
+
+/* Sets the model used inside gd_match_filter: groups whose predicted probability is below
+ * threshold are not aligned.  params == NULL turns the triage off. */
+int gd_triage_set_model(gd_context* ctx, const float* params, float threshold);
+
+/* Feature scales (mean / standard deviation over feat's n rows) and seeded He-uniform
+ * initial weights, zero biases.  Host only. */
+int gd_mlp_init(const float* feat, int64_t n, uint64_t seed, float* params);
+
+/* prob[i] = sigmoid(MLP(feat[i])) on the device, host buffers in and out. */
+int gd_mlp_forward(gd_context* ctx, const float* params, const float* feat, int64_t n, float* prob);
+
+/* Gradient (GD_TRI_NPARAM floats; mean and scale entries 0) and value of the batch-mean
+ * binary cross-entropy with positives weighted pos_weight, over n rows, on the device. */
+int gd_mlp_grad(gd_context* ctx, const float* params, const float* feat, const float* label, int n, float pos_weight,
+                float* grad, float* loss);
+
+/* Mini-batch Adam (beta 0.9 / 0.999, eps 1e-8) on the device for epochs passes over the n
+ * rows in a seeded shuffled order; params holds the initial model on entry and the trained
+ * one on return; epoch_loss (optional, epochs floats) receives each pass's mean loss. */
+int gd_mlp_train(gd_context* ctx, const float* feat, const float* label, int64_t n, int epochs, int batch, float lr,
+                 float pos_weight, uint64_t seed, float* params, float* epoch_loss);
 
 #ifdef __cplusplus
 }

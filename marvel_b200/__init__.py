@@ -50,7 +50,7 @@ class GdStats(C.Structure):
     _fields_ = [("kmers", C.c_int64 * 3), ("hits", C.c_int64 * 2), ("groups", C.c_int64 * 2),
                 ("seeds", C.c_int64 * 2), ("cells", C.c_int64 * 2), ("records", C.c_int64),
                 ("limit", C.c_int32 * 2), ("ms_index", C.c_double * 3), ("ms_merge", C.c_double * 2),
-                ("ms_align", C.c_double * 2)]
+                ("ms_align", C.c_double * 2), ("skipped", C.c_int64 * 2)]
 
 
 # exported symbols of include/gpudalign.h
@@ -59,7 +59,11 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_num_overlaps", "gd_get_overlaps", "gd_write_overlap_buffer", "gd_reset_overlap_buffer",
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
-           "gd_compute_trace_pts"]
+           "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
+           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train"]
+
+TRI_NF = 12        # features per pair group
+TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
 
 
 def lib():
@@ -103,6 +107,17 @@ def lib():
                                        C.c_void_p]
     L.gd_local_alignment_batch_noalloc.argtypes = [C.c_void_p] + [C.c_void_p] * 8 + [C.c_int] * 3 + \
         [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.gd_triage_collect.argtypes = [C.c_void_p, C.c_int]
+    L.gd_triage_get_groups.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+    L.gd_triage_get_groups.restype = C.c_int64
+    L.gd_triage_reset.argtypes = [C.c_void_p]
+    L.gd_triage_set_model.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
+    L.gd_mlp_init.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p]
+    L.gd_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    L.gd_mlp_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p,
+                              C.c_void_p]
+    L.gd_mlp_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_float,
+                               C.c_float, C.c_uint64, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 
@@ -245,6 +260,56 @@ class Context:
         _check(lib().gd_get_stats(self.h, C.byref(st)))
         return {k: (list(getattr(st, k)) if hasattr(getattr(st, k), "__len__") else getattr(st, k))
                 for k, _ in GdStats._fields_}
+
+    # learned triage of pair groups (marvel_b200.triage drives these)
+    def triage_collect(self, on=True):
+        _check(lib().gd_triage_collect(self.h, int(bool(on))))
+
+    def triage_groups(self):
+        """Collected rows: (features n x 12 float32, records uint32, cells uint32)."""
+        n = _check(lib().gd_triage_get_groups(self.h, None, None, None, 0))
+        feat = np.zeros((n, TRI_NF), np.float32)
+        rec = np.zeros(n, np.uint32)
+        cells = np.zeros(n, np.uint32)
+        _check(lib().gd_triage_get_groups(self.h, feat.ctypes.data, rec.ctypes.data, cells.ctypes.data, n))
+        return feat, rec, cells
+
+    def triage_reset(self):
+        _check(lib().gd_triage_reset(self.h))
+
+    def triage_set_model(self, params, threshold=0.0):
+        if params is None:
+            _check(lib().gd_triage_set_model(self.h, None, 0.0))
+            return
+        self._tri_params = np.ascontiguousarray(params, np.float32)
+        assert self._tri_params.size == TRI_NPARAM
+        _check(lib().gd_triage_set_model(self.h, self._tri_params.ctypes.data, float(threshold)))
+
+    def mlp_forward(self, params, feat):
+        params = np.ascontiguousarray(params, np.float32)
+        feat = np.ascontiguousarray(feat, np.float32).reshape(-1, TRI_NF)
+        prob = np.zeros(feat.shape[0], np.float32)
+        _check(lib().gd_mlp_forward(self.h, params.ctypes.data, feat.ctypes.data, feat.shape[0], prob.ctypes.data))
+        return prob
+
+    def mlp_grad(self, params, feat, label, pos_weight=1.0):
+        params = np.ascontiguousarray(params, np.float32)
+        feat = np.ascontiguousarray(feat, np.float32).reshape(-1, TRI_NF)
+        label = np.ascontiguousarray(label, np.float32)
+        grad = np.zeros(TRI_NPARAM, np.float32)
+        loss = np.zeros(1, np.float32)
+        _check(lib().gd_mlp_grad(self.h, params.ctypes.data, feat.ctypes.data, label.ctypes.data, feat.shape[0],
+                                 float(pos_weight), grad.ctypes.data, loss.ctypes.data))
+        return grad, float(loss[0])
+
+    def mlp_train(self, feat, label, params, epochs=20, batch=4096, lr=2e-3, pos_weight=1.0, seed=1):
+        feat = np.ascontiguousarray(feat, np.float32).reshape(-1, TRI_NF)
+        label = np.ascontiguousarray(label, np.float32)
+        out = np.array(params, np.float32, copy=True)
+        losses = np.zeros(epochs, np.float32)
+        _check(lib().gd_mlp_train(self.h, feat.ctypes.data, label.ctypes.data, feat.shape[0], int(epochs), int(batch),
+                                  float(lr), float(pos_weight), int(seed), out.ctypes.data, losses.ctypes.data))
+        return out, losses
 
     def local_alignment_batch(self, abases, aoff, alen, bbases, boff, blen, diag, anti, comp, trstride=None):
         n = len(diag)

@@ -1249,9 +1249,13 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32, 4)
         g = __shfl_sync(GD_FULL, g, 0);
         if (g >= ngroups || st->code != 0)
             break;
-        uint2 grp = groups[order[g]];
+        const unsigned item = order[g];
+        if (out.skip && out.skip[item])
+            continue;
+        uint2 grp = groups[item];
         const int s = (int)grp.x, e = (int)grp.y;
-        w.item = (int)order[g];
+        w.item = (int)item;
+        const long long cells0 = w.cells;
         uint64_t k0 = hkey[s];
         const int ar = (int)((k0 >> P.hb.pbits) & ((1ull << P.hb.abits) - 1));
         const int br = (int)(k0 >> (P.hb.pbits + P.hb.abits));
@@ -1476,6 +1480,9 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32, 4)
         __syncwarp();
         emit_paths(w, P, amatch, novla, tbuf, ar + A.ufirst, br + B.ufirst, out);
         emit_paths(w, P, bmatch, novlb, tbuf, br + B.ufirst, ar + A.ufirst, out);
+        if (out.gstat && lane == 0)
+            out.gstat[item] = make_uint2((unsigned)(novla + novlb),
+                                         (unsigned)min(w.cells - cells0, (long long)0xffffffffll));
         __syncwarp();
     }
     if (lane == 0)

@@ -66,6 +66,8 @@ struct AlignOut
     uint8_t* trace;
     unsigned long long* counters;  // [0] records, [1] trace bytes, [2] cells, [3] seeds, [4] LA calls kept
     uint64_t rcap, tcap;
+    const uint8_t* skip;  // per pair group: 1 = triaged away (may be null)
+    uint2* gstat;         // per pair group: (records emitted, wave cells) (may be null)
 };
 
 size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands);

@@ -19,6 +19,9 @@
 #include "gd_filter.cuh"
 #include "gd_prims.cuh"
 #include "gd_verify.cuh"
+#include "gd_triage.cuh"
+
+static_assert(GD_TRI_NPARAM == gd::TRI_NPARAM && GD_TRI_NF == gd::TRI_NF, "triage parameter layout");
 
 static thread_local char g_err[1024] = "";
 unsigned long long g_gd_launches = 0;
@@ -125,6 +128,13 @@ struct gd_context
     std::vector<uint8_t> trace;
     gd_stats stats;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
+    // learned triage: model (on), per-group feature/outcome collection (collect)
+    int tri_on = 0, tri_collect = 0;
+    float tri_thr = 0.f;
+    DevBuf tri_params, tri_feat, tri_prob, tri_skip, tri_gstat, tri_misc;
+    DevBuf tri_x, tri_y, tri_perm, tri_grad, tri_m, tri_v, tri_loss, tri_w;
+    std::vector<float> tri_hfeat;
+    std::vector<uint32_t> tri_hrec, tri_hcells;
 };
 
 // ----------------------------------------------------------------------------------------
@@ -249,6 +259,24 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
 // Match_Filter
 // ----------------------------------------------------------------------------------------
 
+// appends the features and plain-path outcome (records, cells) of the last call's groups
+static int tri_append(gd_context* c, unsigned ng)
+{
+    size_t f0 = c->tri_hfeat.size(), g0 = c->tri_hrec.size();
+    c->tri_hfeat.resize(f0 + (size_t)ng * gd::TRI_NF);
+    std::vector<uint2> st(ng);
+    GD_CUDA(cudaMemcpy(c->tri_hfeat.data() + f0, c->tri_feat.p, (size_t)ng * gd::TRI_NF * 4, cudaMemcpyDeviceToHost));
+    GD_CUDA(cudaMemcpy(st.data(), c->tri_gstat.p, (size_t)ng * 8, cudaMemcpyDeviceToHost));
+    c->tri_hrec.resize(g0 + ng);
+    c->tri_hcells.resize(g0 + ng);
+    for (unsigned i = 0; i < ng; i++)
+    {
+        c->tri_hrec[g0 + i] = st[i].x;
+        c->tri_hcells[g0 + i] = st[i].y;
+    }
+    return 0;
+}
+
 template <typename K>
 static int match_filter_t(gd_context* c, int bslot, int comp, int self)
 {
@@ -258,6 +286,7 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     Slot& B = c->slot[bslot];
     int oi = comp ? 1 : 0;
     c->stats.hits[oi] = c->stats.groups[oi] = c->stats.seeds[oi] = c->stats.cells[oi] = 0;
+    c->stats.skipped[oi] = 0;
     c->stats.ms_merge[oi] = c->stats.ms_align[oi] = 0;
     c->nhits = 0;
     int64_t na = A.nk, nb = B.nk;
@@ -395,6 +424,26 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     if (gw < 0)
         return -1;
     uint32_t* order = gw ? P<uint32_t>(c->gidx2) : P<uint32_t>(c->gidx);
+    // learned triage: group features, MLP, skip flags (one launch)
+    const uint8_t* skip = nullptr;
+    unsigned* d_nskip = P<unsigned>(c->misc) + 32;
+    if ((c->tri_on || c->tri_collect) && ng > 0)
+    {
+        if (ensure(c->tri_skip, ng) || ensure(c->tri_gstat, (size_t)ng * 8) ||
+            (c->tri_collect && ensure(c->tri_feat, (size_t)ng * TRI_NF * 4)))
+            return -1;
+        GD_CUDA(cudaMemsetAsync(d_nskip, 0, 4, s));
+        if (launch_triage_groups(hkey, hdiag, P<uint2>(c->groups), ng, hb, A.blk, B.blk, comp, c->minover, c->binshift,
+                                 A.has_mask ? P<int64_t>(A.manno) : nullptr, A.has_mask ? P<int32_t>(A.mdata) : nullptr,
+                                 c->tri_on ? P<float>(c->tri_params) : nullptr, c->tri_thr,
+                                 c->tri_collect ? P<float>(c->tri_feat) : nullptr, P<uint8_t>(c->tri_skip),
+                                 d_nskip, s))
+            return -1;
+        if (c->tri_on)
+            skip = P<uint8_t>(c->tri_skip);
+        if (c->tri_collect)
+            GD_CUDA(cudaMemsetAsync(c->tri_gstat.p, 0, (size_t)ng * 8, s));
+    }
     GD_CUDA(cudaEventRecord(c->ev1, s));
     GD_CUDA(cudaEventSynchronize(c->ev1));
     float ms = 0;
@@ -433,19 +482,20 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     {
         AlignScratch sc{};
         size_t need = align_scratch_bytes(nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands);
-        bool fresh = need > c->ascr.n;
         if (ensure(c->ascr, need))
             return -1;
         align_scratch_carve(&sc, c->ascr.p, nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands);
-        if (fresh || attempt > 0)
-            GD_CUDA(cudaMemsetAsync(sc.bands, 0, (size_t)nwarps * 3 * nbands * 4, s));
+        // the band arrays (score, lastp, lasta per warp) start at zero on every launch: their
+        // place in the scratch moves with maxlen and the capacities, so an earlier launch's
+        // clean-up does not cover them
+        GD_CUDA(cudaMemsetAsync(sc.bands, 0, (size_t)nwarps * 3 * nbands * 4, s));
         if (ensure(c->outrec, c->rcap * sizeof(OutRec)) || ensure(c->outtr, c->tbcap) ||
             ensure(c->counters, 8 * 8) || ensure(c->status, sizeof(DevStatus)) || ensure(c->queue, 16))
             return -1;
         GD_CUDA(cudaMemsetAsync(c->counters.p, 0, 64, s));
         GD_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), s));
         AlignOut out{P<OutRec>(c->outrec), P<uint8_t>(c->outtr), P<unsigned long long>(c->counters), c->rcap,
-                     c->tbcap};
+                     c->tbcap, skip, c->tri_collect ? P<uint2>(c->tri_gstat) : nullptr};
         GD_CUDA(cudaEventRecord(c->ev0, s));
         if (launch_align_pairs(A.blk, B.blk, hkey, hdiag, P<uint2>(c->groups), order, ng, ap, sc, out,
                                P<unsigned>(c->queue), P<DevStatus>(c->status), c->agrid, s))
@@ -481,6 +531,14 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
         }
         c->stats.cells[oi] = (int64_t)cnt[2];
         c->stats.seeds[oi] = (int64_t)cnt[3];
+        if (c->tri_on)
+        {
+            unsigned nskip = 0;
+            GD_CUDA(cudaMemcpy(&nskip, d_nskip, 4, cudaMemcpyDeviceToHost));
+            c->stats.skipped[oi] = nskip;
+        }
+        if (c->tri_collect && tri_append(c, ng))
+            return -1;
         // bring the overlaps home
         size_t r0 = c->recs.size();
         size_t t0 = c->trace.size();
@@ -646,7 +704,9 @@ void gd_destroy(gd_context* c)
                       &c->excl,   &c->jb,     &c->cnt,   &c->hoff,   &c->ctrun,  &c->gram,    &c->misc,
                       &c->hk0,    &c->hd0,    &c->hk1,   &c->hd1,    &c->starts, &c->groups,  &c->gcost,
                       &c->gidx,   &c->gcost2, &c->gidx2, &c->ascr,   &c->outrec, &c->outtr,   &c->counters,
-                      &c->status, &c->queue};
+                      &c->status, &c->queue,  &c->tri_params, &c->tri_feat, &c->tri_prob, &c->tri_skip,
+                      &c->tri_gstat, &c->tri_misc, &c->tri_x, &c->tri_y, &c->tri_perm, &c->tri_grad, &c->tri_m,
+                      &c->tri_v, &c->tri_loss, &c->tri_w};
     for (DevBuf* b : bufs)
         release(*b);
     for (Slot& s : c->slot)
@@ -1194,6 +1254,212 @@ int gd_local_alignment_batch(gd_context* c, const uint8_t* abases, int64_t alen_
     for (DevBuf* b : all)
         release(*b);
     return rc;
+}
+
+// ---------------------------------------------------------------------------------------
+// learned triage (no counterpart in the reference)
+// ---------------------------------------------------------------------------------------
+
+int gd_triage_collect(gd_context* c, int on)
+{
+    c->tri_collect = on ? 1 : 0;
+    return 0;
+}
+
+int64_t gd_triage_get_groups(gd_context* c, float* feat, uint32_t* records, uint32_t* cells, int64_t cap)
+{
+    int64_t n = (int64_t)c->tri_hrec.size();
+    int64_t m = std::min(n, cap);
+    if (m > 0)
+    {
+        if (feat)
+            memcpy(feat, c->tri_hfeat.data(), (size_t)m * gd::TRI_NF * 4);
+        if (records)
+            memcpy(records, c->tri_hrec.data(), (size_t)m * 4);
+        if (cells)
+            memcpy(cells, c->tri_hcells.data(), (size_t)m * 4);
+    }
+    return n;
+}
+
+int gd_triage_reset(gd_context* c)
+{
+    c->tri_hfeat.clear();
+    c->tri_hrec.clear();
+    c->tri_hcells.clear();
+    return 0;
+}
+
+int gd_triage_set_model(gd_context* c, const float* params, float threshold)
+{
+    if (!params)
+    {
+        c->tri_on = 0;
+        return 0;
+    }
+    for (int i = 0; i < gd::TRI_NF; i++)
+        if (!(params[gd::TRI_OFF_STD + i] > 0.f))
+        {
+            gd_set_error("triage model: feature %d has a non-positive scale", i);
+            return -1;
+        }
+    if (ensure(c->tri_params, gd::TRI_NPARAM * 4) || ensure(c->tri_misc, 64))
+        return -1;
+    GD_CUDA(cudaMemcpy(c->tri_params.p, params, gd::TRI_NPARAM * 4, cudaMemcpyHostToDevice));
+    c->tri_thr = threshold;
+    c->tri_on = 1;
+    return 0;
+}
+
+int gd_mlp_forward(gd_context* c, const float* params, const float* feat, int64_t n, float* prob)
+{
+    if (n < 0)
+    {
+        gd_set_error("gd_mlp_forward: negative row count");
+        return -1;
+    }
+    if (n == 0)
+        return 0;
+    if (ensure(c->tri_w, gd::TRI_NPARAM * 4) || ensure(c->tri_x, (size_t)n * gd::TRI_NF * 4) ||
+        ensure(c->tri_prob, (size_t)n * 4))
+        return -1;
+    cudaStream_t s = c->s;
+    GD_CUDA(cudaMemcpyAsync(c->tri_w.p, params, gd::TRI_NPARAM * 4, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemcpyAsync(c->tri_x.p, feat, (size_t)n * gd::TRI_NF * 4, cudaMemcpyHostToDevice, s));
+    if (gd::launch_mlp_forward(P<float>(c->tri_w), P<float>(c->tri_x), n, P<float>(c->tri_prob), s))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(prob, c->tri_prob.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int gd_mlp_grad(gd_context* c, const float* params, const float* feat, const float* label, int n, float pos_weight,
+                float* grad, float* loss)
+{
+    if (n <= 0)
+    {
+        gd_set_error("gd_mlp_grad: empty batch");
+        return -1;
+    }
+    if (ensure(c->tri_w, gd::TRI_NPARAM * 4) || ensure(c->tri_x, (size_t)n * gd::TRI_NF * 4) ||
+        ensure(c->tri_y, (size_t)n * 4) || ensure(c->tri_grad, gd::TRI_NPARAM * 4) || ensure(c->tri_loss, 16))
+        return -1;
+    cudaStream_t s = c->s;
+    GD_CUDA(cudaMemcpyAsync(c->tri_w.p, params, gd::TRI_NPARAM * 4, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemcpyAsync(c->tri_x.p, feat, (size_t)n * gd::TRI_NF * 4, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemcpyAsync(c->tri_y.p, label, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    if (gd::launch_mlp_grad(P<float>(c->tri_w), P<float>(c->tri_x), P<float>(c->tri_y), n, pos_weight,
+                            P<float>(c->tri_grad), P<float>(c->tri_loss), s))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(grad, c->tri_grad.p, gd::TRI_NPARAM * 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaMemcpyAsync(loss, c->tri_loss.p, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+static uint64_t splitmix64(uint64_t& x)
+{
+    uint64_t z = (x += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+int gd_mlp_init(const float* feat, int64_t n, uint64_t seed, float* params)
+{
+    using namespace gd;
+    if (n <= 0)
+    {
+        gd_set_error("gd_mlp_init: no rows");
+        return -1;
+    }
+    memset(params, 0, TRI_NPARAM * 4);
+    for (int f = 0; f < TRI_NF; f++)
+    {
+        double s = 0, q = 0;
+        for (int64_t i = 0; i < n; i++)
+        {
+            double v = feat[i * TRI_NF + f];
+            s += v;
+            q += v * v;
+        }
+        double mean = s / n, var = q / n - mean * mean;
+        params[TRI_OFF_MEAN + f] = (float)mean;
+        params[TRI_OFF_STD + f] = (float)(var > 1e-12 ? sqrt(var) : 1.0);
+    }
+    // He-uniform weights, zero biases
+    uint64_t st = seed;
+    auto uni = [&](double bound) {
+        double u = (double)(splitmix64(st) >> 11) * (1.0 / 9007199254740992.0);
+        return (float)((2 * u - 1) * bound);
+    };
+    for (int i = 0; i < TRI_H * TRI_NF; i++)
+        params[TRI_OFF_W1 + i] = uni(sqrt(6.0 / TRI_NF));
+    for (int i = 0; i < TRI_H * TRI_H; i++)
+        params[TRI_OFF_W2 + i] = uni(sqrt(6.0 / TRI_H));
+    for (int i = 0; i < TRI_H; i++)
+        params[TRI_OFF_W3 + i] = uni(sqrt(3.0 / TRI_H));
+    return 0;
+}
+
+int gd_mlp_train(gd_context* c, const float* feat, const float* label, int64_t n, int epochs, int batch, float lr,
+                 float pos_weight, uint64_t seed, float* params, float* epoch_loss)
+{
+    using namespace gd;
+    if (n <= 0 || batch <= 0 || epochs <= 0 || n > INT32_MAX)
+    {
+        gd_set_error("gd_mlp_train: bad sizes (n %lld, batch %d, epochs %d)", (long long)n, batch, epochs);
+        return -1;
+    }
+    const int64_t nb = (n + batch - 1) / batch;
+    cudaStream_t s = c->s;
+    if (ensure(c->tri_w, TRI_NPARAM * 4) || ensure(c->tri_x, (size_t)n * TRI_NF * 4) || ensure(c->tri_y, (size_t)n * 4) ||
+        ensure(c->tri_perm, (size_t)n * 4) || ensure(c->tri_grad, TRI_NPARAM * 4) || ensure(c->tri_m, TRI_NPARAM * 4) ||
+        ensure(c->tri_v, TRI_NPARAM * 4) || ensure(c->tri_loss, (size_t)nb * 4))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(c->tri_w.p, params, TRI_NPARAM * 4, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemcpyAsync(c->tri_x.p, feat, (size_t)n * TRI_NF * 4, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemcpyAsync(c->tri_y.p, label, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemsetAsync(c->tri_m.p, 0, TRI_NPARAM * 4, s));
+    GD_CUDA(cudaMemsetAsync(c->tri_v.p, 0, TRI_NPARAM * 4, s));
+    std::vector<int> perm(n);
+    std::vector<float> bl(nb);
+    uint64_t st = seed ^ 0x5bd1e995ull;
+    int step = 0;
+    for (int ep = 0; ep < epochs; ep++)
+    {
+        for (int64_t i = 0; i < n; i++)
+            perm[i] = (int)i;
+        for (int64_t i = n - 1; i > 0; i--)
+            std::swap(perm[i], perm[splitmix64(st) % (uint64_t)(i + 1)]);
+        GD_CUDA(cudaMemcpyAsync(c->tri_perm.p, perm.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
+        for (int64_t b = 0; b < nb; b++)
+        {
+            int64_t r0 = b * batch;
+            int rows = (int)std::min<int64_t>(batch, n - r0);
+            if (launch_mlp_grad_perm(P<float>(c->tri_w), P<float>(c->tri_x), P<float>(c->tri_y), P<int>(c->tri_perm),
+                                     r0, rows, pos_weight, P<float>(c->tri_grad), P<float>(c->tri_loss) + b, s) ||
+                launch_adam(P<float>(c->tri_w), P<float>(c->tri_grad), P<float>(c->tri_m), P<float>(c->tri_v), ++step,
+                            lr, s))
+                return -1;
+        }
+        GD_CUDA(cudaMemcpyAsync(bl.data(), c->tri_loss.p, (size_t)nb * 4, cudaMemcpyDeviceToHost, s));
+        GD_CUDA(cudaStreamSynchronize(s));
+        if (epoch_loss)
+        {
+            double sum = 0, w = 0;
+            for (int64_t b = 0; b < nb; b++)
+            {
+                double rows = (double)std::min<int64_t>(batch, n - b * batch);
+                sum += bl[b] * rows;
+                w += rows;
+            }
+            epoch_loss[ep] = (float)(sum / w);
+        }
+    }
+    GD_CUDA(cudaMemcpyAsync(params, c->tri_w.p, TRI_NPARAM * 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    return 0;
 }
 
 }  // extern "C"

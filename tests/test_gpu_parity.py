@@ -155,6 +155,26 @@ def test_full_block_cfg1_matches_oracle_and_is_deterministic(mb, tmp_path):
     assert ok, msg
 
 
+def test_context_reuse_across_blocks_matches_fresh_contexts(mb, tmp_path):
+    """One context over blocks of different maximum read lengths (the aligner's scratch
+    layout moves with maxlen) gives every block exactly the output of a fresh context."""
+    blocks = []
+    for name in ("cfg1", "tiny", "tiny_tandem"):
+        reads, _ = synth.generate(name)
+        dazzdb.write_db(str(tmp_path / name), reads, 200)
+        blocks.append(dazzdb.open_block(str(tmp_path / (name + ".1"))))
+    assert len({A.maxlen for A in blocks}) == 3
+    ctx = mb.Context()
+    seq = blocks + [blocks[0], blocks[2], blocks[1]]
+    shared = [mb.daligner_block(ctx, A) for A in seq]
+    ctx.close()
+    for A, (r, t) in zip(seq, shared):
+        f = mb.Context()
+        r0, t0 = mb.daligner_block(f, A)
+        f.close()
+        assert r.size == r0.size and (r == r0).all() and (t == t0).all()
+
+
 def test_size_independent_properties_cfg2(mb, tmp_path):
     """The bacterial workload at full size (~115 Mbp block): the output is sorted by
     (aread, bread, comp, abpos), every A-path has its B-path mirror, traces are consistent
