@@ -100,9 +100,16 @@ int gd_match_filter(gd_context* ctx, int bslot, int comp, int self);
 /* The sorted hits of the last gd_match_filter (rows diag, apos, aread, bread), for tests. */
 int64_t gd_get_hits(gd_context* ctx, int32_t* rows4, int64_t cap);
 
-/* Overlap buffer: count, copy out (sorted as SORT_OVL, dalign/align.c:5786-5813), write
- * .las files as Write_Overlap_Buffer does (dalign/align.c:5815-6043), reset. */
+/* Overlap buffer (kept in device memory): count, sort, copy out, write .las files as
+ * Write_Overlap_Buffer does (dalign/align.c:5815-6043), reset.
+ * gd_num_overlaps: records and trace bytes in the buffer (before the -I identity filter).
+ * gd_sort_overlaps: sorts the buffer on the device in SORT_OVL order (aread, bread,
+ * orientation, abpos; dalign/align.c:5786-5813; ties by aepos, bbpos) with the identity
+ * filter applied; returns the records kept and their trace bytes.  Later reads reuse it.
+ * gd_get_overlaps: copies up to rcap sorted records and their traces (at most tcap bytes;
+ * toff = offset in trace) to host memory; returns the number of records copied. */
 int64_t gd_num_overlaps(gd_context* ctx, int64_t* trace_bytes);
+int64_t gd_sort_overlaps(gd_context* ctx, int64_t* trace_bytes);
 int64_t gd_get_overlaps(gd_context* ctx, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap);
 int gd_write_overlap_buffer(gd_context* ctx, int run_id, const char* ablock, const char* bblock, int last_read);
 int gd_reset_overlap_buffer(gd_context* ctx);

@@ -60,7 +60,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
-           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train"]
+           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -92,6 +92,8 @@ def lib():
     L.gd_num_overlaps.restype = C.c_int64
     L.gd_get_overlaps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
     L.gd_get_overlaps.restype = C.c_int64
+    L.gd_sort_overlaps.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.gd_sort_overlaps.restype = C.c_int64
     L.gd_write_overlap_buffer.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
     L.gd_reset_overlap_buffer.argtypes = [C.c_void_p]
     L.gd_get_stats.argtypes = [C.c_void_p, C.POINTER(GdStats)]
@@ -232,13 +234,28 @@ class Context:
         _check(lib().gd_get_hits(self.h, rows.ctypes.data, n))
         return rows[:n]
 
-    def overlaps(self):
+    def sort_overlaps(self):
+        """Sorts the overlap buffer on the device; returns (records, trace bytes) kept."""
         tb = C.c_int64()
-        n = _check(lib().gd_num_overlaps(self.h, C.byref(tb)))
-        recs = np.zeros(max(n, 1), OVL_DTYPE)
-        tr = np.zeros(max(tb.value, 1), np.uint8)
-        k = _check(lib().gd_get_overlaps(self.h, recs.ctypes.data, tr.ctypes.data, n, tb.value))
-        return recs[:k], tr
+        n = _check(lib().gd_sort_overlaps(self.h, C.byref(tb)))
+        return n, tb.value
+
+    def overlaps(self, out=None):
+        """The overlap buffer, sorted like the .las file: (records, trace bytes).  out may
+        give (records array of OVL_DTYPE, uint8 array) to fill, e.g. views of pinned memory;
+        they must be large enough, and the views returned are their prefixes."""
+        n, tb = self.sort_overlaps()
+        if out is None:
+            recs = np.empty(max(n, 1), OVL_DTYPE)
+            tr = np.empty(max(tb, 1), np.uint8)
+        else:
+            recs, tr = out
+            if recs.dtype != OVL_DTYPE or recs.size < n or tr.size < tb or not (recs.flags.c_contiguous and
+                                                                               tr.flags.c_contiguous):
+                raise ValueError(f"output buffers too small or wrong type for {n} records / {tb} trace bytes")
+        k = _check(lib().gd_get_overlaps(self.h, recs.ctypes.data, tr.ctypes.data, n, tb))
+        assert k == n
+        return recs[:k], tr[:tb]
 
     def write_overlap_buffer(self, run_id, ablock, bblock, last_read):
         _check(lib().gd_write_overlap_buffer(self.h, run_id, ablock.encode(), bblock.encode(), last_read))

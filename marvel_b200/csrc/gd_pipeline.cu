@@ -17,6 +17,7 @@
 #include "../../include/gpudalign.h"
 #include "gd_align.cuh"
 #include "gd_filter.cuh"
+#include "gd_output.cuh"
 #include "gd_prims.cuh"
 #include "gd_verify.cuh"
 #include "gd_triage.cuh"
@@ -79,6 +80,59 @@ T* P(DevBuf& b)
     return (T*)b.p;
 }
 
+// grows b to at least bytes, keeping its first used bytes
+int ensure_keep(DevBuf& b, size_t bytes, size_t used, cudaStream_t s)
+{
+    if (bytes <= b.n)
+        return 0;
+    size_t want = bytes + bytes / 2;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess)
+    {
+        gd_set_error("cudaMalloc of %zu bytes failed: %s", want, cudaGetErrorString(e));
+        return -1;
+    }
+    if (used)
+    {
+        GD_CUDA(cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, s));
+        GD_CUDA(cudaStreamSynchronize(s));
+    }
+    if (b.p)
+        cudaFree(b.p);
+    b.p = p;
+    b.n = want;
+    return 0;
+}
+
+struct HostBuf
+{
+    void* p = nullptr;
+    size_t n = 0;
+};
+
+int ensure_host(HostBuf& b, size_t bytes)
+{
+    if (bytes == 0)
+        bytes = 16;
+    if (bytes <= b.n)
+        return 0;
+    if (b.p)
+        cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.n = 0;
+    size_t want = bytes + bytes / 8;
+    cudaError_t e = cudaMallocHost(&b.p, want);
+    if (e != cudaSuccess)
+    {
+        b.p = nullptr;
+        gd_set_error("cudaMallocHost of %zu bytes failed: %s", want, cudaGetErrorString(e));
+        return -1;
+    }
+    b.n = want;
+    return 0;
+}
+
 struct Slot
 {
     DevBuf bases, boff, rlen, manno, mdata;
@@ -124,8 +178,12 @@ struct gd_context
     int agrid = 0;
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
     uint64_t rcap = 1 << 22, tbcap = 512ull << 20;
-    std::vector<gd_overlap> recs;
-    std::vector<uint8_t> trace;
+    // the overlap buffer: records and trace bytes of every Match_Filter since the last reset,
+    // in HBM in emission order (acc_*), and its sorted, compacted copy (srt_*)
+    DevBuf acc_rec, acc_tr, srt_rec, srt_tr, okey0, okey1, oval0, oval1, olen;
+    uint64_t acc_n = 0, acc_tb = 0, srt_n = 0, srt_tb = 0;
+    bool srt_valid = false;
+    HostBuf h_rec, h_tr;  // pinned staging for file writes
     gd_stats stats;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
     // learned triage: model (on), per-group feature/outcome collection (collect)
@@ -539,32 +597,17 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
         }
         if (c->tri_collect && tri_append(c, ng))
             return -1;
-        // bring the overlaps home
-        size_t r0 = c->recs.size();
-        size_t t0 = c->trace.size();
-        std::vector<OutRec> tmp(cnt[0]);
-        c->trace.resize(t0 + cnt[1]);
-        if (cnt[0])
-            GD_CUDA(cudaMemcpy(tmp.data(), c->outrec.p, cnt[0] * sizeof(OutRec), cudaMemcpyDeviceToHost));
+        // append to the overlap buffer in HBM
+        if (ensure_keep(c->acc_rec, (c->acc_n + cnt[0]) * sizeof(OutRec), c->acc_n * sizeof(OutRec), s) ||
+            ensure_keep(c->acc_tr, c->acc_tb + cnt[1] + 16, c->acc_tb, s))
+            return -1;
+        if (launch_ovl_append(P<OutRec>(c->outrec), cnt[0], c->acc_tb, P<OutRec>(c->acc_rec) + c->acc_n, s))
+            return -1;
         if (cnt[1])
-            GD_CUDA(cudaMemcpy(c->trace.data() + t0, c->outtr.p, cnt[1], cudaMemcpyDeviceToHost));
-        c->recs.resize(r0 + cnt[0]);
-        for (size_t i = 0; i < cnt[0]; i++)
-        {
-            gd_overlap& o = c->recs[r0 + i];
-            const OutRec& x = tmp[i];
-            o.tlen = x.tlen;
-            o.diffs = x.diffs;
-            o.abpos = x.abpos;
-            o.bbpos = x.bbpos;
-            o.aepos = x.aepos;
-            o.bepos = x.bepos;
-            o.flags = x.flags;
-            o.aread = x.aread;
-            o.bread = x.bread;
-            o.pad = 0;
-            o.toff = x.toff + t0;
-        }
+            GD_CUDA(cudaMemcpyAsync(P<uint8_t>(c->acc_tr) + c->acc_tb, c->outtr.p, cnt[1], cudaMemcpyDeviceToDevice, s));
+        c->acc_n += cnt[0];
+        c->acc_tb += cnt[1];
+        c->srt_valid = false;
         return 0;
     }
     gd_set_error("aligner scratch could not be grown enough");
@@ -575,36 +618,104 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
 // overlap sort + .las writing (Write_Overlap_Buffer, dalign/align.c:5786-6043)
 // ----------------------------------------------------------------------------------------
 
-static bool ovl_less(const gd_overlap& l, const gd_overlap& r)
+// Write_Overlap_Buffer's sort (SORT_OVL, dalign/align.c:5786-5813) on the device: order
+// (aread, bread, orientation, abpos), ties by (aepos, bbpos) -- the reference's qsort leaves
+// ties unordered -- with -I's identity filter (only_identity) applied as a drop bit.
+static int sort_overlaps(gd_context* c)
 {
-    if (l.aread != r.aread)
-        return l.aread < r.aread;
-    if (l.bread != r.bread)
-        return l.bread < r.bread;
-    if ((l.flags & 1) != (r.flags & 1))
-        return (l.flags & 1) < (r.flags & 1);
-    if (l.abpos != r.abpos)
-        return l.abpos < r.abpos;
-    // keys tie: the reference's qsort leaves these unordered; fix an order
-    if (l.aepos != r.aepos)
-        return l.aepos < r.aepos;
-    if (l.bbpos != r.bbpos)
-        return l.bbpos < r.bbpos;
-    return l.toff < r.toff;
+    using namespace gd;
+    if (c->srt_valid)
+        return 0;
+    cudaStream_t s = c->s;
+    const uint64_t n = c->acc_n;
+    c->srt_n = c->srt_tb = 0;
+    if (n == 0)
+    {
+        c->srt_valid = true;
+        return 0;
+    }
+    if (n > 0xffffffffull)
+    {
+        gd_set_error("%llu overlaps exceed the 32-bit sort index", (unsigned long long)n);
+        return -1;
+    }
+    if (ensure(c->okey0, n * 8) || ensure(c->okey1, n * 8) || ensure(c->oval0, n * 4) || ensure(c->oval1, n * 4) ||
+        ensure(c->olen, n * 8 + 8) ||
+        ensure(c->scratch, std::max(radix_scratch_bytes((int64_t)n), scan_scratch_bytes<uint64_t>((int64_t)n))) ||
+        ensure(c->misc, 256))
+        return -1;
+    const OutRec* rec = P<OutRec>(c->acc_rec);
+    unsigned* d_ext = P<unsigned>(c->misc) + 40;
+    unsigned long long* d_kept = (unsigned long long*)(P<unsigned>(c->misc) + 44);
+    uint64_t* d_total = (uint64_t*)(P<unsigned>(c->misc) + 46);
+    static const unsigned ext0[3] = {0xffffffffu, 0u, 0u};
+    GD_CUDA(cudaMemcpyAsync(d_ext, ext0, sizeof ext0, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemsetAsync(d_kept, 0, 8, s));
+    if (launch_ovl_extent(rec, n, d_ext, s))
+        return -1;
+    unsigned ext[3];
+    GD_CUDA(cudaMemcpyAsync(ext, d_ext, sizeof ext, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    const int pbits = bits_for(std::max(ext[2], 1u));
+    const int rbits = bits_for(std::max(ext[1] - ext[0], 1u));
+    if (3 * pbits + 1 > 64 || 2 * rbits + 1 > 64)
+    {
+        gd_set_error("overlap sort keys need %d / %d bits", 3 * pbits + 1, 2 * rbits + 1);
+        return -1;
+    }
+    if (launch_ovl_key_lo(rec, n, pbits, P<uint64_t>(c->okey0), P<uint32_t>(c->oval0), s))
+        return -1;
+    int w1 = radix_sort_pairs<uint64_t>(P<uint64_t>(c->okey0), P<uint32_t>(c->oval0), P<uint64_t>(c->okey1),
+                                        P<uint32_t>(c->oval1), n, 0, 3 * pbits + 1, c->scratch.p, s);
+    if (w1 < 0)
+        return -1;
+    uint64_t* ka = w1 ? P<uint64_t>(c->okey1) : P<uint64_t>(c->okey0);
+    uint32_t* va = w1 ? P<uint32_t>(c->oval1) : P<uint32_t>(c->oval0);
+    uint64_t* kb = w1 ? P<uint64_t>(c->okey0) : P<uint64_t>(c->okey1);
+    uint32_t* vb = w1 ? P<uint32_t>(c->oval0) : P<uint32_t>(c->oval1);
+    if (launch_ovl_key_hi(rec, va, n, rbits, ext[0], c->only_identity, ka, d_kept, s))
+        return -1;
+    int w2 = radix_sort_pairs<uint64_t>(ka, va, kb, vb, n, 0, 2 * rbits + 1, c->scratch.p, s);
+    if (w2 < 0)
+        return -1;
+    const uint32_t* perm = w2 ? vb : va;
+    const int tbytes = c->tspace <= 125 ? 1 : 2;
+    uint64_t* off = P<uint64_t>(c->olen);
+    if (launch_ovl_len(rec, perm, n, tbytes, off, s) ||
+        exclusive_scan<uint64_t>(off, off, (int64_t)n, d_total, c->scratch.p, s))
+        return -1;
+    unsigned long long kept = 0;
+    GD_CUDA(cudaMemcpyAsync(&kept, d_kept, 8, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    uint64_t kbytes = 0;
+    GD_CUDA(cudaMemcpyAsync(&kbytes, kept < n ? off + kept : d_total, 8, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    if (ensure(c->srt_rec, kept * sizeof(OutRec)) || ensure(c->srt_tr, kbytes + 16))
+        return -1;
+    if (launch_ovl_gather(rec, P<uint8_t>(c->acc_tr), perm, off, kept, tbytes, P<OutRec>(c->srt_rec),
+                          P<uint8_t>(c->srt_tr), s))
+        return -1;
+    GD_CUDA(cudaStreamSynchronize(s));
+    c->srt_n = kept;
+    c->srt_tb = kbytes;
+    c->srt_valid = true;
+    return 0;
 }
 
-static std::vector<size_t> sorted_order(gd_context* c)
+// the sorted buffer in pinned host memory (h_rec, h_tr)
+static int stage_sorted(gd_context* c)
 {
-    std::vector<size_t> idx;
-    idx.reserve(c->recs.size());
-    for (size_t i = 0; i < c->recs.size(); i++)
-        if (!c->only_identity || c->recs[i].aread == c->recs[i].bread)
-            idx.push_back(i);
-    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return ovl_less(c->recs[a], c->recs[b]); });
-    return idx;
+    if (sort_overlaps(c) || ensure_host(c->h_rec, c->srt_n * sizeof(gd_overlap)) || ensure_host(c->h_tr, c->srt_tb))
+        return -1;
+    if (c->srt_n)
+        GD_CUDA(cudaMemcpyAsync(c->h_rec.p, c->srt_rec.p, c->srt_n * sizeof(gd_overlap), cudaMemcpyDeviceToHost, c->s));
+    if (c->srt_tb)
+        GD_CUDA(cudaMemcpyAsync(c->h_tr.p, c->srt_tr.p, c->srt_tb, cudaMemcpyDeviceToHost, c->s));
+    GD_CUDA(cudaStreamSynchronize(c->s));
+    return 0;
 }
 
-static int write_las(gd_context* c, const char* path, const std::vector<size_t>& idx, size_t from, size_t to)
+static int write_las(gd_context* c, const char* path, size_t from, size_t to)
 {
     FILE* f = fopen(path, "w");
     if (!f)
@@ -612,21 +723,23 @@ static int write_las(gd_context* c, const char* path, const std::vector<size_t>&
         gd_set_error("Cannot open file %s for writing", path);
         return -1;
     }
+    const gd_overlap* recs = (const gd_overlap*)c->h_rec.p;
+    const uint8_t* trace = (const uint8_t*)c->h_tr.p;
     int tbytes = c->tspace <= 125 ? 1 : 2;
     int64_t n = (int64_t)(to - from);
     int32_t ts = c->tspace;
     fwrite(&n, 8, 1, f);
     fwrite(&ts, 4, 1, f);
     std::vector<uint8_t> buf;
-    buf.reserve(1 << 20);
+    buf.reserve(1 << 21);
     for (size_t i = from; i < to; i++)
     {
-        const gd_overlap& o = c->recs[idx[i]];
+        const gd_overlap& o = recs[i];
         int32_t r[10] = {o.tlen, o.diffs, o.abpos, o.bbpos, o.aepos, o.bepos, (int32_t)o.flags, o.aread, o.bread, 0};
         const uint8_t* rb = (const uint8_t*)r;
         buf.insert(buf.end(), rb, rb + 40);
         if (o.tlen > 0)
-            buf.insert(buf.end(), c->trace.data() + o.toff, c->trace.data() + o.toff + (size_t)o.tlen * tbytes);
+            buf.insert(buf.end(), trace + o.toff, trace + o.toff + (size_t)o.tlen * tbytes);
         if (buf.size() > (1 << 20))
         {
             fwrite(buf.data(), 1, buf.size(), f);
@@ -706,9 +819,13 @@ void gd_destroy(gd_context* c)
                       &c->gidx,   &c->gcost2, &c->gidx2, &c->ascr,   &c->outrec, &c->outtr,   &c->counters,
                       &c->status, &c->queue,  &c->tri_params, &c->tri_feat, &c->tri_prob, &c->tri_skip,
                       &c->tri_gstat, &c->tri_misc, &c->tri_x, &c->tri_y, &c->tri_perm, &c->tri_grad, &c->tri_m,
-                      &c->tri_v, &c->tri_loss, &c->tri_w};
+                      &c->tri_v, &c->tri_loss, &c->tri_w, &c->acc_rec, &c->acc_tr, &c->srt_rec, &c->srt_tr,
+                      &c->okey0, &c->okey1, &c->oval0, &c->oval1, &c->olen};
     for (DevBuf* b : bufs)
         release(*b);
+    for (HostBuf* h : {&c->h_rec, &c->h_tr})
+        if (h->p)
+            cudaFreeHost(h->p);
     for (Slot& s : c->slot)
     {
         DevBuf* sb[] = {&s.bases, &s.boff, &s.rlen, &s.manno, &s.mdata, &s.code, &s.read, &s.rpos};
@@ -760,6 +877,7 @@ int gd_new_align_spec(gd_context* c, double ave_corr, int trace_space, const flo
     c->only_identity = only_identity;
     c->no_trace = no_trace_points;
     c->spec_set = 1;
+    c->srt_valid = false;  // the identity filter and trace width enter the sorted copy
     return upload_spec(c);
 }
 
@@ -966,33 +1084,52 @@ int64_t gd_get_hits(gd_context* c, int32_t* rows4, int64_t cap)
 int64_t gd_num_overlaps(gd_context* c, int64_t* trace_bytes)
 {
     if (trace_bytes)
-        *trace_bytes = (int64_t)c->trace.size();
-    return (int64_t)c->recs.size();
+        *trace_bytes = (int64_t)c->acc_tb;
+    return (int64_t)c->acc_n;
+}
+
+int64_t gd_sort_overlaps(gd_context* c, int64_t* trace_bytes)
+{
+    if (sort_overlaps(c))
+        return -1;
+    if (trace_bytes)
+        *trace_bytes = (int64_t)c->srt_tb;
+    return (int64_t)c->srt_n;
 }
 
 int64_t gd_get_overlaps(gd_context* c, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap)
 {
-    std::vector<size_t> idx = sorted_order(c);
+    if (sort_overlaps(c))
+        return -1;
+    int64_t m = std::min<int64_t>(rcap, (int64_t)c->srt_n);
+    if (m <= 0)
+        return 0;
+    GD_CUDA(cudaMemcpyAsync(recs, c->srt_rec.p, (size_t)m * sizeof(gd_overlap), cudaMemcpyDeviceToHost, c->s));
+    GD_CUDA(cudaStreamSynchronize(c->s));
     int tbytes = c->tspace <= 125 ? 1 : 2;
-    uint64_t t = 0;
     int64_t n = 0;
-    for (size_t i = 0; i < idx.size() && n < rcap; i++, n++)
+    uint64_t end = 0;
+    for (; n < m; n++)
     {
-        gd_overlap o = c->recs[idx[i]];
-        size_t len = (size_t)o.tlen * tbytes;
-        if ((int64_t)(t + len) > tcap)
+        uint64_t e2 = recs[n].toff + (uint64_t)recs[n].tlen * tbytes;
+        if ((int64_t)e2 > tcap)
             break;
-        memcpy(trace + t, c->trace.data() + o.toff, len);
-        o.toff = t;
-        recs[n] = o;
-        t += len;
+        end = e2;
+    }
+    if (end)
+    {
+        GD_CUDA(cudaMemcpyAsync(trace, c->srt_tr.p, end, cudaMemcpyDeviceToHost, c->s));
+        GD_CUDA(cudaStreamSynchronize(c->s));
     }
     return n;
 }
 
 int gd_write_overlap_buffer(gd_context* c, int run_id, const char* ablock, const char* bblock, int last_read)
 {
-    std::vector<size_t> idx = sorted_order(c);
+    if (stage_sorted(c))
+        return -1;
+    const size_t nsrt = c->srt_n;
+    const gd_overlap* srt = (const gd_overlap*)c->h_rec.p;
     // block ids and roots from the names (dalign/align.c:5858-5877)
     auto split = [](const char* name, std::string& root, int& id) {
         const char* dot = strrchr(name, '.');
@@ -1020,7 +1157,7 @@ int gd_write_overlap_buffer(gd_context* c, int run_id, const char* ablock, const
             snprintf(path1, sizeof path1, "%s.%s.%d.las", aroot.c_str(), broot.c_str(), bid);
         else
             snprintf(path1, sizeof path1, "%s.%s.las", aroot.c_str(), broot.c_str());
-        return write_las(c, path1, idx, 0, idx.size());
+        return write_las(c, path1, 0, nsrt);
     }
     std::string d1 = dirname_of(run_id, aid), d2 = dirname_of(run_id, bid);
     if (aid > 0)
@@ -1054,11 +1191,11 @@ int gd_write_overlap_buffer(gd_context* c, int run_id, const char* ablock, const
     if (bid < aid)
         std::swap(p1, p2);
     size_t j = 0;
-    while (j < idx.size() && c->recs[idx[j]].aread <= last_read)
+    while (j < nsrt && srt[j].aread <= last_read)
         j++;
-    if (write_las(c, p1, idx, 0, j))
+    if (write_las(c, p1, 0, j))
         return -1;
-    return write_las(c, p2, idx, j, idx.size());
+    return write_las(c, p2, j, nsrt);
 }
 
 int gd_compute_trace_pts(gd_context* c, int aslot, int bslot, int cslot, const gd_overlap* recs, const uint8_t* trace,
@@ -1161,14 +1298,15 @@ int gd_compute_trace_pts(gd_context* c, int aslot, int bslot, int cslot, const g
 
 int gd_reset_overlap_buffer(gd_context* c)
 {
-    c->recs.clear();
-    c->trace.clear();
+    c->acc_n = c->acc_tb = 0;
+    c->srt_n = c->srt_tb = 0;
+    c->srt_valid = false;
     return 0;
 }
 
 int gd_get_stats(gd_context* c, gd_stats* st)
 {
-    c->stats.records = (int64_t)c->recs.size();
+    c->stats.records = (int64_t)c->acc_n;
     *st = c->stats;
     return 0;
 }
