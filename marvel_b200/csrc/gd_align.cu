@@ -34,10 +34,11 @@ namespace gd
 #define RM (RING - 1)
 #define SENT4 0x0404040404040404ull
 
+// wave vectors: [dif & 1] holds wave dif, so a wave reads the previous one while it writes
 struct WaveSmem
 {
-    unsigned long long T[RING];
-    int V[RING], HA[RING], HB[RING], NA[RING], NB[RING];
+    unsigned long long T[2][RING];
+    int V[2][RING], HA[2][RING], HB[2][RING], NA[2][RING], NB[2][RING];
 };
 
 struct LAPath
@@ -270,12 +271,12 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
         }
         if (lane == 0)
         {
-            R.V[k & RM] = c;
-            R.T[k & RM] = PATH_INT;
-            R.HA[k & RM] = ha;
-            R.HB[k & RM] = hb;
-            R.NA[k & RM] = na;
-            R.NB[k & RM] = nb;
+            R.V[0][k & RM] = c;
+            R.T[0][k & RM] = PATH_INT;
+            R.HA[0][k & RM] = ha;
+            R.HB[0][k & RM] = hb;
+            R.NA[0][k & RM] = na;
+            R.NB[0][k & RM] = nb;
         }
         __syncwarp();
     }
@@ -293,15 +294,15 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                     hgh = aclip - 1;
                 else
                     low = aclip + 1;
-                int Mc = __popcll(R.T[aclip & RM] & MASK61);
+                int Mc = __popcll(R.T[dif & 1][aclip & RM] & MASK61);
                 if (morem <= Mc)
                 {
                     morem = Mc;
-                    morea = R.V[aclip & RM];
+                    morea = R.V[dif & 1][aclip & RM];
                     morey = (morea - aclip) / 2;
                     mored = dif;
-                    moreha = R.HA[aclip & RM];
-                    morehb = R.HB[aclip & RM];
+                    moreha = R.HA[dif & 1][aclip & RM];
+                    morehb = R.HB[dif & 1][aclip & RM];
                 }
             }
             if (FWD ? (low <= bclip) : (hgh >= bclip))
@@ -310,15 +311,15 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                     low = bclip + 1;
                 else
                     hgh = bclip - 1;
-                int Mc = __popcll(R.T[bclip & RM] & MASK61);
+                int Mc = __popcll(R.T[dif & 1][bclip & RM] & MASK61);
                 if (morem <= Mc)
                 {
                     morem = Mc;
-                    morea = R.V[bclip & RM];
+                    morea = R.V[dif & 1][bclip & RM];
                     morey = (morea - bclip) / 2;
                     mored = dif;
-                    moreha = R.HA[bclip & RM];
-                    morehb = R.HB[bclip & RM];
+                    moreha = R.HA[dif & 1][bclip & RM];
+                    morehb = R.HB[dif & 1][bclip & RM];
                 }
             }
             aclip = FWD ? INT_MAX : -INT_MAX;
@@ -368,8 +369,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
         }
         const int nch = (width + 31) >> 5;
         const int hgh0 = hgh, low0 = low;
-        int rc[WAVE_CHUNKS], rha[WAVE_CHUNKS], rhb[WAVE_CHUNKS], rna[WAVE_CHUNKS], rnb[WAVE_CHUNKS];
-        unsigned long long rb[WAVE_CHUNKS];
+        const int cur = dif & 1, prv = cur ^ 1;
 #pragma unroll
         for (int ch = 0; ch < WAVE_CHUNKS; ch++)
         {
@@ -385,9 +385,9 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             {
                 // choose the furthest of the three predecessors (align.c:748-797)
                 const int kP = k + S, kN = k - S;
-                int vP = (kP >= olow && kP <= ohgh) ? R.V[kP & RM] : VNONE;
-                int vC = (k >= olow && k <= ohgh) ? R.V[k & RM] : VNONE;
-                int vN = (kN >= olow && kN <= ohgh) ? R.V[kN & RM] : VNONE;
+                int vP = (kP >= olow && kP <= ohgh) ? R.V[prv][kP & RM] : VNONE;
+                int vC = (k >= olow && k <= ohgh) ? R.V[prv][k & RM] : VNONE;
+                int vN = (kN >= olow && kN <= ohgh) ? R.V[prv][kN & RM] : VNONE;
                 int wP = FWD ? vP : -vP, wC = FWD ? vC : -vC, wN = FWD ? vN : -vN;
                 int ks, vs, step;
                 if (wC < wN)
@@ -417,9 +417,9 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                     step = 2;
                 }
                 c = vs + S * step;
-                b = R.T[ks & RM] << 1;
-                ha = R.HA[ks & RM];
-                hb = R.HB[ks & RM];
+                b = R.T[prv][ks & RM] << 1;
+                ha = R.HA[prv][ks & RM];
+                hb = R.HB[prv][ks & RM];
                 y = (c - k) >> 1;
                 int y0 = y;
                 y = snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
@@ -427,8 +427,8 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 b = (L >= 61) ? ~0ull : ((b << L) | ((1ull << L) - 1ull));
                 c = (y << 1) + k;
                 const int kn = k < olow ? olow : (k > ohgh ? ohgh : k);
-                na = R.NA[kn & RM];
-                nb = R.NB[kn & RM];
+                na = R.NA[prv][kn & RM];
+                nb = R.NB[prv][kn & RM];
             }
             // trace points of A and B crossed by this extension (align.c:826-878)
             while (true)
@@ -469,12 +469,15 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 if (needB)
                     nb += FWD ? TS : -TS;
             }
-            rc[ch] = c;
-            rb[ch] = b;
-            rha[ch] = ha;
-            rhb[ch] = hb;
-            rna[ch] = na;
-            rnb[ch] = nb;
+            if (valid)
+            {
+                R.V[cur][k & RM] = c;
+                R.T[cur][k & RM] = b;
+                R.HA[cur][k & RM] = ha;
+                R.HB[cur][k & RM] = hb;
+                R.NA[cur][k & RM] = na;
+                R.NB[cur][k & RM] = nb;
+            }
 
             // clip bookkeeping: bclip = first B-end in scan order, aclip = last A-end
             unsigned bm = __ballot_sync(GD_FULL, valid && bend);
@@ -499,15 +502,18 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             // the records are enumerated with a prefix-max scan.
             int wv = valid ? (FWD ? c : -c) : INT_MIN;
             int wbest = FWD ? besta : -besta;
+            // the PATH_AVE and trim tests of every lane, in parallel with the reduction
+            const bool q1 = valid && __popcll(b & MASK61) >= PATH_AVE;
+            const bool q2 = q1 && trim_ok(b, P.table, P.score);
             int wmax = __reduce_max_sync(GD_FULL, wv);
             if (wmax > wbest)
             {
                 int jm = __ffs(__ballot_sync(GD_FULL, wv == wmax)) - 1;
+                const unsigned mq1 = __ballot_sync(GD_FULL, q1), mq2 = __ballot_sync(GD_FULL, q2);
                 besta = __shfl_sync(GD_FULL, c, jm);
                 besty = __shfl_sync(GD_FULL, y, jm);
-                unsigned long long bj = __shfl_sync(GD_FULL, b, jm);
-                bool p1j = __popcll(bj & MASK61) >= PATH_AVE;
-                bool p2j = p1j && trim_ok(bj, P.table, P.score);
+                bool p1j = (mq1 >> jm) & 1;
+                bool p2j = (mq2 >> jm) & 1;
                 if (p1j)
                     lasta = besta;
                 if (p2j)
@@ -525,12 +531,11 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                     if (lane == 0)
                         excl = INT_MIN;
                     bool rec = valid && wv > max(wbest, excl) && lane < jm;
-                    bool p1 = rec && (__popcll(b & MASK61) >= PATH_AVE);
-                    unsigned m1 = __ballot_sync(GD_FULL, p1);
+                    unsigned mrec = __ballot_sync(GD_FULL, rec);
+                    unsigned m1 = mrec & mq1;
                     if (m1 && !p1j)
                         lasta = __shfl_sync(GD_FULL, c, 31 - __clz(m1));
-                    bool p2 = p1 && trim_ok(b, P.table, P.score);
-                    unsigned m2 = __ballot_sync(GD_FULL, p2);
+                    unsigned m2 = mrec & mq2;
                     if (m2)
                     {
                         int j2 = 31 - __clz(m2);
@@ -544,28 +549,10 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             }
         }
         __syncwarp();
-#pragma unroll
-        for (int ch = 0; ch < WAVE_CHUNKS; ch++)
-        {
-            if (ch >= nch)
-                break;
-            int p = ch * 32 + lane;
-            if (p < width)
-            {
-                int k = FWD ? hgh - p : low + p;
-                R.V[k & RM] = rc[ch];
-                R.T[k & RM] = rb[ch];
-                R.HA[k & RM] = rha[ch];
-                R.HB[k & RM] = rhb[ch];
-                R.NA[k & RM] = rna[ch];
-                R.NB[k & RM] = rnb[ch];
-            }
-        }
-        __syncwarp();
         clip_block();
 
-        // drop diagonals more than WAVE_LAG behind the best (align.c:946-955), from the
-        // new values still in registers; k runs monotonically with the lane position
+        // drop diagonals more than WAVE_LAG behind the best (align.c:946-955), from this
+        // wave's ring; k runs monotonically with the lane position
         {
             const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
             const int hw = FWD ? hgh0 : low0;  // wave origin before clipping
@@ -577,7 +564,12 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                     break;
                 int p = ch * 32 + lane;
                 int k = FWD ? hw - p : hw + p;
-                bool good = p < width && k >= low && k <= hgh && (FWD ? (rc[ch] >= n) : (rc[ch] <= n));
+                bool good = p < width && k >= low && k <= hgh;
+                if (good)
+                {
+                    const int v = R.V[cur][k & RM];
+                    good = FWD ? (v >= n) : (v <= n);
+                }
                 unsigned gm = __ballot_sync(GD_FULL, good);
                 if (gm)
                 {
@@ -1209,7 +1201,7 @@ __device__ void emit_paths(WarpCtx& w, const AlignParams& P, const MPath* m, int
     }
 }
 
-__global__ void __launch_bounds__(ALIGN_WARPS * 32, 4)
+__global__ void __launch_bounds__(ALIGN_WARPS * 32, 5)
     k_align_pairs(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
                   AlignScratch sc, AlignOut out, unsigned* queue, DevStatus* st)

@@ -12,7 +12,8 @@ const int16_t* gd_context_align_tables(gd_context* ctx, int* tspace, int* ave_pa
 namespace gd
 {
 
-constexpr int RING = 256;           // wave-vector ring per warp (diagonal k lives at k & (RING-1))
+constexpr int RING = 128;           // wave-vector rings per warp, one for the previous and one for the
+                                     // current wave (diagonal k lives at k & (RING-1))
 constexpr int WAVE_CHUNKS = 4;      // band width up to 32 * WAVE_CHUNKS diagonals per wave
 constexpr int ALIGN_WARPS = 4;      // warps per CTA of the aligner
 constexpr int TRIM_TABLE = 1 << 15; // TRIM_MASK + 1 (dalign/align.c:154)

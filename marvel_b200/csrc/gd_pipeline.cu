@@ -238,7 +238,10 @@ static int upload_spec(gd_context* c)
     set_table(0, 0, 0, 0, mscore, dscore, t.data(), t.data() + gd::TRIM_TABLE);
     if (ensure(c->tables, t.size() * 2))
         return -1;
-    GD_CUDA(cudaMemcpy(c->tables.p, t.data(), t.size() * 2, cudaMemcpyHostToDevice));
+    // on the context's stream: its kernels must see the tables (the stream does not order
+    // against the legacy default stream)
+    GD_CUDA(cudaMemcpyAsync(c->tables.p, t.data(), t.size() * 2, cudaMemcpyHostToDevice, c->s));
+    GD_CUDA(cudaStreamSynchronize(c->s));
     return 0;
 }
 
@@ -1266,8 +1269,11 @@ int gd_compute_trace_pts(gd_context* c, int aslot, int bslot, int cslot, const g
         if (ensure(dseg, nseg * sizeof(Segment)) || ensure(dscr, (size_t)nthreads * 3 * (2 * R + 1) * 4) ||
             ensure(ddiff, n * 4) || ensure(dst, sizeof(DevStatus)))
             break;
-        if (cudaMemcpy(dseg.p, seg.data(), nseg * sizeof(Segment), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemset(ddiff.p, 0, n * 4) != cudaSuccess || cudaMemset(dst.p, 0, sizeof(DevStatus)) != cudaSuccess)
+        // all on the context's stream, which the kernel runs on: a plain cudaMemcpy/cudaMemset
+        // goes to the legacy stream, which a non-blocking stream does not wait for
+        if (cudaMemcpyAsync(dseg.p, seg.data(), nseg * sizeof(Segment), cudaMemcpyHostToDevice, c->s) != cudaSuccess ||
+            cudaMemsetAsync(ddiff.p, 0, n * 4, c->s) != cudaSuccess ||
+            cudaMemsetAsync(dst.p, 0, sizeof(DevStatus), c->s) != cudaSuccess)
         {
             gd_set_error("gd_compute_trace_pts: copies failed");
             break;
@@ -1443,7 +1449,8 @@ int gd_triage_set_model(gd_context* c, const float* params, float threshold)
         }
     if (ensure(c->tri_params, gd::TRI_NPARAM * 4) || ensure(c->tri_misc, 64))
         return -1;
-    GD_CUDA(cudaMemcpy(c->tri_params.p, params, gd::TRI_NPARAM * 4, cudaMemcpyHostToDevice));
+    GD_CUDA(cudaMemcpyAsync(c->tri_params.p, params, gd::TRI_NPARAM * 4, cudaMemcpyHostToDevice, c->s));
+    GD_CUDA(cudaStreamSynchronize(c->s));
     c->tri_thr = threshold;
     c->tri_on = 1;
     return 0;
