@@ -67,16 +67,11 @@ struct WarpCtx
     long long cells;
 };
 
-__device__ __forceinline__ uint64_t ld8u(const uint8_t* p)
+__device__ __forceinline__ unsigned ld4u(const uint8_t* p)
 {
     uintptr_t a = (uintptr_t)p;
-    const uint64_t* q = (const uint64_t*)(a & ~(uintptr_t)7);
-    unsigned sh = (unsigned)(a & 7) * 8;
-    uint64_t lo = __ldg(q);
-    if (!sh)
-        return lo;
-    uint64_t hi = __ldg(q + 1);
-    return (lo >> sh) | (hi << (64 - sh));
+    const unsigned* q = (const unsigned*)(a & ~(uintptr_t)3);
+    return __funnelshift_r(__ldg(q), __ldg(q + 1), (unsigned)(a & 3) * 8);
 }
 
 // Extend the match on diagonal k from b-position y forward (FWD) or backward.
@@ -88,41 +83,40 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
     if (FWD)
     {
         // the 4 after every read stops the extension; the cap only guards against a bad pointer
-        for (int guard = (lim >> 3) + 2; guard > 0; guard--)
+        for (int guard = (lim >> 2) + 2; guard > 0; guard--)
         {
-            uint64_t wb = ld8u(bseq + y), wa = ld8u(aseq + y + k);
-            uint64_t stop = (wa ^ wb) | (wb & SENT4);
+            unsigned wb = ld4u(bseq + y), wa = ld4u(aseq + y + k);
+            unsigned stop = (wa ^ wb) | (wb & 0x04040404u);
             if (stop)
             {
-                int i = (__ffsll((long long)stop) - 1) >> 3;
+                int i = (__ffs((int)stop) - 1) >> 3;
                 y += i;
-                // the stop bases come from the compare windows themselves
                 int cb = (int)(wb >> (8 * i)) & 0xff;
                 bend = (cb == 4);
                 aend = !bend && (((int)(wa >> (8 * i)) & 0xff) == 4);
                 return y;
             }
-            y += 8;
+            y += 4;
         }
         bend = aend = true;  // unreachable with well-formed blocks (every read ends with a 4)
     }
     else
     {
-        for (int guard = (lim >> 3) + 2; guard > 0; guard--)
+        for (int guard = (lim >> 2) + 2; guard > 0; guard--)
         {
-            uint64_t wb = ld8u(bseq + y - 8), wa = ld8u(aseq + y + k - 8);
-            uint64_t stop = (wa ^ wb) | (wb & SENT4);
+            unsigned wb = ld4u(bseq + y - 4), wa = ld4u(aseq + y + k - 4);
+            unsigned stop = (wa ^ wb) | (wb & 0x04040404u);
             if (stop)
             {
-                int i = __clzll((long long)stop) >> 3;
+                int i = __clz((int)stop) >> 3;
                 y -= i;
-                int sh = 8 * (7 - i);
+                int sh = 8 * (3 - i);
                 int cb = (int)(wb >> sh) & 0xff;
                 bend = (cb == 4);
                 aend = !bend && (((int)(wa >> sh) & 0xff) == 4);
                 return y;
             }
-            y -= 8;
+            y -= 4;
         }
         bend = aend = true;
     }
@@ -135,18 +129,6 @@ __device__ __forceinline__ bool trim_ok(unsigned long long b, const int16_t* tab
 {
     int lo15 = (int)(b & TRIM_MASK), hi15 = (int)((b >> TRIM_LEN) & TRIM_MASK);
     return (__ldg(table + lo15) >= 0) && (__ldg(table + hi15) + __ldg(score + lo15) >= 0);
-}
-
-__device__ __forceinline__ int warp_max_incl(int v, int lane)
-{
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1)
-    {
-        int t = __shfl_up_sync(GD_FULL, v, o);
-        if (lane >= o)
-            v = max(v, t);
-    }
-    return v;
 }
 
 // uniform single-pebble allocation (all lanes call, lane 0 writes)
@@ -370,6 +352,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
         const int nch = (width + 31) >> 5;
         const int hgh0 = hgh, low0 = low;
         const int cur = dif & 1, prv = cur ^ 1;
+        int c0 = 0;  // chunk 0's new V, for the WAVE_LAG test
 #pragma unroll
         for (int ch = 0; ch < WAVE_CHUNKS; ch++)
         {
@@ -469,6 +452,8 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 if (needB)
                     nb += FWD ? TS : -TS;
             }
+            if (ch == 0)
+                c0 = c;
             if (valid)
             {
                 R.V[cur][k & RM] = c;
@@ -526,7 +511,14 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 }
                 else
                 {
-                    int incl = warp_max_incl(wv, lane);
+                    // prefix max over the lanes before jm only (records lie before the maximum)
+                    int incl = wv;
+                    for (int o = 1; o < jm; o <<= 1)
+                    {
+                        int t = __shfl_up_sync(GD_FULL, incl, o);
+                        if (lane >= o)
+                            incl = max(incl, t);
+                    }
                     int excl = __shfl_up_sync(GD_FULL, incl, 1);
                     if (lane == 0)
                         excl = INT_MIN;
@@ -567,7 +559,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 bool good = p < width && k >= low && k <= hgh;
                 if (good)
                 {
-                    const int v = R.V[cur][k & RM];
+                    const int v = ch == 0 ? c0 : R.V[cur][k & RM];
                     good = FWD ? (v >= n) : (v <= n);
                 }
                 unsigned gm = __ballot_sync(GD_FULL, good);
