@@ -182,21 +182,38 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ ke
     counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// Shared memory of one scatter tile: the tile's items re-ordered by digit (stable), the
+// per-warp digit counts, the tile's digit starts and its global digit offsets.
+template <typename K>
+struct RsTile
+{
+    K key[RS_TILE];
+    uint32_t val[RS_TILE];
+    uint32_t wcnt[RS_WARPS][256];
+    uint32_t lstart[256];
+    uint32_t toff[256];
+};
+
+// Ranks every item of the tile (warps own contiguous sub-tiles, rounds walk them in order,
+// match-any groups within a round: stable), places it in a digit-sorted copy of the tile in
+// shared memory, and then writes the copy out in tile order: items of one digit leave as a
+// contiguous run, so the global writes coalesce.
 template <typename K>
 __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                           K* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
                                                           int shift, const uint32_t* __restrict__ offs, int ntiles)
 {
-    __shared__ uint32_t wcnt[RS_WARPS][256];
-    __shared__ uint32_t toff[256];
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    RsTile<K>& S = *reinterpret_cast<RsTile<K>*>(rs_smem);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int i = 0; i < RS_WARPS; i++)
-        wcnt[i][threadIdx.x] = 0;
-    toff[threadIdx.x] = offs[(int64_t)threadIdx.x * ntiles + blockIdx.x];
+        S.wcnt[i][threadIdx.x] = 0;
+    S.toff[threadIdx.x] = offs[(int64_t)threadIdx.x * ntiles + blockIdx.x];
     __syncthreads();
 
-    int64_t base = (int64_t)blockIdx.x * RS_TILE + (int64_t)w * (RS_ROUNDS * 32);
+    const int64_t tbase = (int64_t)blockIdx.x * RS_TILE;
+    const int64_t base = tbase + (int64_t)w * (RS_ROUNDS * 32);
     K key[RS_ROUNDS];
     uint32_t val[RS_ROUNDS];
     uint32_t rank[RS_ROUNDS];
@@ -214,23 +231,42 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
             d = (unsigned)(key[r] >> shift) & 255u;
         }
         unsigned peers = __match_any_sync(GD_FULL, d);
-        unsigned c = valid ? wcnt[w][d] : 0;
+        unsigned c = valid ? S.wcnt[w][d] : 0;
         rank[r] = c + __popc(peers & lt);
         __syncwarp();
         if (valid && (peers & lt) == 0)
-            wcnt[w][d] = c + __popc(peers);
+            S.wcnt[w][d] = c + __popc(peers);
         __syncwarp();
     }
     __syncthreads();
+    // per digit: warp offsets within the digit's run, and the run's length
+    uint32_t tot = 0;
+#pragma unroll
+    for (int i = 0; i < RS_WARPS; i++)
     {
-        uint32_t run = 0;
+        uint32_t t = S.wcnt[i][threadIdx.x];
+        S.wcnt[i][threadIdx.x] = tot;
+        tot += t;
+    }
+    // exclusive scan of the run lengths over the 256 digits (one per thread)
+    {
+        uint32_t x = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            uint32_t t = __shfl_up_sync(GD_FULL, x, o);
+            if (lane >= o)
+                x += t;
+        }
+        __shared__ uint32_t wsum[RS_WARPS];
+        if (lane == 31)
+            wsum[w] = x;
+        __syncthreads();
+        uint32_t wo = 0;
 #pragma unroll
         for (int i = 0; i < RS_WARPS; i++)
-        {
-            uint32_t t = wcnt[i][threadIdx.x];
-            wcnt[i][threadIdx.x] = run;
-            run += t;
-        }
+            wo += i < w ? wsum[i] : 0;
+        S.lstart[threadIdx.x] = wo + x - tot;
     }
     __syncthreads();
 #pragma unroll
@@ -240,10 +276,20 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
         if (idx < n)
         {
             unsigned d = (unsigned)(key[r] >> shift) & 255u;
-            uint32_t dest = toff[d] + wcnt[w][d] + rank[r];
-            kout[dest] = key[r];
-            vout[dest] = val[r];
+            uint32_t pos = S.lstart[d] + S.wcnt[w][d] + rank[r];
+            S.key[pos] = key[r];
+            S.val[pos] = val[r];
         }
+    }
+    __syncthreads();
+    const int tn = (int)min((int64_t)RS_TILE, n - tbase);
+    for (int i = threadIdx.x; i < tn; i += RS_THREADS)
+    {
+        K k = S.key[i];
+        unsigned d = (unsigned)(k >> shift) & 255u;
+        uint32_t dest = S.toff[d] + (uint32_t)i - S.lstart[d];
+        kout[dest] = k;
+        vout[dest] = S.val[i];
     }
 }
 
@@ -260,6 +306,13 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
         return -1;
     }
     int ntiles = (int)tiles64;
+    static bool smem_set = false;
+    if (!smem_set)
+    {
+        GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(RsTile<K>)));
+        smem_set = true;
+    }
     int64_t ncnt = (int64_t)ntiles * 256;
     uint32_t* counts = (uint32_t*)scratch;
     void* sscr = (void*)(((uintptr_t)(counts + ncnt) + 255) & ~(uintptr_t)255);
@@ -274,7 +327,7 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
         GD_LAUNCHED(1);
         if (exclusive_scan<uint32_t>(counts, counts, ncnt, (uint32_t*)nullptr, sscr, s))
             return -1;
-        k_rs_scatter<K><<<ntiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, b, counts, ntiles);
+        k_rs_scatter<K><<<ntiles, RS_THREADS, sizeof(RsTile<K>), s>>>(kin, vin, kout, vout, n, b, counts, ntiles);
         GD_LAUNCHED(1);
         cur ^= 1;
     }

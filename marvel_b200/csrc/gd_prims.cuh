@@ -5,7 +5,8 @@
 // but restructured for the GPU: per pass one kernel builds per-tile digit histograms,
 // one exclusive scan turns them into tile offsets (digit-major), and one kernel ranks
 // every item inside its tile with warp match-any groups (stable: warps own contiguous
-// sub-tiles, rounds walk them in order) and scatters it.
+// sub-tiles, rounds walk them in order), re-orders the tile by digit in shared memory and
+// writes each digit's items out as one contiguous run (coalesced scatter).
 #pragma once
 #include "gd_common.cuh"
 
