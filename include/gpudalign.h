@@ -111,6 +111,12 @@ int64_t gd_get_hits(gd_context* ctx, int32_t* rows4, int64_t cap);
 int64_t gd_num_overlaps(gd_context* ctx, int64_t* trace_bytes);
 int64_t gd_sort_overlaps(gd_context* ctx, int64_t* trace_bytes);
 int64_t gd_get_overlaps(gd_context* ctx, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap);
+
+/* LAsort (dalign/LAsort.c:65-90, 139-256) of one .las file on the device: writes out_path
+ * with the records of in_path ordered by (aread, bread, abpos) -- ties, which the
+ * reference's qsort leaves unordered, by (aepos, bbpos) and then file order -- each record's
+ * bytes (trace and pad word included) unchanged.  Returns the number of records. */
+int64_t gd_las_sort(gd_context* ctx, const char* in_path, const char* out_path);
 int gd_write_overlap_buffer(gd_context* ctx, int run_id, const char* ablock, const char* bblock, int last_read);
 int gd_reset_overlap_buffer(gd_context* ctx);
 

@@ -60,7 +60,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
-           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps"]
+           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -94,6 +94,8 @@ def lib():
     L.gd_get_overlaps.restype = C.c_int64
     L.gd_sort_overlaps.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.gd_sort_overlaps.restype = C.c_int64
+    L.gd_las_sort.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
+    L.gd_las_sort.restype = C.c_int64
     L.gd_write_overlap_buffer.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
     L.gd_reset_overlap_buffer.argtypes = [C.c_void_p]
     L.gd_get_stats.argtypes = [C.c_void_p, C.POINTER(GdStats)]
@@ -268,6 +270,10 @@ class Context:
         _check(lib().gd_compute_trace_pts(self.h, aslot, bslot, cslot, recs.ctypes.data, trace.ctypes.data, recs.size,
                                           out.ctypes.data))
         return out[:recs.size]
+
+    def las_sort(self, in_path, out_path):
+        """LAsort of one .las file on the device; returns the number of records."""
+        return _check(lib().gd_las_sort(self.h, os.fsencode(in_path), os.fsencode(out_path)))
 
     def reset_overlap_buffer(self):
         _check(lib().gd_reset_overlap_buffer(self.h))

@@ -45,14 +45,14 @@ __global__ void k_ovl_extent(const OutRec* __restrict__ r, uint64_t n, unsigned*
     }
 }
 
-__global__ void k_ovl_key_lo(const OutRec* __restrict__ r, uint64_t n, int pbits, uint64_t* __restrict__ key,
-                             uint32_t* __restrict__ val)
+__global__ void k_ovl_key_lo(const OutRec* __restrict__ r, uint64_t n, int pbits, int with_comp,
+                             uint64_t* __restrict__ key, uint32_t* __restrict__ val)
 {
     uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
     if (i >= n)
         return;
     const OutRec& o = r[i];
-    key[i] = ((uint64_t)(o.flags & 1) << (3 * pbits)) | ((uint64_t)o.abpos << (2 * pbits)) |
+    key[i] = ((uint64_t)(with_comp ? o.flags & 1 : 0) << (3 * pbits)) | ((uint64_t)o.abpos << (2 * pbits)) |
              ((uint64_t)o.aepos << pbits) | (uint64_t)o.bbpos;
     val[i] = (uint32_t)i;
 }
@@ -125,6 +125,80 @@ __global__ void k_ovl_gather(const OutRec* __restrict__ r, const uint8_t* __rest
     }
 }
 
+// .las record header: tlen, diffs, abpos, bbpos, aepos, bepos, flags, aread, bread, pad
+// (Overlap without its trace pointer, dalign/align.h:307-312), 40 little-endian bytes.  A
+// record starts at any even byte offset (1-byte trace points), so headers are read and
+// written byte by byte.
+__device__ __forceinline__ int32_t rd32(const uint8_t* q)
+{
+    return (int32_t)((uint32_t)q[0] | ((uint32_t)q[1] << 8) | ((uint32_t)q[2] << 16) | ((uint32_t)q[3] << 24));
+}
+
+__global__ void k_las_parse(const uint8_t* __restrict__ raw, const int64_t* __restrict__ off, uint64_t n,
+                            OutRec* __restrict__ rec)
+{
+    uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint8_t* h = raw + off[i];
+    OutRec o;
+    o.tlen = rd32(h);
+    o.diffs = rd32(h + 4);
+    o.abpos = rd32(h + 8);
+    o.bbpos = rd32(h + 12);
+    o.aepos = rd32(h + 16);
+    o.bepos = rd32(h + 20);
+    o.flags = (uint32_t)rd32(h + 24);
+    o.aread = rd32(h + 28);
+    o.bread = rd32(h + 32);
+    o.pad = rd32(h + 36);
+    o.toff = (uint64_t)off[i] + 40;
+    rec[i] = o;
+}
+
+// one warp per record: lanes write the 40 header bytes, then the trace bytes
+__global__ void k_las_emit(const OutRec* __restrict__ r, const uint8_t* __restrict__ tr,
+                           const uint32_t* __restrict__ perm, const uint64_t* __restrict__ toff, uint64_t n,
+                           int tbytes, uint8_t* __restrict__ out)
+{
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (w >= n)
+        return;
+    const OutRec o = r[perm[w]];
+    uint8_t* dst = out + 40 * w + toff[w];
+    const int32_t f[10] = {o.tlen, o.diffs, o.abpos, o.bbpos, o.aepos, o.bepos, (int32_t)o.flags, o.aread, o.bread,
+                           o.pad};
+    for (int j = lane; j < 40; j += 32)
+        dst[j] = (uint8_t)((uint32_t)f[j >> 2] >> (8 * (j & 3)));
+    const uint8_t* src = tr + o.toff;
+    const uint64_t len = (uint64_t)o.tlen * tbytes;
+    for (uint64_t j = lane; j < len; j += 32)
+        dst[40 + j] = src[j];
+}
+
+int launch_las_parse(const uint8_t* raw, const int64_t* off, uint64_t n, OutRec* rec, cudaStream_t s)
+{
+    if (n == 0)
+        return 0;
+    k_las_parse<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(raw, off, n, rec);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int launch_las_emit(const OutRec* r, const uint8_t* tr, const uint32_t* perm, const uint64_t* toff, uint64_t n,
+                    int tbytes, uint8_t* out, cudaStream_t s)
+{
+    if (n == 0)
+        return 0;
+    const uint64_t threads = n * 32;
+    k_las_emit<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(r, tr, perm, toff, n, tbytes, out);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 static inline unsigned grid256(uint64_t n)
 {
     return (unsigned)((n + 255) / 256);
@@ -150,11 +224,12 @@ int launch_ovl_extent(const OutRec* r, uint64_t n, unsigned* ext, cudaStream_t s
     return 0;
 }
 
-int launch_ovl_key_lo(const OutRec* r, uint64_t n, int pbits, uint64_t* key, uint32_t* val, cudaStream_t s)
+int launch_ovl_key_lo(const OutRec* r, uint64_t n, int pbits, int with_comp, uint64_t* key, uint32_t* val,
+                      cudaStream_t s)
 {
     if (n == 0)
         return 0;
-    k_ovl_key_lo<<<grid256(n), 256, 0, s>>>(r, n, pbits, key, val);
+    k_ovl_key_lo<<<grid256(n), 256, 0, s>>>(r, n, pbits, with_comp, key, val);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;

@@ -14,8 +14,10 @@ int launch_ovl_append(const OutRec* src, uint64_t n, uint64_t t0, OutRec* dst, c
 // coordinates (ext must hold {UINT_MAX, 0, 0} on entry)
 int launch_ovl_extent(const OutRec* r, uint64_t n, unsigned* ext, cudaStream_t s);
 
-// low sort key (orientation, abpos, aepos, bbpos) with pbits bits per position; val[i] = i
-int launch_ovl_key_lo(const OutRec* r, uint64_t n, int pbits, uint64_t* key, uint32_t* val, cudaStream_t s);
+// low sort key (orientation, abpos, aepos, bbpos) with pbits bits per position -- without
+// the orientation when with_comp is 0 (LAsort's key); val[i] = i
+int launch_ovl_key_lo(const OutRec* r, uint64_t n, int pbits, int with_comp, uint64_t* key, uint32_t* val,
+                      cudaStream_t s);
 
 // high sort key of r[perm[i]]: (dropped, aread - rmin, bread - rmin) with rbits per read id;
 // a record is dropped when only_identity and aread != bread; *nkept counts the others
@@ -28,5 +30,14 @@ int launch_ovl_len(const OutRec* r, const uint32_t* perm, uint64_t n, int tbytes
 // out[i] = r[perm[i]] with its trace moved to outtr + off[i] (toff = off[i]); first n records
 int launch_ovl_gather(const OutRec* r, const uint8_t* tr, const uint32_t* perm, const uint64_t* off, uint64_t n,
                       int tbytes, OutRec* out, uint8_t* outtr, cudaStream_t s);
+
+// .las records at byte offsets off[i] of raw (the 40-byte header of each) -> rec[i], with
+// toff = off[i] + 40 (its trace bytes in raw) and the header's pad word kept in pad
+int launch_las_parse(const uint8_t* raw, const int64_t* off, uint64_t n, OutRec* rec, cudaStream_t s);
+
+// the .las byte stream of r[perm[0..n)]: record i's 40-byte header (pad kept) at
+// out + 40 * i + toff[i], its trace bytes right after
+int launch_las_emit(const OutRec* r, const uint8_t* tr, const uint32_t* perm, const uint64_t* toff, uint64_t n,
+                    int tbytes, uint8_t* out, cudaStream_t s);
 
 }  // namespace gd

@@ -184,6 +184,7 @@ struct gd_context
     uint64_t acc_n = 0, acc_tb = 0, srt_n = 0, srt_tb = 0;
     bool srt_valid = false;
     HostBuf h_rec, h_tr;  // pinned staging for file writes
+    DevBuf las_raw, las_off, las_rec, las_out;  // gd_las_sort
     gd_stats stats;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
     // learned triage: model (on), per-group feature/outcome collection (collect)
@@ -621,22 +622,16 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
 // overlap sort + .las writing (Write_Overlap_Buffer, dalign/align.c:5786-6043)
 // ----------------------------------------------------------------------------------------
 
-// Write_Overlap_Buffer's sort (SORT_OVL, dalign/align.c:5786-5813) on the device: order
-// (aread, bread, orientation, abpos), ties by (aepos, bbpos) -- the reference's qsort leaves
-// ties unordered -- with -I's identity filter (only_identity) applied as a drop bit.
-static int sort_overlaps(gd_context* c)
+// The order of n records on the device: two stable radix sorts, by (orientation if
+// with_comp, abpos, aepos, bbpos) and then by (dropped, aread, bread).  Returns the
+// permutation (in oval0 or oval1) in *perm, the records kept (not dropped by the identity
+// filter; they come first) in *kept, and in olen the exclusive scan of their trace bytes
+// (olen[n] = total); *kbytes = trace bytes of the kept records.
+static int sort_perm(gd_context* c, const gd::OutRec* rec, uint64_t n, int with_comp, int only_identity, int tbytes,
+                     const uint32_t** perm_out, uint64_t* kept_out, uint64_t* kbytes_out)
 {
     using namespace gd;
-    if (c->srt_valid)
-        return 0;
     cudaStream_t s = c->s;
-    const uint64_t n = c->acc_n;
-    c->srt_n = c->srt_tb = 0;
-    if (n == 0)
-    {
-        c->srt_valid = true;
-        return 0;
-    }
     if (n > 0xffffffffull)
     {
         gd_set_error("%llu overlaps exceed the 32-bit sort index", (unsigned long long)n);
@@ -647,7 +642,6 @@ static int sort_overlaps(gd_context* c)
         ensure(c->scratch, std::max(radix_scratch_bytes((int64_t)n), scan_scratch_bytes<uint64_t>((int64_t)n))) ||
         ensure(c->misc, 256))
         return -1;
-    const OutRec* rec = P<OutRec>(c->acc_rec);
     unsigned* d_ext = P<unsigned>(c->misc) + 40;
     unsigned long long* d_kept = (unsigned long long*)(P<unsigned>(c->misc) + 44);
     uint64_t* d_total = (uint64_t*)(P<unsigned>(c->misc) + 46);
@@ -666,7 +660,7 @@ static int sort_overlaps(gd_context* c)
         gd_set_error("overlap sort keys need %d / %d bits", 3 * pbits + 1, 2 * rbits + 1);
         return -1;
     }
-    if (launch_ovl_key_lo(rec, n, pbits, P<uint64_t>(c->okey0), P<uint32_t>(c->oval0), s))
+    if (launch_ovl_key_lo(rec, n, pbits, with_comp, P<uint64_t>(c->okey0), P<uint32_t>(c->oval0), s))
         return -1;
     int w1 = radix_sort_pairs<uint64_t>(P<uint64_t>(c->okey0), P<uint32_t>(c->oval0), P<uint64_t>(c->okey1),
                                         P<uint32_t>(c->oval1), n, 0, 3 * pbits + 1, c->scratch.p, s);
@@ -676,13 +670,12 @@ static int sort_overlaps(gd_context* c)
     uint32_t* va = w1 ? P<uint32_t>(c->oval1) : P<uint32_t>(c->oval0);
     uint64_t* kb = w1 ? P<uint64_t>(c->okey0) : P<uint64_t>(c->okey1);
     uint32_t* vb = w1 ? P<uint32_t>(c->oval0) : P<uint32_t>(c->oval1);
-    if (launch_ovl_key_hi(rec, va, n, rbits, ext[0], c->only_identity, ka, d_kept, s))
+    if (launch_ovl_key_hi(rec, va, n, rbits, ext[0], only_identity, ka, d_kept, s))
         return -1;
     int w2 = radix_sort_pairs<uint64_t>(ka, va, kb, vb, n, 0, 2 * rbits + 1, c->scratch.p, s);
     if (w2 < 0)
         return -1;
     const uint32_t* perm = w2 ? vb : va;
-    const int tbytes = c->tspace <= 125 ? 1 : 2;
     uint64_t* off = P<uint64_t>(c->olen);
     if (launch_ovl_len(rec, perm, n, tbytes, off, s) ||
         exclusive_scan<uint64_t>(off, off, (int64_t)n, d_total, c->scratch.p, s))
@@ -693,12 +686,39 @@ static int sort_overlaps(gd_context* c)
     uint64_t kbytes = 0;
     GD_CUDA(cudaMemcpyAsync(&kbytes, kept < n ? off + kept : d_total, 8, cudaMemcpyDeviceToHost, s));
     GD_CUDA(cudaStreamSynchronize(s));
+    *perm_out = perm;
+    *kept_out = kept;
+    *kbytes_out = kbytes;
+    return 0;
+}
+
+// Write_Overlap_Buffer's sort (SORT_OVL, dalign/align.c:5786-5813) of the overlap buffer:
+// order (aread, bread, orientation, abpos), ties by (aepos, bbpos) -- the reference's qsort
+// leaves ties unordered -- with -I's identity filter (only_identity) applied as a drop bit;
+// the kept records and their traces are gathered into srt_rec / srt_tr.
+static int sort_overlaps(gd_context* c)
+{
+    using namespace gd;
+    if (c->srt_valid)
+        return 0;
+    const uint64_t n = c->acc_n;
+    c->srt_n = c->srt_tb = 0;
+    if (n == 0)
+    {
+        c->srt_valid = true;
+        return 0;
+    }
+    const int tbytes = c->tspace <= 125 ? 1 : 2;
+    const uint32_t* perm = nullptr;
+    uint64_t kept = 0, kbytes = 0;
+    if (sort_perm(c, P<OutRec>(c->acc_rec), n, 1, c->only_identity, tbytes, &perm, &kept, &kbytes))
+        return -1;
     if (ensure(c->srt_rec, kept * sizeof(OutRec)) || ensure(c->srt_tr, kbytes + 16))
         return -1;
-    if (launch_ovl_gather(rec, P<uint8_t>(c->acc_tr), perm, off, kept, tbytes, P<OutRec>(c->srt_rec),
-                          P<uint8_t>(c->srt_tr), s))
+    if (launch_ovl_gather(P<OutRec>(c->acc_rec), P<uint8_t>(c->acc_tr), perm, P<uint64_t>(c->olen), kept, tbytes,
+                          P<OutRec>(c->srt_rec), P<uint8_t>(c->srt_tr), c->s))
         return -1;
-    GD_CUDA(cudaStreamSynchronize(s));
+    GD_CUDA(cudaStreamSynchronize(c->s));
     c->srt_n = kept;
     c->srt_tb = kbytes;
     c->srt_valid = true;
@@ -823,7 +843,8 @@ void gd_destroy(gd_context* c)
                       &c->status, &c->queue,  &c->tri_params, &c->tri_feat, &c->tri_prob, &c->tri_skip,
                       &c->tri_gstat, &c->tri_misc, &c->tri_x, &c->tri_y, &c->tri_perm, &c->tri_grad, &c->tri_m,
                       &c->tri_v, &c->tri_loss, &c->tri_w, &c->acc_rec, &c->acc_tr, &c->srt_rec, &c->srt_tr,
-                      &c->okey0, &c->okey1, &c->oval0, &c->oval1, &c->olen};
+                      &c->okey0, &c->okey1, &c->oval0, &c->oval1, &c->olen, &c->las_raw, &c->las_off,
+                      &c->las_rec, &c->las_out};
     for (DevBuf* b : bufs)
         release(*b);
     for (HostBuf* h : {&c->h_rec, &c->h_tr})
@@ -1098,6 +1119,106 @@ int64_t gd_sort_overlaps(gd_context* c, int64_t* trace_bytes)
     if (trace_bytes)
         *trace_bytes = (int64_t)c->srt_tb;
     return (int64_t)c->srt_n;
+}
+
+int64_t gd_las_sort(gd_context* c, const char* in_path, const char* out_path)
+{
+    using namespace gd;
+    FILE* f = fopen(in_path, "rb");
+    if (!f)
+    {
+        gd_set_error("Cannot open %s for reading", in_path);
+        return -1;
+    }
+    int64_t novl = 0;
+    int32_t tspace = 0;
+    fseek(f, 0, SEEK_END);
+    long fsize = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (fsize < 12 || fread(&novl, 8, 1, f) != 1 || fread(&tspace, 4, 1, f) != 1 || novl < 0 || tspace <= 0)
+    {
+        fclose(f);
+        gd_set_error("%s: not a .las file", in_path);
+        return -1;
+    }
+    const uint64_t body = (uint64_t)fsize - 12;
+    if (ensure_host(c->h_tr, body + 16) || ensure_host(c->h_rec, body + 16))
+    {
+        fclose(f);
+        return -1;
+    }
+    if (body && fread(c->h_tr.p, 1, body, f) != body)
+    {
+        fclose(f);
+        gd_set_error("%s: short read", in_path);
+        return -1;
+    }
+    fclose(f);
+    // record offsets: records are variable length (LAsort.c:209-218), a sequential walk
+    const int tbytes = tspace <= 125 ? 1 : 2;  // TRACE_XOVR
+    if ((uint64_t)novl > body / 40)
+    {
+        gd_set_error("%s: header claims %lld records, the file holds at most %llu", in_path, (long long)novl,
+                     (unsigned long long)(body / 40));
+        return -1;
+    }
+    const uint8_t* raw = (const uint8_t*)c->h_tr.p;
+    std::vector<int64_t> off((size_t)novl);
+    uint64_t o = 0;
+    for (int64_t i = 0; i < novl; i++)
+    {
+        int32_t tlen;
+        if (o + 40 > body)
+        {
+            gd_set_error("%s: record %lld runs past the end of the file", in_path, (long long)i);
+            return -1;
+        }
+        memcpy(&tlen, raw + o, 4);
+        if (tlen < 0 || o + 40 + (uint64_t)tlen * tbytes > body)
+        {
+            gd_set_error("%s: record %lld has a bad trace length %d", in_path, (long long)i, tlen);
+            return -1;
+        }
+        off[(size_t)i] = (int64_t)o;
+        o += 40 + (uint64_t)tlen * tbytes;
+    }
+    const uint64_t used = o;
+    cudaStream_t s = c->s;
+    if (ensure(c->las_raw, used + 16) || ensure(c->las_off, (size_t)novl * 8 + 8) ||
+        ensure(c->las_rec, (size_t)novl * sizeof(OutRec) + 16) || ensure(c->las_out, used + 16))
+        return -1;
+    if (used)
+        GD_CUDA(cudaMemcpyAsync(c->las_raw.p, raw, used, cudaMemcpyHostToDevice, s));
+    if (novl)
+        GD_CUDA(cudaMemcpyAsync(c->las_off.p, off.data(), (size_t)novl * 8, cudaMemcpyHostToDevice, s));
+    uint64_t outbytes = 0;
+    if (novl)
+    {
+        const uint32_t* perm = nullptr;
+        uint64_t kept = 0, kbytes = 0;
+        if (launch_las_parse(P<uint8_t>(c->las_raw), P<int64_t>(c->las_off), (uint64_t)novl, P<OutRec>(c->las_rec), s) ||
+            sort_perm(c, P<OutRec>(c->las_rec), (uint64_t)novl, 0, 0, tbytes, &perm, &kept, &kbytes) ||
+            launch_las_emit(P<OutRec>(c->las_rec), P<uint8_t>(c->las_raw), perm, P<uint64_t>(c->olen), kept, tbytes,
+                            P<uint8_t>(c->las_out), s))
+            return -1;
+        outbytes = 40 * kept + kbytes;
+        GD_CUDA(cudaMemcpyAsync(c->h_rec.p, c->las_out.p, outbytes, cudaMemcpyDeviceToHost, s));
+    }
+    GD_CUDA(cudaStreamSynchronize(s));
+    FILE* g = fopen(out_path, "wb");
+    if (!g)
+    {
+        gd_set_error("Cannot open %s for writing", out_path);
+        return -1;
+    }
+    bool ok = fwrite(&novl, 8, 1, g) == 1 && fwrite(&tspace, 4, 1, g) == 1 &&
+              (outbytes == 0 || fwrite(c->h_rec.p, 1, outbytes, g) == outbytes);
+    if (fclose(g) || !ok)
+    {
+        gd_set_error("write to %s failed", out_path);
+        return -1;
+    }
+    return novl;
 }
 
 int64_t gd_get_overlaps(gd_context* c, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap)

@@ -261,17 +261,19 @@ def read_las(path):
     return tspace, recs, traces
 
 
-def las_equal(path_a, path_b):
-    """Record-level comparison that ignores the 4 uninitialised pad bytes and accepts any
-    order among records whose (aread, bread, COMP, abpos) sort keys tie
-    (dalign/align.c:5786-5813).  Returns (equal, message)."""
+def las_equal(path_a, path_b, key="overlap", pad=False):
+    """Record-level comparison of two .las files that accepts any order among records whose
+    sort keys tie: (aread, bread, COMP, abpos) for key="overlap" (Write_Overlap_Buffer,
+    dalign/align.c:5786-5813), (aread, bread, abpos) for key="lasort" (dalign/LAsort.c:65-90).
+    The 4 pad bytes of each record (uninitialised in daligner's output) are ignored unless
+    pad=True.  Returns (equal, message)."""
     ta, ra, xa = read_las(path_a)
     tb, rb, xb = read_las(path_b)
     if ta != tb:
         return False, f"tspace {ta} != {tb}"
     if ra.size != rb.size:
         return False, f"novl {ra.size} != {rb.size}"
-    fields = [f for f in LAS_REC_DTYPE.names if f != "pad"]
+    fields = [f for f in LAS_REC_DTYPE.names if pad or f != "pad"]
 
     def canon(recs, traces):
         keys = []
@@ -285,8 +287,10 @@ def las_equal(path_a, path_b):
         return True, "identical"
     if sorted(ka) == sorted(kb):
         # same multiset: allowed only if differences are among tied sort keys
+        ia, ib, fl, ab = (fields.index(f) for f in ("aread", "bread", "flags", "abpos"))
+
         def sk(k):
-            return (k[7], k[8], k[6] & 1, k[2])
+            return (k[ia], k[ib], k[fl] & 1, k[ab]) if key == "overlap" else (k[ia], k[ib], k[ab])
         for x, y in zip(ka, kb):
             if sk(x) != sk(y):
                 return False, "same records, different order"
