@@ -44,25 +44,7 @@ CPU_SAMPLE_SCALE = 0.2   # CPU baseline: the same genome/read model on a 1/5-siz
 
 def make_db(workload, seed_offset=0, scale=1.0):
     """Generates (or reuses) the DB of a workload; returns the path of block 1."""
-    w = synth.WORKLOADS[workload]
-    import dataclasses
-    w = dataclasses.replace(w, seed=w.seed + 1000 * seed_offset)
-    if scale != 1.0:
-        g = w.genome
-        reps = tuple((max(1, int(round(c * scale))), u, d) for c, u, d in g.repeats)
-        w = dataclasses.replace(w, genome=dataclasses.replace(g, length=int(g.length * scale), repeats=reps))
-    d = os.path.join(CACHE, f"{workload}_s{w.seed}_x{scale}")
-    root = os.path.join(d, "W")
-    if not os.path.exists(root + ".db"):
-        reads, _ = synth.generate(w)
-        tmp = d + f".tmp{os.getpid()}"
-        os.makedirs(tmp, exist_ok=True)
-        dazzdb.write_db(os.path.join(tmp, "W"), reads, 100000)   # a single block
-        try:
-            os.rename(tmp, d)
-        except OSError:   # another process finished first
-            pass
-    return root + ".1"
+    return synth.cached_db(workload, seed_offset, scale, CACHE)
 
 
 class ClockSampler:
@@ -207,6 +189,37 @@ def run_gpu(args):
             d2h = r.size * mb.OVL_DTYPE.itemsize + tr.size
     barrier()
     e_ms_max, = reduce([sum(etimes)], torch.distributed.ReduceOp.MAX if ws > 1 else None)
+
+    # ---- learned triage (beside the exact path): the shipped model, trained on another genome
+    tri = None
+    from marvel_b200 import triage as mtri
+    if args.triage and os.path.exists(mtri.DEFAULT_MODEL):
+        model = mtri.TriageModel.load(mtri.DEFAULT_MODEL)
+        ctx.triage_set_model(model.params, model.threshold)
+        ttimes, trecs, tskip, tgroups = [], 0, 0, 0
+        for i in range(1 + args.steps):
+            ctx.reset_overlap_buffer()
+            ctx.timer_mark(0)
+            mb.run_loaded(ctx, True)
+            ctx.sort_overlaps()
+            ctx.timer_mark(1)
+            if i >= 1:
+                ttimes.append(ctx.timer_elapsed_ms())
+                tst = ctx.stats()
+                trecs += tst["records"]
+                tskip += sum(tst["skipped"])
+                tgroups += sum(tst["groups"])
+        ctx.triage_set_model(None)
+        barrier()
+        t_ms_max, = reduce([sum(ttimes)], torch.distributed.ReduceOp.MAX if ws > 1 else None)
+        trecs_all, = reduce([float(trecs)], torch.distributed.ReduceOp.SUM if ws > 1 else None)
+        tri = {"value": round(trecs_all / (t_ms_max / 1e3), 1), "unit": "overlaps/s",
+               "ms_per_step": round(t_ms_max / args.steps, 3),
+               "record_recall": round(trecs / recs, 5) if recs else None,
+               "groups_skipped": round(tskip / tgroups, 4) if tgroups else None,
+               "model": os.path.relpath(mtri.DEFAULT_MODEL, ROOT) + " (trained on the GPU on another genome of "
+                        "this workload's model, seed offset 1)",
+               "note": "records are a subset of the exact path's; recall < 1, so not the headline"}
     erecs_all, = reduce([float(erecs)], torch.distributed.ReduceOp.SUM if ws > 1 else None)
     e2e = erecs_all / (e_ms_max / 1e3)
 
@@ -262,6 +275,7 @@ def run_gpu(args):
             "e2e": {"value": round(e2e, 1), "unit": "overlaps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
+            "triage": tri,
             "clocks": clocks,
         }
         if args.cpu_baseline:
@@ -378,6 +392,8 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="cfg2", choices=sorted(synth.WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-triage", dest="triage", action="store_false",
+                    help="skip the learned-triage measurement (reported beside the exact path)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

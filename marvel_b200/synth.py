@@ -210,6 +210,9 @@ WORKLOADS = {
                             ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=13),
     "small": Workload("small", GenomeModel(200_000, repeats=((6, 3000, 0.015),)),
                       ReadModel(15, 6000, 3000, 1000, 20000, **PACBIO), seed=12),
+    # reads of 30-150 kbp: a-positions beyond the 50,000-bp panels of the seed scan
+    "long": Workload("long", GenomeModel(250_000, repeats=((4, 3000, 0.01),)),
+                     ReadModel(6, 70000, 20000, 30000, 150000, p_ins=0.03, p_del=0.05, p_sub=0.02), seed=14),
 }
 
 
@@ -233,3 +236,31 @@ def write_fasta(path, reads, width=0):
             f.write(f">sim/{i + 1}/0_{r.size}\n")
             f.write(letters[r].tobytes().decode())
             f.write("\n")
+
+
+def cached_db(workload: str, seed_offset: int = 0, scale: float = 1.0, cache: str | None = None):
+    """Writes (once) a one-block DB of a workload -- seed shifted by 1000 * seed_offset, genome
+    and repeat counts scaled by scale -- under cache and returns the path of block 1."""
+    import os
+    import tempfile
+    from . import dazzdb
+    if cache is None:
+        cache = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
+    w = WORKLOADS[workload]
+    w = dataclasses.replace(w, seed=w.seed + 1000 * seed_offset)
+    if scale != 1.0:
+        g = w.genome
+        reps = tuple((max(1, int(round(c * scale))), u, d) for c, u, d in g.repeats)
+        w = dataclasses.replace(w, genome=dataclasses.replace(g, length=int(g.length * scale), repeats=reps))
+    d = os.path.join(cache, f"{workload}_s{w.seed}_x{scale}")
+    root = os.path.join(d, "W")
+    if not os.path.exists(root + ".db"):
+        reads, _ = generate(w)
+        tmp = d + f".tmp{os.getpid()}"
+        os.makedirs(tmp, exist_ok=True)
+        dazzdb.write_db(os.path.join(tmp, "W"), reads, 100000)   # a single block
+        try:
+            os.rename(tmp, d)
+        except OSError:   # another process finished first
+            pass
+    return root + ".1"

@@ -21,11 +21,15 @@ FP32 accumulation and FP32 optimizer state (libgpudalign.so, gd_triage.cu).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
 
 from . import TRI_NF, TRI_NPARAM, Context, _check, lib, run_loaded
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_MODEL = os.path.join(HERE, "models", "triage_cfg2.npz")
 
 
 @dataclass
@@ -129,3 +133,53 @@ def fit(ctx: Context, feat, records, *, recall=0.999, holdout=0.25, seed=1, **kw
     thr = calibrate(pc, records[cal], recall)
     info = {"losses": losses.tolist(), "calibration": evaluate(pc, records[cal], np.ones(len(cal)), thr)}
     return TriageModel(params, thr, recall), info
+
+
+def train_on_workload(workload: str, seed_offset: int, out: str, recall: float = 0.999, epochs: int = 25,
+                      scale: float = 1.0):
+    """Collects the groups of one synthetic block compared with itself (bench's generator,
+    another seed than the benchmark's), trains on the device and writes the model file."""
+    import json
+    import time
+
+    from . import daligner_block, dazzdb, synth
+
+    A = dazzdb.open_block(synth.cached_db(workload, seed_offset, scale))
+    ctx = Context()
+    ctx.triage_reset()
+    ctx.triage_collect(True)
+    daligner_block(ctx, A)
+    ctx.triage_collect(False)
+    feat, rec, cells = ctx.triage_groups()
+    t0 = time.perf_counter()
+    model, info = fit(ctx, feat, rec, recall=recall, epochs=epochs)
+    info["train_s"] = round(time.perf_counter() - t0, 2)
+    info["groups"] = int(len(rec))
+    info["positive_groups"] = int((rec > 0).sum())
+    info["trained_on"] = f"{workload} genome, seed offset {seed_offset}, scale {scale}"
+    ctx.close()
+    model.save(out)
+    with open(os.path.splitext(out)[0] + ".json", "w") as f:
+        json.dump({k: v for k, v in info.items() if k != "losses"} | {"final_loss": info["losses"][-1]}, f, indent=1)
+    return model, info
+
+
+def main(argv=None):
+    """python -m marvel_b200.triage train [--workload cfg2] [--seed-offset 1] [--out PATH]"""
+    import argparse
+    p = argparse.ArgumentParser(prog="marvel_b200.triage")
+    p.add_argument("cmd", choices=["train"])
+    p.add_argument("--workload", default="cfg2")
+    p.add_argument("--seed-offset", type=int, default=1)
+    p.add_argument("--scale", type=float, default=1.0)
+    p.add_argument("--recall", type=float, default=0.999)
+    p.add_argument("--epochs", type=int, default=25)
+    p.add_argument("--out", default=DEFAULT_MODEL)
+    a = p.parse_args(argv)
+    model, info = train_on_workload(a.workload, a.seed_offset, a.out, a.recall, a.epochs, a.scale)
+    print(f"threshold {model.threshold:.4g}; calibration {info['calibration']}; {info['train_s']} s")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

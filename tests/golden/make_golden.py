@@ -30,6 +30,8 @@ CASES = {
     "self_identity": ("tiny", 0.5, 200, ["-I", "-k12", "-w6", "-h30", "-e.70", "-l500", "-s100"], ["G.1", "G.1"]),
     "self_asym_lowmem": ("tiny", 0.7, 200, ["-A", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100", "-M0"],
                          ["G.1", "G.1"]),
+    # reads of 30-150 kbp: the seed scan's 50,000-bp panels (dalign/filter.c:1717-1745)
+    "self_long_panels": ("long", 1.0, 200, ["-k14", "-w6", "-h35", "-e.75", "-l1000", "-s100"], ["G.1", "G.1"]),
     # tandem repeats masked by the reference DBdust track (-mdust), blocks of ~0.4 Mbp
     "pair_dust": ("tiny_tandem", 1.0, 0.4, ["-mdust", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100"],
                   ["G.1", "G.2"]),
