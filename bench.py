@@ -40,6 +40,9 @@ from marvel_b200 import dazzdb, synth  # noqa: E402
 PARAMS = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=32)
 CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
 CPU_SAMPLE_SCALE = 0.2   # CPU baseline: the same genome/read model on a 1/5-size genome
+# k_align_pairs DRAM bytes (read + write) per wave cell, from the ncu capture of the cfg1
+# N-orientation launch: 121.3 MB over 282 M cells
+ALIGN_DRAM_BYTES_PER_CELL = 121.3e6 / 282.0e6
 
 
 def make_db(workload, seed_offset=0, scale=1.0):
@@ -265,7 +268,10 @@ def run_gpu(args):
             "gcups": round(gcups, 2) if gcups else None,
             "roofline": {"bound": "issue", "kernel": "k_align_pairs", "achieved": round(achieved, 3),
                          "peak": round(issue_peak, 2), "unit": "T int lane-ops/s",
-                         "frac": round(achieved / issue_peak, 4), "traffic": None,
+                         "frac": round(achieved / issue_peak, 4),
+                         "traffic": int(ALIGN_DRAM_BYTES_PER_CELL * cells / 2),
+                         "traffic_source": "bytes per launch: dram read+write per wave cell of the cfg1 ncu capture "
+                                           "(profiles/k_align_pairs_cfg1.md) x this launch's cells",
                          "peak_source": "derived: 148 SM x 128 lanes/clk x median SM clock under load"},
             "roofline_filter": {"bound": "hbm", "kernel": "k-mer index (extract + 4 LSD passes)",
                                 "achieved": round(idx_bytes / (idx_ms / 1e3) / 1e9, 1),
