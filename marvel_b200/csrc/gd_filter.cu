@@ -143,6 +143,35 @@ __device__ __forceinline__ int64_t upper_code(const K* a, int64_t n, K x)
     return l;
 }
 
+// the same searches restricted to [l, r), for keys known to lie in that window
+template <typename K>
+__device__ __forceinline__ int64_t lower_code_in(const K* a, int64_t l, int64_t r, K x)
+{
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] < x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
+template <typename K>
+__device__ __forceinline__ int64_t upper_code_in(const K* a, int64_t l, int64_t r, K x)
+{
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] <= x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(FT) k_suppress(const K* __restrict__ code, int64_t n, int t, uint32_t* keep)
 {
@@ -220,6 +249,17 @@ __global__ void __launch_bounds__(FT) k_pair_count(const K* __restrict__ acode, 
                                                   MergeArgs m, uint32_t* jb_out, uint64_t* cnt_out,
                                                   unsigned long long* ctrun)
 {
+    // A is sorted: the block's codes span [acode[t0], acode[t1]], so every B range it needs
+    // lies in [lower(acode[t0]), upper(acode[t1])) -- two full searches per block, then
+    // short ones per entry
+    __shared__ int64_t s_lo, s_hi;
+    const int64_t t0 = (int64_t)blockIdx.x * FT;
+    const int64_t t1 = min(t0 + FT, m.na) - 1;
+    if (threadIdx.x == 0)
+        s_lo = lower_code(bcode, m.nb, acode[t0]);
+    else if (threadIdx.x == 32)
+        s_hi = upper_code(bcode, m.nb, acode[t1]);
+    __syncthreads();
     int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
     bool act = i < m.na;
     uint64_t n = 0;
@@ -227,10 +267,11 @@ __global__ void __launch_bounds__(FT) k_pair_count(const K* __restrict__ acode, 
     if (act)
     {
         K c = acode[i];
-        int64_t jb = lower_code(bcode, m.nb, c);
+        const int64_t lo = s_lo, hi = s_hi;
+        int64_t jb = lower_code_in(bcode, lo, hi, c);
         int64_t je = jb;
-        if (jb < m.nb && bcode[jb] == c)
-            je = upper_code(bcode, m.nb, c);
+        if (jb < hi && bcode[jb] == c)
+            je = upper_code_in(bcode, jb, hi, c);
         int ar = aread[i], ap = arpos[i];
         int64_t e = je;
         if (m.self)

@@ -218,18 +218,23 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
     uint32_t val[RS_ROUNDS];
     uint32_t rank[RS_ROUNDS];
     const unsigned lt = lanemask_lt();
+    // all of the sub-tile's loads in flight before the ranking
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; r++)
+    {
+        int64_t idx = base + r * 32 + lane;
+        if (idx < n)
+        {
+            key[r] = kin[idx];
+            val[r] = vin[idx];
+        }
+    }
 #pragma unroll
     for (int r = 0; r < RS_ROUNDS; r++)
     {
         int64_t idx = base + r * 32 + lane;
         bool valid = idx < n;
-        unsigned d = 256;
-        if (valid)
-        {
-            key[r] = kin[idx];
-            val[r] = vin[idx];
-            d = (unsigned)(key[r] >> shift) & 255u;
-        }
+        unsigned d = valid ? (unsigned)(key[r] >> shift) & 255u : 256u;
         unsigned peers = __match_any_sync(GD_FULL, d);
         unsigned c = valid ? S.wcnt[w][d] : 0;
         rank[r] = c + __popc(peers & lt);
