@@ -323,12 +323,13 @@ def ref_threads():
     return j
 
 
-def run_reference_once(path, threads):
-    """The reference daligner on a block against itself; returns (records, seconds)."""
+def run_reference_once(path, threads, h=35):
+    """The reference daligner on a block against itself; returns (records, seconds).  With
+    h=100000 no pair group reaches the aligner: the filter alone."""
     b = ref_binary()
     d = os.path.dirname(path)
     name = os.path.basename(path)
-    cmd = [b, f"-j{threads}", "-M32", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100", name, name]
+    cmd = [b, f"-j{threads}", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
     t = time.perf_counter()
     subprocess.run(cmd, cwd=d, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     dt = time.perf_counter() - t
@@ -338,14 +339,27 @@ def run_reference_once(path, threads):
     return n, dt
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(args):
     path = make_db(args.workload, scale=CPU_SAMPLE_SCALE)
     if ref_binary():
         j = ref_threads()
         n, dt = run_reference_once(path, j)
+        _, df = run_reference_once(path, j, h=100000)
         return {"value": round(n / dt, 1), "unit": "overlaps/s", "cores": j, "kind": "reference",
                 "sample": f"reference daligner -j{j} on the {args.workload} model with a {CPU_SAMPLE_SCALE}x genome "
-                          f"({n} overlaps, {dt:.1f} s wall)"}
+                          f"({n} overlaps, {dt:.1f} s wall)",
+                "filter_only_s": round(df, 2), "cpu_model": cpu_model()}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     A = dazzdb.open_block(path)
