@@ -112,6 +112,15 @@ int64_t gd_num_overlaps(gd_context* ctx, int64_t* trace_bytes);
 int64_t gd_sort_overlaps(gd_context* ctx, int64_t* trace_bytes);
 int64_t gd_get_overlaps(gd_context* ctx, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap);
 
+/* DBdust (db/DBdust.c:92-530) on the device for the block in slot: low-complexity
+ * intervals of every read with scan window `window` (-w, 3..128), threshold `thresh` (-t),
+ * intervals of at least `mflag` bases (-m), `biased` (-b, weights from freq, the DB's base
+ * frequencies).  Returns the number of ints of interval data (pairs begin, end); when
+ * anno (nreads + 1 int64) and data (cap int32) are given and cap suffices, fills them in
+ * the .dust.anno / .dust.data layout: anno[r] = byte offset of read r's pairs in data. */
+int64_t gd_dust(gd_context* ctx, int slot, int window, double thresh, int mflag, int biased, const float freq[4],
+                int64_t* anno, int32_t* data, int64_t cap);
+
 /* LAsort (dalign/LAsort.c:65-90, 139-256) of one .las file on the device: writes out_path
  * with the records of in_path ordered by (aread, bread, abpos) -- ties, which the
  * reference's qsort leaves unordered, by (aepos, bbpos) and then file order -- each record's

@@ -60,7 +60,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
-           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort"]
+           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -96,6 +96,9 @@ def lib():
     L.gd_sort_overlaps.restype = C.c_int64
     L.gd_las_sort.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
     L.gd_las_sort.restype = C.c_int64
+    L.gd_dust.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_float),
+                          C.c_void_p, C.c_void_p, C.c_int64]
+    L.gd_dust.restype = C.c_int64
     L.gd_write_overlap_buffer.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
     L.gd_reset_overlap_buffer.argtypes = [C.c_void_p]
     L.gd_get_stats.argtypes = [C.c_void_p, C.POINTER(GdStats)]
@@ -177,6 +180,7 @@ class Context:
         if not self.h:
             raise GpuError(L.gd_last_error().decode())
         self.tspace = 100
+        self._nreads = {}
 
     def close(self):
         if self.h:
@@ -204,6 +208,7 @@ class Context:
     def load_block(self, slot, blk):
         r = _BlockRef(blk)
         _check(lib().gd_load_block(self.h, slot, C.byref(r.s)))
+        self._nreads[slot] = blk.nreads
 
     def complement_block(self, src, dst):
         _check(lib().gd_complement_block(self.h, src, dst))
@@ -270,6 +275,19 @@ class Context:
         _check(lib().gd_compute_trace_pts(self.h, aslot, bslot, cslot, recs.ctypes.data, trace.ctypes.data, recs.size,
                                           out.ctypes.data))
         return out[:recs.size]
+
+    def dust(self, slot, freq, window=64, thresh=2.0, mflag=10, biased=False):
+        """DBdust of the block in slot: (anno int64[nreads+1] byte offsets, data int32 pairs)."""
+        fr = (C.c_float * 4)(*[float(x) for x in freq])
+        anno = np.zeros(self._nreads[slot] + 1, np.int64)
+        data = np.zeros(1 << 20, np.int32)
+        n = _check(lib().gd_dust(self.h, slot, window, thresh, mflag, int(biased), fr, anno.ctypes.data,
+                                 data.ctypes.data, data.size))
+        if n > data.size:   # larger than the first guess: run again with room for all
+            data = np.zeros(n, np.int32)
+            _check(lib().gd_dust(self.h, slot, window, thresh, mflag, int(biased), fr, anno.ctypes.data,
+                                 data.ctypes.data, n))
+        return anno, data[:n]
 
     def las_sort(self, in_path, out_path):
         """LAsort of one .las file on the device; returns the number of records."""

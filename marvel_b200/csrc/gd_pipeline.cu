@@ -17,6 +17,7 @@
 #include "../../include/gpudalign.h"
 #include "gd_align.cuh"
 #include "gd_filter.cuh"
+#include "gd_dust.cuh"
 #include "gd_output.cuh"
 #include "gd_prims.cuh"
 #include "gd_verify.cuh"
@@ -1219,6 +1220,77 @@ int64_t gd_las_sort(gd_context* c, const char* in_path, const char* out_path)
         return -1;
     }
     return novl;
+}
+
+int64_t gd_dust(gd_context* c, int slot, int window, double thresh, int mflag, int biased, const float freq[4],
+                int64_t* anno, int32_t* data, int64_t cap)
+{
+    using namespace gd;
+    if (slot < 0 || slot > 2 || !c->slot[slot].loaded)
+    {
+        gd_set_error("gd_dust: slot %d not loaded", slot);
+        return -1;
+    }
+    if (!(thresh > 0.) || mflag - 1 <= 0)
+    {
+        gd_set_error("gd_dust: threshold must be positive and -m at least 2");
+        return -1;
+    }
+    Slot& S = c->slot[slot];
+    const int n = S.blk.nreads;
+    cudaStream_t s = c->s;
+    // 64 triplet weights for -b, in the reference's precision: the product of three float
+    // frequencies in float, then .015625 / product in double (db/DBdust.c:244-252)
+    double skew[64];
+    for (int a = 0, p = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++)
+            for (int e = 0; e < 4; e++)
+            {
+                float q = freq[a] * freq[b];
+                q = q * freq[e];
+                skew[p++] = .015625 / (double)q;
+            }
+    int64_t boff_end = 0;
+    GD_CUDA(cudaMemcpyAsync(&boff_end, S.blk.boff + n, 8, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    const size_t outints = (size_t)boff_end + 4ull * n + 8;
+    // scratch: per-read slices (k0), counts (flags), offsets (hoff), packed data (k1), weights (misc)
+    if (ensure(c->k0, outints * 4) || ensure(c->flags, (size_t)n * 4 + 4) || ensure(c->hoff, (size_t)n * 8 + 8) ||
+        ensure(c->misc, 1024))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(c->misc.p, skew, sizeof skew, cudaMemcpyHostToDevice, s));
+    if (launch_dust(S.blk, window, thresh, mflag - 1, biased != 0, P<double>(c->misc), P<int>(c->k0),
+                    P<int>(c->flags), s))
+        return -1;
+    std::vector<int> cnt(n);
+    GD_CUDA(cudaMemcpyAsync(cnt.data(), c->flags.p, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    std::vector<int64_t> off(n + 1);
+    int64_t total = 0;
+    for (int r = 0; r < n; r++)
+    {
+        if (cnt[r] < 0)
+        {
+            gd_set_error("gd_dust: read %d overflowed the candidate list", r);
+            return -1;
+        }
+        off[r] = total;
+        total += cnt[r];
+    }
+    off[n] = total;
+    if (!anno || !data || cap < total)
+        return total;
+    if (ensure(c->k1, (size_t)total * 4 + 16))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(c->hoff.p, off.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    if (launch_dust_gather(S.blk, P<int>(c->k0), P<int>(c->flags), P<int64_t>(c->hoff), P<int>(c->k1), s))
+        return -1;
+    if (total)
+        GD_CUDA(cudaMemcpyAsync(data, c->k1.p, (size_t)total * 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    for (int r = 0; r <= n; r++)
+        anno[r] = off[r] * 4;  // the .anno file holds byte offsets
+    return total;
 }
 
 int64_t gd_get_overlaps(gd_context* c, gd_overlap* recs, uint8_t* trace, int64_t rcap, int64_t tcap)

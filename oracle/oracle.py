@@ -203,3 +203,39 @@ def trace_pts_diffs(aread_seq, bread_seq, rec, trace, tspace):
                          int(rec["aepos"]), int(rec["bepos"]), None if t8 is None else t8.ctypes.data,
                          None if t16 is None else t16.ctypes.data, int(rec["tlen"]), tspace, C.byref(out))
     return out.value
+
+
+def dust(block, window=64, thresh=2.0, mflag=10, biased=False):
+    """DBdust's scan of every read of a block (dust_oracle.c): (anno int64[n+1] byte offsets,
+    data int32 pairs), the .dust.anno / .dust.data layout."""
+    fn = lib().or_dust_read
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    f = [np.float32(x) for x in block.freq]
+    skew = np.zeros(64, np.float64)
+    p = 0
+    for a in range(4):
+        for b in range(4):
+            for c in range(4):
+                q = np.float32(f[a] * f[b])
+                q = np.float32(q * f[c])
+                skew[p] = .015625 / float(q)
+                p += 1
+    n = block.nreads
+    anno = np.zeros(n + 1, np.int64)
+    out = []
+    o = 0
+    for r in range(n):
+        seq = np.ascontiguousarray(block.read(r), np.uint8)
+        L_ = seq.size
+        buf = np.zeros(L_ + 8, np.int32)
+        work = np.zeros(L_ + 8, np.int32)
+        k = fn(seq.ctypes.data, L_, window, thresh, mflag - 1, int(biased), skew.ctypes.data, buf.ctypes.data,
+               work.ctypes.data)
+        if k < 0:
+            raise RuntimeError(f"or_dust_read failed on read {r} ({k})")
+        anno[r] = 4 * o
+        out.append(buf[:k].copy())
+        o += k
+    anno[n] = 4 * o
+    return anno, (np.concatenate(out) if out else np.zeros(0, np.int32))
