@@ -126,6 +126,12 @@ int64_t gd_dust(gd_context* ctx, int slot, int window, double thresh, int mflag,
  * reference's qsort leaves unordered, by (aepos, bbpos) and then file order -- each record's
  * bytes (trace and pad word included) unchanged.  Returns the number of records. */
 int64_t gd_las_sort(gd_context* ctx, const char* in_path, const char* out_path);
+
+/* LAmerge's result (utils/LAmerge.c, heap merge ordered by SORT_OVL of
+ * utils/LAmergeUtils.c:50-79: aread, bread, orientation, abpos) for nin .las files of one
+ * trace spacing, in one device sort of all their records; ties by (aepos, bbpos), then
+ * input order.  Record bytes are kept.  Returns the number of records. */
+int64_t gd_las_merge(gd_context* ctx, const char* const* in_paths, int nin, const char* out_path);
 int gd_write_overlap_buffer(gd_context* ctx, int run_id, const char* ablock, const char* bblock, int last_read);
 int gd_reset_overlap_buffer(gd_context* ctx);
 

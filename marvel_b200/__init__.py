@@ -60,7 +60,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
-           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust"]
+           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -96,6 +96,8 @@ def lib():
     L.gd_sort_overlaps.restype = C.c_int64
     L.gd_las_sort.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
     L.gd_las_sort.restype = C.c_int64
+    L.gd_las_merge.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int, C.c_char_p]
+    L.gd_las_merge.restype = C.c_int64
     L.gd_dust.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_float),
                           C.c_void_p, C.c_void_p, C.c_int64]
     L.gd_dust.restype = C.c_int64
@@ -292,6 +294,11 @@ class Context:
     def las_sort(self, in_path, out_path):
         """LAsort of one .las file on the device; returns the number of records."""
         return _check(lib().gd_las_sort(self.h, os.fsencode(in_path), os.fsencode(out_path)))
+
+    def las_merge(self, in_paths, out_path):
+        """LAmerge of .las files on the device; returns the number of records."""
+        arr = (C.c_char_p * len(in_paths))(*[os.fsencode(p) for p in in_paths])
+        return _check(lib().gd_las_merge(self.h, arr, len(in_paths), os.fsencode(out_path)))
 
     def reset_overlap_buffer(self):
         _check(lib().gd_reset_overlap_buffer(self.h))

@@ -1122,68 +1122,97 @@ int64_t gd_sort_overlaps(gd_context* c, int64_t* trace_bytes)
     return (int64_t)c->srt_n;
 }
 
-int64_t gd_las_sort(gd_context* c, const char* in_path, const char* out_path)
+// LAsort / LAmerge core: the records of all input files, ordered on the device by (aread,
+// bread, [orientation,] abpos), ties by (aepos, bbpos) and then input order, written to
+// out_path with every record's bytes unchanged.
+static int64_t las_sort_files(gd_context* c, const char* const* in_paths, int nin, const char* out_path, int with_comp)
 {
     using namespace gd;
-    FILE* f = fopen(in_path, "rb");
-    if (!f)
-    {
-        gd_set_error("Cannot open %s for reading", in_path);
-        return -1;
-    }
     int64_t novl = 0;
     int32_t tspace = 0;
-    fseek(f, 0, SEEK_END);
-    long fsize = ftell(f);
-    fseek(f, 0, SEEK_SET);
-    if (fsize < 12 || fread(&novl, 8, 1, f) != 1 || fread(&tspace, 4, 1, f) != 1 || novl < 0 || tspace <= 0)
+    std::vector<uint64_t> bodies(nin);
+    uint64_t body = 0;
+    for (int f = 0; f < nin; f++)
     {
-        fclose(f);
-        gd_set_error("%s: not a .las file", in_path);
-        return -1;
+        FILE* fp = fopen(in_paths[f], "rb");
+        if (!fp)
+        {
+            gd_set_error("Cannot open %s for reading", in_paths[f]);
+            return -1;
+        }
+        int64_t nf = 0;
+        int32_t ts = 0;
+        fseek(fp, 0, SEEK_END);
+        long fsize = ftell(fp);
+        fclose(fp);
+        fp = fopen(in_paths[f], "rb");
+        if (fsize < 12 || fread(&nf, 8, 1, fp) != 1 || fread(&ts, 4, 1, fp) != 1 || nf < 0 || ts <= 0)
+        {
+            fclose(fp);
+            gd_set_error("%s: not a .las file", in_paths[f]);
+            return -1;
+        }
+        fclose(fp);
+        if (f > 0 && ts != tspace)
+        {
+            gd_set_error("%s: trace spacing %d differs from %d of the first input", in_paths[f], ts, tspace);
+            return -1;
+        }
+        tspace = ts;
+        novl += nf;
+        bodies[f] = (uint64_t)fsize - 12;
+        body += bodies[f];
     }
-    const uint64_t body = (uint64_t)fsize - 12;
     if (ensure_host(c->h_tr, body + 16) || ensure_host(c->h_rec, body + 16))
-    {
-        fclose(f);
         return -1;
-    }
-    if (body && fread(c->h_tr.p, 1, body, f) != body)
-    {
-        fclose(f);
-        gd_set_error("%s: short read", in_path);
-        return -1;
-    }
-    fclose(f);
-    // record offsets: records are variable length (LAsort.c:209-218), a sequential walk
+    uint8_t* raw = (uint8_t*)c->h_tr.p;
     const int tbytes = tspace <= 125 ? 1 : 2;  // TRACE_XOVR
     if ((uint64_t)novl > body / 40)
     {
-        gd_set_error("%s: header claims %lld records, the file holds at most %llu", in_path, (long long)novl,
+        gd_set_error("%s: headers claim %lld records, the files hold at most %llu", in_paths[0], (long long)novl,
                      (unsigned long long)(body / 40));
         return -1;
     }
-    const uint8_t* raw = (const uint8_t*)c->h_tr.p;
+    // record offsets: records are variable length (LAsort.c:209-218), a sequential walk per file
     std::vector<int64_t> off((size_t)novl);
-    uint64_t o = 0;
-    for (int64_t i = 0; i < novl; i++)
+    uint64_t base = 0, used = 0;
+    int64_t k = 0;
+    for (int f = 0; f < nin; f++)
     {
-        int32_t tlen;
-        if (o + 40 > body)
+        FILE* fp = fopen(in_paths[f], "rb");
+        int64_t nf = 0;
+        int32_t ts = 0;
+        if (!fp || fread(&nf, 8, 1, fp) != 1 || fread(&ts, 4, 1, fp) != 1 ||
+            (bodies[f] && fread(raw + base, 1, bodies[f], fp) != bodies[f]))
         {
-            gd_set_error("%s: record %lld runs past the end of the file", in_path, (long long)i);
+            if (fp)
+                fclose(fp);
+            gd_set_error("%s: short read", in_paths[f]);
             return -1;
         }
-        memcpy(&tlen, raw + o, 4);
-        if (tlen < 0 || o + 40 + (uint64_t)tlen * tbytes > body)
+        fclose(fp);
+        uint64_t o = 0;
+        for (int64_t i = 0; i < nf; i++, k++)
         {
-            gd_set_error("%s: record %lld has a bad trace length %d", in_path, (long long)i, tlen);
-            return -1;
+            int32_t tlen;
+            if (o + 40 > bodies[f])
+            {
+                gd_set_error("%s: record %lld runs past the end of the file", in_paths[f], (long long)i);
+                return -1;
+            }
+            memcpy(&tlen, raw + base + o, 4);
+            if (tlen < 0 || o + 40 + (uint64_t)tlen * tbytes > bodies[f])
+            {
+                gd_set_error("%s: record %lld has a bad trace length %d", in_paths[f], (long long)i, tlen);
+                return -1;
+            }
+            off[(size_t)k] = (int64_t)(base + o);
+            o += 40 + (uint64_t)tlen * tbytes;
         }
-        off[(size_t)i] = (int64_t)o;
-        o += 40 + (uint64_t)tlen * tbytes;
+        // bytes after a file's last record are never referenced (the reference ignores them too)
+        base += bodies[f];
+        used = base;
     }
-    const uint64_t used = o;
     cudaStream_t s = c->s;
     if (ensure(c->las_raw, used + 16) || ensure(c->las_off, (size_t)novl * 8 + 8) ||
         ensure(c->las_rec, (size_t)novl * sizeof(OutRec) + 16) || ensure(c->las_out, used + 16))
@@ -1198,7 +1227,7 @@ int64_t gd_las_sort(gd_context* c, const char* in_path, const char* out_path)
         const uint32_t* perm = nullptr;
         uint64_t kept = 0, kbytes = 0;
         if (launch_las_parse(P<uint8_t>(c->las_raw), P<int64_t>(c->las_off), (uint64_t)novl, P<OutRec>(c->las_rec), s) ||
-            sort_perm(c, P<OutRec>(c->las_rec), (uint64_t)novl, 0, 0, tbytes, &perm, &kept, &kbytes) ||
+            sort_perm(c, P<OutRec>(c->las_rec), (uint64_t)novl, with_comp, 0, tbytes, &perm, &kept, &kbytes) ||
             launch_las_emit(P<OutRec>(c->las_rec), P<uint8_t>(c->las_raw), perm, P<uint64_t>(c->olen), kept, tbytes,
                             P<uint8_t>(c->las_out), s))
             return -1;
@@ -1220,6 +1249,21 @@ int64_t gd_las_sort(gd_context* c, const char* in_path, const char* out_path)
         return -1;
     }
     return novl;
+}
+
+int64_t gd_las_sort(gd_context* c, const char* in_path, const char* out_path)
+{
+    return las_sort_files(c, &in_path, 1, out_path, 0);
+}
+
+int64_t gd_las_merge(gd_context* c, const char* const* in_paths, int nin, const char* out_path)
+{
+    if (nin <= 0)
+    {
+        gd_set_error("gd_las_merge: no input files");
+        return -1;
+    }
+    return las_sort_files(c, in_paths, nin, out_path, 1);
 }
 
 int64_t gd_dust(gd_context* c, int slot, int window, double thresh, int mflag, int biased, const float freq[4],

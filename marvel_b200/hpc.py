@@ -55,6 +55,7 @@ class HpcOptions:
     sort: bool = False
     host: str | None = None
     port: int = 0
+    merge_after: bool = False   # --run --merge: the plan's LAmerge calls after its daligner calls
 
 
 def _diag_jobs(o: HpcOptions) -> int:
@@ -307,19 +308,44 @@ def reduce_stats(calls: int, seconds: float):
     return int(c.item()), float(s.item())
 
 
-def run(db: str, o: HpcOptions, fblock: int | None = None, lblock: int | None = None, executor=None):
+def run_merges(db: str, blocks, o: HpcOptions, merger=None):
+    """The plan's LAmerge calls for the given blocks: all .las files of run directory
+    %03d_%05d (run id, block) merged into <db name>.<block>.las beside the DB, on the GPU."""
+    path, name, d = _db_parts(db)
+    for i in blocks:
+        src = os.path.join(d, "%03d_%05d" % (o.run_id, i))
+        out = os.path.join(d, f"{name}.{i}.las")
+        if merger is not None:
+            merger(src, out)
+        else:
+            from . import lamerge
+            if lamerge.main(["-n", str(o.merge), path, out, src]) != 0:
+                raise RuntimeError(f"merging {src} failed")
+    return len(blocks)
+
+
+def run(db: str, o: HpcOptions, fblock: int | None = None, lblock: int | None = None, executor=None, merge=False,
+        merger=None):
     """Plans all block comparisons of db, runs this rank's share (rank and world from the
-    default process group, if any), and returns (calls of all ranks, slowest rank's seconds)."""
+    default process group, if any), and returns (calls of all ranks, slowest rank's seconds).
+    With merge, after all ranks finish their calls, each rank merges its share of the blocks
+    (the plan's LAmerge calls)."""
     import torch.distributed as dist
     world, rank = 1, 0
-    if dist.is_available() and dist.is_initialized():
+    dist_on = dist.is_available() and dist.is_initialized()
+    if dist_on:
         world, rank = dist.get_world_size(), dist.get_rank()
     n = db_blocks(db)
     fb = fblock or 1
     lb = lblock or n
+    t0 = time.perf_counter()
     mine = assign(plan(fb, lb, o), world, rank)
-    calls, secs = run_jobs(db, mine, o, executor)
-    return reduce_stats(calls, secs)
+    calls, _ = run_jobs(db, mine, o, executor)
+    if merge:
+        if dist_on:
+            dist.barrier()   # every block's files are written before any merge reads them
+        run_merges(db, list(range(fb, lb + 1))[rank::world], o, merger)
+    return reduce_stats(calls, time.perf_counter() - t0)
 
 
 def parse_args(argv):
@@ -327,6 +353,7 @@ def parse_args(argv):
     import argparse
     p = argparse.ArgumentParser(prog="marvel_b200.hpc", add_help=False)
     p.add_argument("--run", action="store_true")
+    p.add_argument("--merge", action="store_true")
     p.add_argument("-v", action="count", default=0)
     for c in "AIXTKS":
         p.add_argument("-" + c, action="store_true")
@@ -357,14 +384,16 @@ def parse_args(argv):
             fb = lb = int(a.blocks)
     if fb < 1 or fb > n or lb < fb or lb > n:
         raise SystemExit(f"invalid block range {fb}-{lb} for a DB of {n} blocks")
+    o.merge_after = a.merge
     return a.db, fb, lb, o, a.run
 
 
 def main(argv=None):
-    """python -m marvel_b200.hpc [--run] [HPCdaligner options] DB [first[-last]]
+    """python -m marvel_b200.hpc [--run [--merge]] [HPCdaligner options] DB [first[-last]]
 
     Without --run prints the plan like HPCdaligner.  With --run (one process per GPU, e.g.
-    under torchrun) each rank runs its share of the daligner calls on its own GPU."""
+    under torchrun) each rank runs its share of the daligner calls on its own GPU, and with
+    --merge then its share of the LAmerge calls."""
     import sys
     db, fb, lb, o, do_run = parse_args(sys.argv[1:] if argv is None else argv)
     if not do_run:
@@ -376,7 +405,7 @@ def main(argv=None):
         local = int(os.environ.get("LOCAL_RANK", "0"))
         os.environ.setdefault("CUDA_VISIBLE_DEVICES", str(local))
         dist.init_process_group("gloo", timeout=timedelta(seconds=3600))
-    calls, secs = run(db, o, fb, lb)
+    calls, secs = run(db, o, fb, lb, merge=o.merge_after)
     if not dist.is_initialized() or dist.get_rank() == 0:
         print(f"{calls} daligner calls, slowest rank {secs:.1f} s")
     if dist.is_initialized():

@@ -34,3 +34,27 @@ def las_sort(src, dst):
         for i in order:
             f.write(recs[i][3])
     return n
+
+
+def las_merge(srcs, dst):
+    """LAmerge's result (utils/LAmerge.c): the records of all inputs ordered by SORT_OVL of
+    utils/LAmergeUtils.c:50-79 (aread, bread, orientation, abpos); LAmerge's heap leaves ties
+    in no fixed order, this restatement keeps them in input order."""
+    recs, ts = [], None
+    for s in srcs:
+        n, t, r = read_records(s)
+        if ts is not None and t != ts:
+            raise ValueError("trace spacings differ")
+        ts = t
+        recs += r
+    def key(i):
+        a, b, ab, raw = recs[i]
+        comp = int(np.frombuffer(raw[24:28], "<u4")[0]) & 1
+        return (a, b, comp, ab)
+    order = sorted(range(len(recs)), key=key)
+    with open(dst, "wb") as f:
+        f.write(np.int64(len(recs)).tobytes())
+        f.write(np.int32(ts).tobytes())
+        for i in order:
+            f.write(recs[i][3])
+    return len(recs)

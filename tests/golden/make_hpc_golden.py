@@ -2,8 +2,9 @@
 oracle/Makefile into oracle/_ref:
 
 * hpc_plans.json -- HPCdaligner's printed plan for a 4-block DB under several option sets;
-* hpc_3blocks/ -- a 3-block DB and every .las file its default plan's daligner calls write
-  (run with the reference daligner), for the multi-block driver's GPU test.
+* hpc_3blocks/ -- a 3-block DB, every .las file its default plan's daligner calls write
+  (run with the reference daligner), and the merged G.n.las files the plan's LAmerge calls
+  write (reference LAmerge), for the multi-block driver's and LAmerge's tests.
 
 Run from the repository root:  make -C oracle ref && python tests/golden/make_hpc_golden.py
 """
@@ -58,8 +59,13 @@ def three_blocks():
     for c in calls:
         subprocess.run([os.path.join(REF, "daligner")] + c, cwd=d, check=True, stdout=subprocess.DEVNULL)
     las = sorted(os.path.relpath(os.path.join(r, f), d) for r, _, fs in os.walk(d) for f in fs if f.endswith(".las"))
+    # the plan's LAmerge calls: one merged file per block from its directory
+    merges = [ln.split()[1:] for ln in plan.splitlines() if ln.startswith("LAmerge ")]
+    for m in merges:
+        subprocess.run([os.path.join(REF, "LAmerge")] + m, cwd=d, check=True, stdout=subprocess.DEVNULL)
     with open(os.path.join(d, "hpc.json"), "w") as f:
-        json.dump({"workload": "tiny", "scale": 0.8, "block_mbp": 0.2, "plan": plan, "las": las}, f, indent=1)
+        json.dump({"workload": "tiny", "scale": 0.8, "block_mbp": 0.2, "plan": plan, "las": las,
+                   "merged": [m[-2] for m in merges], "merge_dirs": [m[-1] for m in merges]}, f, indent=1)
 
 
 if __name__ == "__main__":

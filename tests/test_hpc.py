@@ -80,9 +80,11 @@ def _rank_main(rank, world, port, db, out):
         ran.append(args)
         time.sleep(0.01 * (1 + rank))
 
-    calls, secs = h.run(db, h.HpcOptions(dal=2), executor=fake)
+    merged = []
+    calls, secs = h.run(db, h.HpcOptions(dal=2), executor=fake, merge=True,
+                        merger=lambda src, out: merged.append(os.path.basename(out)))
     with open(os.path.join(out, f"rank{rank}.json"), "w") as f:
-        json.dump({"ran": ran, "calls": calls, "secs": secs}, f)
+        json.dump({"ran": ran, "calls": calls, "secs": secs, "merged": merged}, f)
     dist.barrier()
     dist.destroy_process_group()
 
@@ -100,3 +102,4 @@ def test_two_ranks_shard_the_plan_over_gloo(db4, tmp_path):
     assert res[0]["ran"] and res[1]["ran"]                    # both ranks worked
     assert res[0]["calls"] == res[1]["calls"] == len(jobs)    # sum over ranks
     assert res[0]["secs"] == res[1]["secs"] > 0               # max over ranks, same on all
+    assert sorted(res[0]["merged"] + res[1]["merged"]) == [f"G.{i}.las" for i in range(1, 5)]
