@@ -51,6 +51,9 @@ struct WarpSmem
     WaveSmem ws;
     LAPath ap, bp;
     int span_lo, span_hi;
+    int trim[5];  // the trim point (anti-diagonal, y, diffs, A and B pebble heads), written by its lane
+    int clipm[6];  // the clip fallback: M count, anti-diagonal, y, diffs, A and B pebble heads
+    int besty;    // y of the best anti-diagonal
 };
 
 struct WarpCtx
@@ -163,14 +166,20 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
     int more = 1;
     int aclip = FWD ? INT_MAX : -INT_MAX;
     int bclip = FWD ? -INT_MAX : INT_MAX;
-    int besta, besty, trima, trimy, trimd, trimha, trimhb;
-    int morea, morey, mored, moreha, morehb, morem, lasta;
-    besta = trima = morea = lasta = mida;
-    besty = trimy = morey = (mida - hgh) >> 1;
-    trimd = mored = 0;
-    trimha = moreha = 0;
-    trimhb = morehb = 1;
-    morem = -1;
+    int besta, lasta;
+    besta = lasta = mida;
+    int* const trim = w.sm->trim;  // [0] a-diag, [1] y, [2] diffs, [3] A head, [4] B head
+    int* const clipm = w.sm->clipm;  // [0] M count (-1: none), [1] a-diag, [2] y, [3] diffs, [4] A head, [5] B head
+    if (lane == 0)
+    {
+        trim[0] = mida;
+        trim[1] = (mida - hgh) >> 1;
+        trim[2] = 0;
+        trim[3] = 0;
+        trim[4] = 1;
+        clipm[0] = -1;
+        w.sm->besty = (mida - hgh) >> 1;
+    }
     int npeb = 0;
     // the reverse wave compares the bases just before the point (align.c:1117-1118)
     const uint8_t* as = FWD ? aseq0 : aseq0 - 1;
@@ -246,10 +255,15 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
         }
         if (FWD ? (c > besta) : (c < besta))
         {
-            besta = trima = lasta = c;
-            besty = trimy = y;
-            trimha = ha;
-            trimhb = hb;
+            besta = lasta = c;
+            if (lane == 0)
+            {
+                trim[0] = c;
+                trim[1] = y;
+                trim[3] = ha;
+                trim[4] = hb;
+                w.sm->besty = y;
+            }
         }
         if (lane == 0)
         {
@@ -268,6 +282,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
     auto clip_block = [&]() {
         if (!more)
         {
+            const int besty = w.sm->besty;
             if (__ldg(bs + besty) != 4 && __ldg(as + besta - besty) != 4)
                 more = 1;
             if (FWD ? (hgh >= aclip) : (low <= aclip))
@@ -277,15 +292,16 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 else
                     low = aclip + 1;
                 int Mc = __popcll(R.T[dif & 1][aclip & RM] & MASK61);
-                if (morem <= Mc)
+                if (lane == 0 && clipm[0] <= Mc)
                 {
-                    morem = Mc;
-                    morea = R.V[dif & 1][aclip & RM];
-                    morey = (morea - aclip) / 2;
-                    mored = dif;
-                    moreha = R.HA[dif & 1][aclip & RM];
-                    morehb = R.HB[dif & 1][aclip & RM];
+                    clipm[0] = Mc;
+                    clipm[1] = R.V[dif & 1][aclip & RM];
+                    clipm[2] = (clipm[1] - aclip) / 2;
+                    clipm[3] = dif;
+                    clipm[4] = R.HA[dif & 1][aclip & RM];
+                    clipm[5] = R.HB[dif & 1][aclip & RM];
                 }
+                __syncwarp();
             }
             if (FWD ? (low <= bclip) : (hgh >= bclip))
             {
@@ -294,15 +310,16 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 else
                     hgh = bclip - 1;
                 int Mc = __popcll(R.T[dif & 1][bclip & RM] & MASK61);
-                if (morem <= Mc)
+                if (lane == 0 && clipm[0] <= Mc)
                 {
-                    morem = Mc;
-                    morea = R.V[dif & 1][bclip & RM];
-                    morey = (morea - bclip) / 2;
-                    mored = dif;
-                    moreha = R.HA[dif & 1][bclip & RM];
-                    morehb = R.HB[dif & 1][bclip & RM];
+                    clipm[0] = Mc;
+                    clipm[1] = R.V[dif & 1][bclip & RM];
+                    clipm[2] = (clipm[1] - bclip) / 2;
+                    clipm[3] = dif;
+                    clipm[4] = R.HA[dif & 1][bclip & RM];
+                    clipm[5] = R.HB[dif & 1][bclip & RM];
                 }
+                __syncwarp();
             }
             aclip = FWD ? INT_MAX : -INT_MAX;
             bclip = FWD ? -INT_MAX : INT_MAX;
@@ -496,18 +513,22 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                 int jm = __ffs(__ballot_sync(GD_FULL, wv == wmax)) - 1;
                 const unsigned mq1 = __ballot_sync(GD_FULL, q1), mq2 = __ballot_sync(GD_FULL, q2);
                 besta = __shfl_sync(GD_FULL, c, jm);
-                besty = __shfl_sync(GD_FULL, y, jm);
+                if (lane == jm)
+                    w.sm->besty = y;
                 bool p1j = (mq1 >> jm) & 1;
                 bool p2j = (mq2 >> jm) & 1;
                 if (p1j)
                     lasta = besta;
                 if (p2j)
                 {
-                    trima = besta;
-                    trimy = besty;
-                    trimd = dif;
-                    trimha = __shfl_sync(GD_FULL, ha, jm);
-                    trimhb = __shfl_sync(GD_FULL, hb, jm);
+                    if (lane == jm)
+                    {
+                        trim[0] = c;
+                        trim[1] = y;
+                        trim[2] = dif;
+                        trim[3] = ha;
+                        trim[4] = hb;
+                    }
                 }
                 else
                 {
@@ -531,13 +552,17 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
                     if (m2)
                     {
                         int j2 = 31 - __clz(m2);
-                        trima = __shfl_sync(GD_FULL, c, j2);
-                        trimy = __shfl_sync(GD_FULL, y, j2);
-                        trimd = dif;
-                        trimha = __shfl_sync(GD_FULL, ha, j2);
-                        trimhb = __shfl_sync(GD_FULL, hb, j2);
+                        if (lane == j2)
+                        {
+                            trim[0] = c;
+                            trim[1] = y;
+                            trim[2] = dif;
+                            trim[3] = ha;
+                            trim[4] = hb;
+                        }
                     }
                 }
+                __syncwarp();  // a later chunk's best point and trim point overwrite these
             }
         }
         __syncwarp();
@@ -583,17 +608,19 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
     }
 
     // ---- trace points of both paths from the pebble chains (align.c:970-1106, 1710-1902)
+    __syncwarp();
     if (lane == 0)
     {
         int4* cells = w.peb;
         int atlen = 0, btlen = 0, trimx, a, b, k, h, d, e;
-        if (morem >= 0)
+        int trima = trim[0], trimy = trim[1], trimd = trim[2], trimha = trim[3], trimhb = trim[4];
+        if (clipm[0] >= 0)
         {
-            trimx = morea - morey;
-            trimy = morey;
-            trimd = mored;
-            trimha = moreha;
-            trimhb = morehb;
+            trimx = clipm[1] - clipm[2];
+            trimy = clipm[2];
+            trimd = clipm[3];
+            trimha = clipm[4];
+            trimhb = clipm[5];
         }
         else
             trimx = trima - trimy;
@@ -1193,7 +1220,7 @@ __device__ void emit_paths(WarpCtx& w, const AlignParams& P, const MPath* m, int
     }
 }
 
-__global__ void __launch_bounds__(ALIGN_WARPS * 32, 5)
+__global__ void __launch_bounds__(ALIGN_WARPS * 32, 6)
     k_align_pairs(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
                   AlignScratch sc, AlignOut out, unsigned* queue, DevStatus* st)
