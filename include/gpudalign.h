@@ -60,6 +60,7 @@ typedef struct
     double ms_merge[2];   /* device time of merge + hit sort */
     double ms_align[2];   /* device time of seed scan + alignment */
     int64_t skipped[2];   /* pair groups the learned triage skipped (0 with no model set) */
+    int64_t wide[2];      /* pair groups whose band outgrew 128 diagonals (aligned by the wide kernel) */
 } gd_stats;
 
 /* Context on the current CUDA device. */
@@ -120,6 +121,12 @@ int64_t gd_get_overlaps(gd_context* ctx, gd_overlap* recs, uint8_t* trace, int64
  * the .dust.anno / .dust.data layout: anno[r] = byte offset of read r's pairs in data. */
 int64_t gd_dust(gd_context* ctx, int slot, int window, double thresh, int mflag, int biased, const float freq[4],
                 int64_t* anno, int32_t* data, int64_t cap);
+
+/* Test hook, no counterpart in the reference: the widest band (in diagonals) the main
+ * aligner kernel takes before it hands a pair group to the wide kernel: 128 (default) or
+ * 32 (a narrow kernel instance that routes most groups through the wide kernel; the
+ * output must not change). */
+int gd_set_wave_limit(gd_context* ctx, int limit);
 
 /* LAsort (dalign/LAsort.c:65-90, 139-256) of one .las file on the device: writes out_path
  * with the records of in_path ordered by (aread, bread, abpos) -- ties, which the

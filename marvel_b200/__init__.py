@@ -50,7 +50,7 @@ class GdStats(C.Structure):
     _fields_ = [("kmers", C.c_int64 * 3), ("hits", C.c_int64 * 2), ("groups", C.c_int64 * 2),
                 ("seeds", C.c_int64 * 2), ("cells", C.c_int64 * 2), ("records", C.c_int64),
                 ("limit", C.c_int32 * 2), ("ms_index", C.c_double * 3), ("ms_merge", C.c_double * 2),
-                ("ms_align", C.c_double * 2), ("skipped", C.c_int64 * 2)]
+                ("ms_align", C.c_double * 2), ("skipped", C.c_int64 * 2), ("wide", C.c_int64 * 2)]
 
 
 # exported symbols of include/gpudalign.h
@@ -60,7 +60,8 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_get_stats", "gd_local_alignment_batch", "gd_complement_block", "gd_timer_mark",
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
-           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge"]
+           "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge",
+           "gd_set_wave_limit"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -98,6 +99,7 @@ def lib():
     L.gd_las_sort.restype = C.c_int64
     L.gd_las_merge.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int, C.c_char_p]
     L.gd_las_merge.restype = C.c_int64
+    L.gd_set_wave_limit.argtypes = [C.c_void_p, C.c_int]
     L.gd_dust.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_float),
                           C.c_void_p, C.c_void_p, C.c_int64]
     L.gd_dust.restype = C.c_int64
@@ -294,6 +296,10 @@ class Context:
     def las_sort(self, in_path, out_path):
         """LAsort of one .las file on the device; returns the number of records."""
         return _check(lib().gd_las_sort(self.h, os.fsencode(in_path), os.fsencode(out_path)))
+
+    def set_wave_limit(self, limit):
+        """Test hook: the widest band of the main aligner kernel, 128 (default) or 32."""
+        _check(lib().gd_set_wave_limit(self.h, int(limit)))
 
     def las_merge(self, in_paths, out_path):
         """LAmerge of .las files on the device; returns the number of records."""

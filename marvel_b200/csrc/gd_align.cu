@@ -6,15 +6,19 @@
 // GPU mapping.  A warp owns one pair group of the sorted hit list.  The panel band scores
 // are built lane-parallel (match-any groups per diagonal band), candidate seeds are taken
 // in hit order, and each fired seed runs the O(ND) wave with lanes over diagonals: the
-// wave vectors V (furthest anti-diagonal), T (60-column match bit vector; its popcount is
-// the reference's M), HA/HB (pebble heads), NA/NB (next trace-point marks) live in a
-// per-warp shared-memory ring indexed by diagonal.  Each wave reads the previous wave for
-// diagonals k-1, k, k+1, keeps the new values in registers (up to 32*WAVE_CHUNKS
-// diagonals), and writes them back after a __syncwarp, which is the reference's
-// in-place update order.  The reference's sequential "c > besta" scan over diagonals
-// becomes a warp prefix-max in scan order; its clip bookkeeping becomes ballots.  Pebbles
-// go to a per-warp global arena; the two trace-point chains are unwound by lane 0.
-// Match extension compares 8 bases per step with 64-bit XOR windows.
+// wave vectors V (furthest anti-diagonal), T (60-column match bit vector; its popcount
+// is the reference's M), HA/HB (pebble heads), NA/NB (next trace-point marks) live in two
+// per-warp shared-memory rings indexed by diagonal, one per wave parity: each wave reads
+// the previous wave for diagonals k-1, k, k+1 and writes the other ring, which is the
+// reference's in-place update order.  The reference's sequential "c > besta" scan over
+// diagonals becomes a warp prefix-max in scan order; its clip bookkeeping becomes ballots.
+// Pebbles go to a per-warp global arena; the two trace-point chains are unwound by lane 0.
+// Match extension compares 4 bases per step with 32-bit XOR windows.
+//
+// Instances by ring size: RING (128 diagonals, 4 warps per CTA) aligns every pair group; a
+// group whose band grows wider is abandoned there (nothing emitted, its counts dropped) and
+// listed for the WIDE_RING instance (512 diagonals, 1 warp per CTA), which aligns it from
+// scratch.  TEST_RING (32) replaces RING in tests so that most groups take that route.
 #include "gd_align.cuh"
 
 #include <climits>
@@ -31,14 +35,15 @@ namespace gd
 #define WAVE_LAG 30
 #define PANEL_SIZE 50000
 #define PANEL_OVERLAP 10000
-#define RM (RING - 1)
+#define RM (RG - 1)  // ring index mask of the instance (RG diagonals)
 #define SENT4 0x0404040404040404ull
 
 // wave vectors: [dif & 1] holds wave dif, so a wave reads the previous one while it writes
+template <int RG>
 struct WaveSmem
 {
-    unsigned long long T[2][RING];
-    int V[2][RING], HA[2][RING], HB[2][RING], NA[2][RING], NB[2][RING];
+    unsigned long long T[2][RG];
+    int V[2][RG], HA[2][RG], HB[2][RG], NA[2][RG], NB[2][RG];
 };
 
 struct LAPath
@@ -46,9 +51,10 @@ struct LAPath
     int abpos, bbpos, aepos, bepos, diffs, tlen, toff, pad;
 };
 
+template <int RG>
 struct WarpSmem
 {
-    WaveSmem ws;
+    WaveSmem<RG> ws;
     LAPath ap, bp;
     int span_lo, span_hi;
     int trim[5];  // the trim point (anti-diagonal, y, diffs, A and B pebble heads), written by its lane
@@ -56,18 +62,19 @@ struct WarpSmem
     int besty;    // y of the best anti-diagonal
 };
 
+template <int RG>
 struct WarpCtx
 {
-    WarpSmem* sm;
+    WarpSmem<RG>* sm;
     int4* peb;
     int pcap;
     uint16_t* pts;
     int ptscap;
     DevStatus* st;
     int lane;
-    int err;
+    int err;         // 1: failed (status set); 2: the band outgrew this instance (the caller decides)
     int item;
-    long long cells;
+    unsigned cells;  // wave cells of the current pair group (or seed)
 };
 
 __device__ __forceinline__ unsigned ld4u(const uint8_t* p)
@@ -135,7 +142,8 @@ __device__ __forceinline__ bool trim_ok(unsigned long long b, const int16_t* tab
 }
 
 // uniform single-pebble allocation (all lanes call, lane 0 writes)
-__device__ __forceinline__ int peb_one(WarpCtx& w, int& npeb, int ptr, int diag, int diff, int mark)
+template <int RG>
+__device__ __forceinline__ int peb_one(WarpCtx<RG>& w, int& npeb, int ptr, int diag, int diff, int mark)
 {
     int idx = npeb++;
     if (idx >= w.pcap)
@@ -151,12 +159,12 @@ __device__ __forceinline__ int peb_one(WarpCtx& w, int& npeb, int ptr, int diag,
 }
 
 // forward_wave (FWD) / reverse_wave (!FWD) restated, with lanes over diagonals.
-template <bool FWD>
-__device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0, int alen, int blen,
+template <bool FWD, int RG>
+__device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0, int alen, int blen,
                      int comp, LAPath* apath, LAPath* bpath, int* mind, int maxd, int mida, int minp, int maxp,
                      uint16_t* atrace, uint16_t* btrace)
 {
-    WaveSmem& R = w.sm->ws;
+    WaveSmem<RG>& R = w.sm->ws;
     const int lane = w.lane;
     const int TS = P.tspace;
     const int S = FWD ? 1 : -1;
@@ -359,11 +367,16 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             return;
         }
         const int width = hgh - low + 1;
-        if (width <= 0 || width > 32 * WAVE_CHUNKS)
+        if ((unsigned)(width - 1) >= (unsigned)RG)  // empty, or wider than this instance
         {
-            if (lane == 0)
-                gd_fail(w.st, width <= 0 ? GD_ERR_EMPTY_BAND : GD_ERR_BAND_WIDTH, w.item, width);
-            w.err = 1;
+            if (width > RG)
+                w.err = 2;  // a wider instance may take this pair (the caller decides)
+            else
+            {
+                if (lane == 0)
+                    gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, width);
+                w.err = 1;
+            }
             return;
         }
         const int nch = (width + 31) >> 5;
@@ -371,7 +384,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
         const int cur = dif & 1, prv = cur ^ 1;
         int c0 = 0;  // chunk 0's new V, for the WAVE_LAG test
 #pragma unroll
-        for (int ch = 0; ch < WAVE_CHUNKS; ch++)
+        for (int ch = 0; ch < RG / 32; ch++)
         {
             if (ch >= nch)
                 break;
@@ -575,7 +588,7 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
             const int hw = FWD ? hgh0 : low0;  // wave origin before clipping
             int nl = INT_MAX, nh = INT_MIN;
 #pragma unroll
-            for (int ch = 0; ch < WAVE_CHUNKS; ch++)
+            for (int ch = 0; ch < RG / 32; ch++)
             {
                 if (ch >= nch)
                     break;
@@ -851,7 +864,8 @@ __device__ void wave(WarpCtx& w, const AlignParams& P, const uint8_t* aseq0, con
 }
 
 // Local_Alignment from one seed (diag, anti) with lbord = hbord = -1 (align.c:1922-2060).
-__device__ void local_alignment(WarpCtx& w, const AlignParams& P, const uint8_t* aseq, const uint8_t* bseq, int alen,
+template <int RG>
+__device__ void local_alignment(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq, const uint8_t* bseq, int alen,
                                 int blen, int comp, int diag, int anti)
 {
     const int TS = P.tspace;
@@ -1143,7 +1157,8 @@ __device__ __forceinline__ int first_above(const uint64_t* hkey, int lo, int hi,
     return lo;
 }
 
-__device__ void store_path(WarpCtx& w, const LAPath& lp, MPath* dst, PairBuf& pb)
+template <int RG>
+__device__ void store_path(WarpCtx<RG>& w, const LAPath& lp, MPath* dst, PairBuf& pb)
 {
     // all lanes: copy the trace into the pair buffer
     if (pb.ttop + lp.tlen > pb.tcap)
@@ -1166,7 +1181,8 @@ __device__ void store_path(WarpCtx& w, const LAPath& lp, MPath* dst, PairBuf& pb
     pb.ttop += lp.tlen;
 }
 
-__device__ void emit_paths(WarpCtx& w, const AlignParams& P, const MPath* m, int n, const uint16_t* tb, int aread,
+template <int RG>
+__device__ void emit_paths(WarpCtx<RG>& w, const AlignParams& P, const MPath* m, int n, const uint16_t* tb, int aread,
                            int bread, AlignOut& out)
 {
     if (n <= 0)
@@ -1220,18 +1236,26 @@ __device__ void emit_paths(WarpCtx& w, const AlignParams& P, const MPath* m, int
     }
 }
 
-__global__ void __launch_bounds__(ALIGN_WARPS * 32, 6)
+template <int RG>
+constexpr int warps_of()
+{
+    return RG == WIDE_RING ? 1 : ALIGN_WARPS;
+}
+
+template <int RG>
+__global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
     k_align_pairs(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
                   AlignScratch sc, AlignOut out, unsigned* queue, DevStatus* st)
 {
-    __shared__ WarpSmem smem[ALIGN_WARPS];
+    constexpr int NW = warps_of<RG>();
+    __shared__ WarpSmem<RG> smem[NW];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int gw = blockIdx.x * ALIGN_WARPS + wib;
+    const int gw = blockIdx.x * NW + wib;
     if (gw >= sc.nwarps)
         return;
-    WarpCtx w;
+    WarpCtx<RG> w;
     w.sm = &smem[wib];
     w.peb = sc.peb + (size_t)gw * sc.pcap;
     w.pcap = sc.pcap;
@@ -1250,7 +1274,7 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32, 6)
     const int K = P.kmer, BS = P.binshift, TS = P.tspace;
     const int minhit = (P.hitmin - 1) / K + 1;
     const unsigned lt = lanemask_lt();
-    unsigned long long nseeds = 0;
+    unsigned long long tcells = 0, tseeds = 0;  // this warp's totals over the groups it completed
 
     while (true)
     {
@@ -1266,7 +1290,8 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32, 6)
         uint2 grp = groups[item];
         const int s = (int)grp.x, e = (int)grp.y;
         w.item = (int)item;
-        const long long cells0 = w.cells;
+        w.cells = 0;
+        unsigned nseeds = 0;
         uint64_t k0 = hkey[s];
         const int ar = (int)((k0 >> P.hb.pbits) & ((1ull << P.hb.abits) - 1));
         const int br = (int)(k0 >> (P.hb.pbits + P.hb.abits));
@@ -1469,6 +1494,22 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32, 6)
                 lastp[dg] = 0;
             }
         __syncwarp();
+        if (w.err == 2)
+        {
+            if (!out.wide_list)
+            {
+                if (lane == 0)
+                    gd_fail(st, GD_ERR_BAND_WIDTH, w.item, RG);
+                break;
+            }
+            // the band outgrew this instance: the group goes to the wide instance as if this
+            // warp had never seen it (its band arrays are clean again, nothing was emitted)
+            if (lane == 0)
+                out.wide_list[atomicAdd(out.nwide, 1u)] = item;
+            w.err = 0;
+            __syncwarp();
+            continue;
+        }
         if (w.err)
             break;
         // merge redundant paths (filter.c:1922-1938), lane 0
@@ -1492,14 +1533,15 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32, 6)
         emit_paths(w, P, amatch, novla, tbuf, ar + A.ufirst, br + B.ufirst, out);
         emit_paths(w, P, bmatch, novlb, tbuf, br + B.ufirst, ar + A.ufirst, out);
         if (out.gstat && lane == 0)
-            out.gstat[item] = make_uint2((unsigned)(novla + novlb),
-                                         (unsigned)min(w.cells - cells0, (long long)0xffffffffll));
+            out.gstat[item] = make_uint2((unsigned)(novla + novlb), w.cells);
+        tcells += w.cells;
+        tseeds += nseeds;
         __syncwarp();
     }
     if (lane == 0)
     {
-        atomicAdd(&out.counters[2], (unsigned long long)w.cells);
-        atomicAdd(&out.counters[3], nseeds);
+        atomicAdd(&out.counters[2], tcells);
+        atomicAdd(&out.counters[3], tseeds);
     }
 }
 
@@ -1535,26 +1577,43 @@ void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int 
     s->bands = (int*)p;
 }
 
-int align_grid(int* grid_out)
+int align_grid(int* grid_out, int wide)
 {
     int dev = 0, nsm = 0, per = 0;
     GD_CUDA(cudaGetDevice(&dev));
     GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_align_pairs, ALIGN_WARPS * 32, 0));
+    if (wide)
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_align_pairs<WIDE_RING>,
+                                                              warps_of<WIDE_RING>() * 32, 0));
+    else  // the narrow instances (RING, TEST_RING) have the same shape
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_align_pairs<RING>, ALIGN_WARPS * 32, 0));
     if (per < 1)
         per = 1;
     *grid_out = nsm * per;
     return 0;
 }
 
+int align_warps_per_cta(int wide)
+{
+    return wide ? warps_of<WIDE_RING>() : ALIGN_WARPS;
+}
+
 int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hkey, const uint32_t* hdiag,
                        const uint2* groups, const uint32_t* order, unsigned ngroups, AlignParams p, AlignScratch sc,
-                       AlignOut out, unsigned* queue, DevStatus* st, int grid, cudaStream_t s)
+                       AlignOut out, unsigned* queue, DevStatus* st, int grid, cudaStream_t s, int wide)
 {
     GD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), s));
     if (ngroups == 0)
         return 0;
-    k_align_pairs<<<grid, ALIGN_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p, sc, out, queue, st);
+    if (wide)
+        k_align_pairs<WIDE_RING><<<grid, warps_of<WIDE_RING>() * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups,
+                                                                            p, sc, out, queue, st);
+    else if (p.test_narrow)
+        k_align_pairs<TEST_RING><<<grid, ALIGN_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p, sc,
+                                                                   out, queue, st);
+    else
+        k_align_pairs<RING><<<grid, ALIGN_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p, sc, out,
+                                                              queue, st);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
@@ -1570,13 +1629,13 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32)
                AlignParams P, AlignScratch sc, int32_t* out12, uint16_t* tr, int trstride, int64_t* cells,
                DevStatus* st)
 {
-    __shared__ WarpSmem smem[ALIGN_WARPS];
+    __shared__ WarpSmem<RING> smem[ALIGN_WARPS];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int gw = blockIdx.x * ALIGN_WARPS + wib;
     if (gw >= sc.nwarps)
         return;
-    WarpCtx w;
+    WarpCtx<RING> w;
     w.sm = &smem[wib];
     w.peb = sc.peb + (size_t)gw * sc.pcap;
     w.pcap = sc.pcap;
@@ -1593,7 +1652,11 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32)
         const uint8_t* bseq = bbase + boff[sd];
         local_alignment(w, P, aseq, bseq, alen[sd], blen[sd], P.comp, diag[sd], anti[sd]);
         if (w.err)
+        {
+            if (w.err == 2 && lane == 0)
+                gd_fail(st, GD_ERR_BAND_WIDTH, sd, RING);
             continue;
+        }
         LAPath a = w.sm->ap, b = w.sm->bp;
         if (lane == 0)
         {

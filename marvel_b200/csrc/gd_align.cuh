@@ -13,9 +13,10 @@ namespace gd
 {
 
 constexpr int RING = 128;           // wave-vector rings per warp, one for the previous and one for the
-                                     // current wave (diagonal k lives at k & (RING-1))
-constexpr int WAVE_CHUNKS = 4;      // band width up to 32 * WAVE_CHUNKS diagonals per wave
-constexpr int ALIGN_WARPS = 4;      // warps per CTA of the aligner
+                                     // current wave (diagonal k lives at k & (RING-1)): the widest band
+constexpr int WIDE_RING = 512;      // the same for the wide instance, for pair groups whose band outgrows RING
+constexpr int TEST_RING = 32;       // a narrow instance for tests only: most groups then go to the wide one
+constexpr int ALIGN_WARPS = 4;      // warps per CTA of the aligner (the wide instance: 1)
 constexpr int TRIM_TABLE = 1 << 15; // TRIM_MASK + 1 (dalign/align.c:154)
 
 // One path as Local_Alignment returns it (dalign/align.h:76-83); trace is an offset into
@@ -43,6 +44,7 @@ struct AlignParams
     const int16_t* table;  // TABLE and SCORE trim tables (set_table, dalign/align.c:196-210)
     const int16_t* score;
     int mscore, dscore;    // match / edit weights the tables are built from (align.c:238-240)
+    int test_narrow;       // tests only: the main pass runs the TEST_RING instance
 };
 
 // Per-warp global scratch, carved from one allocation.
@@ -69,6 +71,8 @@ struct AlignOut
     uint64_t rcap, tcap;
     const uint8_t* skip;  // per pair group: 1 = triaged away (may be null)
     uint2* gstat;         // per pair group: (records emitted, wave cells) (may be null)
+    unsigned* wide_list;  // groups handed to the wide instance (null: a too-wide band is an error)
+    unsigned* nwide;      // their count
 };
 
 size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands);
@@ -77,7 +81,7 @@ void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int 
 // Persistent seed-scan + alignment over the ordered pair groups.
 int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hkey, const uint32_t* hdiag,
                        const uint2* groups, const uint32_t* order, unsigned ngroups, AlignParams p, AlignScratch sc,
-                       AlignOut out, unsigned* queue, DevStatus* st, int grid, cudaStream_t s);
+                       AlignOut out, unsigned* queue, DevStatus* st, int grid, cudaStream_t s, int wide = 0);
 
 // One Local_Alignment per seed (for parity tests of the wave alone).  out12 per seed:
 // A-path {abpos,bbpos,aepos,bepos,diffs,tlen}, B-path the same; traces at
@@ -87,6 +91,8 @@ int launch_la_batch(const uint8_t* aseq_base, const int64_t* aoff, const int32_t
                     AlignParams p, AlignScratch sc, int32_t* out12, uint16_t* tr, int trstride, int64_t* cells,
                     DevStatus* st, cudaStream_t s);
 
-int align_grid(int* grid_out);
+// CTAs for a persistent launch of the narrow (wide = 0) or wide instance, and its warps per CTA
+int align_grid(int* grid_out, int wide = 0);
+int align_warps_per_cta(int wide);
 
 }  // namespace gd

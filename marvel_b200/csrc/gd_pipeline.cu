@@ -177,6 +177,9 @@ struct gd_context
     gd::HitBits hb{};
     DevBuf ascr, outrec, outtr, counters, status, queue;
     int agrid = 0;
+    DevBuf ascr_w, wide;  // the wide aligner instance's scratch, and its group list + count
+    int agrid_w = 0;
+    int test_narrow = 0;  // tests only: the main aligner pass with the 32-diagonal instance
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
     uint64_t rcap = 1 << 22, tbcap = 512ull << 20;
     // the overlap buffer: records and trace bytes of every Match_Filter since the last reset,
@@ -350,6 +353,7 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     int oi = comp ? 1 : 0;
     c->stats.hits[oi] = c->stats.groups[oi] = c->stats.seeds[oi] = c->stats.cells[oi] = 0;
     c->stats.skipped[oi] = 0;
+    c->stats.wide[oi] = 0;
     c->stats.ms_merge[oi] = c->stats.ms_align[oi] = 0;
     c->nhits = 0;
     int64_t na = A.nk, nb = B.nk;
@@ -535,9 +539,11 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     ap.score = P<int16_t>(c->tables) + TRIM_TABLE;
     ap.mscore = c->mscore;
     ap.dscore = c->dscore;
-    if (!c->agrid && align_grid(&c->agrid))
+    ap.test_narrow = c->test_narrow;
+    if ((!c->agrid && align_grid(&c->agrid, 0)) || (!c->agrid_w && align_grid(&c->agrid_w, 1)))
         return -1;
     int nwarps = c->agrid * ALIGN_WARPS;
+    const int nwarps_w = c->agrid_w * align_warps_per_cta(1);
     int maxlen = std::max(A.blk.maxlen, B.blk.maxlen);
     int ptscap = 4 * (2 * (maxlen / c->tspace + 2)) + 32;
     int nbands = ap.maxdiag - ap.mindiag + 8;
@@ -557,12 +563,38 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
             return -1;
         GD_CUDA(cudaMemsetAsync(c->counters.p, 0, 64, s));
         GD_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), s));
+        if (ensure(c->wide, (size_t)ng * 4 + 16))
+            return -1;
+        unsigned* wide_list = P<unsigned>(c->wide);
+        unsigned* d_nwide = wide_list + ng;
+        GD_CUDA(cudaMemsetAsync(d_nwide, 0, 4, s));
         AlignOut out{P<OutRec>(c->outrec), P<uint8_t>(c->outtr), P<unsigned long long>(c->counters), c->rcap,
-                     c->tbcap, skip, c->tri_collect ? P<uint2>(c->tri_gstat) : nullptr};
+                     c->tbcap, skip, c->tri_collect ? P<uint2>(c->tri_gstat) : nullptr, wide_list, d_nwide};
         GD_CUDA(cudaEventRecord(c->ev0, s));
         if (launch_align_pairs(A.blk, B.blk, hkey, hdiag, P<uint2>(c->groups), order, ng, ap, sc, out,
-                               P<unsigned>(c->queue), P<DevStatus>(c->status), c->agrid, s))
+                               P<unsigned>(c->queue), P<DevStatus>(c->status), c->agrid, s, 0))
             return -1;
+        // pair groups whose band outgrew the main instance: the wide one, appending to the same
+        // output with its own scratch (a band wider than WIDE_RING is an error there)
+        unsigned nwide = 0;
+        GD_CUDA(cudaMemcpyAsync(&nwide, d_nwide, 4, cudaMemcpyDeviceToHost, s));
+        GD_CUDA(cudaStreamSynchronize(s));
+        c->stats.wide[oi] = nwide;
+        if (nwide > 0)
+        {
+            AlignScratch scw{};
+            const size_t need_w = align_scratch_bytes(nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+            if (ensure(c->ascr_w, need_w))
+                return -1;
+            align_scratch_carve(&scw, c->ascr_w.p, nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+            GD_CUDA(cudaMemsetAsync(scw.bands, 0, (size_t)nwarps_w * 3 * nbands * 4, s));
+            AlignOut outw = out;
+            outw.wide_list = nullptr;
+            outw.nwide = nullptr;
+            if (launch_align_pairs(A.blk, B.blk, hkey, hdiag, P<uint2>(c->groups), wide_list, nwide, ap, scw, outw,
+                                   P<unsigned>(c->queue), P<DevStatus>(c->status), c->agrid_w, s, 1))
+                return -1;
+        }
         GD_CUDA(cudaEventRecord(c->ev1, s));
         GD_CUDA(cudaEventSynchronize(c->ev1));
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -845,7 +877,7 @@ void gd_destroy(gd_context* c)
                       &c->tri_gstat, &c->tri_misc, &c->tri_x, &c->tri_y, &c->tri_perm, &c->tri_grad, &c->tri_m,
                       &c->tri_v, &c->tri_loss, &c->tri_w, &c->acc_rec, &c->acc_tr, &c->srt_rec, &c->srt_tr,
                       &c->okey0, &c->okey1, &c->oval0, &c->oval1, &c->olen, &c->las_raw, &c->las_off,
-                      &c->las_rec, &c->las_out};
+                      &c->las_rec, &c->las_out, &c->ascr_w, &c->wide};
     for (DevBuf* b : bufs)
         release(*b);
     for (HostBuf* h : {&c->h_rec, &c->h_tr})
@@ -1544,6 +1576,17 @@ int gd_reset_overlap_buffer(gd_context* c)
     c->acc_n = c->acc_tb = 0;
     c->srt_n = c->srt_tb = 0;
     c->srt_valid = false;
+    return 0;
+}
+
+int gd_set_wave_limit(gd_context* c, int limit)
+{
+    if (limit != gd::RING && limit != gd::TEST_RING)
+    {
+        gd_set_error("gd_set_wave_limit: %d is neither %d nor %d", limit, gd::RING, gd::TEST_RING);
+        return -1;
+    }
+    c->test_narrow = limit == gd::TEST_RING;
     return 0;
 }
 

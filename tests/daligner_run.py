@@ -61,8 +61,9 @@ def write_las(path, recs, traces, tspace):
             f.write(np.asarray(t).astype("<u1" if tb == 1 else "<u2").tobytes())
 
 
-def run(dbdir, flags, blocks, outdir, impl):
-    """Runs `daligner flags blocks[0] blocks[1]` with impl in {"oracle", "gpu"}; returns the paths."""
+def run(dbdir, flags, blocks, outdir, impl, wave_limit=None):
+    """Runs `daligner flags blocks[0] blocks[1]` with impl in {"oracle", "gpu"}; returns the paths.
+    wave_limit (gpu only) sets the widest band of the main aligner kernel (test hook)."""
     o = parse_flags(flags)
     aname, bname = blocks
     A = dazzdb.open_block(os.path.join(dbdir, aname))
@@ -88,6 +89,8 @@ def run(dbdir, flags, blocks, outdir, impl):
     else:
         import marvel_b200 as mb
         ctx = mb.Context()
+        if wave_limit is not None:
+            ctx.set_wave_limit(wave_limit)
         ctx.set_filter_params(o["k"], o["w"], o["t"], o["h"])
         ctx.new_align_spec(o["e"], o["s"], A.freq, symmetric, o["O"], o["T"])
         ctx.set_globals(2 * o["l"], o["I"] or o["O"], mem)

@@ -40,6 +40,17 @@ def _ctx(mb, A, k=14, w=6, t=0, h=35):
     return ctx
 
 
+@pytest.mark.parametrize("name", ["self_default", "pair_blocks", "self_long_panels"])
+def test_wide_band_kernel_matches_reference_golden(mb, name, tmp_path):
+    """The golden cases with a 32-diagonal main kernel, so that many pair groups go to the
+    wide kernel: the .las files are still the reference's."""
+    d, meta = load(name)
+    names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "gpu", wave_limit=32)
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
+        assert ok, f"{name} {n}: {msg}"
+
+
 @pytest.mark.parametrize("name,k", [("self_default", 14), ("self_k16_w5", 16)])
 def test_kmer_index_and_hits_match_oracle(mb, name, k):
     import oracle
@@ -134,7 +145,8 @@ def test_local_alignment_batch_matches_oracle(mb, comp):
 
 
 def test_full_block_cfg1_matches_oracle_and_is_deterministic(mb, tmp_path):
-    """The 1 Mbp / 20x workload (2.5k reads, 21 Mbp) end to end against the oracle."""
+    """The 1 Mbp / 20x workload (2.5k reads, 21 Mbp) end to end against the oracle, also
+    with many pair groups routed through the wide-band kernel."""
     import oracle
     reads, _ = synth.generate("cfg1")
     dazzdb.write_db(str(tmp_path / "C"), reads, 200)
@@ -144,7 +156,15 @@ def test_full_block_cfg1_matches_oracle_and_is_deterministic(mb, tmp_path):
     r2, t2 = mb.daligner_block(ctx, A)
     assert (r1 == r2).all() and (t1 == t2).all()
     st = ctx.stats()
+    # pair groups whose band outgrows 32 diagonals handed to the wide kernel: same output,
+    # same seeds and cells
+    ctx.set_wave_limit(32)
+    r3, t3 = mb.daligner_block(ctx, A)
+    st3 = ctx.stats()
     ctx.close()
+    assert sum(st3["wide"]) > 100 and sum(st["wide"]) == 0
+    assert (r3 == r1).all() and (t3 == t1).all()
+    assert st3["seeds"] == st["seeds"] and st3["cells"] == st["cells"]
     recs, traces, ost = oracle.daligner(A, A, dazzdb.complement_block(A), oracle.make_params(A.freq), True)
     assert r1.size == len(recs)
     assert st["seeds"] == [ost["seeds_n"], ost["seeds_c"]]
