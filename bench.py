@@ -41,8 +41,8 @@ PARAMS = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=32)
 CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
 CPU_SAMPLE_SCALE = 0.2   # CPU baseline: the same genome/read model on a 1/5-size genome
 # k_align_pairs DRAM bytes (read + write) per wave cell, from the ncu capture of the cfg1
-# N-orientation launch: 121.3 MB over 282 M cells
-ALIGN_DRAM_BYTES_PER_CELL = 121.3e6 / 282.0e6
+# N-orientation launch: 160.6 MB over 282 M cells
+ALIGN_DRAM_BYTES_PER_CELL = 160.6e6 / 282.0e6
 
 
 def make_db(workload, seed_offset=0, scale=1.0):
