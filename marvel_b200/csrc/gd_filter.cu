@@ -31,59 +31,140 @@ __device__ __forceinline__ int read_of_slot(const DevBlock& b, int64_t s, int K)
     return lo;
 }
 
+// Four consecutive slots per thread: one read lookup, the codes rolled base by base within
+// a read, keys and values stored as 16-byte vectors.  The value is the slot index, or with
+// pbits >= 0 the packed (read << pbits | first position), so that no search is needed after
+// the sort (the packed values keep the slots' order, so the sort's ties come out the same).
 template <typename K>
 __global__ void __launch_bounds__(FT) k_extract(DevBlock b, const int64_t* __restrict__ mask_anno,
                                                const int32_t* __restrict__ mask_data, int kmer, K* keys, uint32_t* vals,
-                                               int64_t nslots, uint32_t* nmasked)
+                                               int64_t nslots, uint32_t* nmasked, int pbits)
 {
-    int64_t s = (int64_t)blockIdx.x * FT + threadIdx.x;
-    bool masked = false;
-    if (s < nslots)
+    const int64_t s0 = ((int64_t)blockIdx.x * FT + threadIdx.x) * 4;
+    unsigned nm = 0;
+    if (s0 < nslots)
     {
-        int r = read_of_slot(b, s, kmer);
-        int rpos = (int)(s - kstart_of(b, r, kmer)) + kmer - 1;
-        int p0 = rpos - kmer + 1;
-        if (mask_anno)
+        const K kmask = (2 * kmer >= (int)(8 * sizeof(K))) ? ~(K)0 : (((K)1 << (2 * kmer)) - 1);
+        int r = read_of_slot(b, s0, kmer);
+        int64_t kst = kstart_of(b, r, kmer), knext = kstart_of(b, r + 1, kmer);
+        K kv[4], code = 0;
+        uint32_t vv[4];
+        int have = -2;  // first position whose code is in `code`
+        const int nj = (int)min((int64_t)4, nslots - s0);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
         {
-            // the segment of unmasked bases containing p0 must also contain rpos
-            // (segments [0,b0) [e0,b1) ... [e_last,rlen), tuple_thread's loop :428-457)
-            int64_t f0 = mask_anno[r], f1 = mask_anno[r + 1];
-            int q = b.rlen[r];
-            int p = 0;
-            for (int64_t a = f0; a < f1; a += 2)
+            if (j >= nj)
+                break;
+            const int64_t s = s0 + j;
+            while (s >= knext)
             {
-                int ib = mask_data[a], ie = mask_data[a + 1];
-                if (p0 < ib)
-                {
-                    q = ib;
-                    break;
-                }
-                p = ie;
-                q = b.rlen[r];
+                r++;
+                kst = knext;
+                knext = kstart_of(b, r + 1, kmer);
+                have = -2;
             }
-            masked = !(p0 >= p && rpos < q);
+            const int p0 = (int)(s - kst);
+            const int rpos = p0 + kmer - 1;
+            const uint8_t* src = b.bases + b.boff[r];
+            if (have == p0 - 1)
+                code = ((code << 2) | (K)src[rpos]) & kmask;
+            else
+            {
+                code = 0;
+                for (int t = 0; t < kmer; t++)
+                    code = (code << 2) | (K)src[p0 + t];
+            }
+            have = p0;
+            bool masked = false;
+            if (mask_anno)
+            {
+                // the segment of unmasked bases containing p0 must also contain rpos
+                // (segments [0,b0) [e0,b1) ... [e_last,rlen), tuple_thread's loop :428-457)
+                int64_t f0 = mask_anno[r], f1 = mask_anno[r + 1];
+                int q = b.rlen[r];
+                int p = 0;
+                for (int64_t a = f0; a < f1; a += 2)
+                {
+                    int ib = mask_data[a], ie = mask_data[a + 1];
+                    if (p0 < ib)
+                    {
+                        q = ib;
+                        break;
+                    }
+                    p = ie;
+                    q = b.rlen[r];
+                }
+                masked = !(p0 >= p && rpos < q);
+            }
+            nm += masked;
+            kv[j] = masked ? (K)~(K)0 : code;
+            vv[j] = pbits >= 0 ? ((uint32_t)r << pbits) | (uint32_t)p0 : (uint32_t)s;
         }
-        const uint8_t* src = b.bases + b.boff[r] + p0;
-        K c = 0;
-        for (int j = 0; j < kmer; j++)
-            c = (c << 2) | (K)src[j];
-        keys[s] = masked ? (K)~(K)0 : c;
-        vals[s] = (uint32_t)s;
+        if (nj == 4)
+        {
+            if (sizeof(K) == 4)
+                *reinterpret_cast<uint4*>(keys + s0) = make_uint4((uint32_t)kv[0], (uint32_t)kv[1], (uint32_t)kv[2],
+                                                                  (uint32_t)kv[3]);
+            else
+            {
+                *reinterpret_cast<ulonglong2*>(keys + s0) = make_ulonglong2((unsigned long long)kv[0],
+                                                                            (unsigned long long)kv[1]);
+                *reinterpret_cast<ulonglong2*>(keys + s0 + 2) = make_ulonglong2((unsigned long long)kv[2],
+                                                                                (unsigned long long)kv[3]);
+            }
+            *reinterpret_cast<uint4*>(vals + s0) = make_uint4(vv[0], vv[1], vv[2], vv[3]);
+        }
+        else
+            for (int j = 0; j < nj; j++)
+            {
+                keys[s0 + j] = kv[j];
+                vals[s0 + j] = vv[j];
+            }
     }
-    unsigned m = __ballot_sync(GD_FULL, masked);
-    if (m && lane_id() == 0)
-        atomicAdd(nmasked, (unsigned)__popc(m));
+    for (int o = 16; o; o >>= 1)
+        nm += __shfl_xor_sync(GD_FULL, nm, o);
+    if (nm && lane_id() == 0)
+        atomicAdd(nmasked, nm);
 }
 
 template <typename K>
 int launch_extract(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, int kmer, K* keys,
-                   uint32_t* vals, int64_t nslots, uint32_t* nmasked, cudaStream_t s)
+                   uint32_t* vals, int64_t nslots, uint32_t* nmasked, int pbits, cudaStream_t s)
 {
     GD_CUDA(cudaMemsetAsync(nmasked, 0, sizeof(uint32_t), s));
     if (nslots <= 0)
         return 0;
-    k_extract<K><<<(unsigned)gd_cdiv<int64_t>(nslots, FT), FT, 0, s>>>(b, mask_anno, mask_data, kmer, keys, vals,
-                                                                        nslots, nmasked);
+    const int64_t threads = (nslots + 3) / 4;
+    k_extract<K><<<(unsigned)gd_cdiv<int64_t>(threads, FT), FT, 0, s>>>(b, mask_anno, mask_data, kmer, keys, vals,
+                                                                         nslots, nmasked, pbits);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// code/read/rpos of the sorted index from packed values (read << pbits | first position)
+template <typename K>
+__global__ void __launch_bounds__(FT) k_unpack(const K* __restrict__ skeys, const uint32_t* __restrict__ svals,
+                                              int64_t n, int pbits, int kmer, K* __restrict__ code,
+                                              int32_t* __restrict__ read, int32_t* __restrict__ rpos)
+{
+    const int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t v = svals[i];
+    code[i] = skeys[i];
+    read[i] = (int32_t)(v >> pbits);
+    rpos[i] = (int32_t)(v & ((1u << pbits) - 1u)) + kmer - 1;
+}
+
+template <typename K>
+int launch_unpack(const K* skeys, const uint32_t* svals, int64_t n, int pbits, int kmer, K* code, int32_t* read,
+                  int32_t* rpos, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_unpack<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(skeys, svals, n, pbits, kmer, code, read, rpos);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
@@ -582,7 +663,9 @@ int launch_complement(const DevBlock& src, uint8_t* dst_bases, const int64_t* an
 
 #define INST(K)                                                                                                  \
     template int launch_extract<K>(const DevBlock&, const int64_t*, const int32_t*, int, K*, uint32_t*, int64_t, \
-                                   uint32_t*, cudaStream_t);                                                     \
+                                   uint32_t*, int, cudaStream_t);                                                \
+    template int launch_unpack<K>(const K*, const uint32_t*, int64_t, int, int, K*, int32_t*, int32_t*,          \
+                                  cudaStream_t);                                                                 \
     template int launch_decode<K>(const DevBlock&, int, const uint32_t*, int64_t, int32_t*, int32_t*,            \
                                   cudaStream_t);                                                                 \
     template int launch_suppress_flags<K>(const K*, int64_t, int, uint32_t*, cudaStream_t);                      \

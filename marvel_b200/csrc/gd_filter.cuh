@@ -10,9 +10,16 @@ constexpr int MAXGRAM = 10000;  // cap on per-code pair counts (dalign/filter.c:
 // k-mer slots: read r owns slots [kstart[r], kstart[r+1]) with kstart[r] = boff[r] - K*r,
 // slot s of read r ends at rpos = s - kstart[r] + K - 1 (the tuple_thread layout,
 // dalign/filter.c:410-425).
+// keys (code, or all ones where masked) and values (slot index, or with pbits >= 0 the
+// packed read << pbits | first position) of every slot
 template <typename K>
 int launch_extract(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, int kmer, K* keys,
-                   uint32_t* vals, int64_t nslots, uint32_t* nmasked, cudaStream_t s);
+                   uint32_t* vals, int64_t nslots, uint32_t* nmasked, int pbits, cudaStream_t s);
+
+// the index arrays from sorted keys and packed values
+template <typename K>
+int launch_unpack(const K* skeys, const uint32_t* svals, int64_t n, int pbits, int kmer, K* code, int32_t* read,
+                  int32_t* rpos, cudaStream_t s);
 
 template <typename K>
 int launch_decode(const DevBlock& b, int kmer, const uint32_t* slots, int64_t n, int32_t* read, int32_t* rpos,

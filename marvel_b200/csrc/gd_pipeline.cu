@@ -268,9 +268,12 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
         ensure(c->v1, nslots * 4) || ensure(c->scratch, radix_scratch_bytes(nslots)) || ensure(c->misc, 64))
         return -1;
     uint32_t* nmasked = P<uint32_t>(c->misc);
+    // sort values carry (read, first position) when both fit in 32 bits, else the slot index
+    const int pb = bits_for(std::max(sl.blk.maxlen - Kmer, 1));
+    const int pbits = (bits_for(std::max(sl.blk.nreads - 1, 1)) + pb <= 32) ? pb : -1;
     if (launch_extract<K>(sl.blk, sl.has_mask ? P<int64_t>(sl.manno) : nullptr,
                           sl.has_mask ? P<int32_t>(sl.mdata) : nullptr, Kmer, P<K>(c->k0), P<uint32_t>(c->v0), nslots,
-                          nmasked, s))
+                          nmasked, pbits, s))
         return -1;
     int sort_bits = 8 * ((2 * Kmer + 7) / 8);  // mersort bytes (filter.c:713-716)
     if (sort_bits > (int)(8 * sizeof(K)))
@@ -287,9 +290,17 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
     int64_t n = nslots - hmask;
     if (ensure(sl.code, (n + 1) * sizeof(K)) || ensure(sl.read, (n + 1) * 4) || ensure(sl.rpos, (n + 1) * 4))
         return -1;
-    GD_CUDA(cudaMemcpyAsync(sl.code.p, skeys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
-    if (launch_decode<K>(sl.blk, Kmer, svals, n, P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
-        return -1;
+    if (pbits >= 0)
+    {
+        if (launch_unpack<K>(skeys, svals, n, pbits, Kmer, P<K>(sl.code), P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
+            return -1;
+    }
+    else
+    {
+        GD_CUDA(cudaMemcpyAsync(sl.code.p, skeys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+        if (launch_decode<K>(sl.blk, Kmer, svals, n, P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
+            return -1;
+    }
     if (c->suppress > 0 && n > 0)
     {
         // -t: drop codes occurring >= t times (compsize/compress_thread, filter.c:645-696)

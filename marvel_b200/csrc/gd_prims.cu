@@ -162,24 +162,56 @@ template <typename K>
 __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ keys, int64_t n, int shift,
                                                        uint32_t* counts, int ntiles)
 {
-    __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0;
+    // one histogram per warp, plain shared-memory atomics; full tiles of 16-byte aligned keys
+    // are read as 16-byte vectors
+    __shared__ uint32_t h[RS_WARPS][256];
+    const int w = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < RS_WARPS; i++)
+        h[i][threadIdx.x] = 0;
     __syncthreads();
-    int64_t base = (int64_t)blockIdx.x * RS_TILE;
-#pragma unroll 4
-    for (int i = 0; i < RS_ROUNDS; i++)
+    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+    constexpr int PER = 16 / sizeof(K);  // keys per vector
+    if (base + RS_TILE <= n && ((uintptr_t)keys & 15) == 0)
     {
-        int64_t idx = base + i * RS_THREADS + threadIdx.x;
-        if (idx < n)
+        const uint4* v = reinterpret_cast<const uint4*>(keys + base);
+        uint4 x[RS_TILE / PER / RS_THREADS];
+#pragma unroll
+        for (int i = 0; i < RS_TILE / PER / RS_THREADS; i++)
+            x[i] = v[i * RS_THREADS + threadIdx.x];
+#pragma unroll
+        for (int i = 0; i < RS_TILE / PER / RS_THREADS; i++)
         {
-            unsigned d = (unsigned)(keys[idx] >> shift) & 255u;
-            unsigned peers = __match_any_sync(__activemask(), d);
-            if ((peers & lanemask_lt()) == 0)
-                atomicAdd(&h[d], (unsigned)__popc(peers));
+            if (sizeof(K) == 4)
+            {
+                atomicAdd(&h[w][(x[i].x >> shift) & 255u], 1u);
+                atomicAdd(&h[w][(x[i].y >> shift) & 255u], 1u);
+                atomicAdd(&h[w][(x[i].z >> shift) & 255u], 1u);
+                atomicAdd(&h[w][(x[i].w >> shift) & 255u], 1u);
+            }
+            else
+            {
+                const uint64_t k0 = ((uint64_t)x[i].y << 32) | x[i].x, k1 = ((uint64_t)x[i].w << 32) | x[i].z;
+                atomicAdd(&h[w][(unsigned)(k0 >> shift) & 255u], 1u);
+                atomicAdd(&h[w][(unsigned)(k1 >> shift) & 255u], 1u);
+            }
+        }
+    }
+    else
+    {
+        for (int i = 0; i < RS_ROUNDS; i++)
+        {
+            int64_t idx = base + i * RS_THREADS + threadIdx.x;
+            if (idx < n)
+                atomicAdd(&h[w][(unsigned)(keys[idx] >> shift) & 255u], 1u);
         }
     }
     __syncthreads();
-    counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+    uint32_t t = 0;
+#pragma unroll
+    for (int i = 0; i < RS_WARPS; i++)
+        t += h[i][threadIdx.x];
+    counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = t;
 }
 
 // Shared memory of one scatter tile: the tile's items re-ordered by digit (stable), the
