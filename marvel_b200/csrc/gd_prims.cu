@@ -1,6 +1,8 @@
 // gd_prims.cu -- exclusive scan and stable LSD radix sort (see gd_prims.cuh).
 #include "gd_prims.cuh"
 
+#include <algorithm>
+
 namespace gd
 {
 
@@ -330,6 +332,247 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// pipelined scatter: a persistent CTA streams its tiles' keys and values into shared memory
+// with bulk asynchronous copies (two stages, one mbarrier each), so the next tile arrives
+// while this one is ranked, re-ordered in place and written out.  Same ranking as
+// k_rs_scatter, so the same (stable) order.
+// ---------------------------------------------------------------------------------------
+
+__device__ int g_rs_wait_failed;  // set when a stage's copy did not complete within the wait limit
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the phase with the given parity; false if the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity)
+{
+    const uint32_t a = smem_addr(bar);
+    for (int it = 0; it < (1 << 22); it++)
+    {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
+// global -> this CTA's shared memory; both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+template <typename K>
+struct RsPipe
+{
+    K key[2][RS_TILE];
+    uint32_t val[2][RS_TILE];
+    uint32_t wcnt[RS_WARPS][256];
+    uint32_t lstart[256];
+    uint32_t toff[256];
+    uint32_t wsum[RS_WARPS];
+    uint64_t full[2];
+};
+
+template <typename K>
+constexpr int rs_pipe_ctas()
+{
+    return sizeof(K) == 4 ? 3 : 2;
+}
+
+// Full tiles (all but possibly the last) arrive by bulk copy; a ragged last tile is read
+// with plain loads.  Requires 16-byte aligned kin and vin.
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
+    k_rs_scatter_pipe(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
+                      uint32_t* __restrict__ vout, int64_t n, int shift, const uint32_t* __restrict__ offs, int ntiles)
+{
+    extern __shared__ __align__(128) unsigned char rs_smem[];
+    RsPipe<K>& S = *reinterpret_cast<RsPipe<K>*>(rs_smem);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nfull = (int)(n / RS_TILE);
+    constexpr unsigned TILE_BYTES = RS_TILE * (sizeof(K) + sizeof(uint32_t));
+    if (threadIdx.x == 0)
+    {
+        mbar_init(&S.full[0], 1);
+        mbar_init(&S.full[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int tile = blockIdx.x;
+    if (threadIdx.x == 0 && tile < nfull)
+    {
+        mbar_expect_tx(&S.full[0], TILE_BYTES);
+        bulk_load(S.key[0], kin + (int64_t)tile * RS_TILE, RS_TILE * sizeof(K), &S.full[0]);
+        bulk_load(S.val[0], vin + (int64_t)tile * RS_TILE, RS_TILE * 4, &S.full[0]);
+    }
+    uint32_t toff = tile < ntiles ? offs[(int64_t)threadIdx.x * ntiles + tile] : 0;
+    unsigned parity = 0;  // bit st: phase of stage st's barrier
+    const unsigned lt = lanemask_lt();
+    for (int st = 0; tile < ntiles; tile += gridDim.x, st ^= 1)
+    {
+        const int next = tile + gridDim.x;
+        // the other stage was released by the barrier that ended the previous tile
+        if (threadIdx.x == 0 && next < nfull)
+        {
+            mbar_expect_tx(&S.full[st ^ 1], TILE_BYTES);
+            bulk_load(S.key[st ^ 1], kin + (int64_t)next * RS_TILE, RS_TILE * sizeof(K), &S.full[st ^ 1]);
+            bulk_load(S.val[st ^ 1], vin + (int64_t)next * RS_TILE, RS_TILE * 4, &S.full[st ^ 1]);
+        }
+        const uint32_t toff_next = next < ntiles ? offs[(int64_t)threadIdx.x * ntiles + next] : 0;
+        S.toff[threadIdx.x] = toff;
+#pragma unroll
+        for (int i = 0; i < RS_WARPS; i++)
+            S.wcnt[i][threadIdx.x] = 0;
+        const int64_t tbase = (int64_t)tile * RS_TILE;
+        const int tn = (int)min((int64_t)RS_TILE, n - tbase);
+        K* skey = S.key[st];
+        uint32_t* sval = S.val[st];
+        bool ok = true;
+        if (tile < nfull)
+        {
+            ok = mbar_wait(&S.full[st], (parity >> st) & 1u);
+            parity ^= 1u << st;
+        }
+        else
+            for (int i = threadIdx.x; i < tn; i += RS_THREADS)
+            {
+                skey[i] = kin[tbase + i];
+                sval[i] = vin[tbase + i];
+            }
+        if (__syncthreads_or(!ok))
+        {
+            // all threads leave; wait (bounded) for the copies still in flight first
+            if (threadIdx.x == 0)
+                atomicExch(&g_rs_wait_failed, 1);
+            if (ok == false)
+                mbar_wait(&S.full[st], ((parity >> st) & 1u) ^ 1u);
+            if (next < nfull)
+                mbar_wait(&S.full[st ^ 1], (parity >> (st ^ 1)) & 1u);
+            return;
+        }
+
+        K key[RS_ROUNDS];
+        uint32_t val[RS_ROUNDS];
+        uint32_t rank2[RS_ROUNDS / 2];  // two 16-bit ranks per register (a rank is < RS_TILE)
+#pragma unroll
+        for (int r = 0; r < RS_ROUNDS; r++)
+        {
+            const int i = w * (RS_ROUNDS * 32) + r * 32 + lane;
+            const bool valid = i < tn;
+            key[r] = valid ? skey[i] : (K)0;
+            val[r] = valid ? sval[i] : 0u;
+            unsigned d = valid ? (unsigned)(key[r] >> shift) & 255u : 256u;
+            unsigned peers = __match_any_sync(GD_FULL, d);
+            unsigned c = valid ? S.wcnt[w][d] : 0;
+            const uint32_t rk = c + __popc(peers & lt);
+            if (r & 1)
+                rank2[r >> 1] |= rk << 16;
+            else
+                rank2[r >> 1] = rk;
+            __syncwarp();
+            if (valid && (peers & lt) == 0)
+                S.wcnt[w][d] = c + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        uint32_t tot = 0;
+#pragma unroll
+        for (int i = 0; i < RS_WARPS; i++)
+        {
+            uint32_t t = S.wcnt[i][threadIdx.x];
+            S.wcnt[i][threadIdx.x] = tot;
+            tot += t;
+        }
+        {
+            uint32_t x = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                uint32_t t = __shfl_up_sync(GD_FULL, x, o);
+                if (lane >= o)
+                    x += t;
+            }
+            if (lane == 31)
+                S.wsum[w] = x;
+            __syncthreads();
+            uint32_t wo = 0;
+#pragma unroll
+            for (int i = 0; i < RS_WARPS; i++)
+                wo += i < w ? S.wsum[i] : 0;
+            S.lstart[threadIdx.x] = wo + x - tot;
+        }
+        __syncthreads();
+        // the stage's tile is in registers: re-order it in place
+#pragma unroll
+        for (int r = 0; r < RS_ROUNDS; r++)
+        {
+            const int i = w * (RS_ROUNDS * 32) + r * 32 + lane;
+            if (i < tn)
+            {
+                unsigned d = (unsigned)(key[r] >> shift) & 255u;
+                uint32_t pos = S.lstart[d] + S.wcnt[w][d] + ((rank2[r >> 1] >> (16 * (r & 1))) & 0xffffu);
+                skey[pos] = key[r];
+                sval[pos] = val[r];
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < tn; i += RS_THREADS)
+        {
+            K k = skey[i];
+            unsigned d = (unsigned)(k >> shift) & 255u;
+            uint32_t dest = S.toff[d] + (uint32_t)i - S.lstart[d];
+            kout[dest] = k;
+            vout[dest] = sval[i];
+        }
+        // this stage is refilled by the bulk copy engine two tiles on: order these generic
+        // accesses before it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        toff = toff_next;
+    }
+}
+
+int radix_sort_wait_check(cudaStream_t s)
+{
+    int h = 0;
+    GD_CUDA(cudaMemcpyFromSymbolAsync(&h, g_rs_wait_failed, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    if (h)
+    {
+        int z = 0;
+        GD_CUDA(cudaMemcpyToSymbolAsync(g_rs_wait_failed, &z, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+        GD_CUDA(cudaStreamSynchronize(s));
+        gd_set_error("radix sort: a tile copy did not complete within the wait limit");
+        return -1;
+    }
+    return 0;
+}
+
 template <typename K>
 int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int begin_bit, int end_bit, void* scratch,
                      cudaStream_t s)
@@ -343,13 +586,23 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
         return -1;
     }
     int ntiles = (int)tiles64;
-    static bool smem_set = false;
-    if (!smem_set)
+    static int pipe_grid = 0;
+    if (!pipe_grid)
     {
         GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(RsTile<K>)));
-        smem_set = true;
+        GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter_pipe<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(RsPipe<K>)));
+        int dev = 0, sms = 0, per = 0;
+        GD_CUDA(cudaGetDevice(&dev));
+        GD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rs_scatter_pipe<K>, RS_THREADS,
+                                                              sizeof(RsPipe<K>)));
+        pipe_grid = sms * std::max(per, 1);
     }
+    // the bulk copies need 16-byte aligned sources (tile starts are then aligned too)
+    const bool pipe = ((uintptr_t)k0 & 15) == 0 && ((uintptr_t)k1 & 15) == 0 && ((uintptr_t)v0 & 15) == 0 &&
+                      ((uintptr_t)v1 & 15) == 0;
     int64_t ncnt = (int64_t)ntiles * 256;
     uint32_t* counts = (uint32_t*)scratch;
     void* sscr = (void*)(((uintptr_t)(counts + ncnt) + 255) & ~(uintptr_t)255);
@@ -364,11 +617,17 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
         GD_LAUNCHED(1);
         if (exclusive_scan<uint32_t>(counts, counts, ncnt, (uint32_t*)nullptr, sscr, s))
             return -1;
-        k_rs_scatter<K><<<ntiles, RS_THREADS, sizeof(RsTile<K>), s>>>(kin, vin, kout, vout, n, b, counts, ntiles);
+        if (pipe)
+            k_rs_scatter_pipe<K><<<std::min(ntiles, pipe_grid), RS_THREADS, sizeof(RsPipe<K>), s>>>(
+                kin, vin, kout, vout, n, b, counts, ntiles);
+        else
+            k_rs_scatter<K><<<ntiles, RS_THREADS, sizeof(RsTile<K>), s>>>(kin, vin, kout, vout, n, b, counts, ntiles);
         GD_LAUNCHED(1);
         cur ^= 1;
     }
     GD_CUDA(cudaGetLastError());
+    if (pipe && radix_sort_wait_check(s))
+        return -1;
     return cur;
 }
 
