@@ -1496,8 +1496,9 @@ static void tbuf_reserve(TBuf* t, int64_t extra)
     }
 }
 
-/* Entwine (filter.c:1249-1342) */
-static int entwine(MPath* jpath, MPath* kpath, TBuf* tb, int TS, int* where)
+/* Entwine (filter.c:1249-1342).  d2: daligner2's version (dalign2/filter.c:1707-1825),
+ * which also compares the B coordinates at a common start and a common end point. */
+static int entwine(MPath* jpath, MPath* kpath, TBuf* tb, int TS, int* where, int d2)
 {
     int ac, b2, y2, ae, i, j, k, num = 0, den = 0, min = 10000;
     uint16_t* ktrace = tb->tr + kpath->toff;
@@ -1506,6 +1507,12 @@ static int entwine(MPath* jpath, MPath* kpath, TBuf* tb, int TS, int* where)
     j = jpath->abpos / TS;
     b2 = kpath->bbpos;
     k = kpath->abpos / TS;
+    if (d2 && jpath->abpos == kpath->abpos)
+    {
+        min = abs(y2 - b2);
+        if (min == 0)
+            *where = kpath->abpos;
+    }
     if (j < k)
     {
         ac = k * TS;
@@ -1543,6 +1550,16 @@ static int entwine(MPath* jpath, MPath* kpath, TBuf* tb, int TS, int* where)
         }
         num += i;
         den += 1;
+    }
+    if (d2 && jpath->aepos == kpath->aepos)
+    {
+        i = abs(jpath->bepos - kpath->bepos);
+        if (i <= min)
+        {
+            min = i;
+            if (i == 0)
+                *where = kpath->aepos;
+        }
     }
     return den == 0 ? -1 : min;
 }
@@ -1600,7 +1617,7 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
             {
                 if (kpath->abpos <= jpath->aepos && kpath->bbpos <= jpath->bepos)
                 {
-                    dist = entwine(jpath, kpath, tb, TS, &awhen);
+                    dist = entwine(jpath, kpath, tb, TS, &awhen, 0);
                     if (dist == 0)
                     {
                         if (kpath->aepos > jpath->aepos)
@@ -1609,7 +1626,7 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
                             {
                                 if (comp)
                                 {
-                                    dist = entwine(bmatch + k, bmatch + j, tb, TS, &bwhen);
+                                    dist = entwine(bmatch + k, bmatch + j, tb, TS, &bwhen, 0);
                                     if (dist != 0)
                                         continue;
                                     fusion(jpath, awhen, kpath, tb, TS);
@@ -1618,7 +1635,7 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
                                 }
                                 else
                                 {
-                                    dist = entwine(bmatch + j, bmatch + k, tb, TS, &bwhen);
+                                    dist = entwine(bmatch + j, bmatch + k, tb, TS, &bwhen, 0);
                                     if (dist != 0)
                                         continue;
                                     fusion(jpath, awhen, kpath, tb, TS);
@@ -1647,7 +1664,7 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
             {
                 if (jpath->abpos <= kpath->aepos && jpath->bbpos <= kpath->bepos)
                 {
-                    dist = entwine(kpath, jpath, tb, TS, &awhen);
+                    dist = entwine(kpath, jpath, tb, TS, &awhen, 0);
                     if (dist == 0)
                     {
                         if (kpath->abpos == jpath->abpos)
@@ -1665,7 +1682,7 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
                             {
                                 if (comp)
                                 {
-                                    dist = entwine(bmatch + j, bmatch + k, tb, TS, &bwhen);
+                                    dist = entwine(bmatch + j, bmatch + k, tb, TS, &bwhen, 0);
                                     if (dist != 0)
                                         continue;
                                     fusion(kpath, awhen, jpath, tb, TS);
@@ -1674,7 +1691,7 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
                                 }
                                 else
                                 {
-                                    dist = entwine(bmatch + k, bmatch + j, tb, TS, &bwhen);
+                                    dist = entwine(bmatch + k, bmatch + j, tb, TS, &bwhen, 0);
                                     if (dist != 0)
                                         continue;
                                     fusion(kpath, awhen, jpath, tb, TS);
@@ -1698,6 +1715,182 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
         }
     }
     return no + 1;
+}
+
+/* daligner2's Handle_Redundancies (dalign2/filter.c:1952-2272): paths fused into the later
+ * index j, the absorbed one marked with abpos = -1 and the scan restarted after a fusion,
+ * then compacted.  Its bridging pass (:2124-2262, Compute_Bridge_Path / Bridge) is detected,
+ * not computed: returns -1 when a pair of paths would be bridged. */
+static int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, TBuf* tb, int TS, int comp)
+{
+    int j, k, no, dist, awhen = 0, bwhen = 0;
+    int hasB = (bmatch != NULL);
+    for (j = 1; j < novls; j++)
+    {
+        MPath* jpath = amatch + j;
+        for (k = j - 1; k >= 0; k--)
+        {
+            MPath* kpath = amatch + k;
+            if (kpath->abpos < 0)
+                continue;
+            if (jpath->abpos < kpath->abpos)
+            {
+                if (kpath->abpos <= jpath->aepos && kpath->bbpos <= jpath->bepos)
+                {
+                    dist = entwine(jpath, kpath, tb, TS, &awhen, 1);
+                    if (dist == 0)
+                    {
+                        if (kpath->aepos > jpath->aepos)
+                        {
+                            if (hasB)
+                            {
+                                if (comp)
+                                {
+                                    dist = entwine(bmatch + k, bmatch + j, tb, TS, &bwhen, 1);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(jpath, awhen, kpath, tb, TS);
+                                    fusion(bmatch + k, bwhen, bmatch + j, tb, TS);
+                                    bmatch[j] = bmatch[k];
+                                }
+                                else
+                                {
+                                    dist = entwine(bmatch + j, bmatch + k, tb, TS, &bwhen, 1);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(jpath, awhen, kpath, tb, TS);
+                                    fusion(bmatch + j, bwhen, bmatch + k, tb, TS);
+                                }
+                            }
+                            else
+                                fusion(jpath, awhen, kpath, tb, TS);
+                            kpath->abpos = -1;
+                            k = j;
+                            continue;
+                        }
+                        kpath->abpos = -1;
+                    }
+                }
+            }
+            else
+            {
+                if (jpath->abpos <= kpath->aepos && jpath->bbpos <= kpath->bepos)
+                {
+                    dist = entwine(kpath, jpath, tb, TS, &awhen, 1);
+                    if (dist == 0)
+                    {
+                        int restart = 0;
+                        if (kpath->abpos == jpath->abpos)
+                        {
+                            if (kpath->aepos > jpath->aepos)
+                            {
+                                *jpath = *kpath;
+                                if (hasB)
+                                    bmatch[j] = bmatch[k];
+                            }
+                        }
+                        else if (jpath->aepos > kpath->aepos)
+                        {
+                            if (hasB)
+                            {
+                                if (comp)
+                                {
+                                    dist = entwine(bmatch + j, bmatch + k, tb, TS, &bwhen, 1);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(kpath, awhen, jpath, tb, TS);
+                                    *jpath = *kpath;
+                                    fusion(bmatch + j, bwhen, bmatch + k, tb, TS);
+                                }
+                                else
+                                {
+                                    dist = entwine(bmatch + k, bmatch + j, tb, TS, &bwhen, 1);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(kpath, awhen, jpath, tb, TS);
+                                    *jpath = *kpath;
+                                    fusion(bmatch + k, bwhen, bmatch + j, tb, TS);
+                                    bmatch[j] = bmatch[k];
+                                }
+                            }
+                            else
+                            {
+                                fusion(kpath, awhen, jpath, tb, TS);
+                                *jpath = *kpath;
+                            }
+                            restart = 1;
+                        }
+                        else
+                        {
+                            *jpath = *kpath;
+                            if (hasB)
+                                bmatch[j] = bmatch[k];
+                        }
+                        kpath->abpos = -1;
+                        if (restart)
+                            k = j;
+                    }
+                }
+            }
+        }
+    }
+    /* the bridging pass's entry test (dalign2/filter.c:2126-2175) */
+    for (j = 1; j < novls; j++)
+    {
+        MPath* jpath = amatch + j;
+        if (jpath->abpos < 0)
+            continue;
+        for (k = j - 1; k >= 0; k--)
+        {
+            MPath* kpath = amatch + k;
+            if (kpath->abpos < 0)
+                continue;
+            MPath *path1, *path2;
+            if (jpath->abpos < kpath->abpos)
+            {
+                path1 = jpath;
+                path2 = kpath;
+            }
+            else
+            {
+                path1 = kpath;
+                path2 = jpath;
+            }
+            if (path2->abpos >= path1->aepos || path1->aepos >= path2->aepos || path1->bbpos >= path2->bbpos ||
+                path2->bbpos >= path1->bepos || path1->bepos >= path2->bepos)
+                continue;
+            int aovl = path1->aepos - path2->abpos;
+            int bovl = path1->bepos - path2->bbpos;
+            if (abs(aovl - bovl) > .2 * (aovl + bovl))
+                continue;
+            if (hasB)
+            {
+                MPath *bath1, *bath2;
+                if (comp == (jpath->abpos < kpath->abpos))
+                {
+                    bath1 = bmatch + k;
+                    bath2 = bmatch + j;
+                }
+                else
+                {
+                    bath1 = bmatch + j;
+                    bath2 = bmatch + k;
+                }
+                if (bath1->abpos > bath2->abpos)
+                    continue;
+            }
+            return -1;
+        }
+    }
+    no = 0;
+    for (j = 0; j < novls; j++)
+        if (amatch[j].abpos >= 0)
+        {
+            if (hasB)
+                bmatch[no] = bmatch[j];
+            amatch[no++] = amatch[j];
+        }
+    return no;
 }
 
 /* Diagonal_Span (filter.c:1568-1599) */
@@ -1770,9 +1963,14 @@ static void obuf_add(OBuf* ob, const MPath* mp, const uint16_t* trace, uint32_t 
 }
 
 /* report_thread (filter.c:1617-1989) over the whole sorted hit list */
+/* p->variant == 2: daligner2's report_thread (dalign2/filter_reporter_cpu.c:16-411): the last
+ * group of the list is scanned too (nidx <= eidx), -H is live, the B-side record of a read
+ * against itself is dropped in both orientations, its Handle_Redundancies, and the 8-bit
+ * trace compression checked.  *status receives the daligner2 failure codes of or_result. */
 static void report(const or_block* A, const or_block* B, const Hit* hits, int64_t nhits, const or_params* p,
-                   const Spec* sp, Work* w, int self, int comp, OBuf* ob, int64_t* nseed)
+                   const Spec* sp, Work* w, int self, int comp, OBuf* ob, int64_t* nseed, int32_t* status)
 {
+    const int d2 = p->variant == 2;
     const int K = p->kmer, BS = p->binshift, TS = sp->tspace;
     int maxdiag = (A->maxlen >> BS);
     int mindiag = ((-B->maxlen) >> BS);
@@ -1784,7 +1982,8 @@ static void report(const or_block* A, const or_block* B, const Hit* hits, int64_
     int* lastp = score + wdt;
     int* lasta = lastp + wdt;
     int minhit = (p->hitmin - 1) / K + 1;
-    int HGAP_MIN = 0; /* -H is a no-op: main() shadows the global (daligner.c:63 vs 641) */
+    /* daligner: -H is a no-op, main() shadows the global (daligner.c:63 vs 641) */
+    int HGAP_MIN = d2 ? p->hgap : 0;
     int64_t AOmax = 100, BOmax = 100;
     MPath* amatch = (MPath*)malloc(sizeof(MPath) * AOmax);
     MPath* bmatch = (MPath*)malloc(sizeof(MPath) * BOmax);
@@ -1796,7 +1995,7 @@ static void report(const or_block* A, const or_block* B, const Hit* hits, int64_
 #define PAIR(i) (((u64)(uint32_t)hits[i].bread << 32) | (uint32_t)hits[i].aread)
     int64_t nidx = 0, eidx = nhits - minhit;
     u64 cpair, npair = 0;
-    for (cpair = PAIR(0); nidx < eidx; cpair = npair)
+    for (cpair = PAIR(0); d2 ? nidx <= eidx : nidx < eidx; cpair = npair)
     {
         if (PAIR(nidx + minhit - 1) != cpair)
         {
@@ -1854,7 +2053,10 @@ static void report(const or_block* A, const or_block* B, const Hit* hits, int64_
                     {
                         setaln = 0;
                         doA = (alen >= HGAP_MIN);
-                        doB = (p->symmetric && blen >= HGAP_MIN && (ar != br || !self || !comp));
+                        if (d2)
+                            doB = (p->symmetric && blen >= HGAP_MIN && !(ar == br && self));
+                        else
+                            doB = (p->symmetric && blen >= HGAP_MIN && (ar != br || !self || !comp));
                     }
                     nfilt += 1;
                     local_alignment(w, sp, aseq, bseq, alen, blen, comp, ap - bp, ap + bp, &apath, &bpath);
@@ -1932,7 +2134,42 @@ static void report(const or_block* A, const or_block* B, const Hit* hits, int64_
                 else
                     lasta[d2] = 0;
         }
-        if (novla > 1)
+        if (d2)
+        {
+            int r1 = novla, r2 = novlb;
+            if (novla > 1)
+            {
+                if (novlb > 1)
+                    r1 = r2 = handle_redundancies_d2(amatch, novla, bmatch, &tb, TS, comp);
+                else
+                    r1 = handle_redundancies_d2(amatch, novla, NULL, &tb, TS, comp);
+            }
+            else if (novlb > 1)
+                r2 = handle_redundancies_d2(bmatch, novlb, NULL, &tb, TS, comp);
+            if (r1 < 0 || r2 < 0)
+            {
+                *status = 1;
+                break;
+            }
+            novla = r1;
+            novlb = r2;
+            if (ob->tbytes == 1 && !p->no_trace)
+            {
+                int big = 0;
+                for (int i = 0; i < novla; i++)
+                    for (int t = 0; t < amatch[i].tlen; t++)
+                        big |= tb.tr[amatch[i].toff + t] > 255;
+                for (int i = 0; i < novlb; i++)
+                    for (int t = 0; t < bmatch[i].tlen; t++)
+                        big |= tb.tr[bmatch[i].toff + t] > 255;
+                if (big)
+                {
+                    *status = 2;
+                    break;
+                }
+            }
+        }
+        else if (novla > 1)
         {
             if (novlb > 1)
                 novla = novlb = handle_redundancies(amatch, novla, bmatch, &tb, TS, comp);
@@ -2001,7 +2238,7 @@ int or_daligner(const or_block* a, const or_block* b, const or_block* bc, const 
             Hit* h = sorted_hits(a, b, al, alen, bl, blen, p, self, 0, self, &nh, &limit);
             res->hits_n = nh;
             if (nh > 0)
-                report(a, b, h, nh, p, &sp, &w, self, 0, &ob, &res->seeds_n);
+                report(a, b, h, nh, p, &sp, &w, self, 0, &ob, &res->seeds_n, &res->status);
             free(h);
         }
         if (!self)
@@ -2013,7 +2250,7 @@ int or_daligner(const or_block* a, const or_block* b, const or_block* bc, const 
             Hit* h = sorted_hits(a, bc, al, alen, bl, blen, p, self, 1, 0, &nh, &limit);
             res->hits_c = nh;
             if (nh > 0)
-                report(a, bc, h, nh, p, &sp, &w, self, 1, &ob, &res->seeds_c);
+                report(a, bc, h, nh, p, &sp, &w, self, 1, &ob, &res->seeds_c, &res->status);
             free(h);
         }
         free(bl);
@@ -2042,6 +2279,348 @@ int or_daligner(const or_block* a, const or_block* b, const or_block* bc, const 
     free(w.cells);
     free(w.pts);
     return 0;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/*  daligner2 (dalign2/): modimizer index, one join for both orientations                */
+/* ------------------------------------------------------------------------------------ */
+
+#define D2_MODULUS 101
+#define D2_MODTHR 28
+
+/* The k-mer list (mask_thread/tuple_thread, dalign2/filter.c:147-769, MODIFER on): at every
+ * position p of an unmasked segment, after k-1 bases of warm-up, two codes: the canonical
+ * k-mer min(c, u) of the forward code c and the reverse-complement code u, and the
+ * "half-shifted" code min(d, v) whose high half comes from the previous code.  A code is
+ * listed when code % 101 < 28, with read = (i << 1) | (1 if the complement code won). */
+static int64_t extract_kmers2(const or_block* b, int K, KPos* list)
+{
+    const int Kshift = K >= 32 ? 64 : 2 * K;
+    const u64 Kmask = K >= 32 ? ~0ull : ((1ull << Kshift) - 1);
+    const u64 LFmask = (1ull << (Kshift / 2)) - 1, HFmask = Kmask - LFmask;
+    const u64 LRmask = (1ull << ((Kshift + 1) / 2)) - 1, HRmask = Kmask - LRmask;
+    u64 cumber[4];
+    for (int x = 0; x < 4; x++)
+        cumber[x] = (u64)(3 - x) << (Kshift - 2);
+    int64_t n = 0;
+    for (int i = 0; i < b->nreads; i++)
+    {
+        const uint8_t* s = b->bases + b->boff[i];
+        const int rlen = b->rlen[i], r = i << 1;
+        int64_t f0 = 0, f1 = 0;
+        if (b->mask_anno)
+        {
+            f0 = b->mask_anno[i];
+            f1 = b->mask_anno[i + 1];
+        }
+        for (int64_t a = f0; a <= f1; a += 2)
+        {
+            int p = (a == f0) ? 0 : b->mask_data[a - 1];
+            int q = (a == f1) ? rlen : b->mask_data[a];
+            if (q - p > K - 1)
+            {
+                u64 c = 0, u = 0, d, v;
+                for (int x = 1; x < K; x++)
+                {
+                    c = (c << 2) | s[p];
+                    u = (u >> 2) | cumber[s[p]];
+                    p++;
+                }
+                for (; p < q; p++)
+                {
+                    int x = s[p];
+                    d = c & HFmask;
+                    c = ((c << 2) | (u64)x) & Kmask;
+                    d |= c & LFmask;
+                    v = u & LRmask;
+                    u = (u >> 2) | cumber[x];
+                    v |= u & HRmask;
+                    if (u < c)
+                    {
+                        if (u % D2_MODULUS < D2_MODTHR)
+                        {
+                            list[n].code = u;
+                            list[n].read = r | 1;
+                            list[n++].rpos = p;
+                        }
+                    }
+                    else if (c % D2_MODULUS < D2_MODTHR)
+                    {
+                        list[n].code = c;
+                        list[n].read = r;
+                        list[n++].rpos = p;
+                    }
+                    if (v < d)
+                    {
+                        if (v % D2_MODULUS < D2_MODTHR)
+                        {
+                            list[n].code = v;
+                            list[n].read = r | 1;
+                            list[n++].rpos = p;
+                        }
+                    }
+                    else if (d % D2_MODULUS < D2_MODTHR)
+                    {
+                        list[n].code = d;
+                        list[n].read = r;
+                        list[n++].rpos = p;
+                    }
+                }
+            }
+            if (!b->mask_anno)
+                break;
+        }
+    }
+    return n;
+}
+
+/* Sort_Kmers (dalign2/filter.c:834-1106): stable radix sort on (k-1)/4+1 code bytes, -t */
+static KPos* build_index2(const or_block* b, const or_params* p, int64_t* len)
+{
+    int K = p->kmer;
+    KPos* list = (KPos*)malloc(sizeof(KPos) * (2 * (size_t)b->totlen + 2));
+    int64_t n = extract_kmers2(b, K, list);
+    sort_kpos(list, n, (K - 1) / 4 + 1);
+    if (p->suppress > 0 && n > 0)
+    {
+        int64_t w = 0, i = 0;
+        while (i < n)
+        {
+            int64_t j = i + 1;
+            while (j < n && list[j].code == list[i].code)
+                j++;
+            if (j - i < p->suppress)
+                for (int64_t q = i; q < j; q++)
+                    list[w++] = list[q];
+            i = j;
+        }
+        n = w;
+    }
+    list[n].code = ~0ull; /* MAX_CODE_64 sentinel (dalign2/filter.c:991) */
+    *len = n;
+    return list;
+}
+
+int64_t or_sort_kmers2(const or_block* b, const or_params* p, uint64_t* code, int32_t* read, int32_t* rpos)
+{
+    int64_t n;
+    KPos* l = build_index2(b, p, &n);
+    for (int64_t i = 0; i < n; i++)
+    {
+        code[i] = l[i].code;
+        read[i] = l[i].read;
+        rpos[i] = l[i].rpos;
+    }
+    free(l);
+    return n;
+}
+
+/* count_thread + the -M cap + merge_thread (dalign2/filter.c:1136-1466, 2401-2520).
+ * Within a block, entry ka of a code run pairs with the run's earlier entries of a smaller
+ * read (all earlier entries with -I); across blocks every A entry with every B entry.  A
+ * pair is a forward hit when both strands agree, else a complement hit whose B position is
+ * reflected (rlen - bpos + k - 2).  Hits of each orientation are returned in the
+ * reference's generation order. */
+static void merge_hits2(const or_block* B, const KPos* al, int64_t alen, const KPos* bl, int64_t blen,
+                        const or_params* p, int self, Hit** hf, int64_t* nf, Hit** hc, int64_t* nc,
+                        int* limit_out)
+{
+    const int Koff = p->kmer - 2;
+    int64_t hist[MAXGRAM];
+    memset(hist, 0, sizeof(hist));
+    int64_t total = 0;
+#define RUN_CT(ja, ia, jb, ib, ct)                                                \
+    do                                                                            \
+    {                                                                             \
+        ct = 0;                                                                   \
+        if (self)                                                                 \
+        {                                                                         \
+            for (int64_t ka = ja + 1; ka < ia; ka++)                              \
+                if (p->identity)                                                  \
+                    ct += ka - ja;                                                \
+                else                                                              \
+                {                                                                 \
+                    int64_t a = ja;                                               \
+                    while (a < ka && (al[a].read >> 1) < (al[ka].read >> 1))      \
+                        a++;                                                      \
+                    ct += a - ja;                                                 \
+                }                                                                 \
+        }                                                                         \
+        else                                                                      \
+            ct = (ia - ja) * (ib - jb);                                           \
+    } while (0)
+    /* pass 1: the histogram of per-code pair counts */
+    {
+        int64_t ia = 0, ib = 0;
+        while (ia < alen)
+        {
+            int64_t ja = ia;
+            u64 ca = al[ia].code;
+            while (ia < alen && al[ia].code == ca)
+                ia++;
+            int64_t jb = 0, ct;
+            if (!self)
+            {
+                while (ib < blen && bl[ib].code < ca)
+                    ib++;
+                if (ib >= blen || bl[ib].code != ca)
+                    continue;
+                jb = ib;
+                while (ib < blen && bl[ib].code == ca)
+                    ib++;
+            }
+            RUN_CT(ja, ia, jb, ib, ct);
+            total += ct;
+            if (ct < MAXGRAM)
+                hist[ct]++;
+        }
+    }
+    int limit = INT_MAX;
+    if (p->mem_limit > 0)
+    {
+        int64_t avail = (int64_t)(p->mem_limit / 16);
+        if (self || avail > alen + 2 * blen)
+            avail = (avail - alen) / 2;
+        else
+            avail = avail - (alen + blen);
+        avail = (int64_t)(avail * .98);
+        int64_t tom = 0;
+        int j;
+        for (j = 0; j < MAXGRAM; j++)
+        {
+            tom += j * hist[j];
+            if (tom > avail)
+                break;
+        }
+        limit = j;
+    }
+    *limit_out = limit;
+    /* pass 2: emission; sizes first */
+    int64_t cap = total + 1;
+    Hit* F = (Hit*)malloc(sizeof(Hit) * (cap + 1));
+    Hit* Cm = (Hit*)malloc(sizeof(Hit) * (cap + 1));
+    int64_t n1 = 0, n2 = 0;
+    int64_t ia = 0, ib = 0;
+    while (ia < alen)
+    {
+        int64_t ja = ia;
+        u64 ca = al[ia].code;
+        while (ia < alen && al[ia].code == ca)
+            ia++;
+        int64_t jb = 0, ct;
+        if (!self)
+        {
+            while (ib < blen && bl[ib].code < ca)
+                ib++;
+            if (ib >= blen || bl[ib].code != ca)
+                continue;
+            jb = ib;
+            while (ib < blen && bl[ib].code == ca)
+                ib++;
+        }
+        RUN_CT(ja, ia, jb, ib, ct);
+        if (ct >= limit)
+            continue;
+#define EMIT(A_, B_)                                                                 \
+    do                                                                               \
+    {                                                                                \
+        int ar = (A_).read >> 1, as = (A_).read & 1, ap = (A_).rpos;                 \
+        int br = (B_).read >> 1, bs = (B_).read & 1, bp = (B_).rpos;                 \
+        Hit* h;                                                                      \
+        if (bs == as)                                                                \
+            h = F + n1++;                                                            \
+        else                                                                         \
+        {                                                                            \
+            bp = (B->rlen[br] - bp) + Koff;                                          \
+            h = Cm + n2++;                                                           \
+        }                                                                            \
+        h->aread = ar;                                                               \
+        h->bread = br;                                                               \
+        h->apos = ap;                                                                \
+        h->diag = ap - bp;                                                           \
+    } while (0)
+        if (self)
+        {
+            for (int64_t ka = ja + 1; ka < ia; ka++)
+                for (int64_t a = ja; a < ka; a++)
+                {
+                    if (!p->identity && (al[a].read >> 1) >= (al[ka].read >> 1))
+                        break;
+                    EMIT(al[ka], al[a]);
+                }
+        }
+        else
+            for (int64_t a = ja; a < ia; a++)
+                for (int64_t q = jb; q < ib; q++)
+                    EMIT(al[a], bl[q]);
+#undef EMIT
+    }
+#undef RUN_CT
+    *hf = F;
+    *nf = n1;
+    *hc = Cm;
+    *nc = n2;
+}
+
+int or_daligner2(const or_block* a, const or_block* b, const or_block* bc, const or_params* p, int self,
+                 or_result* res)
+{
+    Spec sp;
+    Work w;
+    OBuf ob;
+    memset(res, 0, sizeof(*res));
+    memset(&w, 0, sizeof(w));
+    memset(&ob, 0, sizeof(ob));
+    if (p->variant != 2)
+        return -1;
+    make_spec(&sp, p);
+    ob.tbytes = (p->tspace <= 125) ? 1 : 2;
+    int64_t alen, blen;
+    KPos* al = build_index2(a, p, &alen);
+    KPos* bl = self ? al : build_index2(b, p, &blen);
+    if (self)
+        blen = alen;
+    res->kmers_a = alen;
+    res->kmers_b = blen;
+    if (alen > 0 && blen > 0)
+    {
+        Hit *hf, *hc;
+        int64_t nf, nc;
+        int limit;
+        merge_hits2(b, al, alen, bl, blen, p, self, &hf, &nf, &hc, &nc, &limit);
+        res->hits_n = nf;
+        res->hits_c = nc;
+        /* the hit sort orders (aread', bread, apos) with aread' = aread + nreads(A) for the
+         * complement; per orientation that is (aread, bread, apos), and groups are
+         * independent, so each orientation is sorted and scanned on its own */
+        sort_hits(hf, nf, nbytes_for(a->maxlen), nbytes_for(a->nreads), nbytes_for(b->nreads));
+        sort_hits(hc, nc, nbytes_for(a->maxlen), nbytes_for(a->nreads), nbytes_for(b->nreads));
+        hf[nf].aread = hf[nf].bread = hf[nf].diag = 0x7fffffff;
+        hf[nf].apos = 0;
+        hc[nc].aread = hc[nc].bread = hc[nc].diag = 0x7fffffff;
+        hc[nc].apos = 0;
+        if (nf > 0)
+            report(a, b, hf, nf, p, &sp, &w, self, 0, &ob, &res->seeds_n, &res->status);
+        if (nc > 0 && res->status == 0)
+            report(a, bc, hc, nc, p, &sp, &w, self, 1, &ob, &res->seeds_c, &res->status);
+        free(hf);
+        free(hc);
+    }
+    if (!self)
+        free(bl);
+    free(al);
+    qsort(ob.o, ob.n, sizeof(or_overlap), cmp_ovl);
+    res->novl = ob.n;
+    res->ovl = ob.o;
+    res->trace = ob.tr;
+    res->tbytes_total = ob.ttop;
+    res->tbytes = ob.tbytes;
+    res->cells = w.cells_count;
+    res->snake_steps = w.snakes;
+    free(w.mem);
+    free(w.cells);
+    free(w.pts);
+    return res->status ? -1 : 0;
 }
 
 /* iter_np (align.c:4556-4917), the distance part: the O(np) waves between A[0..M) and

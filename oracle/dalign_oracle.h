@@ -41,6 +41,8 @@ typedef struct
     int32_t symmetric, identity, only_identity, no_trace;
     uint64_t mem_limit;                       /* bytes (-M << 30), 0 = no cap */
     float freq[4];                            /* A-block base frequencies */
+    int32_t hgap;                             /* daligner2 -H (its HGAP_MIN is live) */
+    int32_t variant;                          /* 1 = daligner, 2 = daligner2 (dalign2/) */
 } or_params;
 
 typedef struct
@@ -60,6 +62,9 @@ typedef struct
     int32_t tbytes;
     /* statistics */
     int64_t kmers_a, kmers_b, hits_n, hits_c, seeds_n, seeds_c, cells, snake_steps;
+    /* 0, or daligner2 only: 1 = a pair would be bridged (Compute_Bridge_Path, not restated),
+     * 2 = a trace value above 255 met the 8-bit compression check (Compress_TraceTo8) */
+    int32_t status;
 } or_result;
 
 /* Sorted k-mer index of a block (Sort_Kmers, dalign/filter.c:698-903).
@@ -84,6 +89,16 @@ int or_local_alignment(const uint8_t* aseq, const uint8_t* bseq, int alen, int b
  * sorted as Write_Overlap_Buffer sorts them (dalign/align.c:5786-5853). */
 int or_daligner(const or_block* a, const or_block* b, const or_block* bc, const or_params* p, int self,
                 or_result* res);
+
+/* daligner2's overlap path for block A against block B (dalign2/daligner.c:654-790): the
+ * modimizer index of both blocks, one join giving both orientations, the seed scan and
+ * alignment per orientation (bc = the complemented B block), records sorted as
+ * Write_Overlap_Buffer sorts them (dalign2/ovlbuffer.c:160-312).  p->variant must be 2. */
+int or_daligner2(const or_block* a, const or_block* b, const or_block* bc, const or_params* p, int self,
+                 or_result* res);
+
+/* daligner2's sorted k-mer index (dalign2/filter.c:834-1106): read = (read << 1) | strand. */
+int64_t or_sort_kmers2(const or_block* b, const or_params* p, uint64_t* code, int32_t* read, int32_t* rpos);
 
 /* Exact diffs between trace points (Compute_Trace_PTS, dalign/align.c:5286-5397). */
 int or_trace_pts_diffs(const uint8_t* aseq, const uint8_t* bseq, int alen, int blen, int abpos, int bbpos,

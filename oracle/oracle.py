@@ -22,7 +22,8 @@ class or_params(C.Structure):
     _fields_ = [("kmer", C.c_int32), ("binshift", C.c_int32), ("suppress", C.c_int32), ("hitmin", C.c_int32),
                 ("ave_corr", C.c_double), ("tspace", C.c_int32), ("minover", C.c_int32),
                 ("symmetric", C.c_int32), ("identity", C.c_int32), ("only_identity", C.c_int32),
-                ("no_trace", C.c_int32), ("mem_limit", C.c_uint64), ("freq", C.c_float * 4)]
+                ("no_trace", C.c_int32), ("mem_limit", C.c_uint64), ("freq", C.c_float * 4),
+                ("hgap", C.c_int32), ("variant", C.c_int32)]
 
 
 class or_overlap(C.Structure):
@@ -35,7 +36,8 @@ class or_result(C.Structure):
     _fields_ = [("novl", C.c_int64), ("ovl", C.POINTER(or_overlap)), ("trace", C.POINTER(C.c_uint8)),
                 ("tbytes_total", C.c_int64), ("tbytes", C.c_int32),
                 ("kmers_a", C.c_int64), ("kmers_b", C.c_int64), ("hits_n", C.c_int64), ("hits_c", C.c_int64),
-                ("seeds_n", C.c_int64), ("seeds_c", C.c_int64), ("cells", C.c_int64), ("snake_steps", C.c_int64)]
+                ("seeds_n", C.c_int64), ("seeds_c", C.c_int64), ("cells", C.c_int64), ("snake_steps", C.c_int64),
+                ("status", C.c_int32)]
 
 
 def lib():
@@ -46,7 +48,10 @@ def lib():
             raise RuntimeError("oracle/liboracle.so is not built (make -C oracle liboracle.so)")
         _lib = C.CDLL(path)
         _lib.or_daligner.argtypes = [C.POINTER(or_block)] * 3 + [C.POINTER(or_params), C.c_int, C.POINTER(or_result)]
+        _lib.or_daligner2.argtypes = [C.POINTER(or_block)] * 3 + [C.POINTER(or_params), C.c_int, C.POINTER(or_result)]
         _lib.or_free_result.argtypes = [C.POINTER(or_result)]
+        _lib.or_sort_kmers2.argtypes = [C.POINTER(or_block), C.POINTER(or_params), C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.or_sort_kmers2.restype = C.c_int64
         _lib.or_sort_kmers.argtypes = [C.POINTER(or_block), C.POINTER(or_params), C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.or_sort_kmers.restype = C.c_int64
         _lib.or_match_hits.argtypes = [C.POINTER(or_block), C.POINTER(or_block), C.POINTER(or_params), C.c_int,
@@ -95,8 +100,11 @@ class BlockRef:
 
 
 def make_params(freq, k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=32, symmetric=True, identity=False,
-                only_identity=False, no_trace=False):
+                only_identity=False, no_trace=False, H=0, variant=1):
+    """variant 1 = daligner (dalign/), 2 = daligner2 (dalign2/, where -H is live)."""
     p = or_params()
+    p.hgap = int(H)
+    p.variant = int(variant)
     p.kmer, p.binshift, p.suppress, p.hitmin = k, w, t, h
     p.ave_corr = e
     p.tspace = s
@@ -114,9 +122,10 @@ def make_params(freq, k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=32, symmetr
 def daligner(a, b, bc, params, self_cmp):
     """Run the restated overlap path; returns (records list of dicts-as-tuples, traces, stats)."""
     L = lib()
+    fn = L.or_daligner2 if params.variant == 2 else L.or_daligner
     ra, rb, rc = BlockRef(a), BlockRef(b), BlockRef(bc)
     res = or_result()
-    L.or_daligner(C.byref(ra.s), C.byref(rb.s), C.byref(rc.s), C.byref(params), int(self_cmp), C.byref(res))
+    fn(C.byref(ra.s), C.byref(rb.s), C.byref(rc.s), C.byref(params), int(self_cmp), C.byref(res))
     n = res.novl
     tb = res.tbytes
     recs = []
@@ -133,7 +142,8 @@ def daligner(a, b, bc, params, self_cmp):
             o = int(ov["toff"][i])
             L_ = int(ov["tlen"][i]) * tb
             traces.append(tr[o:o + L_].view("<u1" if tb == 1 else "<u2").copy())
-    stats = {k: getattr(res, k) for k in ("kmers_a", "kmers_b", "hits_n", "hits_c", "seeds_n", "seeds_c", "cells")}
+    stats = {k: getattr(res, k) for k in ("kmers_a", "kmers_b", "hits_n", "hits_c", "seeds_n", "seeds_c", "cells",
+                                          "status")}
     L.or_free_result(C.byref(res))
     return recs, traces, stats
 
@@ -160,6 +170,18 @@ def sort_kmers(blk, params):
     read = np.zeros(n, np.int32)
     rpos = np.zeros(n, np.int32)
     k = L.or_sort_kmers(C.byref(r.s), C.byref(params), code.ctypes.data, read.ctypes.data, rpos.ctypes.data)
+    return code[:k], read[:k], rpos[:k]
+
+
+def sort_kmers2(blk, params):
+    """daligner2's sorted modimizer index: (code, (read << 1) | strand, rpos)."""
+    L = lib()
+    r = BlockRef(blk)
+    n = 2 * blk.totlen + 2
+    code = np.zeros(n, np.uint64)
+    read = np.zeros(n, np.int32)
+    rpos = np.zeros(n, np.int32)
+    k = L.or_sort_kmers2(C.byref(r.s), C.byref(params), code.ctypes.data, read.ctypes.data, rpos.ctypes.data)
     return code[:k], read[:k], rpos[:k]
 
 

@@ -11,12 +11,12 @@ from marvel_b200 import dazzdb
 
 
 def parse_flags(flags):
-    o = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=None, A=False, I=False, O=False, T=False, r=1, m=[])
+    o = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=None, A=False, I=False, O=False, T=False, r=1, m=[],
+             H=0)
     for f in flags:
         c, v = f[1], f[2:]
         if c in "kwhtlsHr":
-            if c != "H":
-                o[c] = int(v)
+            o[c] = int(v)
         elif c == "M":
             o["M"] = int(v)
         elif c == "e":
@@ -48,6 +48,21 @@ def las_names(aname, bname, run_id, symmetric):
     return [p2, p1] if bi < ai else [p1, p2]
 
 
+def las_names2(aname, bname, base, symmetric):
+    """daligner2's paths (pathLas / Write_Overlap_Buffer, dalign2/ovlbuffer.c:226-421): under
+    <base>_<block>/, in (first, second) order."""
+    def split(n):
+        root, _, b = n.rpartition(".")
+        return root, int(b)
+    ar, ai = split(aname)
+    br, bi = split(bname)
+    p1 = "%s_%05d/%s.%d.%s.%d.las" % (base, ai, ar, ai, br, bi)
+    if aname == bname or not symmetric:
+        return [p1]
+    p2 = "%s_%05d/%s.%d.%s.%d.las" % (base, bi, br, bi, ar, ai)
+    return [p2, p1] if bi < ai else [p1, p2]
+
+
 def write_las(path, recs, traces, tspace):
     os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
     tb = 1 if tspace <= 125 else 2
@@ -61,9 +76,10 @@ def write_las(path, recs, traces, tspace):
             f.write(np.asarray(t).astype("<u1" if tb == 1 else "<u2").tobytes())
 
 
-def run(dbdir, flags, blocks, outdir, impl, wave_limit=None):
-    """Runs `daligner flags blocks[0] blocks[1]` with impl in {"oracle", "gpu"}; returns the paths.
-    wave_limit (gpu only) sets the widest band of the main aligner kernel (test hook)."""
+def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1):
+    """Runs `daligner flags blocks[0] blocks[1]` (variant 2: `daligner2 -Pout ...`) with impl in
+    {"oracle", "gpu"}; returns the paths.  wave_limit (gpu only) sets the widest band of the
+    main aligner kernel (test hook)."""
     o = parse_flags(flags)
     aname, bname = blocks
     A = dazzdb.open_block(os.path.join(dbdir, aname))
@@ -83,9 +99,12 @@ def run(dbdir, flags, blocks, outdir, impl, wave_limit=None):
     if impl == "oracle":
         import oracle
         p = oracle.make_params(A.freq, k=o["k"], w=o["w"], h=o["h"], t=o["t"], e=o["e"], l=o["l"], s=o["s"],
-                               M=0, symmetric=symmetric, identity=o["I"], only_identity=o["O"], no_trace=o["T"])
+                               M=0, symmetric=symmetric, identity=o["I"], only_identity=o["O"], no_trace=o["T"],
+                               H=o["H"], variant=variant)
         p.mem_limit = mem
-        recs, traces, _ = oracle.daligner(A, B, dazzdb.complement_block(B), p, self_cmp)
+        recs, traces, st = oracle.daligner(A, B, dazzdb.complement_block(B), p, self_cmp)
+        if st["status"]:
+            raise RuntimeError(f"oracle: daligner2 status {st['status']}")
     else:
         import marvel_b200 as mb
         ctx = mb.Context()
@@ -104,7 +123,7 @@ def run(dbdir, flags, blocks, outdir, impl, wave_limit=None):
         recs = r
         traces = [tr[int(x["toff"]):int(x["toff"]) + int(x["tlen"]) * tb].view("<u1" if tb == 1 else "<u2")
                   for x in r]
-    names = las_names(aname, bname, o["r"], symmetric)
+    names = las_names2(aname, bname, "out", symmetric) if variant == 2 else las_names(aname, bname, o["r"], symmetric)
     paths = [os.path.join(outdir, n) for n in names]
     if len(paths) == 1:
         write_las(paths[0], recs, traces, tspace)

@@ -4,7 +4,7 @@ import os
 import pytest
 
 import daligner_run
-from golden_cases import cases, load
+from golden_cases import cases, d2_cases, load
 from marvel_b200 import dazzdb
 
 
@@ -12,6 +12,18 @@ from marvel_b200 import dazzdb
 def test_oracle_matches_reference_golden(name, tmp_path):
     d, meta = load(name)
     names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "oracle")
+    assert sorted(names) == sorted(meta["las"])
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
+        assert ok, f"{name} {n}: {msg}"
+
+
+@pytest.mark.parametrize("name", d2_cases())
+def test_oracle_matches_reference_daligner2_golden(name, tmp_path):
+    """The daligner2 restatement (modimizer index, one join for both orientations, its
+    report and Handle_Redundancies) reproduces the reference daligner2's .las files."""
+    d, meta = load(name)
+    names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "oracle", variant=2)
     assert sorted(names) == sorted(meta["las"])
     for n in names:
         ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
