@@ -98,6 +98,22 @@ int64_t gd_get_kmers(gd_context* ctx, int slot, uint64_t* code, int32_t* read, i
  * Appends the overlaps it finds to the context's overlap buffer. */
 int gd_match_filter(gd_context* ctx, int bslot, int comp, int self);
 
+/* daligner2 mode (the reference's dalign2/, modimizer seeds).  variant 1 = daligner (the
+ * default), 2 = daligner2; hgap = daligner2's -H (HGAP_MIN, dalign2/daligner.c:29,570: pairs
+ * whose reads are both shorter are skipped, shorter reads get no record of their own).
+ * In mode 2, gd_sort_kmers builds daligner2's index (Sort_Kmers, dalign2/filter.c:834-1106:
+ * canonical and half-shifted codes with code % 101 < 28; read = (read << 1) | strand) and
+ * Match_Filter is gd_match_filter2.  Changing the mode drops the slots' indices. */
+int gd_set_variant(gd_context* ctx, int variant, int hgap);
+
+/* daligner2's Match_Filter (dalign2/filter.c:2344-2700 with report_thread,
+ * dalign2/filter_reporter_cpu.c:16-411): A (slot 0) against bslot in both orientations from
+ * one join; cslot holds the complemented B block (gd_complement_block) the complement pairs
+ * are aligned against.  Fails (GD_ERR_BRIDGE in the message) where daligner2 would bridge
+ * two paths of a pair (Compute_Bridge_Path, dalign2/filter.c:1579-1705), which this build
+ * does not compute, and where a trace value above 255 meets the 8-bit compression check. */
+int gd_match_filter2(gd_context* ctx, int bslot, int cslot, int self);
+
 /* The sorted hits of the last gd_match_filter (rows diag, apos, aread, bread), for tests. */
 int64_t gd_get_hits(gd_context* ctx, int32_t* rows4, int64_t cap);
 

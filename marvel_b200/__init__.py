@@ -61,7 +61,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
            "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge",
-           "gd_set_wave_limit"]
+           "gd_set_wave_limit", "gd_set_variant", "gd_match_filter2"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -82,6 +82,8 @@ def lib():
     L.gd_new_align_spec.argtypes = [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int]
     L.gd_set_globals.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64]
     L.gd_load_block.argtypes = [C.c_void_p, C.c_int, C.POINTER(GdBlock)]
+    L.gd_set_variant.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.gd_match_filter2.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.gd_sort_kmers.argtypes = [C.c_void_p, C.c_int]
     L.gd_sort_kmers.restype = C.c_int64
     L.gd_get_kmers.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
@@ -235,6 +237,14 @@ class Context:
         rpos = np.zeros(max(n, 1), np.int32)
         k = _check(lib().gd_get_kmers(self.h, slot, code.ctypes.data, read.ctypes.data, rpos.ctypes.data, n))
         return code[:k], read[:k], rpos[:k]
+
+    def set_variant(self, variant, hgap=0):
+        """1 = daligner (default), 2 = daligner2 (modimizer seeds; hgap = its -H)."""
+        _check(lib().gd_set_variant(self.h, int(variant), int(hgap)))
+
+    def match_filter2(self, bslot, cslot, self_cmp):
+        """daligner2's Match_Filter: A against bslot in both orientations (cslot = complemented B)."""
+        _check(lib().gd_match_filter2(self.h, bslot, cslot, int(self_cmp)))
 
     def match_filter(self, bslot, comp, self_cmp):
         _check(lib().gd_match_filter(self.h, bslot, int(comp), int(self_cmp)))
@@ -413,6 +423,38 @@ def run_loaded(ctx: Context, self_cmp: bool):
         ctx.complement_block(1, 2)
     ctx.sort_kmers(2)
     ctx.match_filter(2, 1, int(self_cmp))
+
+
+def daligner2_block(ctx: Context, A: dazzdb.Block, B: dazzdb.Block | None = None, *, k=14, w=6, h=35, t=0,
+                    e=0.70, l=1000, s=100, M=32, H=0, symmetric=True, identity=False):
+    """One daligner2 block comparison on the GPU (dalign2/daligner.c:654-790): A against B (or
+    against itself when B is None), both orientations from one join.  Returns the overlap
+    buffer as (records, trace bytes), sorted like the .las file."""
+    self_cmp = B is None
+    ctx.set_variant(2, H)
+    ctx.set_filter_params(k, w, t, h)
+    ctx.new_align_spec(e, s, A.freq, symmetric, False, False)
+    ctx.set_globals(2 * l, identity, int(M) * 0x40000000)
+    ctx.reset_overlap_buffer()
+    ctx.load_block(0, A)
+    if not self_cmp:
+        ctx.load_block(1, B)
+    run_loaded2(ctx, self_cmp)
+    return ctx.overlaps()
+
+
+def run_loaded2(ctx: Context, self_cmp: bool):
+    """daligner2's per-block device pipeline once the blocks are resident (context in variant
+    2): Sort_Kmers(A), Sort_Kmers(B), the complemented B block for the complement pairs'
+    alignments (CopyAndComp per pair in the reference), Match_Filter(A, B)."""
+    ctx.sort_kmers(0)
+    if self_cmp:
+        ctx.complement_block(0, 2)
+        ctx.match_filter2(0, 2, 1)
+    else:
+        ctx.sort_kmers(1)
+        ctx.complement_block(1, 2)
+        ctx.match_filter2(1, 2, 0)
 
 
 def write_las(path, recs, trace, tspace):

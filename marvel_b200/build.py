@@ -10,7 +10,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpudalign.so")
 CLI = os.path.join(HERE, "daligner_gpu")
-SOURCES = ["gd_prims.cu", "gd_filter.cu", "gd_align.cu", "gd_pipeline.cu", "gd_noalloc.cu", "gd_verify.cu", "gd_triage.cu", "gd_output.cu", "gd_dust.cu"]
+SOURCES = ["gd_prims.cu", "gd_filter.cu", "gd_filter2.cu", "gd_align.cu", "gd_pipeline.cu", "gd_noalloc.cu", "gd_verify.cu", "gd_triage.cu", "gd_output.cu", "gd_dust.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -930,7 +930,9 @@ struct PairBuf
     int err;
 };
 
-__device__ int entwine(const MPath* jpath, const MPath* kpath, const uint16_t* tb, int TS, int* where)
+// Entwine (filter.c:1249-1342); d2: daligner2's version (dalign2/filter.c:1707-1825), which
+// also compares the B coordinates at a common start and a common end point
+__device__ int entwine(const MPath* jpath, const MPath* kpath, const uint16_t* tb, int TS, int* where, bool d2 = false)
 {
     int ac, b2, y2, ae, i, j, k, den = 0, min = 10000;
     const uint16_t* ktrace = tb + kpath->toff;
@@ -939,6 +941,12 @@ __device__ int entwine(const MPath* jpath, const MPath* kpath, const uint16_t* t
     j = jpath->abpos / TS;
     b2 = kpath->bbpos;
     k = kpath->abpos / TS;
+    if (d2 && jpath->abpos == kpath->abpos)
+    {
+        min = abs(y2 - b2);
+        if (min == 0)
+            *where = kpath->abpos;
+    }
     if (j < k)
     {
         ac = k * TS;
@@ -975,6 +983,16 @@ __device__ int entwine(const MPath* jpath, const MPath* kpath, const uint16_t* t
                 *where = ac;
         }
         den += 1;
+    }
+    if (d2 && jpath->aepos == kpath->aepos)
+    {
+        i = abs(jpath->bepos - kpath->bepos);
+        if (i <= min)
+        {
+            min = i;
+            if (i == 0)
+                *where = kpath->aepos;
+        }
     }
     return den == 0 ? -1 : min;
 }
@@ -1134,6 +1152,199 @@ __device__ int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, Pair
     return no + 1;
 }
 
+// daligner2's Handle_Redundancies (dalign2/filter.c:1952-2272): the surviving path of a fused
+// or contained pair stays at the later index j, the other is marked abpos = -1, a fusion
+// restarts j's scan; compaction at the end.  Its bridging pass (:2124-2262) is detected, not
+// computed: returns -1 when two paths would go to Compute_Bridge_Path.
+__device__ int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, PairBuf& pb, int TS, int comp)
+{
+    int j, k, dist, awhen = 0, bwhen = 0;
+    const bool hasB = (bmatch != nullptr);
+    for (j = 1; j < novls; j++)
+    {
+        MPath* jpath = amatch + j;
+        for (k = j - 1; k >= 0; k--)
+        {
+            MPath* kpath = amatch + k;
+            if (kpath->abpos < 0)
+                continue;
+            if (jpath->abpos < kpath->abpos)
+            {
+                if (kpath->abpos <= jpath->aepos && kpath->bbpos <= jpath->bepos)
+                {
+                    dist = entwine(jpath, kpath, pb.tb, TS, &awhen, true);
+                    if (dist == 0)
+                    {
+                        if (kpath->aepos > jpath->aepos)
+                        {
+                            if (hasB)
+                            {
+                                if (comp)
+                                {
+                                    dist = entwine(bmatch + k, bmatch + j, pb.tb, TS, &bwhen, true);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(jpath, awhen, kpath, pb, TS);
+                                    fusion(bmatch + k, bwhen, bmatch + j, pb, TS);
+                                    bmatch[j] = bmatch[k];
+                                }
+                                else
+                                {
+                                    dist = entwine(bmatch + j, bmatch + k, pb.tb, TS, &bwhen, true);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(jpath, awhen, kpath, pb, TS);
+                                    fusion(bmatch + j, bwhen, bmatch + k, pb, TS);
+                                }
+                            }
+                            else
+                                fusion(jpath, awhen, kpath, pb, TS);
+                            kpath->abpos = -1;
+                            k = j;
+                            continue;
+                        }
+                        kpath->abpos = -1;
+                    }
+                }
+            }
+            else
+            {
+                if (jpath->abpos <= kpath->aepos && jpath->bbpos <= kpath->bepos)
+                {
+                    dist = entwine(kpath, jpath, pb.tb, TS, &awhen, true);
+                    if (dist == 0)
+                    {
+                        bool restart = false;
+                        if (kpath->abpos == jpath->abpos)
+                        {
+                            if (kpath->aepos > jpath->aepos)
+                            {
+                                *jpath = *kpath;
+                                if (hasB)
+                                    bmatch[j] = bmatch[k];
+                            }
+                        }
+                        else if (jpath->aepos > kpath->aepos)
+                        {
+                            if (hasB)
+                            {
+                                if (comp)
+                                {
+                                    dist = entwine(bmatch + j, bmatch + k, pb.tb, TS, &bwhen, true);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(kpath, awhen, jpath, pb, TS);
+                                    *jpath = *kpath;
+                                    fusion(bmatch + j, bwhen, bmatch + k, pb, TS);
+                                }
+                                else
+                                {
+                                    dist = entwine(bmatch + k, bmatch + j, pb.tb, TS, &bwhen, true);
+                                    if (dist != 0)
+                                        continue;
+                                    fusion(kpath, awhen, jpath, pb, TS);
+                                    *jpath = *kpath;
+                                    fusion(bmatch + k, bwhen, bmatch + j, pb, TS);
+                                    bmatch[j] = bmatch[k];
+                                }
+                            }
+                            else
+                            {
+                                fusion(kpath, awhen, jpath, pb, TS);
+                                *jpath = *kpath;
+                            }
+                            restart = true;
+                        }
+                        else
+                        {
+                            *jpath = *kpath;
+                            if (hasB)
+                                bmatch[j] = bmatch[k];
+                        }
+                        kpath->abpos = -1;
+                        if (restart)
+                            k = j;
+                    }
+                }
+            }
+        }
+    }
+    // the bridging pass's entry test (dalign2/filter.c:2126-2175)
+    for (j = 1; j < novls; j++)
+    {
+        const MPath* jpath = amatch + j;
+        if (jpath->abpos < 0)
+            continue;
+        for (k = j - 1; k >= 0; k--)
+        {
+            const MPath* kpath = amatch + k;
+            if (kpath->abpos < 0)
+                continue;
+            const MPath* path1 = jpath->abpos < kpath->abpos ? jpath : kpath;
+            const MPath* path2 = jpath->abpos < kpath->abpos ? kpath : jpath;
+            if (path2->abpos >= path1->aepos || path1->aepos >= path2->aepos || path1->bbpos >= path2->bbpos ||
+                path2->bbpos >= path1->bepos || path1->bepos >= path2->bepos)
+                continue;
+            const int aovl = path1->aepos - path2->abpos;
+            const int bovl = path1->bepos - path2->bbpos;
+            if (abs(aovl - bovl) > .2 * (aovl + bovl))
+                continue;
+            if (hasB)
+            {
+                const bool first = (comp != 0) == (jpath->abpos < kpath->abpos);
+                const MPath* bath1 = first ? bmatch + k : bmatch + j;
+                const MPath* bath2 = first ? bmatch + j : bmatch + k;
+                if (bath1->abpos > bath2->abpos)
+                    continue;
+            }
+            return -1;
+        }
+    }
+    int no = 0;
+    for (j = 0; j < novls; j++)
+        if (amatch[j].abpos >= 0)
+        {
+            if (hasB)
+                bmatch[no] = bmatch[j];
+            amatch[no++] = amatch[j];
+        }
+    return no;
+}
+
+// daligner2's end of a pair (filter_reporter_cpu.c:330-371): Handle_Redundancies, then the
+// check of Compress_TraceTo8 (dalign2/align.c:3391-3412).  Returns 0 or the GD_ERR_ code the
+// pair fails with.  Kept out of line: the pair kernel's hot loop stays compact.
+__device__ __noinline__ int finish_pair_d2(MPath* amatch, int* novla, MPath* bmatch, int* novlb, PairBuf& pb, int TS,
+                                           int comp, bool check8)
+{
+    int r1 = *novla, r2 = *novlb;
+    if (r1 > 1)
+    {
+        if (r2 > 1)
+            r1 = r2 = handle_redundancies_d2(amatch, r1, bmatch, pb, TS, comp);
+        else
+            r1 = handle_redundancies_d2(amatch, r1, nullptr, pb, TS, comp);
+    }
+    else if (r2 > 1)
+        r2 = handle_redundancies_d2(bmatch, r2, nullptr, pb, TS, comp);
+    if (r1 < 0 || r2 < 0)
+        return GD_ERR_BRIDGE;
+    *novla = r1;
+    *novlb = r2;
+    if (check8)
+    {
+        for (int i = 0; i < r1; i++)
+            for (int t = 0; t < amatch[i].tlen; t++)
+                if (pb.tb[amatch[i].toff + t] > 255)
+                    return GD_ERR_TRACE8;
+        for (int i = 0; i < r2; i++)
+            for (int t = 0; t < bmatch[i].tlen; t++)
+                if (pb.tb[bmatch[i].toff + t] > 255)
+                    return GD_ERR_TRACE8;
+    }
+    return 0;
+}
+
 // ------------------------------------------------------------------------------------------
 // the pair kernel
 // ------------------------------------------------------------------------------------------
@@ -1242,7 +1453,10 @@ constexpr int warps_of()
     return RG == WIDE_RING ? 1 : ALIGN_WARPS;
 }
 
-template <int RG>
+// D2: daligner2's report (dalign2/filter_reporter_cpu.c) -- its -H, its rule for the B-side
+// record of a read against itself, its Handle_Redundancies; a separate instance, so that
+// daligner's keeps its code layout.
+template <int RG, bool D2 = false>
 __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
     k_align_pairs(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
@@ -1298,7 +1512,11 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
         const int alen = A.rlen[ar], blen = B.rlen[br];
         const uint8_t* aseq = A.bases + A.boff[ar];
         const uint8_t* bseq = B.bases + B.boff[br];
-        const bool doB = P.symmetric && (ar != br || !P.self || !P.comp);
+        if (D2 && alen < P.hgap && blen < P.hgap)
+            continue;  // daligner2 -H: neither read is long enough (filter_reporter_cpu.c:156-162)
+        const bool doA = !D2 || alen >= P.hgap;
+        const bool doB = D2 ? (P.symmetric && blen >= P.hgap && !(ar == br && P.self))
+                            : (P.symmetric && (ar != br || !P.self || !P.comp));
         PairBuf pb;
         pb.am = amatch;
         pb.bm = bmatch;
@@ -1447,15 +1665,18 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
                     __syncwarp();
                     if ((apth.aepos - apth.abpos) + (apth.bepos - apth.bbpos) >= P.minover)
                     {
-                        if (novla >= sc.mcap || (doB && novlb >= sc.mcap))
+                        if ((doA && novla >= sc.mcap) || (doB && novlb >= sc.mcap))
                         {
                             if (lane == 0)
                                 gd_fail(st, GD_ERR_MATCHES, w.item, sc.mcap);
                             w.err = 1;
                             break;
                         }
-                        store_path(w, apth, amatch + novla, pb);
-                        novla++;
+                        if (doA)
+                        {
+                            store_path(w, apth, amatch + novla, pb);
+                            novla++;
+                        }
                         if (doB)
                         {
                             store_path(w, bpth, bmatch + novlb, pb);
@@ -1513,9 +1734,16 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
         if (w.err)
             break;
         // merge redundant paths (filter.c:1922-1938), lane 0
+        int d2fail = 0;
         if (lane == 0)
         {
-            if (novla > 1)
+            if (D2)
+            {
+                d2fail = finish_pair_d2(amatch, &novla, bmatch, &novlb, pb, TS, P.comp, P.trace8 && !P.no_trace);
+                if (d2fail)
+                    gd_fail(st, d2fail, w.item, 0);
+            }
+            else if (novla > 1)
             {
                 if (novlb > 1)
                     novla = novlb = handle_redundancies(amatch, novla, bmatch, pb, TS, P.comp);
@@ -1529,7 +1757,10 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
         }
         novla = __shfl_sync(GD_FULL, novla, 0);
         novlb = __shfl_sync(GD_FULL, novlb, 0);
+        d2fail = __shfl_sync(GD_FULL, d2fail, 0);
         __syncwarp();
+        if (d2fail)
+            break;
         emit_paths(w, P, amatch, novla, tbuf, ar + A.ufirst, br + B.ufirst, out);
         emit_paths(w, P, bmatch, novlb, tbuf, br + B.ufirst, ar + A.ufirst, out);
         if (out.gstat && lane == 0)
@@ -1605,7 +1836,16 @@ int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hke
     GD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), s));
     if (ngroups == 0)
         return 0;
-    if (wide)
+    if (p.d2)
+    {
+        if (wide)
+            k_align_pairs<WIDE_RING, true><<<grid, warps_of<WIDE_RING>() * 32, 0, s>>>(A, B, hkey, hdiag, groups, order,
+                                                                                      ngroups, p, sc, out, queue, st);
+        else
+            k_align_pairs<RING, true><<<grid, ALIGN_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p,
+                                                                        sc, out, queue, st);
+    }
+    else if (wide)
         k_align_pairs<WIDE_RING><<<grid, warps_of<WIDE_RING>() * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups,
                                                                             p, sc, out, queue, st);
     else if (p.test_narrow)

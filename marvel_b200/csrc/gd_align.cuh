@@ -45,6 +45,7 @@ struct AlignParams
     const int16_t* score;
     int mscore, dscore;    // match / edit weights the tables are built from (align.c:238-240)
     int test_narrow;       // tests only: the main pass runs the TEST_RING instance
+    int d2, hgap;          // daligner2's report (dalign2/filter_reporter_cpu.c) and its -H
 };
 
 // Per-warp global scratch, carved from one allocation.

@@ -39,6 +39,28 @@ struct DevBlock
     int32_t ufirst;
 };
 
+// k-mer slots of a block: read r owns slots [kstart(r), kstart(r+1)), one per position p of
+// its last k-mer base (p >= k-1); slot kstart(r) + p - (k-1).  A block's reads are >= k long.
+__device__ __forceinline__ int64_t kstart_of(const DevBlock& b, int r, int K)
+{
+    return b.boff[r] - (int64_t)K * r;
+}
+
+// largest r in [0, nreads) with kstart(r) <= s
+__device__ __forceinline__ int read_of_slot(const DevBlock& b, int64_t s, int K)
+{
+    int lo = 0, hi = b.nreads - 1;
+    while (lo < hi)
+    {
+        int mid = (lo + hi + 1) >> 1;
+        if (kstart_of(b, mid, K) <= s)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 // Device-side error status shared by all kernels of a context.  Kernels never trap:
 // they record the first failure here and skip the remaining work.
 struct DevStatus
@@ -59,6 +81,8 @@ enum
     GD_ERR_OUTPUT = 5,       // overlap output buffer exhausted
     GD_ERR_EMPTY_BAND = 6,   // wave band emptied while the wave continues
     GD_ERR_RING = 7,         // band left the ring window
+    GD_ERR_BRIDGE = 8,       // daligner2: a pair of paths would be bridged (not built)
+    GD_ERR_TRACE8 = 9,       // daligner2: a trace value above 255 fails the 8-bit compression check
 };
 
 __device__ __forceinline__ void gd_fail(DevStatus* st, int code, int where, int info)

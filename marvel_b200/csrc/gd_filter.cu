@@ -11,26 +11,6 @@ namespace gd
 
 constexpr int FT = 256;
 
-__device__ __forceinline__ int64_t kstart_of(const DevBlock& b, int r, int K)
-{
-    return b.boff[r] - (int64_t)K * r;
-}
-
-// largest r in [0, nreads) with kstart(r) <= s
-__device__ __forceinline__ int read_of_slot(const DevBlock& b, int64_t s, int K)
-{
-    int lo = 0, hi = b.nreads - 1;
-    while (lo < hi)
-    {
-        int mid = (lo + hi + 1) >> 1;
-        if (kstart_of(b, mid, K) <= s)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
 // Four consecutive slots per thread: one read lookup, the codes rolled base by base within
 // a read, keys and values stored as 16-byte vectors.  The value is the slot index, or with
 // pbits >= 0 the packed (read << pbits | first position), so that no search is needed after
@@ -192,65 +172,6 @@ int launch_decode(const DevBlock& b, int kmer, const uint32_t* slots, int64_t n,
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
-}
-
-template <typename K>
-__device__ __forceinline__ int64_t lower_code(const K* a, int64_t n, K x)
-{
-    int64_t l = 0, r = n;
-    while (l < r)
-    {
-        int64_t m = (l + r) >> 1;
-        if (a[m] < x)
-            l = m + 1;
-        else
-            r = m;
-    }
-    return l;
-}
-
-template <typename K>
-__device__ __forceinline__ int64_t upper_code(const K* a, int64_t n, K x)
-{
-    int64_t l = 0, r = n;
-    while (l < r)
-    {
-        int64_t m = (l + r) >> 1;
-        if (a[m] <= x)
-            l = m + 1;
-        else
-            r = m;
-    }
-    return l;
-}
-
-// the same searches restricted to [l, r), for keys known to lie in that window
-template <typename K>
-__device__ __forceinline__ int64_t lower_code_in(const K* a, int64_t l, int64_t r, K x)
-{
-    while (l < r)
-    {
-        int64_t m = (l + r) >> 1;
-        if (a[m] < x)
-            l = m + 1;
-        else
-            r = m;
-    }
-    return l;
-}
-
-template <typename K>
-__device__ __forceinline__ int64_t upper_code_in(const K* a, int64_t l, int64_t r, K x)
-{
-    while (l < r)
-    {
-        int64_t m = (l + r) >> 1;
-        if (a[m] <= x)
-            l = m + 1;
-        else
-            r = m;
-    }
-    return l;
 }
 
 template <typename K>

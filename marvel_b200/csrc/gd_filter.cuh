@@ -74,4 +74,64 @@ int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits,
 int launch_complement(const DevBlock& src, uint8_t* dst_bases, const int64_t* anno, const int32_t* mdata,
                       int32_t* mdata_dst, cudaStream_t s);
 
+// binary searches over a sorted code array: first index with a[i] >= x (lower) / > x (upper)
+template <typename K>
+__device__ __forceinline__ int64_t lower_code(const K* a, int64_t n, K x)
+{
+    int64_t l = 0, r = n;
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] < x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
+template <typename K>
+__device__ __forceinline__ int64_t upper_code(const K* a, int64_t n, K x)
+{
+    int64_t l = 0, r = n;
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] <= x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
+// the same searches restricted to [l, r), for keys known to lie in that window
+template <typename K>
+__device__ __forceinline__ int64_t lower_code_in(const K* a, int64_t l, int64_t r, K x)
+{
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] < x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
+template <typename K>
+__device__ __forceinline__ int64_t upper_code_in(const K* a, int64_t l, int64_t r, K x)
+{
+    while (l < r)
+    {
+        int64_t m = (l + r) >> 1;
+        if (a[m] <= x)
+            l = m + 1;
+        else
+            r = m;
+    }
+    return l;
+}
+
 }  // namespace gd

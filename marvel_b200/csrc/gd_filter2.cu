@@ -1,0 +1,396 @@
+// gd_filter2.cu -- daligner2's modimizer filter (dalign2/filter.c) on sm_100a.
+//
+// Index build: one thread per k-mer slot evaluates the slot's two candidate codes from the
+// bases alone (no per-read serial state), a scan of the per-slot counts places them in the
+// reference's list order (read, position, canonical before half-shifted), and the shared LSD
+// radix sort orders them by code.  Join: one thread per A entry finds its B range by binary
+// search, splits it by orientation with a prefix count of strands, and writes its hits of
+// each orientation into that orientation's own list in the reference's generation order.
+#include "gd_filter2.cuh"
+
+namespace gd
+{
+
+constexpr int F2T = 256;
+constexpr unsigned D2_MODULUS = 101;  // MODULUS / MODTHR (dalign2/filter.c:47-48)
+constexpr unsigned D2_MODTHR = 28;
+
+D2Masks d2_masks(int kmer)
+{
+    D2Masks m;
+    m.kshift = kmer >= 32 ? 64 : 2 * kmer;
+    m.kmask = kmer >= 32 ? ~0ull : ((1ull << m.kshift) - 1);
+    m.lf = (1ull << (m.kshift / 2)) - 1;
+    m.hf = m.kmask - m.lf;
+    m.lr = (1ull << ((m.kshift + 1) / 2)) - 1;
+    m.hr = m.kmask - m.lr;
+    return m;
+}
+
+__device__ __forceinline__ bool d2_keep(uint64_t code, int kshift)
+{
+    if (kshift <= 32)
+        return (uint32_t)code % D2_MODULUS < D2_MODTHR;
+    return code % D2_MODULUS < D2_MODTHR;
+}
+
+// The slot's two candidates (tuple_thread's loop body, dalign2/filter.c:485-565).  For the
+// k-mer ending at p of the unmasked segment starting at ps: c / u are the forward /
+// reverse-complement codes of bases [p-k+1, p]; the codes one step earlier cover bases
+// [max(ps, p-k), p-1] (k-1 bases at the segment's first k-mer, where the reference's
+// warm-up leaves them).  d = high half of the earlier c | low half of c, v likewise from u.
+struct D2Codes
+{
+    uint64_t code1, code2;
+    unsigned strand1, strand2;
+    bool keep1, keep2;
+    int read, pos;
+};
+
+__device__ __forceinline__ bool d2_slot(const DevBlock& b, const int64_t* __restrict__ manno,
+                                        const int32_t* __restrict__ mdata, int kmer, const D2Masks& M, int64_t s,
+                                        D2Codes& o)
+{
+    const int r = read_of_slot(b, s, kmer);
+    const int p0 = (int)(s - kstart_of(b, r, kmer));
+    const int p = p0 + kmer - 1;
+    int ps = 0;
+    if (manno)
+    {
+        // the unmasked segment containing p0 must also contain p (the segments between the
+        // mask intervals, tuple_thread's loop :436-460)
+        int64_t f0 = manno[r], f1 = manno[r + 1];
+        int q = b.rlen[r];
+        for (int64_t a = f0; a < f1; a += 2)
+        {
+            int ib = mdata[a], ie = mdata[a + 1];
+            if (p0 < ib)
+            {
+                q = ib;
+                break;
+            }
+            ps = ie;
+            q = b.rlen[r];
+        }
+        if (!(p0 >= ps && p < q))
+            return false;
+    }
+    const uint8_t* src = b.bases + b.boff[r];
+    const int top = M.kshift - 2;
+    uint64_t c = 0, u = 0, cp = 0, up = 0;
+    const int lo = max(ps, p - kmer);
+    for (int t = lo; t < p; t++)
+    {
+        const uint64_t x = src[t];
+        cp = (cp << 2) | x;
+        up = (up >> 2) | ((3ull - x) << top);
+    }
+    for (int t = p - kmer + 1; t <= p; t++)
+    {
+        const uint64_t x = src[t];
+        c = (c << 2) | x;
+        u = (u >> 2) | ((3ull - x) << top);
+    }
+    c &= M.kmask;
+    cp &= M.kmask;
+    const uint64_t d = (cp & M.hf) | (c & M.lf);
+    const uint64_t v = (up & M.lr) | (u & M.hr);
+    if (u < c)
+    {
+        o.code1 = u;
+        o.strand1 = 1;
+    }
+    else
+    {
+        o.code1 = c;
+        o.strand1 = 0;
+    }
+    if (v < d)
+    {
+        o.code2 = v;
+        o.strand2 = 1;
+    }
+    else
+    {
+        o.code2 = d;
+        o.strand2 = 0;
+    }
+    o.keep1 = d2_keep(o.code1, M.kshift);
+    o.keep2 = d2_keep(o.code2, M.kshift);
+    o.read = r;
+    o.pos = p;
+    return true;
+}
+
+__global__ void __launch_bounds__(F2T) k_d2_count(DevBlock b, const int64_t* __restrict__ manno,
+                                                 const int32_t* __restrict__ mdata, int kmer, D2Masks M,
+                                                 int64_t nslots, uint32_t* count)
+{
+    const int64_t s = (int64_t)blockIdx.x * F2T + threadIdx.x;
+    if (s >= nslots)
+        return;
+    D2Codes o;
+    count[s] = d2_slot(b, manno, mdata, kmer, M, s, o) ? (uint32_t)o.keep1 + (uint32_t)o.keep2 : 0u;
+}
+
+int launch_d2_count(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, int kmer,
+                    const D2Masks& m, int64_t nslots, uint32_t* count, cudaStream_t s)
+{
+    if (nslots <= 0)
+        return 0;
+    k_d2_count<<<(unsigned)gd_cdiv<int64_t>(nslots, F2T), F2T, 0, s>>>(b, mask_anno, mask_data, kmer, m, nslots,
+                                                                       count);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(F2T) k_d2_emit(DevBlock b, const int64_t* __restrict__ manno,
+                                                const int32_t* __restrict__ mdata, int kmer, D2Masks M,
+                                                int64_t nslots, const uint32_t* __restrict__ off, K* keys,
+                                                uint32_t* vals, int32_t* rd, int32_t* rp)
+{
+    const int64_t s = (int64_t)blockIdx.x * F2T + threadIdx.x;
+    if (s >= nslots)
+        return;
+    D2Codes o;
+    if (!d2_slot(b, manno, mdata, kmer, M, s, o))
+        return;
+    uint32_t e = off[s];
+    if (o.keep1)
+    {
+        keys[e] = (K)o.code1;
+        vals[e] = e;
+        rd[e] = (o.read << 1) | (int)o.strand1;
+        rp[e] = o.pos;
+        e++;
+    }
+    if (o.keep2)
+    {
+        keys[e] = (K)o.code2;
+        vals[e] = e;
+        rd[e] = (o.read << 1) | (int)o.strand2;
+        rp[e] = o.pos;
+    }
+}
+
+template <typename K>
+int launch_d2_emit(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, int kmer,
+                   const D2Masks& m, int64_t nslots, const uint32_t* off, K* keys, uint32_t* vals, int32_t* rd,
+                   int32_t* rp, cudaStream_t s)
+{
+    if (nslots <= 0)
+        return 0;
+    k_d2_emit<K><<<(unsigned)gd_cdiv<int64_t>(nslots, F2T), F2T, 0, s>>>(b, mask_anno, mask_data, kmer, m, nslots,
+                                                                         off, keys, vals, rd, rp);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(F2T) k_d2_gather(const K* __restrict__ skeys, const uint32_t* __restrict__ svals,
+                                                  int64_t n, const int32_t* __restrict__ rd,
+                                                  const int32_t* __restrict__ rp, K* code, int32_t* read,
+                                                  int32_t* rpos)
+{
+    const int64_t i = (int64_t)blockIdx.x * F2T + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t e = svals[i];
+    code[i] = skeys[i];
+    read[i] = rd[e];
+    rpos[i] = rp[e];
+}
+
+template <typename K>
+int launch_d2_gather(const K* skeys, const uint32_t* svals, int64_t n, const int32_t* rd, const int32_t* rp, K* code,
+                     int32_t* read, int32_t* rpos, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_d2_gather<K><<<(unsigned)gd_cdiv<int64_t>(n, F2T), F2T, 0, s>>>(skeys, svals, n, rd, rp, code, read, rpos);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(F2T) k_d2_strand_flags(const int32_t* __restrict__ read, int64_t n,
+                                                        uint32_t* flags)
+{
+    const int64_t i = (int64_t)blockIdx.x * F2T + threadIdx.x;
+    if (i < n)
+        flags[i] = (uint32_t)read[i] & 1u;
+}
+
+int launch_d2_strand_flags(const int32_t* read, int64_t n, uint32_t* flags, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_d2_strand_flags<<<(unsigned)gd_cdiv<int64_t>(n, F2T), F2T, 0, s>>>(read, n, flags);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// count_thread (dalign2/filter.c:1136-1256), per A entry.  Within a block (self) the entry
+// pairs with the earlier entries of its code run whose read is smaller (all earlier entries
+// with -I); across blocks with the whole B run of its code.  bstrand_excl[j] = number of
+// complement-strand entries among B[0, j).
+template <typename K>
+__global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ acode, const int32_t* __restrict__ aread,
+                                                      const uint32_t* __restrict__ arun_excl,
+                                                      const uint32_t* __restrict__ arun_flag,
+                                                      const K* __restrict__ bcode, const int32_t* __restrict__ bread,
+                                                      const uint32_t* __restrict__ bstrand_excl, int64_t na,
+                                                      int64_t nb, int self, int identity, uint32_t* jb_out,
+                                                      uint64_t* cnt_f, uint64_t* cnt_c, unsigned long long* ctrun)
+{
+    __shared__ int64_t s_lo, s_hi;
+    const int64_t t0 = (int64_t)blockIdx.x * F2T;
+    const int64_t t1 = min(t0 + F2T, na) - 1;
+    if (threadIdx.x == 0)
+        s_lo = lower_code(bcode, nb, acode[t0]);
+    else if (threadIdx.x == 32)
+        s_hi = upper_code(bcode, nb, acode[t1]);
+    __syncthreads();
+    const int64_t i = t0 + threadIdx.x;
+    const bool act = i < na;
+    uint64_t n = 0;
+    uint32_t run = 0;
+    if (act)
+    {
+        const K c = acode[i];
+        const int64_t jb = lower_code_in(bcode, s_lo, s_hi, c);
+        int64_t je = jb;
+        if (jb < s_hi && bcode[jb] == c)
+            je = upper_code_in(bcode, jb, s_hi, c);
+        const int ar = aread[i];
+        int64_t e = je;
+        if (self)
+        {
+            if (identity)
+                e = i;  // every earlier entry of the run (A and B are the same index)
+            else
+            {
+                int64_t l = jb, r = je;
+                while (l < r)
+                {
+                    const int64_t md = (l + r) >> 1;
+                    if ((bread[md] >> 1) < (ar >> 1))
+                        l = md + 1;
+                    else
+                        r = md;
+                }
+                e = l;
+            }
+        }
+        n = (uint64_t)(e - jb);
+        const uint64_t ncomp_strand = bstrand_excl[e] - bstrand_excl[jb];
+        const uint64_t fwd = (ar & 1) ? ncomp_strand : n - ncomp_strand;
+        jb_out[i] = (uint32_t)jb;
+        cnt_f[i] = fwd;
+        cnt_c[i] = n - fwd;
+        run = arun_excl[i] + arun_flag[i] - 1;
+    }
+    const unsigned long long key = act ? (unsigned long long)run : ~0ull;
+    const unsigned peers = __match_any_sync(GD_FULL, key);
+    unsigned long long tot = 0;
+    for (unsigned mm = peers; mm; mm &= mm - 1)
+        tot += __shfl_sync(peers, n, __ffs(mm) - 1);
+    if (act && (peers & lanemask_lt()) == 0 && tot)
+        atomicAdd(&ctrun[run], tot);
+}
+
+template <typename K>
+int launch_d2_pair_count(const K* acode, const int32_t* aread, const uint32_t* arun_excl, const uint32_t* arun_flag,
+                         const K* bcode, const int32_t* bread, const uint32_t* bstrand_excl, int64_t na, int64_t nb,
+                         int self, int identity, uint32_t* jb, uint64_t* cnt_f, uint64_t* cnt_c,
+                         unsigned long long* ctrun, cudaStream_t s)
+{
+    if (na <= 0)
+        return 0;
+    k_d2_pair_count<K><<<(unsigned)gd_cdiv<int64_t>(na, F2T), F2T, 0, s>>>(
+        acode, aread, arun_excl, arun_flag, bcode, bread, bstrand_excl, na, nb, self, identity, jb, cnt_f, cnt_c,
+        ctrun);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// merge_thread's emission (dalign2/filter.c:1358-1463) for one A entry: its B entries in
+// index order, each to the list of its orientation; a complement hit's B position is
+// reflected into the complemented read (rlen - bpos + k - 2).
+__global__ void __launch_bounds__(F2T) k_d2_emit_hits(const int32_t* __restrict__ aread,
+                                                     const int32_t* __restrict__ arpos,
+                                                     const int32_t* __restrict__ bread,
+                                                     const int32_t* __restrict__ brpos,
+                                                     const int32_t* __restrict__ brlen,
+                                                     const uint32_t* __restrict__ jb,
+                                                     const uint64_t* __restrict__ cnt_f,
+                                                     const uint64_t* __restrict__ cnt_c,
+                                                     const uint64_t* __restrict__ foff,
+                                                     const uint64_t* __restrict__ coff, int64_t na, int koff,
+                                                     HitBits hb, uint64_t* fkey, uint32_t* fdiag, uint64_t* ckey,
+                                                     uint32_t* cdiag)
+{
+    const int64_t i = (int64_t)blockIdx.x * F2T + threadIdx.x;
+    if (i >= na)
+        return;
+    const uint64_t n = cnt_f[i] + cnt_c[i];
+    if (!n)
+        return;
+    uint64_t of = foff[i], oc = coff[i];
+    const int ar = aread[i] >> 1, as = aread[i] & 1, ap = arpos[i];
+    const uint64_t akey = ((uint64_t)ar << hb.pbits) | (uint64_t)ap;
+    const int sh = hb.pbits + hb.abits;
+    const uint32_t b0 = jb[i];
+    for (uint64_t j = 0; j < n; j++)
+    {
+        const uint32_t q = b0 + (uint32_t)j;
+        const int br = bread[q] >> 1, bs = bread[q] & 1;
+        const uint64_t key = ((uint64_t)br << sh) | akey;
+        if (bs == as)
+        {
+            fkey[of] = key;
+            fdiag[of] = (uint32_t)(ap - brpos[q]);
+            of++;
+        }
+        else
+        {
+            ckey[oc] = key;
+            cdiag[oc] = (uint32_t)(ap - ((brlen[br] - brpos[q]) + koff));
+            oc++;
+        }
+    }
+}
+
+int launch_d2_emit_hits(const int32_t* aread, const int32_t* arpos, const int32_t* bread, const int32_t* brpos,
+                        const int32_t* brlen, const uint32_t* jb, const uint64_t* cnt_f, const uint64_t* cnt_c,
+                        const uint64_t* foff, const uint64_t* coff, int64_t na, int kmer, HitBits hb, uint64_t* fkey,
+                        uint32_t* fdiag, uint64_t* ckey, uint32_t* cdiag, cudaStream_t s)
+{
+    if (na <= 0)
+        return 0;
+    k_d2_emit_hits<<<(unsigned)gd_cdiv<int64_t>(na, F2T), F2T, 0, s>>>(aread, arpos, bread, brpos, brlen, jb, cnt_f,
+                                                                       cnt_c, foff, coff, na, kmer - 2, hb, fkey,
+                                                                       fdiag, ckey, cdiag);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+#define INST2(K)                                                                                                 \
+    template int launch_d2_emit<K>(const DevBlock&, const int64_t*, const int32_t*, int, const D2Masks&, int64_t, \
+                                   const uint32_t*, K*, uint32_t*, int32_t*, int32_t*, cudaStream_t);            \
+    template int launch_d2_gather<K>(const K*, const uint32_t*, int64_t, const int32_t*, const int32_t*, K*,     \
+                                     int32_t*, int32_t*, cudaStream_t);                                          \
+    template int launch_d2_pair_count<K>(const K*, const int32_t*, const uint32_t*, const uint32_t*, const K*,   \
+                                         const int32_t*, const uint32_t*, int64_t, int64_t, int, int, uint32_t*,  \
+                                         uint64_t*, uint64_t*, unsigned long long*, cudaStream_t);
+INST2(uint32_t)
+INST2(uint64_t)
+#undef INST2
+
+}  // namespace gd

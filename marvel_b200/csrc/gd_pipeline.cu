@@ -17,6 +17,7 @@
 #include "../../include/gpudalign.h"
 #include "gd_align.cuh"
 #include "gd_filter.cuh"
+#include "gd_filter2.cuh"
 #include "gd_dust.cuh"
 #include "gd_output.cuh"
 #include "gd_prims.cuh"
@@ -180,6 +181,8 @@ struct gd_context
     DevBuf ascr_w, wide;  // the wide aligner instance's scratch, and its group list + count
     int agrid_w = 0;
     int test_narrow = 0;  // tests only: the main aligner pass with the 32-diagonal instance
+    int variant = 1, hgap = 0;  // 2 = daligner2 (modimizer seeds, dalign2/), its -H
+    DevBuf d2rd, d2rp, d2sgn, cnt2, hoff2, hk2, hd2;
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
     uint64_t rcap = 1 << 22, tbcap = 512ull << 20;
     // the overlap buffer: records and trace bytes of every Match_Filter since the last reset,
@@ -255,6 +258,9 @@ static int upload_spec(gd_context* c)
 // ----------------------------------------------------------------------------------------
 
 template <typename K>
+static int suppress_index(gd_context* c, Slot& sl, int64_t& n);
+
+template <typename K>
 static int64_t index_slot_t(gd_context* c, Slot& sl)
 {
     using namespace gd;
@@ -301,9 +307,22 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
         if (launch_decode<K>(sl.blk, Kmer, svals, n, P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
             return -1;
     }
+    if (suppress_index<K>(c, sl, n))
+        return -1;
+    GD_CUDA(cudaStreamSynchronize(s));
+    sl.nk = n;
+    return n;
+}
+
+// -t: drop codes occurring >= t times (compsize/compress_thread, filter.c:645-696 and
+// dalign2/filter.c:771-832); k0, k1 (2n int32), v0 and v1 hold at least n entries
+template <typename K>
+static int suppress_index(gd_context* c, Slot& sl, int64_t& n)
+{
+    using namespace gd;
+    cudaStream_t s = c->s;
     if (c->suppress > 0 && n > 0)
     {
-        // -t: drop codes occurring >= t times (compsize/compress_thread, filter.c:645-696)
         uint32_t* keep = P<uint32_t>(c->v0);
         uint32_t* pos = P<uint32_t>(c->v1);
         if (ensure(c->misc, 64))
@@ -327,6 +346,58 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
         GD_CUDA(cudaMemcpyAsync(sl.rpos.p, rpos2, kept * 4ull, cudaMemcpyDeviceToDevice, s));
         n = kept;
     }
+    return 0;
+}
+
+// daligner2's Sort_Kmers (dalign2/filter.c:834-1106): the modimizer list in the reference's
+// order (per slot counts, their scan, emission), the stable radix sort on (k-1)/4+1 code
+// bytes, the gather of (read << 1 | strand, position), -t.
+template <typename K>
+static int64_t index_slot_d2_t(gd_context* c, Slot& sl)
+{
+    using namespace gd;
+    const int Kmer = c->kmer;
+    const int64_t nslots = sl.nslots;
+    cudaStream_t s = c->s;
+    sl.nk = 0;
+    if (nslots <= 0)
+        return 0;
+    const D2Masks M = d2_masks(Kmer);
+    const int64_t* manno = sl.has_mask ? P<int64_t>(sl.manno) : nullptr;
+    const int32_t* mdata = sl.has_mask ? P<int32_t>(sl.mdata) : nullptr;
+    if (ensure(c->flags, nslots * 4) || ensure(c->excl, nslots * 4 + 4) ||
+        ensure(c->scratch, scan_scratch_bytes<uint32_t>(nslots)) || ensure(c->misc, 64))
+        return -1;
+    uint32_t* d_tot = P<uint32_t>(c->misc) + 4;
+    if (launch_d2_count(sl.blk, manno, mdata, Kmer, M, nslots, P<uint32_t>(c->flags), s) ||
+        exclusive_scan<uint32_t>(P<uint32_t>(c->flags), P<uint32_t>(c->excl), nslots, d_tot, c->scratch.p, s))
+        return -1;
+    uint32_t ne = 0;
+    GD_CUDA(cudaMemcpyAsync(&ne, d_tot, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    int64_t n = ne;
+    if (n == 0)
+        return 0;
+    if (ensure(c->k0, n * sizeof(K)) || ensure(c->k1, n * 8) || ensure(c->v0, n * 4) || ensure(c->v1, n * 4) ||
+        ensure(c->d2rd, n * 4) || ensure(c->d2rp, n * 4) || ensure(c->scratch, radix_scratch_bytes(n)) ||
+        ensure(sl.code, (n + 1) * sizeof(K)) || ensure(sl.read, (n + 1) * 4) || ensure(sl.rpos, (n + 1) * 4))
+        return -1;
+    if (launch_d2_emit<K>(sl.blk, manno, mdata, Kmer, M, nslots, P<uint32_t>(c->excl), P<K>(c->k0),
+                          P<uint32_t>(c->v0), P<int32_t>(c->d2rd), P<int32_t>(c->d2rp), s))
+        return -1;
+    int sort_bits = 8 * ((Kmer - 1) / 4 + 1);  // mersort bytes (dalign2/filter.c:942-953)
+    if (sort_bits > (int)(8 * sizeof(K)))
+        sort_bits = 8 * sizeof(K);
+    int which = radix_sort_pairs<K>(P<K>(c->k0), P<uint32_t>(c->v0), P<K>(c->k1), P<uint32_t>(c->v1), n, 0,
+                                    sort_bits, c->scratch.p, s);
+    if (which < 0)
+        return -1;
+    if (launch_d2_gather<K>(which ? P<K>(c->k1) : P<K>(c->k0), which ? P<uint32_t>(c->v1) : P<uint32_t>(c->v0), n,
+                            P<int32_t>(c->d2rd), P<int32_t>(c->d2rp), P<K>(sl.code), P<int32_t>(sl.read),
+                            P<int32_t>(sl.rpos), s))
+        return -1;
+    if (suppress_index<K>(c, sl, n))
+        return -1;
     GD_CUDA(cudaStreamSynchronize(s));
     sl.nk = n;
     return n;
@@ -353,6 +424,11 @@ static int tri_append(gd_context* c, unsigned ng)
     }
     return 0;
 }
+
+static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBits hb, int comp, int self);
+static int pair_cap(gd_context* c, int64_t na, int64_t nb, int same_index, int* limit_out);
+template <typename K>
+static int match_emit_t(gd_context* c, Slot& A, Slot& B, int64_t na, uint64_t* d_nhits, int comp, int self);
 
 template <typename K>
 static int match_filter_t(gd_context* c, int bslot, int comp, int self)
@@ -392,15 +468,31 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
                              P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<unsigned long long>(c->ctrun), s) ||
         launch_gram(P<unsigned long long>(c->ctrun), nruns, P<unsigned long long>(c->gram), s))
         return -1;
+    int limit;
+    if (pair_cap(c, na, nb, self && !comp, &limit))  // asort == bsort only for the self N call
+        return -1;
+    c->stats.limit[oi] = limit;
+    uint64_t* d_nhits = (uint64_t*)(P<uint32_t>(c->misc) + 16);
+    if (launch_cnt_mask(P<uint32_t>(c->excl), P<uint32_t>(c->flags), P<unsigned long long>(c->ctrun), na, limit,
+                        self && c->identity && comp, P<uint64_t>(c->cnt), s) ||
+        exclusive_scan<uint64_t>(P<uint64_t>(c->cnt), P<uint64_t>(c->hoff), na, d_nhits, c->scratch.p, s))
+        return -1;
+    return match_emit_t<K>(c, A, B, na, d_nhits, comp, self);
+}
+
+// The pair cap from the memory limit (filter.c:2107-2174, dalign2/filter.c:2430-2480), from
+// the histogram of per-code pair counts in c->gram.
+static int pair_cap(gd_context* c, int64_t na, int64_t nb, int same_index, int* limit_out)
+{
+    using namespace gd;
+    cudaStream_t s = c->s;
     std::vector<unsigned long long> gram(MAXGRAM);
     GD_CUDA(cudaMemcpyAsync(gram.data(), c->gram.p, MAXGRAM * 8, cudaMemcpyDeviceToHost, s));
     GD_CUDA(cudaStreamSynchronize(s));
-    // the pair cap from the memory limit (filter.c:2107-2174)
     int limit = INT32_MAX;
     if (c->mem_limit > 0)
     {
         int64_t avail;
-        int same_index = self && !comp;  // asort == bsort only for the self N call
         uint64_t dsz = c->mem_limit / 16;
         if (same_index || (int64_t)dsz > na + 2 * nb)
             avail = ((int64_t)dsz - na) / 2;
@@ -426,12 +518,18 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
             fprintf(stderr, "\nWarning: Sensitivity hampered by low memory allocation (%.1fGb)\n",
                     (1. * c->mem_limit) / 0x40000000ll);
     }
-    c->stats.limit[oi] = limit;
-    uint64_t* d_nhits = (uint64_t*)(P<uint32_t>(c->misc) + 16);
-    if (launch_cnt_mask(P<uint32_t>(c->excl), P<uint32_t>(c->flags), P<unsigned long long>(c->ctrun), na, limit,
-                        self && c->identity && comp, P<uint64_t>(c->cnt), s) ||
-        exclusive_scan<uint64_t>(P<uint64_t>(c->cnt), P<uint64_t>(c->hoff), na, d_nhits, c->scratch.p, s))
-        return -1;
+    *limit_out = limit;
+    return 0;
+}
+
+// daligner's emission of one orientation's hits (merge_thread, filter.c:1061-1231) after the
+// per-entry counts are capped and scanned, then the hit sort, groups and alignment.
+template <typename K>
+static int match_emit_t(gd_context* c, Slot& A, Slot& B, int64_t na, uint64_t* d_nhits, int comp, int self)
+{
+    using namespace gd;
+    cudaStream_t s = c->s;
+    const int oi = comp ? 1 : 0;
     uint64_t nhits = 0;
     GD_CUDA(cudaMemcpyAsync(&nhits, d_nhits, 8, cudaMemcpyDeviceToHost, s));
     GD_CUDA(cudaStreamSynchronize(s));
@@ -460,6 +558,127 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
                     P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<uint64_t>(c->hoff), na, hb, P<uint64_t>(c->hk0),
                     P<uint32_t>(c->hd0), s))
         return -1;
+    return align_hits(c, A, B, nhits, hb, comp, self);
+}
+
+// daligner2's Match_Filter (dalign2/filter.c:2344-2700) for A (slot 0) against B (bslot),
+// both orientations from one join: per A entry the B range of its code split by strand
+// agreement, the pair cap over both, and the hits of each orientation in generation order;
+// then each orientation's hit sort, groups and alignment (complement groups against the
+// complemented B block in cslot).
+template <typename K>
+static int match_filter_d2_t(gd_context* c, int bslot, int cslot, int self)
+{
+    using namespace gd;
+    cudaStream_t s = c->s;
+    Slot& A = c->slot[0];
+    Slot& B = c->slot[bslot];
+    Slot& C = c->slot[cslot];
+    for (int oi = 0; oi < 2; oi++)
+    {
+        c->stats.hits[oi] = c->stats.groups[oi] = c->stats.seeds[oi] = c->stats.cells[oi] = 0;
+        c->stats.skipped[oi] = 0;
+        c->stats.wide[oi] = 0;
+        c->stats.ms_merge[oi] = c->stats.ms_align[oi] = 0;
+    }
+    c->nhits = 0;
+    const int64_t na = A.nk, nb = B.nk;
+    if (na <= 0 || nb <= 0)
+        return 0;
+    GD_CUDA(cudaEventRecord(c->ev0, s));
+    if (ensure(c->flags, na * 4) || ensure(c->excl, na * 4) || ensure(c->jb, na * 4) || ensure(c->cnt, na * 8) ||
+        ensure(c->cnt2, na * 8) || ensure(c->hoff, na * 8) || ensure(c->hoff2, na * 8) ||
+        ensure(c->d2sgn, (nb + 1) * 4) ||
+        ensure(c->scratch, std::max(std::max(scan_scratch_bytes<uint64_t>(na), scan_scratch_bytes<uint32_t>(nb)),
+                                    (size_t)4096)) ||
+        ensure(c->misc, 256) || ensure(c->gram, MAXGRAM * 8))
+        return -1;
+    uint32_t* d_nruns = P<uint32_t>(c->misc) + 8;
+    uint32_t* sgn = P<uint32_t>(c->d2sgn);
+    if (launch_run_flags<K>(P<K>(A.code), na, P<uint32_t>(c->flags), s) ||
+        exclusive_scan<uint32_t>(P<uint32_t>(c->flags), P<uint32_t>(c->excl), na, d_nruns, c->scratch.p, s) ||
+        launch_d2_strand_flags(P<int32_t>(B.read), nb, sgn, s) ||
+        exclusive_scan<uint32_t>(sgn, sgn, nb, sgn + nb, c->scratch.p, s))
+        return -1;
+    uint32_t nruns = 0;
+    GD_CUDA(cudaMemcpyAsync(&nruns, d_nruns, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    if (ensure(c->ctrun, (size_t)nruns * 8 + 8))
+        return -1;
+    GD_CUDA(cudaMemsetAsync(c->ctrun.p, 0, (size_t)nruns * 8, s));
+    if (launch_d2_pair_count<K>(P<K>(A.code), P<int32_t>(A.read), P<uint32_t>(c->excl), P<uint32_t>(c->flags),
+                                P<K>(B.code), P<int32_t>(B.read), sgn, na, nb, self, c->identity,
+                                P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<uint64_t>(c->cnt2),
+                                P<unsigned long long>(c->ctrun), s) ||
+        launch_gram(P<unsigned long long>(c->ctrun), nruns, P<unsigned long long>(c->gram), s))
+        return -1;
+    int limit;
+    if (pair_cap(c, na, nb, self, &limit))
+        return -1;
+    c->stats.limit[0] = c->stats.limit[1] = limit;
+    uint64_t* d_nf = (uint64_t*)(P<uint32_t>(c->misc) + 16);
+    uint64_t* d_nc = (uint64_t*)(P<uint32_t>(c->misc) + 20);
+    if (launch_cnt_mask(P<uint32_t>(c->excl), P<uint32_t>(c->flags), P<unsigned long long>(c->ctrun), na, limit, 0,
+                        P<uint64_t>(c->cnt), s) ||
+        launch_cnt_mask(P<uint32_t>(c->excl), P<uint32_t>(c->flags), P<unsigned long long>(c->ctrun), na, limit, 0,
+                        P<uint64_t>(c->cnt2), s) ||
+        exclusive_scan<uint64_t>(P<uint64_t>(c->cnt), P<uint64_t>(c->hoff), na, d_nf, c->scratch.p, s) ||
+        exclusive_scan<uint64_t>(P<uint64_t>(c->cnt2), P<uint64_t>(c->hoff2), na, d_nc, c->scratch.p, s))
+        return -1;
+    uint64_t nf = 0, nc = 0;
+    GD_CUDA(cudaMemcpyAsync(&nf, d_nf, 8, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaMemcpyAsync(&nc, d_nc, 8, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    c->stats.hits[0] = (int64_t)nf;
+    c->stats.hits[1] = (int64_t)nc;
+    if (nf == 0 && nc == 0)
+        return 0;
+    const uint64_t nmax = std::max(nf, nc);
+    if (nmax > 0xffffffffull)
+    {
+        gd_set_error("%llu hits exceed the 32-bit hit index of this build", (unsigned long long)nmax);
+        return -1;
+    }
+    HitBits hb;
+    hb.pbits = bits_for(std::max(A.blk.maxlen - 1, 1));
+    hb.abits = bits_for(std::max(A.blk.nreads - 1, 1));
+    hb.bbits = bits_for(std::max(B.blk.nreads - 1, 1));
+    if (hb.pbits + hb.abits + hb.bbits > 64)
+    {
+        gd_set_error("hit key needs %d bits (> 64): block too large for this build", hb.pbits + hb.abits + hb.bbits);
+        return -1;
+    }
+    if (ensure(c->hk0, nmax * 8 + 8) || ensure(c->hk1, nmax * 8 + 8) || ensure(c->hd0, nmax * 4 + 4) ||
+        ensure(c->hd1, nmax * 4 + 4) || ensure(c->hk2, nc * 8 + 8) || ensure(c->hd2, nc * 4 + 4) ||
+        ensure(c->scratch, radix_scratch_bytes(nmax)))
+        return -1;
+    if (launch_d2_emit_hits(P<int32_t>(A.read), P<int32_t>(A.rpos), P<int32_t>(B.read), P<int32_t>(B.rpos),
+                            P<int32_t>(B.rlen), P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<uint64_t>(c->cnt2),
+                            P<uint64_t>(c->hoff), P<uint64_t>(c->hoff2), na, c->kmer, hb, P<uint64_t>(c->hk0),
+                            P<uint32_t>(c->hd0), P<uint64_t>(c->hk2), P<uint32_t>(c->hd2), s))
+        return -1;
+    if (nf > 0 && align_hits(c, A, B, nf, hb, 0, self))
+        return -1;
+    if (nc > 0)
+    {
+        GD_CUDA(cudaEventRecord(c->ev0, s));
+        GD_CUDA(cudaMemcpyAsync(c->hk0.p, c->hk2.p, nc * 8, cudaMemcpyDeviceToDevice, s));
+        GD_CUDA(cudaMemcpyAsync(c->hd0.p, c->hd2.p, nc * 4, cudaMemcpyDeviceToDevice, s));
+        if (align_hits(c, A, C, nc, hb, 1, self))
+            return -1;
+    }
+    return 0;
+}
+
+// The hits of one orientation in (hk0, hd0), in generation order, through the hit sort, the
+// pair groups, the learned triage and the seed scan + alignment; records are appended to the
+// overlap buffer in HBM.  c->ev0 marks the start of this orientation's merge stage.
+static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBits hb, int comp, int self)
+{
+    using namespace gd;
+    cudaStream_t s = c->s;
+    const int oi = comp ? 1 : 0;
+    const int hbits = hb.pbits + hb.abits + hb.bbits;
     // hit sort by (bread, aread, apos), stable (pairsort, filter.c:2030-2054, 2239-2252)
     int which = radix_sort_pairs<uint64_t>(P<uint64_t>(c->hk0), P<uint32_t>(c->hd0), P<uint64_t>(c->hk1),
                                            P<uint32_t>(c->hd1), nhits, 0, hbits, c->scratch.p, s);
@@ -551,6 +770,8 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     ap.mscore = c->mscore;
     ap.dscore = c->dscore;
     ap.test_narrow = c->test_narrow;
+    ap.d2 = c->variant == 2;
+    ap.hgap = c->hgap;
     if ((!c->agrid && align_grid(&c->agrid, 0)) || (!c->agrid_w && align_grid(&c->agrid_w, 1)))
         return -1;
     int nwarps = c->agrid * ALIGN_WARPS;
@@ -1081,7 +1302,11 @@ int64_t gd_sort_kmers(gd_context* c, int slot)
         return -1;
     }
     GD_CUDA(cudaEventRecord(c->ev0, c->s));
-    int64_t n = c->kmer <= 15 ? index_slot_t<uint32_t>(c, c->slot[slot]) : index_slot_t<uint64_t>(c, c->slot[slot]);
+    int64_t n;
+    if (c->variant == 2)
+        n = c->kmer <= 15 ? index_slot_d2_t<uint32_t>(c, c->slot[slot]) : index_slot_d2_t<uint64_t>(c, c->slot[slot]);
+    else
+        n = c->kmer <= 15 ? index_slot_t<uint32_t>(c, c->slot[slot]) : index_slot_t<uint64_t>(c, c->slot[slot]);
     GD_CUDA(cudaEventRecord(c->ev1, c->s));
     GD_CUDA(cudaEventSynchronize(c->ev1));
     float ms = 0;
@@ -1116,6 +1341,11 @@ int64_t gd_get_kmers(gd_context* c, int slot, uint64_t* code, int32_t* read, int
 
 int gd_match_filter(gd_context* c, int bslot, int comp, int self)
 {
+    if (c->variant != 1)
+    {
+        gd_set_error("gd_match_filter runs daligner's filter; daligner2 mode uses gd_match_filter2");
+        return -1;
+    }
     if (!c->spec_set)
     {
         gd_set_error("gd_new_align_spec has not been called");
@@ -1128,6 +1358,42 @@ int gd_match_filter(gd_context* c, int bslot, int comp, int self)
     }
     return c->kmer <= 15 ? match_filter_t<uint32_t>(c, bslot, comp, self)
                          : match_filter_t<uint64_t>(c, bslot, comp, self);
+}
+
+int gd_set_variant(gd_context* c, int variant, int hgap)
+{
+    if (variant != 1 && variant != 2)
+    {
+        gd_set_error("variant must be 1 (daligner) or 2 (daligner2), got %d", variant);
+        return -1;
+    }
+    c->variant = variant;
+    c->hgap = variant == 2 ? std::max(hgap, 0) : 0;
+    for (int i = 0; i < 3; i++)
+        c->slot[i].nk = -1;  // an index of the other kind must be rebuilt
+    return 0;
+}
+
+int gd_match_filter2(gd_context* c, int bslot, int cslot, int self)
+{
+    if (c->variant != 2)
+    {
+        gd_set_error("gd_match_filter2 needs gd_set_variant(ctx, 2, ...)");
+        return -1;
+    }
+    if (!c->spec_set)
+    {
+        gd_set_error("gd_new_align_spec has not been called");
+        return -1;
+    }
+    if (bslot < 0 || bslot > 2 || cslot < 0 || cslot > 2 || cslot == bslot || c->slot[0].nk < 0 ||
+        c->slot[bslot].nk < 0 || !c->slot[cslot].loaded)
+    {
+        gd_set_error("gd_match_filter2: both indices must be built and the complemented B block loaded");
+        return -1;
+    }
+    return c->kmer <= 15 ? match_filter_d2_t<uint32_t>(c, bslot, cslot, self)
+                         : match_filter_d2_t<uint64_t>(c, bslot, cslot, self);
 }
 
 int64_t gd_get_hits(gd_context* c, int32_t* rows4, int64_t cap)

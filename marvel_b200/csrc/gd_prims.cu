@@ -411,8 +411,8 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
     k_rs_scatter_pipe(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
                       uint32_t* __restrict__ vout, int64_t n, int shift, const uint32_t* __restrict__ offs, int ntiles)
 {
-    extern __shared__ __align__(128) unsigned char rs_smem[];
-    RsPipe<K>& S = *reinterpret_cast<RsPipe<K>*>(rs_smem);
+    extern __shared__ __align__(128) unsigned char rs_pipe_smem[];
+    RsPipe<K>& S = *reinterpret_cast<RsPipe<K>*>(rs_pipe_smem);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nfull = (int)(n / RS_TILE);
     constexpr unsigned TILE_BYTES = RS_TILE * (sizeof(K) + sizeof(uint32_t));

@@ -110,13 +110,18 @@ def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1):
         ctx = mb.Context()
         if wave_limit is not None:
             ctx.set_wave_limit(wave_limit)
+        if variant == 2:
+            ctx.set_variant(2, o["H"])
         ctx.set_filter_params(o["k"], o["w"], o["t"], o["h"])
         ctx.new_align_spec(o["e"], o["s"], A.freq, symmetric, o["O"], o["T"])
         ctx.set_globals(2 * o["l"], o["I"] or o["O"], mem)
         ctx.load_block(0, A)
         if not self_cmp:
             ctx.load_block(1, B)
-        mb.run_loaded(ctx, self_cmp)
+        if variant == 2:
+            mb.run_loaded2(ctx, self_cmp)
+        else:
+            mb.run_loaded(ctx, self_cmp)
         r, tr = ctx.overlaps()
         ctx.close()
         tb = 1 if tspace <= 125 else 2
