@@ -223,6 +223,33 @@ def run_gpu(args):
                "model": os.path.relpath(mtri.DEFAULT_MODEL, ROOT) + " (trained on the GPU on another genome of "
                         "this workload's model, seed offset 1)",
                "note": "records are a subset of the exact path's; recall < 1, so not the headline"}
+    # ---- daligner2 (modimizer seeds) on the same resident block, beside the headline path
+    d2 = None
+    if args.d2:
+        ctx.set_variant(2)
+        ctx.set_filter_params(14, 6, 0, 35)
+        ctx.load_block(0, A)
+        d2times, d2recs = [], 0
+        for i in range(1 + args.steps):
+            ctx.reset_overlap_buffer()
+            ctx.timer_mark(0)
+            mb.run_loaded2(ctx, True)
+            ctx.sort_overlaps()
+            ctx.timer_mark(1)
+            if i >= 1:
+                d2times.append(ctx.timer_elapsed_ms())
+                d2recs += ctx.stats()["records"]
+        d2st = ctx.stats()
+        ctx.set_variant(1)
+        barrier()
+        d2_ms, = reduce([sum(d2times)], torch.distributed.ReduceOp.MAX if ws > 1 else None)
+        d2recs_all, = reduce([float(d2recs)], torch.distributed.ReduceOp.SUM if ws > 1 else None)
+        d2 = {"value": round(d2recs_all / (d2_ms / 1e3), 1), "unit": "overlaps/s",
+              "ms_per_step": round(d2_ms / args.steps, 3), "records_per_step": d2recs // args.steps,
+              "stages_ms": {"index": round(d2st["ms_index"][0], 3), "merge_hitsort": round(sum(d2st["ms_merge"]), 3),
+                            "seed_scan_align": round(sum(d2st["ms_align"]), 3)},
+              "kmers": int(d2st["kmers"][0]), "hits": [int(x) for x in d2st["hits"]],
+              "note": "daligner2 (dalign2/, modimizer seeds), same block and flags, device-resident like value"}
     erecs_all, = reduce([float(erecs)], torch.distributed.ReduceOp.SUM if ws > 1 else None)
     e2e = erecs_all / (e_ms_max / 1e3)
 
@@ -282,10 +309,18 @@ def run_gpu(args):
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "triage": tri,
+            "daligner2": d2,
             "clocks": clocks,
         }
         if args.cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args)
+            if d2 is not None and ref_binary("daligner2"):
+                j = ref_threads()
+                n2, dt2 = run_reference_once(make_db(args.workload, scale=CPU_SAMPLE_SCALE), j, prog="daligner2")
+                d2["cpu_baseline"] = {"value": round(n2 / dt2, 1), "unit": "overlaps/s", "cores": j,
+                                      "kind": "reference",
+                                      "sample": f"reference daligner2 -T{j} on the {args.workload} model with a "
+                                                f"{CPU_SAMPLE_SCALE}x genome ({n2} overlaps, {dt2:.1f} s wall)"}
         print(json.dumps(out), flush=True)
     ctx.close()
     if ws > 1:
@@ -310,8 +345,8 @@ def load_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
-def ref_binary():
-    b = os.path.join(ROOT, "oracle", "_ref", "daligner")
+def ref_binary(prog="daligner"):
+    b = os.path.join(ROOT, "oracle", "_ref", prog)
     return b if os.path.exists(b) and os.access(b, os.X_OK) else None
 
 
@@ -323,17 +358,21 @@ def ref_threads():
     return j
 
 
-def run_reference_once(path, threads, h=35):
-    """The reference daligner on a block against itself; returns (records, seconds).  With
-    h=100000 no pair group reaches the aligner: the filter alone."""
-    b = ref_binary()
+def run_reference_once(path, threads, h=35, prog="daligner"):
+    """The reference daligner (or daligner2) on a block against itself; returns (records,
+    seconds).  With h=100000 no pair group reaches the aligner: the filter alone."""
+    b = ref_binary(prog)
     d = os.path.dirname(path)
     name = os.path.basename(path)
-    cmd = [b, f"-j{threads}", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
+    if prog == "daligner2":
+        cmd = [b, f"-T{threads}", "-Pd2out", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
+        las = os.path.join(d, "d2out_00001", "W.1.W.1.las")
+    else:
+        cmd = [b, f"-j{threads}", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
+        las = os.path.join(d, "001_00001", "W.1.W.1.las")
     t = time.perf_counter()
     subprocess.run(cmd, cwd=d, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     dt = time.perf_counter() - t
-    las = os.path.join(d, "001_00001", "W.1.W.1.las")
     with open(las, "rb") as f:
         n = int(np.frombuffer(f.read(8), "<i8")[0])
     return n, dt
@@ -414,6 +453,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-triage", dest="triage", action="store_false",
                     help="skip the learned-triage measurement (reported beside the exact path)")
+    ap.add_argument("--no-d2", dest="d2", action="store_false",
+                    help="skip the daligner2 (modimizer seeds) measurement (reported beside the exact path)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
