@@ -231,6 +231,28 @@ __global__ void __launch_bounds__(FT) k_run_flags(const K* __restrict__ code, in
         flags[i] = (i == 0 || code[i] != code[i - 1]) ? 1u : 0u;
 }
 
+__global__ void __launch_bounds__(FT) k_run_starts(const uint32_t* __restrict__ flags,
+                                                  const uint32_t* __restrict__ excl, int64_t n, uint32_t nruns,
+                                                  uint32_t* runstart)
+{
+    int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i < n && flags[i])
+        runstart[excl[i]] = (uint32_t)i;
+    if (i == 0)
+        runstart[nruns] = (uint32_t)n;
+}
+
+int launch_run_starts(const uint32_t* flags, const uint32_t* excl, int64_t n, uint32_t nruns, uint32_t* runstart,
+                      cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_run_starts<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(flags, excl, n, nruns, runstart);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 template <typename K>
 int launch_run_flags(const K* code, int64_t n, uint32_t* flags, cudaStream_t s)
 {
@@ -257,23 +279,37 @@ __global__ void __launch_bounds__(FT) k_pair_count(const K* __restrict__ acode, 
     __shared__ int64_t s_lo, s_hi;
     const int64_t t0 = (int64_t)blockIdx.x * FT;
     const int64_t t1 = min(t0 + FT, m.na) - 1;
-    if (threadIdx.x == 0)
-        s_lo = lower_code(bcode, m.nb, acode[t0]);
-    else if (threadIdx.x == 32)
-        s_hi = upper_code(bcode, m.nb, acode[t1]);
+    if (!m.runstart)
+    {
+        if (threadIdx.x == 0)
+            s_lo = lower_code(bcode, m.nb, acode[t0]);
+        else if (threadIdx.x == 32)
+            s_hi = upper_code(bcode, m.nb, acode[t1]);
+    }
     __syncthreads();
     int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
     bool act = i < m.na;
     uint64_t n = 0;
     uint32_t run = 0;
-    if (act)
+    if (act && m.runstart)
+    {
+        // B is A's own index: the run is i's own run; the entries pairing with i are the
+        // run's earlier entries of smaller reads (of any earlier entry with -I, filter.c:984-998)
+        run = arun_excl[i] + arun_flag[i] - 1;
+        const int64_t jb = m.runstart[run];
+        const int64_t e = m.identity ? i : same_read_start(aread, jb, i, 0);
+        n = (uint64_t)(e - jb);
+        jb_out[i] = (uint32_t)jb;
+        cnt_out[i] = n;
+    }
+    else if (act)
     {
         K c = acode[i];
         const int64_t lo = s_lo, hi = s_hi;
         int64_t jb = lower_code_in(bcode, lo, hi, c);
         int64_t je = jb;
         if (jb < hi && bcode[jb] == c)
-            je = upper_code_in(bcode, jb, hi, c);
+            je = upper_code_from(bcode, jb, hi, c);
         int ar = aread[i], ap = arpos[i];
         int64_t e = je;
         if (m.self)

@@ -38,7 +38,14 @@ struct MergeArgs
 {
     int64_t na, nb;
     int self, identity, comp;
+    // non-null when B is A's own index (a block against itself, forward): the start of every
+    // code run of A (nruns + 1 entries, the last = na), so no searches are needed
+    const uint32_t* runstart;
 };
+
+// runstart[excl[i]] = i for every run head i, runstart[nruns] = n
+int launch_run_starts(const uint32_t* flags, const uint32_t* excl, int64_t n, uint32_t nruns, uint32_t* runstart,
+                      cudaStream_t s);
 
 template <typename K>
 int launch_run_flags(const K* code, int64_t n, uint32_t* flags, cudaStream_t s);
@@ -130,6 +137,56 @@ __device__ __forceinline__ int64_t upper_code_in(const K* a, int64_t l, int64_t 
             l = m + 1;
         else
             r = m;
+    }
+    return l;
+}
+
+// First index of the run end after jb (the first entry > x), galloping from jb: runs are short.
+template <typename K>
+__device__ __forceinline__ int64_t upper_code_from(const K* a, int64_t jb, int64_t r, K x)
+{
+    int64_t l = jb, step = 1;  // a[l] <= x
+    while (true)
+    {
+        const int64_t j = l + step;
+        if (j >= r || a[j] > x)
+            return upper_code_in(a, l + 1, min(j, r), x);
+        l = j;
+        step <<= 1;
+    }
+}
+
+// The first index j in [lo, i] from which read[j] >> shift equals read[i] >> shift (the
+// entries are sorted by read within their code run), galloping back from i.
+__device__ __forceinline__ int64_t same_read_start(const int32_t* __restrict__ read, int64_t lo, int64_t i,
+                                                   int shift)
+{
+    const int key = read[i] >> shift;
+    int64_t l = i, step = 1;  // read[l] matches
+    int64_t j;
+    while (true)
+    {
+        j = l - step;
+        if (j < lo)
+        {
+            if ((read[lo] >> shift) == key)
+                return lo;
+            j = lo;
+            break;
+        }
+        if ((read[j] >> shift) != key)
+            break;
+        l = j;
+        step <<= 1;
+    }
+    // read[j] does not match, read[l] does
+    while (l - j > 1)
+    {
+        const int64_t md = (j + l) >> 1;
+        if ((read[md] >> shift) == key)
+            l = md;
+        else
+            j = md;
     }
     return l;
 }

@@ -242,6 +242,7 @@ template <typename K>
 __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ acode, const int32_t* __restrict__ aread,
                                                       const uint32_t* __restrict__ arun_excl,
                                                       const uint32_t* __restrict__ arun_flag,
+                                                      const uint32_t* __restrict__ runstart,
                                                       const K* __restrict__ bcode, const int32_t* __restrict__ bread,
                                                       const uint32_t* __restrict__ bstrand_excl, int64_t na,
                                                       int64_t nb, int self, int identity, uint32_t* jb_out,
@@ -250,10 +251,13 @@ __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ aco
     __shared__ int64_t s_lo, s_hi;
     const int64_t t0 = (int64_t)blockIdx.x * F2T;
     const int64_t t1 = min(t0 + F2T, na) - 1;
-    if (threadIdx.x == 0)
-        s_lo = lower_code(bcode, nb, acode[t0]);
-    else if (threadIdx.x == 32)
-        s_hi = upper_code(bcode, nb, acode[t1]);
+    if (!runstart)
+    {
+        if (threadIdx.x == 0)
+            s_lo = lower_code(bcode, nb, acode[t0]);
+        else if (threadIdx.x == 32)
+            s_hi = upper_code(bcode, nb, acode[t1]);
+    }
     __syncthreads();
     const int64_t i = t0 + threadIdx.x;
     const bool act = i < na;
@@ -261,29 +265,40 @@ __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ aco
     uint32_t run = 0;
     if (act)
     {
-        const K c = acode[i];
-        const int64_t jb = lower_code_in(bcode, s_lo, s_hi, c);
-        int64_t je = jb;
-        if (jb < s_hi && bcode[jb] == c)
-            je = upper_code_in(bcode, jb, s_hi, c);
         const int ar = aread[i];
-        int64_t e = je;
-        if (self)
+        int64_t jb, e;
+        if (runstart)
         {
-            if (identity)
-                e = i;  // every earlier entry of the run (A and B are the same index)
-            else
+            // B is A's own index: i's own run; the earlier entries of smaller reads (any
+            // earlier entry with -I), found by galloping back over i's read
+            jb = runstart[arun_excl[i] + arun_flag[i] - 1];
+            e = identity ? i : same_read_start(aread, jb, i, 1);
+        }
+        else
+        {
+            const K c = acode[i];
+            jb = lower_code_in(bcode, s_lo, s_hi, c);
+            int64_t je = jb;
+            if (jb < s_hi && bcode[jb] == c)
+                je = upper_code_from(bcode, jb, s_hi, c);
+            e = je;
+            if (self)
             {
-                int64_t l = jb, r = je;
-                while (l < r)
+                if (identity)
+                    e = i;  // every earlier entry of the run (A and B are the same index)
+                else
                 {
-                    const int64_t md = (l + r) >> 1;
-                    if ((bread[md] >> 1) < (ar >> 1))
-                        l = md + 1;
-                    else
-                        r = md;
+                    int64_t l = jb, r = je;
+                    while (l < r)
+                    {
+                        const int64_t md = (l + r) >> 1;
+                        if ((bread[md] >> 1) < (ar >> 1))
+                            l = md + 1;
+                        else
+                            r = md;
+                    }
+                    e = l;
                 }
-                e = l;
             }
         }
         n = (uint64_t)(e - jb);
@@ -305,15 +320,15 @@ __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ aco
 
 template <typename K>
 int launch_d2_pair_count(const K* acode, const int32_t* aread, const uint32_t* arun_excl, const uint32_t* arun_flag,
-                         const K* bcode, const int32_t* bread, const uint32_t* bstrand_excl, int64_t na, int64_t nb,
-                         int self, int identity, uint32_t* jb, uint64_t* cnt_f, uint64_t* cnt_c,
-                         unsigned long long* ctrun, cudaStream_t s)
+                         const uint32_t* runstart, const K* bcode, const int32_t* bread, const uint32_t* bstrand_excl,
+                         int64_t na, int64_t nb, int self, int identity, uint32_t* jb, uint64_t* cnt_f,
+                         uint64_t* cnt_c, unsigned long long* ctrun, cudaStream_t s)
 {
     if (na <= 0)
         return 0;
     k_d2_pair_count<K><<<(unsigned)gd_cdiv<int64_t>(na, F2T), F2T, 0, s>>>(
-        acode, aread, arun_excl, arun_flag, bcode, bread, bstrand_excl, na, nb, self, identity, jb, cnt_f, cnt_c,
-        ctrun);
+        acode, aread, arun_excl, arun_flag, runstart, bcode, bread, bstrand_excl, na, nb, self, identity, jb, cnt_f,
+        cnt_c, ctrun);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
@@ -386,9 +401,10 @@ int launch_d2_emit_hits(const int32_t* aread, const int32_t* arpos, const int32_
                                    const uint32_t*, K*, uint32_t*, int32_t*, int32_t*, cudaStream_t);            \
     template int launch_d2_gather<K>(const K*, const uint32_t*, int64_t, const int32_t*, const int32_t*, K*,     \
                                      int32_t*, int32_t*, cudaStream_t);                                          \
-    template int launch_d2_pair_count<K>(const K*, const int32_t*, const uint32_t*, const uint32_t*, const K*,   \
-                                         const int32_t*, const uint32_t*, int64_t, int64_t, int, int, uint32_t*,  \
-                                         uint64_t*, uint64_t*, unsigned long long*, cudaStream_t);
+    template int launch_d2_pair_count<K>(const K*, const int32_t*, const uint32_t*, const uint32_t*,             \
+                                         const uint32_t*, const K*, const int32_t*, const uint32_t*, int64_t,    \
+                                         int64_t, int, int, uint32_t*, uint64_t*, uint64_t*, unsigned long long*, \
+                                         cudaStream_t);
 INST2(uint32_t)
 INST2(uint64_t)
 #undef INST2

@@ -182,7 +182,7 @@ struct gd_context
     int agrid_w = 0;
     int test_narrow = 0;  // tests only: the main aligner pass with the 32-diagonal instance
     int variant = 1, hgap = 0;  // 2 = daligner2 (modimizer seeds, dalign2/), its -H
-    DevBuf d2rd, d2rp, d2sgn, cnt2, hoff2, hk2, hd2;
+    DevBuf d2rd, d2rp, d2sgn, cnt2, hoff2, hk2, hd2, runstart;
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
     uint64_t rcap = 1 << 22, tbcap = 512ull << 20;
     // the overlap buffer: records and trace bytes of every Match_Filter since the last reset,
@@ -462,7 +462,14 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     if (ensure(c->ctrun, (size_t)nruns * 8 + 8))
         return -1;
     GD_CUDA(cudaMemsetAsync(c->ctrun.p, 0, (size_t)nruns * 8, s));
-    MergeArgs m{na, nb, self, c->identity, comp};
+    MergeArgs m{na, nb, self, c->identity, comp, nullptr};
+    if (&B == &A)  // the block against its own index: run bounds without searches
+    {
+        if (ensure(c->runstart, ((size_t)nruns + 1) * 4) ||
+            launch_run_starts(P<uint32_t>(c->flags), P<uint32_t>(c->excl), na, nruns, P<uint32_t>(c->runstart), s))
+            return -1;
+        m.runstart = P<uint32_t>(c->runstart);
+    }
     if (launch_pair_count<K>(P<K>(A.code), P<int32_t>(A.read), P<int32_t>(A.rpos), P<uint32_t>(c->excl),
                              P<uint32_t>(c->flags), P<K>(B.code), P<int32_t>(B.read), P<int32_t>(B.rpos), m,
                              P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<unsigned long long>(c->ctrun), s) ||
@@ -606,8 +613,16 @@ static int match_filter_d2_t(gd_context* c, int bslot, int cslot, int self)
     if (ensure(c->ctrun, (size_t)nruns * 8 + 8))
         return -1;
     GD_CUDA(cudaMemsetAsync(c->ctrun.p, 0, (size_t)nruns * 8, s));
+    const uint32_t* runstart = nullptr;
+    if (&B == &A)  // the block against its own index: run bounds without searches
+    {
+        if (ensure(c->runstart, ((size_t)nruns + 1) * 4) ||
+            launch_run_starts(P<uint32_t>(c->flags), P<uint32_t>(c->excl), na, nruns, P<uint32_t>(c->runstart), s))
+            return -1;
+        runstart = P<uint32_t>(c->runstart);
+    }
     if (launch_d2_pair_count<K>(P<K>(A.code), P<int32_t>(A.read), P<uint32_t>(c->excl), P<uint32_t>(c->flags),
-                                P<K>(B.code), P<int32_t>(B.read), sgn, na, nb, self, c->identity,
+                                runstart, P<K>(B.code), P<int32_t>(B.read), sgn, na, nb, self, c->identity,
                                 P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<uint64_t>(c->cnt2),
                                 P<unsigned long long>(c->ctrun), s) ||
         launch_gram(P<unsigned long long>(c->ctrun), nruns, P<unsigned long long>(c->gram), s))
