@@ -1717,11 +1717,460 @@ static int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, TBuf* tb
     return no + 1;
 }
 
+/* ---- daligner2 bridging (DO_BRIDGING, dalign2/filter.c:1479-1705, 2124-2262) ---------- */
+
+/* split_nd (dalign2/align.c:4355-4523): bidirectional O(nd) waves over A[0,M) x B[0,N) until
+ * they meet; returns the edit distance D and the meeting point (x, y).  VF/VB as the
+ * reference places them in its vector (Compute_Alignment, :4815-4826). */
+static int split_nd(const uint8_t* A, int M, const uint8_t* B, int N, int* VF, int* VB, int* px, int* py)
+{
+    int x, y, D, flow, blow, bhgh;
+    const uint8_t* a;
+    y = 0;
+    if (N < M)
+        while (y < N && B[y] == A[y])
+            y += 1;
+    else
+    {
+        while (y < M && B[y] == A[y])
+            y += 1;
+        if (y >= M && N == M)
+        {
+            *px = *py = M;
+            return 0;
+        }
+    }
+    flow = 0;
+    VF[0] = y;
+    VF[-1] = -2;
+    x = N - M;
+    a = A - x;
+    y = N - 1;
+    if (N > M)
+        while (y >= x && B[y] == a[y])
+            y -= 1;
+    else
+        while (y >= 0 && B[y] == a[y])
+            y -= 1;
+    blow = bhgh = -x;
+    VB += x;
+    VB[blow] = y;
+    VB[blow - 1] = N + 1;
+    for (D = 1;; D += 1)
+    {
+        int k, r, am, ac, ap;
+        flow -= 1;
+        am = ac = VF[flow - 1] = -2;
+        a = A + D;
+        x = M - D;
+        for (k = D; k >= flow; k--)
+        {
+            ap = ac;
+            ac = am + 1;
+            am = VF[k - 1];
+            if (ac < am)
+                y = (ap < am) ? am : ap;
+            else
+                y = (ap < ac) ? ac : ap;
+            if (blow <= k && k <= bhgh)
+            {
+                r = VB[k];
+                if (y > r)
+                {
+                    D = (D << 1) - 1;
+                    if (ap > r)
+                        y = ap;
+                    else if (ac > r)
+                        y = ac;
+                    else
+                        y = r + 1;
+                    *px = k + y;
+                    *py = y;
+                    return D;
+                }
+            }
+            if (N < x)
+                while (y < N && B[y] == a[y])
+                    y += 1;
+            else
+                while (y < x && B[y] == a[y])
+                    y += 1;
+            VF[k] = y;
+            a -= 1;
+            x += 1;
+        }
+        bhgh += 1;
+        blow -= 1;
+        am = ac = VB[blow - 1] = N + 1;
+        a = A + bhgh;
+        x = -bhgh;
+        for (k = bhgh; k >= blow; k--)
+        {
+            ap = ac + 1;
+            ac = am;
+            am = VB[k - 1];
+            if (ac > am)
+                y = (ap > am) ? am : ap;
+            else
+                y = (ap > ac) ? ac : ap;
+            if (flow <= k && k <= D)
+            {
+                r = VF[k];
+                if (y <= r)
+                {
+                    D = (D << 1);
+                    if (ap <= r)
+                        y = ap;
+                    else if (ac <= r)
+                        y = ac;
+                    else
+                        y = r;
+                    *px = k + y;
+                    *py = y;
+                    return D;
+                }
+            }
+            y -= 1;
+            if (x > 0)
+                while (y >= x && B[y] == a[y])
+                    y -= 1;
+            else
+                while (y >= 0 && B[y] == a[y])
+                    y -= 1;
+            VB[k] = y;
+            a -= 1;
+            x += 1;
+        }
+    }
+}
+
+typedef struct
+{
+    const uint8_t* Aabs;
+    uint16_t* Trace; /* indexed by 2 * (absolute A position / tspace) */
+    int *VF, *VB;
+} TWave;
+
+/* trace_nd (dalign2/align.c:4525-4679): the trace-point counts (diffs, b-advance) of an
+ * optimal alignment of A[0,M) x B[0,N), split at midpoints until a piece lies inside one
+ * trace interval.  Every update is an addition, so the order of the pieces is free. */
+static int trace_nd(const uint8_t* A, int M, const uint8_t* B, int N, TWave* w, int tspace)
+{
+    int x, y, D, s;
+    if (M <= 0)
+    {
+        y = (int)(((A - w->Aabs) / tspace) << 1);
+        w->Trace[y] += N;
+        w->Trace[y + 1] += N;
+        return N;
+    }
+    if (N <= 0)
+    {
+        x = (int)(A - w->Aabs);
+        y = x / tspace;
+        x = (y + 1) * tspace - x;
+        y <<= 1;
+        for (s = M; s > 0; s -= x, x = tspace)
+        {
+            if (x > s)
+                x = s;
+            w->Trace[y] += x;
+            y += 2;
+        }
+        return M;
+    }
+    D = split_nd(A, M, B, N, w->VF, w->VB, &x, &y);
+    if (D > 1)
+    {
+        s = (int)(A - w->Aabs);
+        if ((s / tspace + 1) * tspace - s >= x)
+        {
+            s = ((s / tspace) << 1);
+            w->Trace[s] += (D + 1) / 2;
+            w->Trace[s + 1] += y;
+        }
+        else
+            trace_nd(A, x, B, y, w, tspace);
+        s = (int)((A + x) - w->Aabs);
+        if ((s / tspace + 1) * tspace - s >= M - x)
+        {
+            s = ((s / tspace) << 1);
+            w->Trace[s] += D / 2;
+            w->Trace[s + 1] += N - y;
+        }
+        else
+            trace_nd(A + x, M - x, B + y, N - y, w, tspace);
+    }
+    else
+    {
+        int u, v;
+        s = (D == 0 || M < N) ? x : x - 1;
+        if (s > 0)
+        {
+            u = (int)(A - w->Aabs);
+            v = u / tspace;
+            u = (v + 1) * tspace - u;
+            for (v <<= 1; s > 0; s -= u, u = tspace)
+            {
+                if (u > s)
+                    u = s;
+                w->Trace[v + 1] += u;
+                v += 2;
+            }
+        }
+        if (D == 0)
+            return D;
+        if (M < N)
+            y = (int)((((A + x) - w->Aabs) / tspace) << 1);
+        else
+            y = (int)((((A + (x - 1)) - w->Aabs) / tspace) << 1);
+        w->Trace[y] += 1;
+        if (M <= N)
+            w->Trace[y + 1] += 1;
+        s = M - x;
+        if (s > 0)
+        {
+            u = (int)((A + x) - w->Aabs);
+            v = u / tspace;
+            u = (v + 1) * tspace - u;
+            for (v <<= 1; s > 0; s -= u, u = tspace)
+            {
+                if (u > s)
+                    u = s;
+                w->Trace[v + 1] += u;
+                v += 2;
+            }
+        }
+    }
+    return D;
+}
+
+/* A bridge path: coordinates, diffs and its own trace (Compute_Alignment's alnpts). */
+typedef struct
+{
+    int abpos, bbpos, aepos, bepos, diffs, tlen;
+    uint16_t* trace;
+    int cap;
+} BPath;
+
+/* Compute_Alignment(align, work, DIFF_TRACE, tspace) (dalign2/align.c:4762-4913) for the box
+ * of p over aseq (its absolute base) and bseq. */
+static void compute_alignment_trace(const uint8_t* aseq, const uint8_t* bseq, BPath* p, int tspace)
+{
+    int asub = p->aepos - p->abpos, bsub = p->bepos - p->bbpos;
+    int n = 2 * (((p->aepos + (tspace - 1)) / tspace - p->abpos / tspace) + 1);
+    if (n > p->cap)
+    {
+        p->cap = 2 * n + 64;
+        p->trace = (uint16_t*)realloc(p->trace, sizeof(uint16_t) * p->cap);
+    }
+    int m = asub > bsub ? asub : bsub;
+    int* vec = (int*)malloc(sizeof(int) * (4 * (size_t)m + 6 + 8));
+    TWave w;
+    w.VF = vec + (m + 1);
+    w.VB = w.VF + (2 * m + 3);
+    w.Aabs = aseq;
+    w.Trace = p->trace - 2 * (p->abpos / tspace);
+    memset(p->trace, 0, sizeof(uint16_t) * n);
+    p->diffs = trace_nd(aseq + p->abpos, asub, bseq + p->bbpos, bsub, &w, tspace);
+    if (p->trace[n - 1] != 0)
+    {
+        p->trace[n - 3] += p->trace[n - 1];
+        p->trace[n - 4] += p->trace[n - 2];
+    }
+    p->tlen = n - 2;
+    free(vec);
+}
+
+/* MapToTPAbove / MapToTPBelow (dalign2/filter.c:1481-1563): the first trace point of path at
+ * or past *x (above) or at or before *x (below), in A (isA) or B; *x becomes it, the other
+ * coordinate is returned. */
+static int map_tp_above(const MPath* path, int* x, int isA, const TBuf* tb, int TS)
+{
+    const uint16_t* trace = tb->tr + path->toff;
+    int a = (path->abpos / TS) * TS, b = path->bbpos;
+    for (int i = 1; i < path->tlen; i += 2)
+    {
+        a += TS;
+        b += trace[i];
+        if (a > path->aepos)
+            a = path->aepos;
+        if (isA ? a >= *x : b >= *x)
+        {
+            int r = isA ? b : a;
+            *x = isA ? a : b;
+            return r;
+        }
+    }
+    int r = isA ? b : a;
+    *x = isA ? a : b;
+    return r;
+}
+
+static int map_tp_below(const MPath* path, int* x, int isA, const TBuf* tb, int TS)
+{
+    const uint16_t* trace = tb->tr + path->toff;
+    int a = ((path->aepos + (TS - 1)) / TS) * TS, b = path->bepos;
+    for (int i = path->tlen - 1; i >= 0; i -= 2)
+    {
+        a -= TS;
+        b -= trace[i];
+        if (a < path->abpos)
+            a = path->abpos;
+        if (isA ? a <= *x : b <= *x)
+        {
+            int r = isA ? b : a;
+            *x = isA ? a : b;
+            return r;
+        }
+    }
+    int r = isA ? b : a;
+    *x = isA ? a : b;
+    return r;
+}
+
+/* Compute_Bridge_Path (dalign2/filter.c:1579-1705): the box from two trace points before
+ * path2's start to two after path1's end, aligned afresh with trace points; with comp the
+ * box is aligned in the complemented frame, shifted so its trace points fall on multiples of
+ * the spacing.  (The bin/bout/err tail of the reference only feeds its debug print.) */
+static void compute_bridge_path(const MPath* path1, const MPath* path2, const uint8_t* aseq, const uint8_t* bseq,
+                                int alen, int blen, int comp, int aovl, int bovl, const TBuf* tb, int TS, BPath* ap)
+{
+    int ain, aout, bin, bout, boff = 0, p;
+    if (bovl > aovl)
+    {
+        bin = path2->bbpos;
+        bout = path1->bepos;
+        ain = map_tp_below(path1, &bin, 0, tb, TS);
+        aout = map_tp_above(path2, &bout, 0, tb, TS);
+    }
+    else
+    {
+        ain = path2->abpos;
+        aout = path1->aepos;
+        bin = map_tp_below(path1, &ain, 1, tb, TS);
+        bout = map_tp_above(path2, &aout, 1, tb, TS);
+    }
+    (void)bin;
+    (void)bout;
+    ap->abpos = ain - 2 * TS;
+    ap->aepos = aout + 2 * TS;
+    ap->bbpos = map_tp_below(path1, &ap->abpos, 1, tb, TS);
+    ap->bepos = map_tp_above(path2, &ap->aepos, 1, tb, TS);
+    const uint8_t* A = aseq;
+    if (comp)
+    {
+        boff = TS - ap->aepos % TS;
+        p = alen - ap->abpos;
+        ap->abpos = alen - ap->aepos;
+        ap->aepos = p;
+        p = blen - ap->bbpos;
+        ap->bbpos = blen - ap->bepos;
+        ap->bepos = p;
+        boff = boff - ap->abpos % TS;
+        A -= boff;
+        ap->abpos += boff;
+        ap->aepos += boff;
+    }
+    compute_alignment_trace(A, bseq, ap, TS);
+    if (comp)
+    {
+        uint16_t* trk = ap->trace;
+        int j = ap->tlen - 2, i = 0;
+        while (i < j)
+        {
+            uint16_t t = trk[i];
+            trk[i] = trk[j];
+            trk[j] = t;
+            t = trk[i + 1];
+            trk[i + 1] = trk[j + 1];
+            trk[j + 1] = t;
+            i += 2;
+            j -= 2;
+        }
+        ap->abpos -= boff;
+        ap->aepos -= boff;
+        p = alen - ap->abpos;
+        ap->abpos = alen - ap->aepos;
+        ap->aepos = p;
+        p = blen - ap->bbpos;
+        ap->bbpos = blen - ap->bepos;
+        ap->bepos = p;
+    }
+}
+
+/* Check_Bridge (dalign2/filter.c:1565-1577) */
+static int check_bridge(const BPath* p, int TS)
+{
+    if (TS <= 125)
+        for (int i = 0; i < p->tlen; i++)
+            if (p->trace[i] > 250)
+                return 1;
+    return 0;
+}
+
+/* Bridge (dalign2/filter.c:1885-1948): path1 up to the bridge, the bridge, path3 after it */
+static void bridge(MPath* path1, const BPath* path2, const MPath* path3, TBuf* tb, int TS)
+{
+    int k, k1, k2, len, diff;
+    k1 = 2 * ((path2->abpos / TS) - (path1->abpos / TS));
+    if (path2->aepos == path3->aepos)
+        k2 = path3->tlen;
+    else
+        k2 = 2 * ((path2->aepos / TS) - (path3->abpos / TS));
+    len = k1 + path2->tlen + (path3->tlen - k2);
+    tbuf_reserve(tb, len);
+    int64_t base = tb->top;
+    tb->top += len;
+    uint16_t* trace = tb->tr + base;
+    diff = 0;
+    len = 0;
+    if (k1 > 0)
+    {
+        const uint16_t* t = tb->tr + path1->toff;
+        for (k = 0; k < k1; k += 2)
+        {
+            trace[len++] = t[k];
+            trace[len++] = t[k + 1];
+            diff += t[k];
+        }
+    }
+    for (k = 0; k < path2->tlen; k += 2)
+    {
+        trace[len++] = path2->trace[k];
+        trace[len++] = path2->trace[k + 1];
+        diff += path2->trace[k];
+    }
+    if (k2 < path3->tlen)
+    {
+        const uint16_t* t = tb->tr + path3->toff;
+        for (k = k2; k < path3->tlen; k += 2)
+        {
+            trace[len++] = t[k];
+            trace[len++] = t[k + 1];
+            diff += t[k];
+        }
+    }
+    path1->aepos = path3->aepos;
+    path1->bepos = path3->bepos;
+    path1->diffs = diff;
+    path1->toff = base;
+    path1->tlen = len;
+}
+
+/* The sequences of a pair as Handle_Redundancies sees them: align (A against B, B
+ * complemented for a complement pair) and blign (the roles swapped). */
+typedef struct
+{
+    const uint8_t *aseq, *bseq;
+    int alen, blen, comp;
+} PairSeq;
+
 /* daligner2's Handle_Redundancies (dalign2/filter.c:1952-2272): paths fused into the later
- * index j, the absorbed one marked with abpos = -1 and the scan restarted after a fusion,
- * then compacted.  Its bridging pass (:2124-2262, Compute_Bridge_Path / Bridge) is detected,
- * not computed: returns -1 when a pair of paths would be bridged. */
-static int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, TBuf* tb, int TS, int comp)
+ * index j, the absorbed one marked with abpos = -1 and the scan restarted after a fusion;
+ * then the bridging pass; then compaction. */
+static int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, TBuf* tb, int TS, int comp,
+                                  const PairSeq* ps)
 {
     int j, k, no, dist, awhen = 0, bwhen = 0;
     int hasB = (bmatch != NULL);
@@ -1834,7 +2283,10 @@ static int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, TBuf*
             }
         }
     }
-    /* the bridging pass's entry test (dalign2/filter.c:2126-2175) */
+    /* the bridging pass (dalign2/filter.c:2124-2262): a pair of paths with a narrow
+     * parallel overlap is joined through a fresh alignment of the overlap's box; the A-side
+     * box is aligned uncomplemented, the B side in its pair's orientation */
+    BPath bp = {0, 0, 0, 0, 0, 0, NULL, 0};
     for (j = 1; j < novls; j++)
     {
         MPath* jpath = amatch + j;
@@ -1845,7 +2297,7 @@ static int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, TBuf*
             MPath* kpath = amatch + k;
             if (kpath->abpos < 0)
                 continue;
-            MPath *path1, *path2;
+            MPath *path1, *path2, *bath1 = NULL, *bath2 = NULL;
             if (jpath->abpos < kpath->abpos)
             {
                 path1 = jpath;
@@ -1865,7 +2317,6 @@ static int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, TBuf*
                 continue;
             if (hasB)
             {
-                MPath *bath1, *bath2;
                 if (comp == (jpath->abpos < kpath->abpos))
                 {
                     bath1 = bmatch + k;
@@ -1879,9 +2330,29 @@ static int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, TBuf*
                 if (bath1->abpos > bath2->abpos)
                     continue;
             }
-            return -1;
+            compute_bridge_path(path1, path2, ps->aseq, ps->bseq, ps->alen, ps->blen, 0, aovl, bovl, tb, TS, &bp);
+            if (check_bridge(&bp, TS))
+                continue;
+            MPath jback = *jpath, kback = *kpath;
+            bridge(path1, &bp, path2, tb, TS);
+            *jpath = *path1;
+            kpath->abpos = -1;
+            if (hasB)
+            {
+                compute_bridge_path(bath1, bath2, ps->bseq, ps->aseq, ps->blen, ps->alen, comp, bovl, aovl, tb, TS,
+                                    &bp);
+                if (check_bridge(&bp, TS))
+                {
+                    *jpath = jback;
+                    *kpath = kback;
+                    continue;
+                }
+                bridge(bath1, &bp, bath2, tb, TS);
+                bmatch[j] = *bath1;
+            }
         }
     }
+    free(bp.trace);
     no = 0;
     for (j = 0; j < novls; j++)
         if (amatch[j].abpos >= 0)
@@ -2137,15 +2608,18 @@ static void report(const or_block* A, const or_block* B, const Hit* hits, int64_
         if (d2)
         {
             int r1 = novla, r2 = novlb;
+            /* the pair's align (B complemented for a complement pair); a B-only call is
+             * handed the same align, as the reference does (filter_reporter_cpu.c:392-400) */
+            PairSeq ps = {aseq, bseq, alen, blen, comp};
             if (novla > 1)
             {
                 if (novlb > 1)
-                    r1 = r2 = handle_redundancies_d2(amatch, novla, bmatch, &tb, TS, comp);
+                    r1 = r2 = handle_redundancies_d2(amatch, novla, bmatch, &tb, TS, comp, &ps);
                 else
-                    r1 = handle_redundancies_d2(amatch, novla, NULL, &tb, TS, comp);
+                    r1 = handle_redundancies_d2(amatch, novla, NULL, &tb, TS, comp, &ps);
             }
             else if (novlb > 1)
-                r2 = handle_redundancies_d2(bmatch, novlb, NULL, &tb, TS, comp);
+                r2 = handle_redundancies_d2(bmatch, novlb, NULL, &tb, TS, comp, &ps);
             if (r1 < 0 || r2 < 0)
             {
                 *status = 1;
@@ -2560,6 +3034,57 @@ static void merge_hits2(const or_block* B, const KPos* al, int64_t alen, const K
     *nf = n1;
     *hc = Cm;
     *nc = n2;
+}
+
+int or_handle_redundancies_d2(const uint8_t* aseq, const uint8_t* bseq, int alen, int blen, int tspace, int comp,
+                              int novls, int hasB, const int32_t* hdr, const uint16_t* traces, int32_t* out_hdr,
+                              uint16_t* out_traces, int64_t tcap)
+{
+    TBuf tb = {0, 0, 0};
+    int npath = novls * (hasB ? 2 : 1);
+    MPath* m = (MPath*)malloc(sizeof(MPath) * (size_t)(npath + 1));
+    int64_t off = 0;
+    for (int i = 0; i < npath; i++)
+    {
+        const int32_t* h = hdr + 6 * i;
+        m[i].abpos = h[0];
+        m[i].bbpos = h[1];
+        m[i].aepos = h[2];
+        m[i].bepos = h[3];
+        m[i].diffs = h[4];
+        m[i].tlen = h[5];
+        tbuf_reserve(&tb, h[5] + 16);
+        memcpy(tb.tr + tb.top, traces + off, sizeof(uint16_t) * h[5]);
+        m[i].toff = tb.top;
+        tb.top += h[5];
+        off += h[5];
+    }
+    PairSeq ps = {aseq, bseq, alen, blen, comp};
+    int n = handle_redundancies_d2(m, novls, hasB ? m + novls : NULL, &tb, tspace, comp, &ps);
+    int64_t o = 0;
+    for (int side = 0; side < (hasB ? 2 : 1); side++)
+        for (int i = 0; i < n; i++)
+        {
+            const MPath* q = m + side * novls + i;
+            int32_t* h = out_hdr + 6 * (side * n + i);
+            h[0] = q->abpos;
+            h[1] = q->bbpos;
+            h[2] = q->aepos;
+            h[3] = q->bepos;
+            h[4] = q->diffs;
+            h[5] = q->tlen;
+            if (o + q->tlen > tcap)
+            {
+                free(m);
+                free(tb.tr);
+                return -1;
+            }
+            memcpy(out_traces + o, tb.tr + q->toff, sizeof(uint16_t) * q->tlen);
+            o += q->tlen;
+        }
+    free(m);
+    free(tb.tr);
+    return n;
 }
 
 int or_daligner2(const or_block* a, const or_block* b, const or_block* bc, const or_params* p, int self,

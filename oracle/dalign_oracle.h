@@ -97,6 +97,15 @@ int or_daligner(const or_block* a, const or_block* b, const or_block* bc, const 
 int or_daligner2(const or_block* a, const or_block* b, const or_block* bc, const or_params* p, int self,
                  or_result* res);
 
+/* daligner2's Handle_Redundancies (fusion, bridging, compaction; dalign2/filter.c:1952-2272)
+ * on one pair's paths: aseq/bseq with a 4 before and after, bseq complemented when comp;
+ * hdr = 6 ints per path (abpos, bbpos, aepos, bepos, diffs, tlen) of the novls A-side paths
+ * and, with hasB, the novls B-side paths; traces = their trace values back to back.
+ * Returns the number of paths kept and writes them the same way (A side, then B side). */
+int or_handle_redundancies_d2(const uint8_t* aseq, const uint8_t* bseq, int alen, int blen, int tspace, int comp,
+                              int novls, int hasB, const int32_t* hdr, const uint16_t* traces, int32_t* out_hdr,
+                              uint16_t* out_traces, int64_t tcap);
+
 /* daligner2's sorted k-mer index (dalign2/filter.c:834-1106): read = (read << 1) | strand. */
 int64_t or_sort_kmers2(const or_block* b, const or_params* p, uint64_t* code, int32_t* read, int32_t* rpos);
 

@@ -1,6 +1,8 @@
 """The CPU restatement (oracle) reproduces the reference daligner's golden .las files."""
 import os
 
+import numpy as np
+
 import pytest
 
 import daligner_run
@@ -57,3 +59,22 @@ def test_oracle_hits_sorted_by_bread_aread_apos():
     k = list(zip(h[:, 3], h[:, 2], h[:, 1], -h[:, 0]))
     assert k == sorted(k)
     assert (h[:, 3] < h[:, 2]).all()   # within a block only b-read < a-read pairs
+
+
+def test_oracle_d2_bridging_matches_reference():
+    """daligner2's Handle_Redundancies with its bridging pass (Compute_Bridge_Path ->
+    Compute_Alignment(DIFF_TRACE) -> trace_nd/split_nd, Bridge) against the reference's own
+    function on the one-pair fixtures (tests/golden/make_d2_bridge_golden.py): paths kept,
+    coordinates, diffs and every trace value."""
+    import d2_bridge_cases as dbc
+    cases, expected = dbc.load(os.path.join(os.path.dirname(__file__), "golden", "d2_bridge", "cases.npz"))
+    bridged = 0
+    for i, (c, (ea, eb)) in enumerate(zip(cases, expected)):
+        ga, gb = dbc.oracle_run(c)
+        assert [h for h, _ in ga] == [h for h, _ in ea], i
+        assert all(np.array_equal(x, y) for (_, x), (_, y) in zip(ga, ea)), i
+        if eb is not None:
+            assert [h for h, _ in gb] == [h for h, _ in eb], i
+            assert all(np.array_equal(x, y) for (_, x), (_, y) in zip(gb, eb)), i
+        bridged += dbc.was_bridged(c, (ea, eb))
+    assert bridged >= len(cases) // 2
