@@ -109,10 +109,20 @@ int gd_set_variant(gd_context* ctx, int variant, int hgap);
 /* daligner2's Match_Filter (dalign2/filter.c:2344-2700 with report_thread,
  * dalign2/filter_reporter_cpu.c:16-411): A (slot 0) against bslot in both orientations from
  * one join; cslot holds the complemented B block (gd_complement_block) the complement pairs
- * are aligned against.  Fails (GD_ERR_BRIDGE in the message) where daligner2 would bridge
- * two paths of a pair (Compute_Bridge_Path, dalign2/filter.c:1579-1705), which this build
- * does not compute, and where a trace value above 255 meets the 8-bit compression check. */
+ * are aligned against.  Two paths of a pair with a narrow parallel overlap are bridged as
+ * daligner2 bridges them (Compute_Bridge_Path, dalign2/filter.c:1579-1705); the call fails
+ * where a trace value above 255 meets the 8-bit compression check (Compress_TraceTo8). */
 int gd_match_filter2(gd_context* ctx, int bslot, int cslot, int self);
+
+/* Test hook, no counterpart in the reference: daligner2's Handle_Redundancies (fusion, bridging,
+ * compaction; dalign2/filter.c:1952-2272) of one pair on the device, with the calling
+ * convention of the oracle's or_handle_redundancies_d2: aseq/bseq point at the first base
+ * with a 4 before and after (bseq complemented when comp); hdr = 6 ints per path (abpos,
+ * bbpos, aepos, bepos, diffs, tlen) of the novls A-side paths and, with hasB, the B-side
+ * paths; traces back to back.  Returns the number of paths kept (written the same way). */
+int gd_test_handle_redundancies_d2(gd_context* ctx, const uint8_t* aseq, const uint8_t* bseq, int alen, int blen,
+                                   int tspace, int comp, int novls, int hasB, const int32_t* hdr,
+                                   const uint16_t* traces, int32_t* out_hdr, uint16_t* out_traces, int64_t tcap);
 
 /* The sorted hits of the last gd_match_filter (rows diag, apos, aread, bread), for tests. */
 int64_t gd_get_hits(gd_context* ctx, int32_t* rows4, int64_t cap);

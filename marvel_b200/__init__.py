@@ -61,7 +61,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
            "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge",
-           "gd_set_wave_limit", "gd_set_variant", "gd_match_filter2"]
+           "gd_set_wave_limit", "gd_set_variant", "gd_match_filter2", "gd_test_handle_redundancies_d2"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -245,6 +245,25 @@ class Context:
     def match_filter2(self, bslot, cslot, self_cmp):
         """daligner2's Match_Filter: A against bslot in both orientations (cslot = complemented B)."""
         _check(lib().gd_match_filter2(self.h, bslot, cslot, int(self_cmp)))
+
+    def test_handle_redundancies_d2(self, aseq, bseq, tspace, comp, hdr, traces, novls, has_b, tcap):
+        """Test hook: daligner2's Handle_Redundancies of one pair on the device.  aseq/bseq
+        carry a 4 before and after the read."""
+        L = lib()
+        fn = L.gd_test_handle_redundancies_d2
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+        aseq = np.ascontiguousarray(aseq, np.uint8)
+        bseq = np.ascontiguousarray(bseq, np.uint8)
+        hdr = np.ascontiguousarray(hdr, np.int32)
+        traces = np.ascontiguousarray(traces, np.uint16)
+        oh = np.zeros(max(hdr.size, 6), np.int32)
+        ot = np.zeros(max(int(tcap), 1), np.uint16)
+        n = _check(fn(self.h, aseq.ctypes.data + 1, bseq.ctypes.data + 1, aseq.size - 2, bseq.size - 2, tspace, comp,
+                      novls, int(has_b), hdr.ctypes.data, traces.ctypes.data, oh.ctypes.data, ot.ctypes.data,
+                      int(tcap)))
+        return n, oh.reshape(-1, 6), ot
 
     def match_filter(self, bslot, comp, self_cmp):
         _check(lib().gd_match_filter(self.h, bslot, int(comp), int(self_cmp)))

@@ -1152,11 +1152,459 @@ __device__ int handle_redundancies(MPath* amatch, int novls, MPath* bmatch, Pair
     return no + 1;
 }
 
+// ---- daligner2 bridging (DO_BRIDGING, dalign2/filter.c:1479-1705, 2124-2262), lane 0 ------
+
+// The bridge scratch of one warp and the sequences of its pair.
+struct BridgeCtx
+{
+    const uint8_t *aseq, *bseq;  // the pair's align: A, and B complemented for a complement pair
+    int alen, blen;
+    int* vec;                    // Compute_Alignment's wave vectors
+    int vcap;
+    uint16_t* tr;                // the bridge's trace
+    int tcap;
+    int need;                    // > 0: ints of vec (or values of tr) a bridge needed but did not have
+};
+
+// split_nd (dalign2/align.c:4355-4523): bidirectional O(nd) waves over A[0,M) x B[0,N) until
+// they meet; the edit distance and the meeting point (x, y)
+__device__ int d2_split_nd(const uint8_t* A, int M, const uint8_t* B, int N, int* VF, int* VB, int* px, int* py)
+{
+    int x, y, D, flow, blow, bhgh;
+    const uint8_t* a;
+    y = 0;
+    if (N < M)
+        while (y < N && B[y] == A[y])
+            y += 1;
+    else
+    {
+        while (y < M && B[y] == A[y])
+            y += 1;
+        if (y >= M && N == M)
+        {
+            *px = *py = M;
+            return 0;
+        }
+    }
+    flow = 0;
+    VF[0] = y;
+    VF[-1] = -2;
+    x = N - M;
+    a = A - x;
+    y = N - 1;
+    if (N > M)
+        while (y >= x && B[y] == a[y])
+            y -= 1;
+    else
+        while (y >= 0 && B[y] == a[y])
+            y -= 1;
+    blow = bhgh = -x;
+    VB += x;
+    VB[blow] = y;
+    VB[blow - 1] = N + 1;
+    for (D = 1;; D += 1)
+    {
+        int k, r, am, ac, ap;
+        flow -= 1;
+        am = ac = VF[flow - 1] = -2;
+        a = A + D;
+        x = M - D;
+        for (k = D; k >= flow; k--)
+        {
+            ap = ac;
+            ac = am + 1;
+            am = VF[k - 1];
+            if (ac < am)
+                y = (ap < am) ? am : ap;
+            else
+                y = (ap < ac) ? ac : ap;
+            if (blow <= k && k <= bhgh)
+            {
+                r = VB[k];
+                if (y > r)
+                {
+                    D = (D << 1) - 1;
+                    y = (ap > r) ? ap : ((ac > r) ? ac : r + 1);
+                    *px = k + y;
+                    *py = y;
+                    return D;
+                }
+            }
+            if (N < x)
+                while (y < N && B[y] == a[y])
+                    y += 1;
+            else
+                while (y < x && B[y] == a[y])
+                    y += 1;
+            VF[k] = y;
+            a -= 1;
+            x += 1;
+        }
+        bhgh += 1;
+        blow -= 1;
+        am = ac = VB[blow - 1] = N + 1;
+        a = A + bhgh;
+        x = -bhgh;
+        for (k = bhgh; k >= blow; k--)
+        {
+            ap = ac + 1;
+            ac = am;
+            am = VB[k - 1];
+            if (ac > am)
+                y = (ap > am) ? am : ap;
+            else
+                y = (ap > ac) ? ac : ap;
+            if (flow <= k && k <= D)
+            {
+                r = VF[k];
+                if (y <= r)
+                {
+                    D = (D << 1);
+                    y = (ap <= r) ? ap : ((ac <= r) ? ac : r);
+                    *px = k + y;
+                    *py = y;
+                    return D;
+                }
+            }
+            y -= 1;
+            if (x > 0)
+                while (y >= x && B[y] == a[y])
+                    y -= 1;
+            else
+                while (y >= 0 && B[y] == a[y])
+                    y -= 1;
+            VB[k] = y;
+            a -= 1;
+            x += 1;
+        }
+    }
+}
+
+// adds s bases of one side, from absolute A position u on, to the trace intervals they fall in
+__device__ __forceinline__ void d2_spread(uint16_t* Trace, int u, int s, int tspace, int side)
+{
+    int v = u / tspace;
+    u = (v + 1) * tspace - u;
+    for (v <<= 1; s > 0; s -= u, u = tspace)
+    {
+        if (u > s)
+            u = s;
+        Trace[v + side] += u;
+        v += 2;
+    }
+}
+
+// trace_nd (dalign2/align.c:4525-4679) without recursion: every update is an addition to a
+// trace interval, so the pieces go on a small stack in any order.  Returns the top-level
+// distance, or -1 if the stack ran out.
+__device__ int d2_trace_nd(const uint8_t* Aabs, int a0, int M0, const uint8_t* B0, int N0, uint16_t* Trace, int* VF,
+                           int* VB, int tspace)
+{
+    struct Piece
+    {
+        int a, M, N;
+        const uint8_t* B;
+    };
+    Piece stk[48];
+    int top = 0, D0 = -1;
+    stk[top++] = Piece{a0, M0, N0, B0};
+    while (top > 0)
+    {
+        const Piece pc = stk[--top];
+        const uint8_t* A = Aabs + pc.a;
+        const int M = pc.M, N = pc.N;
+        int x, y, D, s;
+        if (M <= 0)
+        {
+            y = ((pc.a / tspace) << 1);
+            Trace[y] += N;
+            Trace[y + 1] += N;
+            D = N;
+        }
+        else if (N <= 0)
+        {
+            x = pc.a;
+            y = x / tspace;
+            x = (y + 1) * tspace - x;
+            y <<= 1;
+            for (s = M; s > 0; s -= x, x = tspace)
+            {
+                if (x > s)
+                    x = s;
+                Trace[y] += x;
+                y += 2;
+            }
+            D = M;
+        }
+        else
+        {
+            D = d2_split_nd(A, M, pc.B, N, VF, VB, &x, &y);
+            if (D > 1)
+            {
+                s = pc.a;
+                if ((s / tspace + 1) * tspace - s >= x)
+                {
+                    s = ((s / tspace) << 1);
+                    Trace[s] += (D + 1) / 2;
+                    Trace[s + 1] += y;
+                }
+                else
+                {
+                    if (top >= 48)
+                        return -1;
+                    stk[top++] = Piece{pc.a, x, y, pc.B};
+                }
+                s = pc.a + x;
+                if ((s / tspace + 1) * tspace - s >= M - x)
+                {
+                    s = ((s / tspace) << 1);
+                    Trace[s] += D / 2;
+                    Trace[s + 1] += N - y;
+                }
+                else
+                {
+                    if (top >= 48)
+                        return -1;
+                    stk[top++] = Piece{pc.a + x, M - x, N - y, pc.B + y};
+                }
+            }
+            else
+            {
+                s = (D == 0 || M < N) ? x : x - 1;
+                if (s > 0)
+                    d2_spread(Trace, pc.a, s, tspace, 1);
+                if (D != 0)
+                {
+                    y = (((M < N) ? pc.a + x : pc.a + (x - 1)) / tspace) << 1;
+                    Trace[y] += 1;
+                    if (M <= N)
+                        Trace[y + 1] += 1;
+                    s = M - x;
+                    if (s > 0)
+                        d2_spread(Trace, pc.a + x, s, tspace, 1);
+                }
+            }
+        }
+        if (D0 < 0)
+            D0 = D;
+    }
+    return D0;
+}
+
+// A bridge path: coordinates, diffs and its trace in the warp's bridge buffer.
+struct BPath
+{
+    int abpos, bbpos, aepos, bepos, diffs, tlen;
+};
+
+// Compute_Alignment(align, work, DIFF_TRACE, tspace) (dalign2/align.c:4762-4913) for the box of
+// p over aseq (its absolute base) and bseq; false if the scratch is too small (bc.need set)
+__device__ bool d2_compute_alignment(const uint8_t* aseq, const uint8_t* bseq, BPath* p, int tspace, BridgeCtx& bc)
+{
+    const int asub = p->aepos - p->abpos, bsub = p->bepos - p->bbpos;
+    const int n = 2 * (((p->aepos + (tspace - 1)) / tspace - p->abpos / tspace) + 1);
+    const int m = asub > bsub ? asub : bsub;
+    if (4 * m + 6 > bc.vcap || n > bc.tcap)
+    {
+        bc.need = max(4 * m + 6 > bc.vcap ? 4 * m + 6 : 0, n > bc.tcap ? n : 0);
+        return false;
+    }
+    int* VF = bc.vec + (m + 1);
+    int* VB = VF + (2 * m + 3);
+    uint16_t* strace = bc.tr;
+    for (int i = 0; i < n; i++)
+        strace[i] = 0;
+    uint16_t* Trace = strace - 2 * (p->abpos / tspace);
+    const int d = d2_trace_nd(aseq, p->abpos, asub, bseq + p->bbpos, bsub, Trace, VF, VB, tspace);
+    if (d < 0)
+    {
+        bc.need = 1;  // the piece stack ran out: reported like a scratch shortage
+        return false;
+    }
+    p->diffs = d;
+    if (strace[n - 1] != 0)
+    {
+        strace[n - 3] += strace[n - 1];
+        strace[n - 4] += strace[n - 2];
+    }
+    p->tlen = n - 2;
+    return true;
+}
+
+// MapToTPAbove / MapToTPBelow (dalign2/filter.c:1481-1563)
+__device__ int d2_map_tp_above(const MPath* path, int* x, bool isA, const uint16_t* tb, int TS)
+{
+    const uint16_t* trace = tb + path->toff;
+    int a = (path->abpos / TS) * TS, b = path->bbpos;
+    for (int i = 1; i < path->tlen; i += 2)
+    {
+        a += TS;
+        b += trace[i];
+        if (a > path->aepos)
+            a = path->aepos;
+        if (isA ? a >= *x : b >= *x)
+            break;
+    }
+    const int r = isA ? b : a;
+    *x = isA ? a : b;
+    return r;
+}
+
+__device__ int d2_map_tp_below(const MPath* path, int* x, bool isA, const uint16_t* tb, int TS)
+{
+    const uint16_t* trace = tb + path->toff;
+    int a = ((path->aepos + (TS - 1)) / TS) * TS, b = path->bepos;
+    for (int i = path->tlen - 1; i >= 0; i -= 2)
+    {
+        a -= TS;
+        b -= trace[i];
+        if (a < path->abpos)
+            a = path->abpos;
+        if (isA ? a <= *x : b <= *x)
+            break;
+    }
+    const int r = isA ? b : a;
+    *x = isA ? a : b;
+    return r;
+}
+
+// Compute_Bridge_Path (dalign2/filter.c:1579-1705): the box from two trace points before
+// path2's start to two after path1's end, aligned afresh with trace points; with comp in the
+// complemented frame, shifted so its trace points fall on multiples of the spacing
+__device__ bool d2_bridge_path(const MPath* path1, const MPath* path2, const uint8_t* aseq, const uint8_t* bseq,
+                               int alen, int blen, int comp, int aovl, int bovl, const uint16_t* tb, int TS, BPath* ap,
+                               BridgeCtx& bc)
+{
+    int ain, aout, bin, bout, boff = 0, p;
+    if (bovl > aovl)
+    {
+        bin = path2->bbpos;
+        bout = path1->bepos;
+        ain = d2_map_tp_below(path1, &bin, false, tb, TS);
+        aout = d2_map_tp_above(path2, &bout, false, tb, TS);
+    }
+    else
+    {
+        ain = path2->abpos;
+        aout = path1->aepos;
+        bin = d2_map_tp_below(path1, &ain, true, tb, TS);
+        bout = d2_map_tp_above(path2, &aout, true, tb, TS);
+    }
+    ap->abpos = ain - 2 * TS;
+    ap->aepos = aout + 2 * TS;
+    ap->bbpos = d2_map_tp_below(path1, &ap->abpos, true, tb, TS);
+    ap->bepos = d2_map_tp_above(path2, &ap->aepos, true, tb, TS);
+    const uint8_t* A = aseq;
+    if (comp)
+    {
+        boff = TS - ap->aepos % TS;
+        p = alen - ap->abpos;
+        ap->abpos = alen - ap->aepos;
+        ap->aepos = p;
+        p = blen - ap->bbpos;
+        ap->bbpos = blen - ap->bepos;
+        ap->bepos = p;
+        boff = boff - ap->abpos % TS;
+        A -= boff;
+        ap->abpos += boff;
+        ap->aepos += boff;
+    }
+    if (!d2_compute_alignment(A, bseq, ap, TS, bc))
+        return false;
+    if (comp)
+    {
+        uint16_t* trk = bc.tr;
+        int j = ap->tlen - 2, i = 0;
+        while (i < j)
+        {
+            uint16_t t = trk[i];
+            trk[i] = trk[j];
+            trk[j] = t;
+            t = trk[i + 1];
+            trk[i + 1] = trk[j + 1];
+            trk[j + 1] = t;
+            i += 2;
+            j -= 2;
+        }
+        ap->abpos -= boff;
+        ap->aepos -= boff;
+        p = alen - ap->abpos;
+        ap->abpos = alen - ap->aepos;
+        ap->aepos = p;
+        p = blen - ap->bbpos;
+        ap->bbpos = blen - ap->bepos;
+        ap->bepos = p;
+    }
+    return true;
+}
+
+// Check_Bridge (dalign2/filter.c:1565-1577)
+__device__ bool d2_check_bridge(const BPath* p, const BridgeCtx& bc, int TS)
+{
+    if (TS <= 125)
+        for (int i = 0; i < p->tlen; i++)
+            if (bc.tr[i] > 250)
+                return true;
+    return false;
+}
+
+// Bridge (dalign2/filter.c:1885-1948): path1 up to the bridge, the bridge, path3 after it
+__device__ void d2_bridge(MPath* path1, const BPath* path2, const uint16_t* btr, const MPath* path3, PairBuf& pb,
+                          int TS)
+{
+    int k, k1, k2, len, diff;
+    k1 = 2 * ((path2->abpos / TS) - (path1->abpos / TS));
+    k2 = (path2->aepos == path3->aepos) ? path3->tlen : 2 * ((path2->aepos / TS) - (path3->abpos / TS));
+    len = k1 + path2->tlen + (path3->tlen - k2);
+    if (len < 0 || pb.ttop + len > pb.tcap)
+    {
+        pb.err = 1;
+        return;
+    }
+    const int base = pb.ttop;
+    pb.ttop += len;
+    uint16_t* trace = pb.tb + base;
+    diff = 0;
+    len = 0;
+    if (k1 > 0)
+    {
+        const uint16_t* t = pb.tb + path1->toff;
+        for (k = 0; k < k1; k += 2)
+        {
+            trace[len++] = t[k];
+            trace[len++] = t[k + 1];
+            diff += t[k];
+        }
+    }
+    for (k = 0; k < path2->tlen; k += 2)
+    {
+        trace[len++] = btr[k];
+        trace[len++] = btr[k + 1];
+        diff += btr[k];
+    }
+    if (k2 < path3->tlen)
+    {
+        const uint16_t* t = pb.tb + path3->toff;
+        for (k = k2; k < path3->tlen; k += 2)
+        {
+            trace[len++] = t[k];
+            trace[len++] = t[k + 1];
+            diff += t[k];
+        }
+    }
+    path1->aepos = path3->aepos;
+    path1->bepos = path3->bepos;
+    path1->diffs = diff;
+    path1->toff = base;
+    path1->tlen = len;
+}
+
 // daligner2's Handle_Redundancies (dalign2/filter.c:1952-2272): the surviving path of a fused
 // or contained pair stays at the later index j, the other is marked abpos = -1, a fusion
-// restarts j's scan; compaction at the end.  Its bridging pass (:2124-2262) is detected, not
-// computed: returns -1 when two paths would go to Compute_Bridge_Path.
-__device__ int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, PairBuf& pb, int TS, int comp)
+// restarts j's scan; then the bridging pass; compaction at the end.  Returns -1 when the
+// bridge scratch was too small (bc.need says how much), or the pair trace buffer filled.
+__device__ int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, PairBuf& pb, int TS, int comp,
+                                      BridgeCtx& bc)
 {
     int j, k, dist, awhen = 0, bwhen = 0;
     const bool hasB = (bmatch != nullptr);
@@ -1269,19 +1717,21 @@ __device__ int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, P
             }
         }
     }
-    // the bridging pass's entry test (dalign2/filter.c:2126-2175)
+    // the bridging pass (dalign2/filter.c:2124-2262): a pair of paths with a narrow parallel
+    // overlap joined through a fresh alignment of the overlap's box; the A side's box is
+    // aligned uncomplemented, the B side's in the pair's orientation
     for (j = 1; j < novls; j++)
     {
-        const MPath* jpath = amatch + j;
+        MPath* jpath = amatch + j;
         if (jpath->abpos < 0)
             continue;
         for (k = j - 1; k >= 0; k--)
         {
-            const MPath* kpath = amatch + k;
+            MPath* kpath = amatch + k;
             if (kpath->abpos < 0)
                 continue;
-            const MPath* path1 = jpath->abpos < kpath->abpos ? jpath : kpath;
-            const MPath* path2 = jpath->abpos < kpath->abpos ? kpath : jpath;
+            MPath* path1 = jpath->abpos < kpath->abpos ? jpath : kpath;
+            MPath* path2 = jpath->abpos < kpath->abpos ? kpath : jpath;
             if (path2->abpos >= path1->aepos || path1->aepos >= path2->aepos || path1->bbpos >= path2->bbpos ||
                 path2->bbpos >= path1->bepos || path1->bepos >= path2->bepos)
                 continue;
@@ -1289,15 +1739,42 @@ __device__ int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, P
             const int bovl = path1->bepos - path2->bbpos;
             if (abs(aovl - bovl) > .2 * (aovl + bovl))
                 continue;
+            MPath *bath1 = nullptr, *bath2 = nullptr;
             if (hasB)
             {
                 const bool first = (comp != 0) == (jpath->abpos < kpath->abpos);
-                const MPath* bath1 = first ? bmatch + k : bmatch + j;
-                const MPath* bath2 = first ? bmatch + j : bmatch + k;
+                bath1 = first ? bmatch + k : bmatch + j;
+                bath2 = first ? bmatch + j : bmatch + k;
                 if (bath1->abpos > bath2->abpos)
                     continue;
             }
-            return -1;
+            BPath bp;
+            if (!d2_bridge_path(path1, path2, bc.aseq, bc.bseq, bc.alen, bc.blen, 0, aovl, bovl, pb.tb, TS, &bp, bc))
+                return -1;
+            if (d2_check_bridge(&bp, bc, TS))
+                continue;
+            const MPath jback = *jpath, kback = *kpath;
+            d2_bridge(path1, &bp, bc.tr, path2, pb, TS);
+            if (pb.err)
+                return -1;
+            *jpath = *path1;
+            kpath->abpos = -1;
+            if (hasB)
+            {
+                if (!d2_bridge_path(bath1, bath2, bc.bseq, bc.aseq, bc.blen, bc.alen, comp, bovl, aovl, pb.tb, TS, &bp,
+                                    bc))
+                    return -1;
+                if (d2_check_bridge(&bp, bc, TS))
+                {
+                    *jpath = jback;
+                    *kpath = kback;
+                    continue;
+                }
+                d2_bridge(bath1, &bp, bc.tr, bath2, pb, TS);
+                if (pb.err)
+                    return -1;
+                bmatch[j] = *bath1;
+            }
         }
     }
     int no = 0;
@@ -1315,20 +1792,21 @@ __device__ int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, P
 // check of Compress_TraceTo8 (dalign2/align.c:3391-3412).  Returns 0 or the GD_ERR_ code the
 // pair fails with.  Kept out of line: the pair kernel's hot loop stays compact.
 __device__ __noinline__ int finish_pair_d2(MPath* amatch, int* novla, MPath* bmatch, int* novlb, PairBuf& pb, int TS,
-                                           int comp, bool check8)
+                                           int comp, bool check8, BridgeCtx& bc)
 {
     int r1 = *novla, r2 = *novlb;
+    // a B-only call gets the pair's align too, as the reference hands it (filter_reporter_cpu.c:392-400)
     if (r1 > 1)
     {
         if (r2 > 1)
-            r1 = r2 = handle_redundancies_d2(amatch, r1, bmatch, pb, TS, comp);
+            r1 = r2 = handle_redundancies_d2(amatch, r1, bmatch, pb, TS, comp, bc);
         else
-            r1 = handle_redundancies_d2(amatch, r1, nullptr, pb, TS, comp);
+            r1 = handle_redundancies_d2(amatch, r1, nullptr, pb, TS, comp, bc);
     }
     else if (r2 > 1)
-        r2 = handle_redundancies_d2(bmatch, r2, nullptr, pb, TS, comp);
+        r2 = handle_redundancies_d2(bmatch, r2, nullptr, pb, TS, comp, bc);
     if (r1 < 0 || r2 < 0)
-        return GD_ERR_BRIDGE;
+        return pb.err ? GD_ERR_TRACE : GD_ERR_BRIDGE;
     *novla = r1;
     *novlb = r2;
     if (check8)
@@ -1739,9 +2217,11 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
         {
             if (D2)
             {
-                d2fail = finish_pair_d2(amatch, &novla, bmatch, &novlb, pb, TS, P.comp, P.trace8 && !P.no_trace);
+                BridgeCtx bc{aseq, bseq, alen, blen, sc.bvec + (size_t)gw * sc.bvcap, sc.bvcap,
+                             sc.btr + (size_t)gw * sc.btcap, sc.btcap, 0};
+                d2fail = finish_pair_d2(amatch, &novla, bmatch, &novlb, pb, TS, P.comp, P.trace8 && !P.no_trace, bc);
                 if (d2fail)
-                    gd_fail(st, d2fail, w.item, 0);
+                    gd_fail(st, d2fail, w.item, d2fail == GD_ERR_BRIDGE ? bc.need : sc.tcap);
             }
             else if (novla > 1)
             {
@@ -1776,10 +2256,64 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
     }
 }
 
-size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands)
+// Test hook: daligner2's Handle_Redundancies (fusion, bridging, compaction) of one pair on
+// the device, single thread.  hdr = 6 ints per path (A side, then B side with hasB), trace =
+// their trace values back to back (capacity tcap in the pair buffer, which also receives
+// fusions and bridges); out_hdr receives the kept paths, out_n their count (or -code).
+__global__ void k_test_hr_d2(const uint8_t* aseq, const uint8_t* bseq, int alen, int blen, int tspace, int comp,
+                             int novls, int hasB, const int32_t* hdr, MPath* paths, uint16_t* tbuf, int ttop,
+                             int tcap, int* vec, int vcap, uint16_t* btr, int btcap, int32_t* out_hdr, int* out_n)
+{
+    const int npath = novls * (hasB ? 2 : 1);
+    int off = 0;
+    for (int i = 0; i < npath; i++)
+    {
+        const int32_t* h = hdr + 6 * i;
+        paths[i] = MPath{off, h[5], h[4], h[0], h[1], h[2], h[3], 0};
+        off += h[5];
+    }
+    PairBuf pb{paths, hasB ? paths + novls : nullptr, tbuf, ttop, tcap, 0};
+    BridgeCtx bc{aseq, bseq, alen, blen, vec, vcap, btr, btcap, 0};
+    const int n = handle_redundancies_d2(paths, novls, hasB ? paths + novls : nullptr, pb, tspace, comp, bc);
+    if (n < 0)
+    {
+        *out_n = pb.err ? -GD_ERR_TRACE : -GD_ERR_BRIDGE;
+        return;
+    }
+    for (int side = 0; side < (hasB ? 2 : 1); side++)
+        for (int i = 0; i < n; i++)
+        {
+            const MPath& q = paths[side * novls + i];
+            int32_t* h = out_hdr + 6 * (side * n + i);
+            h[0] = q.abpos;
+            h[1] = q.bbpos;
+            h[2] = q.aepos;
+            h[3] = q.bepos;
+            h[4] = q.diffs;
+            h[5] = q.tlen;
+        }
+    // the kept paths' trace offsets, for the host to gather
+    for (int side = 0; side < (hasB ? 2 : 1); side++)
+        for (int i = 0; i < n; i++)
+            out_hdr[6 * npath + side * n + i] = paths[side * novls + i].toff;
+    *out_n = n;
+}
+
+int launch_test_hr_d2(const uint8_t* aseq, const uint8_t* bseq, int alen, int blen, int tspace, int comp, int novls,
+                      int hasB, const int32_t* hdr, MPath* paths, uint16_t* tbuf, int ttop, int tcap, int* vec,
+                      int vcap, uint16_t* btr, int btcap, int32_t* out_hdr, int* out_n, cudaStream_t s)
+{
+    k_test_hr_d2<<<1, 1, 0, s>>>(aseq, bseq, alen, blen, tspace, comp, novls, hasB, hdr, paths, tbuf, ttop, tcap, vec,
+                                 vcap, btr, btcap, out_hdr, out_n);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands, int bvcap, int btcap)
 {
     size_t per = (size_t)pcap * sizeof(int4) + (size_t)ptscap * 2 + (size_t)2 * mcap * sizeof(MPath) +
-                 (size_t)tcap * 2 + (size_t)3 * nbands * 4 + 4 * 256;
+                 (size_t)tcap * 2 + (size_t)3 * nbands * 4 + (size_t)bvcap * 4 + (size_t)btcap * 2 + 6 * 256;
     return per * nwarps + 4096;
 }
 
@@ -1788,7 +2322,8 @@ static inline char* align_up(char* p, size_t a)
     return (char*)(((uintptr_t)p + a - 1) & ~(uintptr_t)(a - 1));
 }
 
-void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands)
+void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands,
+                         int bvcap, int btcap)
 {
     char* p = align_up((char*)base, 256);
     s->nwarps = nwarps;
@@ -1806,6 +2341,12 @@ void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int 
     p = align_up(p + (size_t)tcap * 2 * nwarps, 256);
     s->nbands = nbands;
     s->bands = (int*)p;
+    p = align_up(p + (size_t)3 * nbands * 4 * nwarps, 256);
+    s->bvcap = bvcap;
+    s->bvec = bvcap ? (int*)p : nullptr;
+    p = align_up(p + (size_t)bvcap * 4 * nwarps, 256);
+    s->btcap = btcap;
+    s->btr = btcap ? (uint16_t*)p : nullptr;
 }
 
 int align_grid(int* grid_out, int wide)

@@ -62,6 +62,10 @@ struct AlignScratch
     int* bands;        // score | lastp | lasta, each nbands ints
     int nbands;
     int nwarps;
+    int* bvec;         // daligner2 bridging: the O(nd) wave vectors of Compute_Alignment (bvcap ints
+    int bvcap;         //   per warp; 0 outside daligner2 mode)
+    uint16_t* btr;     //   and the bridge's trace (btcap values per warp)
+    int btcap;
 };
 
 struct AlignOut
@@ -76,8 +80,10 @@ struct AlignOut
     unsigned* nwide;      // their count
 };
 
-size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands);
-void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands);
+size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands, int bvcap = 0,
+                           int btcap = 0);
+void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands,
+                         int bvcap = 0, int btcap = 0);
 
 // Persistent seed-scan + alignment over the ordered pair groups.
 int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hkey, const uint32_t* hdiag,
@@ -91,6 +97,11 @@ int launch_la_batch(const uint8_t* aseq_base, const int64_t* aoff, const int32_t
                     const int64_t* boff, const int32_t* blen, const int32_t* diag, const int32_t* anti, int nseeds,
                     AlignParams p, AlignScratch sc, int32_t* out12, uint16_t* tr, int trstride, int64_t* cells,
                     DevStatus* st, cudaStream_t s);
+
+// Test hook: daligner2's Handle_Redundancies of one pair on one device thread (see gd_align.cu).
+int launch_test_hr_d2(const uint8_t* aseq, const uint8_t* bseq, int alen, int blen, int tspace, int comp, int novls,
+                      int hasB, const int32_t* hdr, MPath* paths, uint16_t* tbuf, int ttop, int tcap, int* vec,
+                      int vcap, uint16_t* btr, int btcap, int32_t* out_hdr, int* out_n, cudaStream_t s);
 
 // CTAs for a persistent launch of the narrow (wide = 0) or wide instance, and its warps per CTA
 int align_grid(int* grid_out, int wide = 0);

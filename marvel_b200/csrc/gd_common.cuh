@@ -81,7 +81,7 @@ enum
     GD_ERR_OUTPUT = 5,       // overlap output buffer exhausted
     GD_ERR_EMPTY_BAND = 6,   // wave band emptied while the wave continues
     GD_ERR_RING = 7,         // band left the ring window
-    GD_ERR_BRIDGE = 8,       // daligner2: a pair of paths would be bridged (not built)
+    GD_ERR_BRIDGE = 8,       // daligner2: bridging scratch exhausted (info: ints needed)
     GD_ERR_TRACE8 = 9,       // daligner2: a trace value above 255 fails the 8-bit compression check
 };
 

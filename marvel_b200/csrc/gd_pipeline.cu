@@ -184,6 +184,7 @@ struct gd_context
     int variant = 1, hgap = 0;  // 2 = daligner2 (modimizer seeds, dalign2/), its -H
     DevBuf d2rd, d2rp, d2sgn, cnt2, hoff2, hk2, hd2, runstart;
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
+    int bvcap = 8192, btcap = 1024;  // daligner2 bridging scratch per warp (ints, trace values)
     uint64_t rcap = 1 << 22, tbcap = 512ull << 20;
     // the overlap buffer: records and trace bytes of every Match_Filter since the last reset,
     // in HBM in emission order (acc_*), and its sorted, compacted copy (srt_*)
@@ -796,11 +797,12 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     int nbands = ap.maxdiag - ap.mindiag + 8;
     for (int attempt = 0; attempt < 6; attempt++)
     {
+        const int bvcap = ap.d2 ? c->bvcap : 0, btcap = ap.d2 ? c->btcap : 0;
         AlignScratch sc{};
-        size_t need = align_scratch_bytes(nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+        size_t need = align_scratch_bytes(nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
         if (ensure(c->ascr, need))
             return -1;
-        align_scratch_carve(&sc, c->ascr.p, nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+        align_scratch_carve(&sc, c->ascr.p, nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
         // the band arrays (score, lastp, lasta per warp) start at zero on every launch: their
         // place in the scratch moves with maxlen and the capacities, so an earlier launch's
         // clean-up does not cover them
@@ -830,10 +832,12 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
         if (nwide > 0)
         {
             AlignScratch scw{};
-            const size_t need_w = align_scratch_bytes(nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+            const size_t need_w =
+                align_scratch_bytes(nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
             if (ensure(c->ascr_w, need_w))
                 return -1;
-            align_scratch_carve(&scw, c->ascr_w.p, nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands);
+            align_scratch_carve(&scw, c->ascr_w.p, nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap,
+                                btcap);
             GD_CUDA(cudaMemsetAsync(scw.bands, 0, (size_t)nwarps_w * 3 * nbands * 4, s));
             AlignOut outw = out;
             outw.wide_list = nullptr;
@@ -858,6 +862,13 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
                 c->tcap *= 2;
             else if (st.code == GD_ERR_MATCHES)
                 c->mcap *= 2;
+            else if (st.code == GD_ERR_BRIDGE && st.info > 1)
+            {
+                // a daligner2 bridge box larger than the bridging scratch: grow both and re-run
+                c->bvcap = std::max(2 * c->bvcap, st.info + 64);
+                c->btcap = std::max(2 * c->btcap, st.info + 64);
+                continue;
+            }
             else
             {
                 gd_set_error("aligner failed on pair group %d: code %d info %d", st.where, st.code, st.info);
@@ -1409,6 +1420,77 @@ int gd_match_filter2(gd_context* c, int bslot, int cslot, int self)
     }
     return c->kmer <= 15 ? match_filter_d2_t<uint32_t>(c, bslot, cslot, self)
                          : match_filter_d2_t<uint64_t>(c, bslot, cslot, self);
+}
+
+int gd_test_handle_redundancies_d2(gd_context* c, const uint8_t* aseq, const uint8_t* bseq, int alen, int blen,
+                                   int tspace, int comp, int novls, int hasB, const int32_t* hdr,
+                                   const uint16_t* traces, int32_t* out_hdr, uint16_t* out_traces, int64_t tcap)
+{
+    using namespace gd;
+    cudaStream_t s = c->s;
+    const int npath = novls * (hasB ? 2 : 1);
+    if (novls <= 0 || alen <= 0 || blen <= 0 || tspace <= 0)
+    {
+        gd_set_error("gd_test_handle_redundancies_d2: empty case");
+        return -1;
+    }
+    int64_t ttot = 0;
+    for (int i = 0; i < npath; i++)
+        ttot += hdr[6 * i + 5];
+    const int m = std::max(alen, blen);
+    const int pcap_tr = (int)(ttot + 8 * (int64_t)(m / tspace + 8) * npath + 4096);
+    const int vcap = 4 * m + 64, btcap = 2 * (m / tspace + 8) + 64;
+    DevBuf da, db, dh, dp, dt, dv, dbt, doh, dn;
+    struct Frees  // the hook's buffers are its own; cudaFree waits for the device
+    {
+        DevBuf* b[9];
+        ~Frees()
+        {
+            for (DevBuf* x : b)
+                if (x->p)
+                    cudaFree(x->p);
+        }
+    } frees{{&da, &db, &dh, &dp, &dt, &dv, &dbt, &doh, &dn}};
+    if (ensure(da, alen + 2) || ensure(db, blen + 2) || ensure(dh, npath * 24) ||
+        ensure(dp, (npath + 1) * sizeof(MPath)) || ensure(dt, (size_t)pcap_tr * 2) || ensure(dv, (size_t)vcap * 4) ||
+        ensure(dbt, (size_t)btcap * 2) || ensure(doh, (size_t)npath * 7 * 4) || ensure(dn, 4))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(da.p, aseq - 1, alen + 2, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemcpyAsync(db.p, bseq - 1, blen + 2, cudaMemcpyHostToDevice, s));
+    GD_CUDA(cudaMemcpyAsync(dh.p, hdr, npath * 24, cudaMemcpyHostToDevice, s));
+    if (ttot)
+        GD_CUDA(cudaMemcpyAsync(dt.p, traces, ttot * 2, cudaMemcpyHostToDevice, s));
+    if (launch_test_hr_d2((const uint8_t*)da.p + 1, (const uint8_t*)db.p + 1, alen, blen, tspace, comp, novls, hasB,
+                          P<int32_t>(dh), P<MPath>(dp), P<uint16_t>(dt), (int)ttot, pcap_tr, P<int>(dv), vcap,
+                          P<uint16_t>(dbt), btcap, P<int32_t>(doh), P<int>(dn), s))
+        return -1;
+    int n = 0;
+    std::vector<int32_t> oh((size_t)npath * 7);
+    GD_CUDA(cudaMemcpyAsync(&n, dn.p, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaMemcpyAsync(oh.data(), doh.p, oh.size() * 4, cudaMemcpyDeviceToHost, s));
+    std::vector<uint16_t> tb((size_t)pcap_tr);
+    GD_CUDA(cudaMemcpyAsync(tb.data(), dt.p, tb.size() * 2, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    if (n < 0)
+    {
+        gd_set_error("gd_test_handle_redundancies_d2: device code %d", -n);
+        return -1;
+    }
+    const int nk = n * (hasB ? 2 : 1);
+    int64_t o = 0;
+    for (int i = 0; i < nk; i++)
+    {
+        memcpy(out_hdr + 6 * i, oh.data() + 6 * i, 24);
+        const int tl = oh[6 * i + 5], toff = oh[6 * npath + i];
+        if (o + tl > tcap || toff < 0 || toff + tl > pcap_tr)
+        {
+            gd_set_error("gd_test_handle_redundancies_d2: output trace capacity");
+            return -1;
+        }
+        memcpy(out_traces + o, tb.data() + toff, (size_t)tl * 2);
+        o += tl;
+    }
+    return n;
 }
 
 int64_t gd_get_hits(gd_context* c, int32_t* rows4, int64_t cap)

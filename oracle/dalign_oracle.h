@@ -62,8 +62,8 @@ typedef struct
     int32_t tbytes;
     /* statistics */
     int64_t kmers_a, kmers_b, hits_n, hits_c, seeds_n, seeds_c, cells, snake_steps;
-    /* 0, or daligner2 only: 1 = a pair would be bridged (Compute_Bridge_Path, not restated),
-     * 2 = a trace value above 255 met the 8-bit compression check (Compress_TraceTo8) */
+    /* 0, or daligner2 only: 2 = a trace value above 255 met the 8-bit compression check
+     * (Compress_TraceTo8) */
     int32_t status;
 } or_result;
 

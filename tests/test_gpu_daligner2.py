@@ -86,3 +86,28 @@ def test_d2_stats_split_orientations(mb):
     with pytest.raises(mb.GpuError):
         ctx.match_filter(0, 0, 1)
     ctx.close()
+
+
+def test_d2_bridging_matches_reference(mb):
+    """daligner2's Handle_Redundancies with its bridging pass on the device, one pair per call,
+    against the reference's own function on the one-pair fixtures
+    (tests/golden/make_d2_bridge_golden.py): paths kept, coordinates, diffs, trace values."""
+    import d2_bridge_cases as dbc
+    cases, expected = dbc.load(os.path.join(os.path.dirname(__file__), "golden", "d2_bridge", "cases.npz"))
+    ctx = mb.Context()
+    for i, (c, (ea, eb)) in enumerate(zip(cases, expected)):
+        ps = c.amatch + (c.bmatch or [])
+        hdr, tr = dbc.flat(ps)
+        a = np.concatenate([[4], c.a, [4]]).astype(np.uint8)
+        b = np.concatenate([[4], c.b, [4]]).astype(np.uint8)
+        tcap = int(tr.size) + 8 * (max(c.a.size, c.b.size) // c.tspace + 8) * len(ps) + 1024
+        n, oh, ot = ctx.test_handle_redundancies_d2(a, b, c.tspace, c.comp, hdr, tr, len(c.amatch),
+                                                    c.bmatch is not None, tcap)
+        want = ea + (eb or [])
+        assert n == len(ea), i
+        o = 0
+        for j, (h, t) in enumerate(want):
+            assert [int(x) for x in oh[j]] == h, (i, j)
+            assert np.array_equal(ot[o:o + h[5]], t), (i, j)
+            o += h[5]
+    ctx.close()
