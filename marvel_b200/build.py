@@ -10,6 +10,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpudalign.so")
 CLI = os.path.join(HERE, "daligner_gpu")
+CLI2 = os.path.join(HERE, "daligner2_gpu")
 SOURCES = ["gd_prims.cu", "gd_filter.cu", "gd_filter2.cu", "gd_align.cu", "gd_pipeline.cu", "gd_noalloc.cu", "gd_verify.cu", "gd_triage.cu", "gd_output.cu", "gd_dust.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -39,11 +40,12 @@ def build(verbose=False, force=False):
             objs.append(o)
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         subprocess.run(cmd, check=True)
-    cli_src = os.path.join(CSRC, "host", "daligner_main.c")
-    if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB, os.path.join(CSRC, "host", "dazz_db.c")])):
-        cmd = ["gcc", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), "-o", CLI, cli_src,
-               os.path.join(CSRC, "host", "dazz_db.c"), "-L" + HERE, "-lgpudalign", "-Wl,-rpath,$ORIGIN"]
-        subprocess.run(cmd, check=True)
+    for cli, main in ((CLI, "daligner_main.c"), (CLI2, "daligner2_main.c")):
+        cli_src = os.path.join(CSRC, "host", main)
+        if force or _stale(cli, [cli_src, LIB, os.path.join(CSRC, "host", "dazz_db.c")]):
+            cmd = ["gcc", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), "-o", cli, cli_src,
+                   os.path.join(CSRC, "host", "dazz_db.c"), "-L" + HERE, "-lgpudalign", "-Wl,-rpath,$ORIGIN"]
+            subprocess.run(cmd, check=True)
     return LIB
 
 

@@ -1789,12 +1789,16 @@ __device__ int handle_redundancies_d2(MPath* amatch, int novls, MPath* bmatch, P
 }
 
 // daligner2's end of a pair (filter_reporter_cpu.c:330-371): Handle_Redundancies, then the
-// check of Compress_TraceTo8 (dalign2/align.c:3391-3412).  Returns 0 or the GD_ERR_ code the
-// pair fails with.  Kept out of line: the pair kernel's hot loop stays compact.
-__device__ __noinline__ int finish_pair_d2(MPath* amatch, int* novla, MPath* bmatch, int* novlb, PairBuf& pb, int TS,
-                                           int comp, bool check8, BridgeCtx& bc)
+// check of Compress_TraceTo8 (dalign2/align.c:3391-3412).  Returns (paths kept on the A side,
+// on the B side, 0 or the GD_ERR_ code the pair fails with, the bridging scratch it needed).
+// Kept out of line and given everything by value, so that the pair kernel's own registers
+// and hot loop stay as they are.
+__device__ __noinline__ int4 finish_pair_d2(MPath* amatch, int novla, MPath* bmatch, int novlb, PairBuf pb, int TS,
+                                            int comp, bool check8, const uint8_t* aseq, const uint8_t* bseq, int alen,
+                                            int blen, int* bvec, int bvcap, uint16_t* btr, int btcap)
 {
-    int r1 = *novla, r2 = *novlb;
+    BridgeCtx bc{aseq, bseq, alen, blen, bvec, bvcap, btr, btcap, 0};
+    int r1 = novla, r2 = novlb;
     // a B-only call gets the pair's align too, as the reference hands it (filter_reporter_cpu.c:392-400)
     if (r1 > 1)
     {
@@ -1806,21 +1810,19 @@ __device__ __noinline__ int finish_pair_d2(MPath* amatch, int* novla, MPath* bma
     else if (r2 > 1)
         r2 = handle_redundancies_d2(bmatch, r2, nullptr, pb, TS, comp, bc);
     if (r1 < 0 || r2 < 0)
-        return pb.err ? GD_ERR_TRACE : GD_ERR_BRIDGE;
-    *novla = r1;
-    *novlb = r2;
+        return make_int4(novla, novlb, pb.err ? GD_ERR_TRACE : GD_ERR_BRIDGE, bc.need);
     if (check8)
     {
         for (int i = 0; i < r1; i++)
             for (int t = 0; t < amatch[i].tlen; t++)
                 if (pb.tb[amatch[i].toff + t] > 255)
-                    return GD_ERR_TRACE8;
+                    return make_int4(r1, r2, GD_ERR_TRACE8, 0);
         for (int i = 0; i < r2; i++)
             for (int t = 0; t < bmatch[i].tlen; t++)
                 if (pb.tb[bmatch[i].toff + t] > 255)
-                    return GD_ERR_TRACE8;
+                    return make_int4(r1, r2, GD_ERR_TRACE8, 0);
     }
-    return 0;
+    return make_int4(r1, r2, 0, 0);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -2217,11 +2219,14 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
         {
             if (D2)
             {
-                BridgeCtx bc{aseq, bseq, alen, blen, sc.bvec + (size_t)gw * sc.bvcap, sc.bvcap,
-                             sc.btr + (size_t)gw * sc.btcap, sc.btcap, 0};
-                d2fail = finish_pair_d2(amatch, &novla, bmatch, &novlb, pb, TS, P.comp, P.trace8 && !P.no_trace, bc);
+                const int4 f = finish_pair_d2(amatch, novla, bmatch, novlb, pb, TS, P.comp, P.trace8 && !P.no_trace,
+                                              aseq, bseq, alen, blen, sc.bvec + (size_t)gw * sc.bvcap, sc.bvcap,
+                                              sc.btr + (size_t)gw * sc.btcap, sc.btcap);
+                novla = f.x;
+                novlb = f.y;
+                d2fail = f.z;
                 if (d2fail)
-                    gd_fail(st, d2fail, w.item, d2fail == GD_ERR_BRIDGE ? bc.need : sc.tcap);
+                    gd_fail(st, d2fail, w.item, d2fail == GD_ERR_BRIDGE ? f.w : sc.tcap);
             }
             else if (novla > 1)
             {
