@@ -108,6 +108,17 @@ __device__ __forceinline__ int lane_id()
     return l;
 }
 
+// Per-device one-time set-up (kernel attributes, occupancy-derived grids) is kept in arrays
+// indexed by the current device, so that contexts on several GPUs of one process each get it.
+constexpr int GD_MAX_DEVICES = 64;
+
+// the current device, or -1 if it cannot be had or is beyond GD_MAX_DEVICES
+inline int gd_device()
+{
+    int d = 0;
+    return (cudaGetDevice(&d) == cudaSuccess && d >= 0 && d < GD_MAX_DEVICES) ? d : -1;
+}
+
 template <typename T>
 __host__ __device__ inline T gd_cdiv(T a, T b)
 {

@@ -39,98 +39,150 @@ __device__ __forceinline__ bool d2_keep(uint64_t code, int kshift)
 // reverse-complement codes of bases [p-k+1, p]; the codes one step earlier cover bases
 // [max(ps, p-k), p-1] (k-1 bases at the segment's first k-mer, where the reference's
 // warm-up leaves them).  d = high half of the earlier c | low half of c, v likewise from u.
+// A thread takes four consecutive slots: within one read and segment the codes roll base by
+// base (the earlier codes are the previous slot's), otherwise they are built from the bases.
 struct D2Codes
 {
     uint64_t code1, code2;
     unsigned strand1, strand2;
     bool keep1, keep2;
-    int read, pos;
 };
 
-__device__ __forceinline__ bool d2_slot(const DevBlock& b, const int64_t* __restrict__ manno,
-                                        const int32_t* __restrict__ mdata, int kmer, const D2Masks& M, int64_t s,
-                                        D2Codes& o)
+// the unmasked segment [ps, q) holding the k-mer [p0, p], or false (tuple_thread :436-460)
+__device__ __forceinline__ bool d2_segment(const DevBlock& b, const int64_t* __restrict__ manno,
+                                           const int32_t* __restrict__ mdata, int r, int p0, int p, int& ps)
 {
-    const int r = read_of_slot(b, s, kmer);
-    const int p0 = (int)(s - kstart_of(b, r, kmer));
-    const int p = p0 + kmer - 1;
-    int ps = 0;
-    if (manno)
+    ps = 0;
+    if (!manno)
+        return true;
+    const int64_t f0 = manno[r], f1 = manno[r + 1];
+    int q = b.rlen[r];
+    for (int64_t a = f0; a < f1; a += 2)
     {
-        // the unmasked segment containing p0 must also contain p (the segments between the
-        // mask intervals, tuple_thread's loop :436-460)
-        int64_t f0 = manno[r], f1 = manno[r + 1];
-        int q = b.rlen[r];
-        for (int64_t a = f0; a < f1; a += 2)
+        const int ib = mdata[a], ie = mdata[a + 1];
+        if (p0 < ib)
         {
-            int ib = mdata[a], ie = mdata[a + 1];
-            if (p0 < ib)
-            {
-                q = ib;
-                break;
-            }
-            ps = ie;
-            q = b.rlen[r];
+            q = ib;
+            break;
         }
-        if (!(p0 >= ps && p < q))
-            return false;
+        ps = ie;
+        q = b.rlen[r];
     }
-    const uint8_t* src = b.bases + b.boff[r];
-    const int top = M.kshift - 2;
-    uint64_t c = 0, u = 0, cp = 0, up = 0;
-    const int lo = max(ps, p - kmer);
-    for (int t = lo; t < p; t++)
-    {
-        const uint64_t x = src[t];
-        cp = (cp << 2) | x;
-        up = (up >> 2) | ((3ull - x) << top);
-    }
-    for (int t = p - kmer + 1; t <= p; t++)
-    {
-        const uint64_t x = src[t];
-        c = (c << 2) | x;
-        u = (u >> 2) | ((3ull - x) << top);
-    }
-    c &= M.kmask;
-    cp &= M.kmask;
-    const uint64_t d = (cp & M.hf) | (c & M.lf);
-    const uint64_t v = (up & M.lr) | (u & M.hr);
-    if (u < c)
-    {
-        o.code1 = u;
-        o.strand1 = 1;
-    }
-    else
-    {
-        o.code1 = c;
-        o.strand1 = 0;
-    }
-    if (v < d)
-    {
-        o.code2 = v;
-        o.strand2 = 1;
-    }
-    else
-    {
-        o.code2 = d;
-        o.strand2 = 0;
-    }
-    o.keep1 = d2_keep(o.code1, M.kshift);
-    o.keep2 = d2_keep(o.code2, M.kshift);
-    o.read = r;
-    o.pos = p;
-    return true;
+    return p0 >= ps && p < q;
 }
 
-__global__ void __launch_bounds__(F2T) k_d2_count(DevBlock b, const int64_t* __restrict__ manno,
-                                                 const int32_t* __restrict__ mdata, int kmer, D2Masks M,
-                                                 int64_t nslots, uint32_t* count)
+__device__ __forceinline__ void d2_pick(uint64_t c, uint64_t u, uint64_t cp, uint64_t up, const D2Masks& M,
+                                        D2Codes& o)
 {
-    const int64_t s = (int64_t)blockIdx.x * F2T + threadIdx.x;
-    if (s >= nslots)
+    const uint64_t d = (cp & M.hf) | (c & M.lf);
+    const uint64_t v = (up & M.lr) | (u & M.hr);
+    o.code1 = u < c ? u : c;
+    o.strand1 = u < c;
+    o.code2 = v < d ? v : d;
+    o.strand2 = v < d;
+    o.keep1 = d2_keep(o.code1, M.kshift);
+    o.keep2 = d2_keep(o.code2, M.kshift);
+}
+
+// EMIT = false: count[s] = codes the slot lists; EMIT = true: the slot's entries at off[s]
+template <bool EMIT, typename K>
+__global__ void __launch_bounds__(F2T) k_d2_slots(DevBlock b, const int64_t* __restrict__ manno,
+                                                 const int32_t* __restrict__ mdata, int kmer, D2Masks M,
+                                                 int64_t nslots, uint32_t* count, const uint32_t* __restrict__ off,
+                                                 K* keys, uint32_t* vals, int32_t* rd, int32_t* rp)
+{
+    const int64_t s0 = ((int64_t)blockIdx.x * F2T + threadIdx.x) * 4;
+    if (s0 >= nslots)
         return;
-    D2Codes o;
-    count[s] = d2_slot(b, manno, mdata, kmer, M, s, o) ? (uint32_t)o.keep1 + (uint32_t)o.keep2 : 0u;
+    const int nj = (int)min((int64_t)4, nslots - s0);
+    const int top = M.kshift - 2;
+    int r = read_of_slot(b, s0, kmer);
+    int64_t kst = kstart_of(b, r, kmer), knext = kstart_of(b, r + 1, kmer);
+    uint64_t c = 0, u = 0;
+    int have = -2, seg = -1;  // position whose codes are in (c, u), and its segment start
+    unsigned cnt[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+    {
+        if (j >= nj)
+            break;
+        const int64_t s = s0 + j;
+        while (s >= knext)
+        {
+            r++;
+            kst = knext;
+            knext = kstart_of(b, r + 1, kmer);
+            have = -2;
+        }
+        const int p0 = (int)(s - kst), p = p0 + kmer - 1;
+        int ps;
+        if (!d2_segment(b, manno, mdata, r, p0, p, ps))
+        {
+            have = -2;
+            continue;
+        }
+        const uint8_t* src = b.bases + b.boff[r];
+        uint64_t cp, up;
+        if (have == p - 1 && seg == ps)
+        {
+            const uint64_t x = src[p];
+            cp = c;
+            up = u;
+            c = ((c << 2) | x) & M.kmask;
+            u = (u >> 2) | ((3ull - x) << top);
+        }
+        else
+        {
+            cp = up = c = u = 0;
+            for (int t = max(ps, p - kmer); t < p; t++)
+            {
+                const uint64_t x = src[t];
+                cp = (cp << 2) | x;
+                up = (up >> 2) | ((3ull - x) << top);
+            }
+            for (int t = p - kmer + 1; t <= p; t++)
+            {
+                const uint64_t x = src[t];
+                c = (c << 2) | x;
+                u = (u >> 2) | ((3ull - x) << top);
+            }
+            c &= M.kmask;
+            cp &= M.kmask;
+        }
+        have = p;
+        seg = ps;
+        D2Codes o;
+        d2_pick(c, u, cp, up, M, o);
+        if (!EMIT)
+            cnt[j] = (unsigned)o.keep1 + (unsigned)o.keep2;
+        else
+        {
+            uint32_t e = off[s];
+            if (o.keep1)
+            {
+                keys[e] = (K)o.code1;
+                vals[e] = e;
+                rd[e] = (r << 1) | (int)o.strand1;
+                rp[e] = p;
+                e++;
+            }
+            if (o.keep2)
+            {
+                keys[e] = (K)o.code2;
+                vals[e] = e;
+                rd[e] = (r << 1) | (int)o.strand2;
+                rp[e] = p;
+            }
+        }
+    }
+    if (!EMIT)
+    {
+        if (nj == 4)
+            *reinterpret_cast<uint4*>(count + s0) = make_uint4(cnt[0], cnt[1], cnt[2], cnt[3]);
+        else
+            for (int j = 0; j < nj; j++)
+                count[s0 + j] = cnt[j];
+    }
 }
 
 int launch_d2_count(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, int kmer,
@@ -138,41 +190,12 @@ int launch_d2_count(const DevBlock& b, const int64_t* mask_anno, const int32_t* 
 {
     if (nslots <= 0)
         return 0;
-    k_d2_count<<<(unsigned)gd_cdiv<int64_t>(nslots, F2T), F2T, 0, s>>>(b, mask_anno, mask_data, kmer, m, nslots,
-                                                                       count);
+    const int64_t threads = (nslots + 3) / 4;
+    k_d2_slots<false, uint32_t><<<(unsigned)gd_cdiv<int64_t>(threads, F2T), F2T, 0, s>>>(
+        b, mask_anno, mask_data, kmer, m, nslots, count, nullptr, nullptr, nullptr, nullptr, nullptr);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
-}
-
-template <typename K>
-__global__ void __launch_bounds__(F2T) k_d2_emit(DevBlock b, const int64_t* __restrict__ manno,
-                                                const int32_t* __restrict__ mdata, int kmer, D2Masks M,
-                                                int64_t nslots, const uint32_t* __restrict__ off, K* keys,
-                                                uint32_t* vals, int32_t* rd, int32_t* rp)
-{
-    const int64_t s = (int64_t)blockIdx.x * F2T + threadIdx.x;
-    if (s >= nslots)
-        return;
-    D2Codes o;
-    if (!d2_slot(b, manno, mdata, kmer, M, s, o))
-        return;
-    uint32_t e = off[s];
-    if (o.keep1)
-    {
-        keys[e] = (K)o.code1;
-        vals[e] = e;
-        rd[e] = (o.read << 1) | (int)o.strand1;
-        rp[e] = o.pos;
-        e++;
-    }
-    if (o.keep2)
-    {
-        keys[e] = (K)o.code2;
-        vals[e] = e;
-        rd[e] = (o.read << 1) | (int)o.strand2;
-        rp[e] = o.pos;
-    }
 }
 
 template <typename K>
@@ -182,8 +205,9 @@ int launch_d2_emit(const DevBlock& b, const int64_t* mask_anno, const int32_t* m
 {
     if (nslots <= 0)
         return 0;
-    k_d2_emit<K><<<(unsigned)gd_cdiv<int64_t>(nslots, F2T), F2T, 0, s>>>(b, mask_anno, mask_data, kmer, m, nslots,
-                                                                         off, keys, vals, rd, rp);
+    const int64_t threads = (nslots + 3) / 4;
+    k_d2_slots<true, K><<<(unsigned)gd_cdiv<int64_t>(threads, F2T), F2T, 0, s>>>(
+        b, mask_anno, mask_data, kmer, m, nslots, nullptr, off, keys, vals, rd, rp);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;

@@ -586,7 +586,14 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
         return -1;
     }
     int ntiles = (int)tiles64;
-    static int pipe_grid = 0;
+    static int pipe_grids[GD_MAX_DEVICES] = {};
+    const int dv = gd_device();
+    if (dv < 0)
+    {
+        gd_set_error("radix sort: no usable current device");
+        return -1;
+    }
+    int& pipe_grid = pipe_grids[dv];
     if (!pipe_grid)
     {
         GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,

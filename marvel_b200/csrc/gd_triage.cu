@@ -594,7 +594,11 @@ static int mlp_smem_attr(const void* fn)
 
 static int infer_grid(int64_t ntiles)
 {
-    static int blocks = 0;
+    static int grids[GD_MAX_DEVICES] = {};
+    const int dv = gd_device();
+    if (dv < 0)
+        return -1;
+    int& blocks = grids[dv];
     if (!blocks)
     {
         int dev = 0, nsm = 0, per = 0;
@@ -624,12 +628,15 @@ int launch_mlp_forward(const float* params, const float* x, int64_t n, float* p,
 int launch_mlp_grad_perm(const float* params, const float* x, const float* y, const int* perm, int64_t n0, int n,
                          float pos_weight, float* grad, float* loss, cudaStream_t s)
 {
-    static bool once = false;
-    if (!once)
+    static bool done[GD_MAX_DEVICES] = {};
+    const int dv = gd_device();
+    if (dv < 0)
+        return -1;
+    if (!done[dv])
     {
         if (mlp_smem_attr((const void*)k_mlp_grad))
             return -1;
-        once = true;
+        done[dv] = true;
     }
     GD_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * TRI_NPARAM, s));
     GD_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), s));
