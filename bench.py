@@ -300,7 +300,11 @@ def run_gpu(args):
                          "traffic": int(ALIGN_DRAM_BYTES_PER_CELL * cells / 2),
                          "traffic_source": "bytes per launch: dram read+write per wave cell of the cfg1 ncu capture "
                                            "(profiles/k_align_pairs_cfg1.md) x this launch's cells",
-                         "peak_source": "derived: 148 SM x 128 lanes/clk x median SM clock under load"},
+                         "peak_source": "derived: 148 SM x 128 lanes/clk x median SM clock under load",
+                         "issue_slots_busy": 0.727,
+                         "issue_source": "smsp__issue_active of the cfg1 ncu capture (profiles/k_align_pairs_cfg1.md): "
+                                         "the kernel issues on 73 % of cycles; a wave is ~11 diagonals wide, so a "
+                                         "warp instruction carries about a third of a warp of cells"},
             "roofline_filter": {"bound": "hbm", "kernel": "k-mer index (extract + 4 LSD passes)",
                                 "achieved": round(idx_bytes / (idx_ms / 1e3) / 1e9, 1),
                                 "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
