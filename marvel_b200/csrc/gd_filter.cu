@@ -231,6 +231,38 @@ __global__ void __launch_bounds__(FT) k_run_flags(const K* __restrict__ code, in
         flags[i] = (i == 0 || code[i] != code[i - 1]) ? 1u : 0u;
 }
 
+template <typename K>
+__global__ void __launch_bounds__(FT) k_code_buckets(const K* __restrict__ code, int64_t n, int shift, uint32_t nb,
+                                                    uint32_t* table)
+{
+    // entry i opens the buckets (prefix of entry i-1, prefix of entry i]; the last entry also
+    // closes the ones after it
+    const int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t pc = code_bucket(code[i], shift, nb);
+    const uint32_t p0 = i == 0 ? 0u : code_bucket(code[i - 1], shift, nb) + 1u;
+    for (uint32_t p = p0; p <= pc; p++)
+        table[p] = (uint32_t)i;
+    if (i == n - 1)
+        for (uint32_t p = pc + 1; p <= nb + 1; p++)
+            table[p] = (uint32_t)n;
+}
+
+template <typename K>
+int launch_code_buckets(const K* code, int64_t n, int shift, uint32_t nb, uint32_t* table, cudaStream_t s)
+{
+    if (n <= 0)
+    {
+        GD_CUDA(cudaMemsetAsync(table, 0, ((size_t)nb + 2) * 4, s));
+        return 0;
+    }
+    k_code_buckets<K><<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(code, n, shift, nb, table);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 __global__ void __launch_bounds__(FT) k_run_starts(const uint32_t* __restrict__ flags,
                                                   const uint32_t* __restrict__ excl, int64_t n, uint32_t nruns,
                                                   uint32_t* runstart)
@@ -273,20 +305,6 @@ __global__ void __launch_bounds__(FT) k_pair_count(const K* __restrict__ acode, 
                                                   MergeArgs m, uint32_t* jb_out, uint64_t* cnt_out,
                                                   unsigned long long* ctrun)
 {
-    // A is sorted: the block's codes span [acode[t0], acode[t1]], so every B range it needs
-    // lies in [lower(acode[t0]), upper(acode[t1])) -- two full searches per block, then
-    // short ones per entry
-    __shared__ int64_t s_lo, s_hi;
-    const int64_t t0 = (int64_t)blockIdx.x * FT;
-    const int64_t t1 = min(t0 + FT, m.na) - 1;
-    if (!m.runstart)
-    {
-        if (threadIdx.x == 0)
-            s_lo = lower_code(bcode, m.nb, acode[t0]);
-        else if (threadIdx.x == 32)
-            s_hi = upper_code(bcode, m.nb, acode[t1]);
-    }
-    __syncthreads();
     int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
     bool act = i < m.na;
     uint64_t n = 0;
@@ -304,8 +322,10 @@ __global__ void __launch_bounds__(FT) k_pair_count(const K* __restrict__ acode, 
     }
     else if (act)
     {
+        // the B run of the code: a search inside the code's bucket
         K c = acode[i];
-        const int64_t lo = s_lo, hi = s_hi;
+        const uint32_t bk = code_bucket(c, m.bshift, m.nbuckets);
+        const int64_t lo = m.btable[bk], hi = m.btable[bk + 1];
         int64_t jb = lower_code_in(bcode, lo, hi, c);
         int64_t je = jb;
         if (jb < hi && bcode[jb] == c)
@@ -629,6 +649,7 @@ int launch_complement(const DevBlock& src, uint8_t* dst_bases, const int64_t* an
     template int launch_compact_index<K>(const K*, const int32_t*, const int32_t*, const uint32_t*,              \
                                          const uint32_t*, int64_t, K*, int32_t*, int32_t*, cudaStream_t);        \
     template int launch_run_flags<K>(const K*, int64_t, uint32_t*, cudaStream_t);                                \
+    template int launch_code_buckets<K>(const K*, int64_t, int, uint32_t, uint32_t*, cudaStream_t);              \
     template int launch_pair_count<K>(const K*, const int32_t*, const int32_t*, const uint32_t*, const uint32_t*, \
                                       const K*, const int32_t*, const int32_t*, MergeArgs, uint32_t*, uint64_t*, \
                                       unsigned long long*, cudaStream_t);

@@ -41,7 +41,34 @@ struct MergeArgs
     // non-null when B is A's own index (a block against itself, forward): the start of every
     // code run of A (nruns + 1 entries, the last = na), so no searches are needed
     const uint32_t* runstart;
+    // otherwise: btable[p] = the first B entry whose code >> bshift is >= p (code_buckets)
+    const uint32_t* btable;
+    int bshift;
+    uint32_t nbuckets;
 };
+
+// Bucket table of a sorted code array: with bucket(code) = min(code >> shift, nb), table[p] =
+// the first index whose bucket is >= p, for p in [0, nb + 1]: a code's run lies in
+// [table[b], table[b + 1]).  Bucket nb holds codes beyond 4^k (the all-ones code of a masked
+// slot that the 4-byte sort for k = 16 can leave inside the index).  bucket_shift: the shift
+// that gives at most 2^20 buckets for k-mers of length kmer.
+inline int bucket_shift(int kmer)
+{
+    return 2 * kmer > 20 ? 2 * kmer - 20 : 0;
+}
+inline uint32_t bucket_count(int kmer)
+{
+    return 1u << (2 * kmer - bucket_shift(kmer));
+}
+template <typename K>
+int launch_code_buckets(const K* code, int64_t n, int shift, uint32_t nb, uint32_t* table, cudaStream_t s);
+
+template <typename K>
+__device__ __forceinline__ uint32_t code_bucket(K code, int shift, uint32_t nb)
+{
+    const K b = code >> shift;
+    return b < (K)nb ? (uint32_t)b : nb;
+}
 
 // runstart[excl[i]] = i for every run head i, runstart[nruns] = n
 int launch_run_starts(const uint32_t* flags, const uint32_t* excl, int64_t n, uint32_t nruns, uint32_t* runstart,

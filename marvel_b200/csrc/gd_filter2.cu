@@ -267,23 +267,14 @@ __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ aco
                                                       const uint32_t* __restrict__ arun_excl,
                                                       const uint32_t* __restrict__ arun_flag,
                                                       const uint32_t* __restrict__ runstart,
+                                                      const uint32_t* __restrict__ btable, int bshift,
+                                                      uint32_t nbuckets,
                                                       const K* __restrict__ bcode, const int32_t* __restrict__ bread,
                                                       const uint32_t* __restrict__ bstrand_excl, int64_t na,
                                                       int64_t nb, int self, int identity, uint32_t* jb_out,
                                                       uint64_t* cnt_f, uint64_t* cnt_c, unsigned long long* ctrun)
 {
-    __shared__ int64_t s_lo, s_hi;
-    const int64_t t0 = (int64_t)blockIdx.x * F2T;
-    const int64_t t1 = min(t0 + F2T, na) - 1;
-    if (!runstart)
-    {
-        if (threadIdx.x == 0)
-            s_lo = lower_code(bcode, nb, acode[t0]);
-        else if (threadIdx.x == 32)
-            s_hi = upper_code(bcode, nb, acode[t1]);
-    }
-    __syncthreads();
-    const int64_t i = t0 + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * F2T + threadIdx.x;
     const bool act = i < na;
     uint64_t n = 0;
     uint32_t run = 0;
@@ -301,10 +292,12 @@ __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ aco
         else
         {
             const K c = acode[i];
-            jb = lower_code_in(bcode, s_lo, s_hi, c);
+            const uint32_t bk = code_bucket(c, bshift, nbuckets);
+            const int64_t lo = btable[bk], hi = btable[bk + 1];
+            jb = lower_code_in(bcode, lo, hi, c);
             int64_t je = jb;
-            if (jb < s_hi && bcode[jb] == c)
-                je = upper_code_from(bcode, jb, s_hi, c);
+            if (jb < hi && bcode[jb] == c)
+                je = upper_code_from(bcode, jb, hi, c);
             e = je;
             if (self)
             {
@@ -344,15 +337,16 @@ __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ aco
 
 template <typename K>
 int launch_d2_pair_count(const K* acode, const int32_t* aread, const uint32_t* arun_excl, const uint32_t* arun_flag,
-                         const uint32_t* runstart, const K* bcode, const int32_t* bread, const uint32_t* bstrand_excl,
-                         int64_t na, int64_t nb, int self, int identity, uint32_t* jb, uint64_t* cnt_f,
-                         uint64_t* cnt_c, unsigned long long* ctrun, cudaStream_t s)
+                         const uint32_t* runstart, const uint32_t* btable, int bshift, uint32_t nbuckets,
+                         const K* bcode, const int32_t* bread, const uint32_t* bstrand_excl, int64_t na, int64_t nb,
+                         int self, int identity, uint32_t* jb, uint64_t* cnt_f, uint64_t* cnt_c,
+                         unsigned long long* ctrun, cudaStream_t s)
 {
     if (na <= 0)
         return 0;
     k_d2_pair_count<K><<<(unsigned)gd_cdiv<int64_t>(na, F2T), F2T, 0, s>>>(
-        acode, aread, arun_excl, arun_flag, runstart, bcode, bread, bstrand_excl, na, nb, self, identity, jb, cnt_f,
-        cnt_c, ctrun);
+        acode, aread, arun_excl, arun_flag, runstart, btable, bshift, nbuckets, bcode, bread, bstrand_excl, na, nb,
+        self, identity, jb, cnt_f, cnt_c, ctrun);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
@@ -426,9 +420,10 @@ int launch_d2_emit_hits(const int32_t* aread, const int32_t* arpos, const int32_
     template int launch_d2_gather<K>(const K*, const uint32_t*, int64_t, const int32_t*, const int32_t*, K*,     \
                                      int32_t*, int32_t*, cudaStream_t);                                          \
     template int launch_d2_pair_count<K>(const K*, const int32_t*, const uint32_t*, const uint32_t*,             \
-                                         const uint32_t*, const K*, const int32_t*, const uint32_t*, int64_t,    \
-                                         int64_t, int, int, uint32_t*, uint64_t*, uint64_t*, unsigned long long*, \
-                                         cudaStream_t);
+                                         const uint32_t*, const uint32_t*, int, uint32_t, const K*,              \
+                                         const int32_t*,                                                         \
+                                         const uint32_t*, int64_t, int64_t, int, int, uint32_t*, uint64_t*,      \
+                                         uint64_t*, unsigned long long*, cudaStream_t);
 INST2(uint32_t)
 INST2(uint64_t)
 #undef INST2

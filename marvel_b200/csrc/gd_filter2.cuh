@@ -40,12 +40,14 @@ int launch_d2_strand_flags(const int32_t* read, int64_t n, uint32_t* flags, cuda
 
 // Per A entry: the B range [jb, jb + n) it pairs with, split by orientation (cnt_f forward,
 // cnt_c complement), and the per-code-run totals (count_thread, dalign2/filter.c:1136-1256).
-// runstart (non-null when B is A's own index): the start of every code run of A.
+// runstart (non-null when B is A's own index): the start of every code run of A; otherwise
+// btable / bshift: B's bucket table (launch_code_buckets).
 template <typename K>
 int launch_d2_pair_count(const K* acode, const int32_t* aread, const uint32_t* arun_excl, const uint32_t* arun_flag,
-                         const uint32_t* runstart, const K* bcode, const int32_t* bread, const uint32_t* bstrand_excl,
-                         int64_t na, int64_t nb, int self, int identity, uint32_t* jb, uint64_t* cnt_f,
-                         uint64_t* cnt_c, unsigned long long* ctrun, cudaStream_t s);
+                         const uint32_t* runstart, const uint32_t* btable, int bshift, uint32_t nbuckets,
+                         const K* bcode, const int32_t* bread, const uint32_t* bstrand_excl, int64_t na, int64_t nb,
+                         int self, int identity, uint32_t* jb, uint64_t* cnt_f, uint64_t* cnt_c,
+                         unsigned long long* ctrun, cudaStream_t s);
 
 // The hits of each orientation in generation order (merge_thread, dalign2/filter.c:1259-1466):
 // forward into (fkey, fdiag) at foff, complement -- B position reflected -- into (ckey, cdiag)

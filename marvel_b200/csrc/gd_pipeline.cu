@@ -182,7 +182,7 @@ struct gd_context
     int agrid_w = 0;
     int test_narrow = 0;  // tests only: the main aligner pass with the 32-diagonal instance
     int variant = 1, hgap = 0;  // 2 = daligner2 (modimizer seeds, dalign2/), its -H
-    DevBuf d2rd, d2rp, d2sgn, cnt2, hoff2, hk2, hd2, runstart;
+    DevBuf d2rd, d2rp, d2sgn, cnt2, hoff2, hk2, hd2, runstart, btable;
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
     int bvcap = 8192, btcap = 1024;  // daligner2 bridging scratch per warp (ints, trace values)
     uint64_t rcap = 1 << 22, tbcap = 512ull << 20;
@@ -463,13 +463,23 @@ static int match_filter_t(gd_context* c, int bslot, int comp, int self)
     if (ensure(c->ctrun, (size_t)nruns * 8 + 8))
         return -1;
     GD_CUDA(cudaMemsetAsync(c->ctrun.p, 0, (size_t)nruns * 8, s));
-    MergeArgs m{na, nb, self, c->identity, comp, nullptr};
+    MergeArgs m{na, nb, self, c->identity, comp, nullptr, nullptr, 0, 0};
     if (&B == &A)  // the block against its own index: run bounds without searches
     {
         if (ensure(c->runstart, ((size_t)nruns + 1) * 4) ||
             launch_run_starts(P<uint32_t>(c->flags), P<uint32_t>(c->excl), na, nruns, P<uint32_t>(c->runstart), s))
             return -1;
         m.runstart = P<uint32_t>(c->runstart);
+    }
+    else  // the B index's bucket table: each search stays inside its code's bucket
+    {
+        m.bshift = bucket_shift(c->kmer);
+        m.nbuckets = bucket_count(c->kmer);
+        const uint32_t nbk = m.nbuckets;
+        if (ensure(c->btable, ((size_t)nbk + 2) * 4) ||
+            launch_code_buckets<K>(P<K>(B.code), nb, m.bshift, nbk, P<uint32_t>(c->btable), s))
+            return -1;
+        m.btable = P<uint32_t>(c->btable);
     }
     if (launch_pair_count<K>(P<K>(A.code), P<int32_t>(A.read), P<int32_t>(A.rpos), P<uint32_t>(c->excl),
                              P<uint32_t>(c->flags), P<K>(B.code), P<int32_t>(B.read), P<int32_t>(B.rpos), m,
@@ -615,6 +625,9 @@ static int match_filter_d2_t(gd_context* c, int bslot, int cslot, int self)
         return -1;
     GD_CUDA(cudaMemsetAsync(c->ctrun.p, 0, (size_t)nruns * 8, s));
     const uint32_t* runstart = nullptr;
+    const uint32_t* btable = nullptr;
+    const int bshift = bucket_shift(c->kmer);
+    const uint32_t nbk = bucket_count(c->kmer);
     if (&B == &A)  // the block against its own index: run bounds without searches
     {
         if (ensure(c->runstart, ((size_t)nruns + 1) * 4) ||
@@ -622,8 +635,15 @@ static int match_filter_d2_t(gd_context* c, int bslot, int cslot, int self)
             return -1;
         runstart = P<uint32_t>(c->runstart);
     }
+    else  // the B index's bucket table: each search stays inside its code's bucket
+    {
+        if (ensure(c->btable, ((size_t)nbk + 2) * 4) ||
+            launch_code_buckets<K>(P<K>(B.code), nb, bshift, nbk, P<uint32_t>(c->btable), s))
+            return -1;
+        btable = P<uint32_t>(c->btable);
+    }
     if (launch_d2_pair_count<K>(P<K>(A.code), P<int32_t>(A.read), P<uint32_t>(c->excl), P<uint32_t>(c->flags),
-                                runstart, P<K>(B.code), P<int32_t>(B.read), sgn, na, nb, self, c->identity,
+                                runstart, btable, bshift, nbk, P<K>(B.code), P<int32_t>(B.read), sgn, na, nb, self, c->identity,
                                 P<uint32_t>(c->jb), P<uint64_t>(c->cnt), P<uint64_t>(c->cnt2),
                                 P<unsigned long long>(c->ctrun), s) ||
         launch_gram(P<unsigned long long>(c->ctrun), nruns, P<unsigned long long>(c->gram), s))
