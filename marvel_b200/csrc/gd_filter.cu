@@ -485,12 +485,43 @@ __global__ void __launch_bounds__(FT) k_emit(const int32_t* __restrict__ aread, 
     uint64_t akey = ((uint64_t)ar << hb.pbits) | (uint64_t)ap;
     int sh = hb.pbits + hb.abits;
     uint32_t b0 = jb[i];
-    for (uint64_t j = 0; j < n; j++)
-    {
-        uint32_t b = b0 + (uint32_t)j;
-        hkey[o + j] = ((uint64_t)bread[b] << sh) | akey;
-        hdiag[o + j] = (uint32_t)(ap - brpos[b]);
-    }
+    if (hb.qbits > 0)
+        for (uint64_t j = 0; j < n; j++)
+        {
+            uint32_t b = b0 + (uint32_t)j;
+            hkey[o + j] = ((((uint64_t)bread[b] << sh) | akey) << hb.qbits) | (uint64_t)(uint32_t)brpos[b];
+        }
+    else
+        for (uint64_t j = 0; j < n; j++)
+        {
+            uint32_t b = b0 + (uint32_t)j;
+            hkey[o + j] = ((uint64_t)bread[b] << sh) | akey;
+            hdiag[o + j] = (uint32_t)(ap - brpos[b]);
+        }
+}
+
+__global__ void __launch_bounds__(FT) k_hit_unpack(const uint64_t* __restrict__ packed, int64_t n, HitBits hb,
+                                                  uint64_t* __restrict__ hkey, uint32_t* __restrict__ hdiag)
+{
+    const int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint64_t v = packed[i];
+    const uint64_t k = v >> hb.qbits;
+    const int bpos = (int)(v & ((1ull << hb.qbits) - 1));
+    const int apos = (int)(k & ((1ull << hb.pbits) - 1));
+    hkey[i] = k;
+    hdiag[i] = (uint32_t)(apos - bpos);
+}
+
+int launch_hit_unpack(const uint64_t* packed, int64_t n, HitBits hb, uint64_t* hkey, uint32_t* hdiag, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_hit_unpack<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(packed, n, hb, hkey, hdiag);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
 }
 
 int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread, const int32_t* brpos,

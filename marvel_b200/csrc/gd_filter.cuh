@@ -90,11 +90,18 @@ int launch_cnt_mask(const uint32_t* arun_excl, const uint32_t* arun_flag, const 
 struct HitBits
 {
     int pbits, abits, bbits;
+    // > 0: the emitted hits are packed keys (bread, aread, apos, bpos) with the B position in
+    // the low qbits (no separate diag array), sorted keys-only on the upper bits and then
+    // unpacked by launch_hit_unpack; 0: (key, diag) pairs
+    int qbits;
 };
 
 int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread, const int32_t* brpos,
                 const uint32_t* jb, const uint64_t* cnt, const uint64_t* hoff, int64_t na, HitBits hb,
                 uint64_t* hkey, uint32_t* hdiag, cudaStream_t s);
+
+// sorted packed hits -> hkey (bread, aread, apos) and hdiag (apos - bpos)
+int launch_hit_unpack(const uint64_t* packed, int64_t n, HitBits hb, uint64_t* hkey, uint32_t* hdiag, cudaStream_t s);
 
 // Pair groups of the sorted hits: start flags, then (start, end) of groups with >= minhit hits.
 int launch_pair_flags(const uint64_t* hkey, int64_t n, int pbits, uint32_t* flags, cudaStream_t s);

@@ -384,18 +384,19 @@ __global__ void __launch_bounds__(F2T) k_d2_emit_hits(const int32_t* __restrict_
         const uint32_t q = b0 + (uint32_t)j;
         const int br = bread[q] >> 1, bs = bread[q] & 1;
         const uint64_t key = ((uint64_t)br << sh) | akey;
-        if (bs == as)
-        {
-            fkey[of] = key;
-            fdiag[of] = (uint32_t)(ap - brpos[q]);
-            of++;
-        }
+        const int bp = (bs == as) ? brpos[q] : (brlen[br] - brpos[q]) + koff;
+        uint64_t* dk = (bs == as) ? fkey + of : ckey + oc;
+        if (hb.qbits > 0)
+            *dk = (key << hb.qbits) | (uint64_t)(uint32_t)bp;
         else
         {
-            ckey[oc] = key;
-            cdiag[oc] = (uint32_t)(ap - ((brlen[br] - brpos[q]) + koff));
-            oc++;
+            *dk = key;
+            ((bs == as) ? fdiag + of : cdiag + oc)[0] = (uint32_t)(ap - bp);
         }
+        if (bs == as)
+            of++;
+        else
+            oc++;
     }
 }
 

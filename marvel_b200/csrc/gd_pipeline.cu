@@ -427,6 +427,13 @@ static int tri_append(gd_context* c, unsigned ng)
 }
 
 static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBits hb, int comp, int self);
+
+// bits of the B position when (bread, aread, apos, bpos) fits one 64-bit word, else 0
+static int hit_qbits(const gd::HitBits& hb, const Slot& B)
+{
+    const int q = bits_for(std::max(B.blk.maxlen - 1, 1));
+    return hb.pbits + hb.abits + hb.bbits + q <= 64 ? q : 0;
+}
 static int pair_cap(gd_context* c, int64_t na, int64_t nb, int same_index, int* limit_out);
 template <typename K>
 static int match_emit_t(gd_context* c, Slot& A, Slot& B, int64_t na, uint64_t* d_nhits, int comp, int self);
@@ -569,6 +576,7 @@ static int match_emit_t(gd_context* c, Slot& A, Slot& B, int64_t na, uint64_t* d
         gd_set_error("hit key needs %d bits (> 64): block too large for this build", hbits);
         return -1;
     }
+    hb.qbits = hit_qbits(hb, B);
     if (ensure(c->hk0, nhits * 8) || ensure(c->hk1, nhits * 8) || ensure(c->hd0, nhits * 4) ||
         ensure(c->hd1, nhits * 4) || ensure(c->scratch, radix_scratch_bytes(nhits)))
         return -1;
@@ -684,6 +692,7 @@ static int match_filter_d2_t(gd_context* c, int bslot, int cslot, int self)
         gd_set_error("hit key needs %d bits (> 64): block too large for this build", hb.pbits + hb.abits + hb.bbits);
         return -1;
     }
+    hb.qbits = hit_qbits(hb, B);
     if (ensure(c->hk0, nmax * 8 + 8) || ensure(c->hk1, nmax * 8 + 8) || ensure(c->hd0, nmax * 4 + 4) ||
         ensure(c->hd1, nmax * 4 + 4) || ensure(c->hk2, nc * 8 + 8) || ensure(c->hd2, nc * 4 + 4) ||
         ensure(c->scratch, radix_scratch_bytes(nmax)))
@@ -699,7 +708,8 @@ static int match_filter_d2_t(gd_context* c, int bslot, int cslot, int self)
     {
         GD_CUDA(cudaEventRecord(c->ev0, s));
         GD_CUDA(cudaMemcpyAsync(c->hk0.p, c->hk2.p, nc * 8, cudaMemcpyDeviceToDevice, s));
-        GD_CUDA(cudaMemcpyAsync(c->hd0.p, c->hd2.p, nc * 4, cudaMemcpyDeviceToDevice, s));
+        if (hb.qbits == 0)
+            GD_CUDA(cudaMemcpyAsync(c->hd0.p, c->hd2.p, nc * 4, cudaMemcpyDeviceToDevice, s));
         if (align_hits(c, A, C, nc, hb, 1, self))
             return -1;
     }
@@ -716,19 +726,39 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     const int oi = comp ? 1 : 0;
     const int hbits = hb.pbits + hb.abits + hb.bbits;
     // hit sort by (bread, aread, apos), stable (pairsort, filter.c:2030-2054, 2239-2252)
-    int which = radix_sort_pairs<uint64_t>(P<uint64_t>(c->hk0), P<uint32_t>(c->hd0), P<uint64_t>(c->hk1),
-                                           P<uint32_t>(c->hd1), nhits, 0, hbits, c->scratch.p, s);
-    if (which < 0)
-        return -1;
-    uint64_t* hkey = which ? P<uint64_t>(c->hk1) : P<uint64_t>(c->hk0);
-    uint32_t* hdiag = which ? P<uint32_t>(c->hd1) : P<uint32_t>(c->hd0);
+    uint64_t* hkey;
+    uint32_t *hdiag, *pflags, *ppos;  // pflags / ppos: free ping-pong halves
+    if (hb.qbits > 0)
+    {
+        // packed hits: keys alone through the passes, the B position riding below the key
+        int which = radix_sort_keys<uint64_t>(P<uint64_t>(c->hk0), P<uint64_t>(c->hk1), nhits, hb.qbits,
+                                              hb.qbits + hbits, c->scratch.p, s);
+        if (which < 0)
+            return -1;
+        uint64_t* packed = which ? P<uint64_t>(c->hk1) : P<uint64_t>(c->hk0);
+        hkey = which ? P<uint64_t>(c->hk0) : P<uint64_t>(c->hk1);
+        hdiag = P<uint32_t>(c->hd0);
+        if (launch_hit_unpack(packed, nhits, hb, hkey, hdiag, s))
+            return -1;
+        pflags = P<uint32_t>(c->hd1);
+        ppos = (uint32_t*)packed;
+    }
+    else
+    {
+        int which = radix_sort_pairs<uint64_t>(P<uint64_t>(c->hk0), P<uint32_t>(c->hd0), P<uint64_t>(c->hk1),
+                                               P<uint32_t>(c->hd1), nhits, 0, hbits, c->scratch.p, s);
+        if (which < 0)
+            return -1;
+        hkey = which ? P<uint64_t>(c->hk1) : P<uint64_t>(c->hk0);
+        hdiag = which ? P<uint32_t>(c->hd1) : P<uint32_t>(c->hd0);
+        pflags = which ? P<uint32_t>(c->hd0) : P<uint32_t>(c->hd1);
+        ppos = (uint32_t*)(which ? P<uint64_t>(c->hk0) : P<uint64_t>(c->hk1));
+    }
     c->hkey = hkey;
     c->hdiag = hdiag;
     c->nhits = (int64_t)nhits;
     c->hb = hb;
     // pair groups with >= ceil(h/k) hits (report_thread's minhit test, filter.c:1699-1709)
-    uint32_t* pflags = which ? P<uint32_t>(c->hd0) : P<uint32_t>(c->hd1);  // free ping-pong half
-    uint32_t* ppos = (uint32_t*)(which ? P<uint64_t>(c->hk0) : P<uint64_t>(c->hk1));
     uint32_t* d_nst = P<uint32_t>(c->misc) + 24;
     if (launch_pair_flags(hkey, nhits, hb.pbits, pflags, s) ||
         exclusive_scan<uint32_t>(pflags, ppos, nhits, d_nst, c->scratch.p, s))

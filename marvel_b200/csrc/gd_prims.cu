@@ -386,11 +386,21 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                  : "memory");
 }
 
-template <typename K>
-struct RsPipe
+template <bool V>
+struct RsPipeVals
+{
+    uint32_t val[2][RS_TILE];
+};
+template <>
+struct RsPipeVals<false>
+{
+};
+
+// V = false: a keys-only sort (no value arrays)
+template <typename K, bool V = true>
+struct RsPipe : RsPipeVals<V>
 {
     K key[2][RS_TILE];
-    uint32_t val[2][RS_TILE];
     uint32_t wcnt[RS_WARPS][256];
     uint32_t lstart[256];
     uint32_t toff[256];
@@ -398,24 +408,24 @@ struct RsPipe
     uint64_t full[2];
 };
 
-template <typename K>
+template <typename K, bool V>
 constexpr int rs_pipe_ctas()
 {
-    return sizeof(K) == 4 ? 3 : 2;
+    return (sizeof(K) == 4 || !V) ? 3 : 2;
 }
 
 // Full tiles (all but possibly the last) arrive by bulk copy; a ragged last tile is read
-// with plain loads.  Requires 16-byte aligned kin and vin.
-template <typename K>
-__global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
+// with plain loads.  Requires 16-byte aligned kin and vin.  V = false: keys only.
+template <typename K, bool V = true>
+__global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
     k_rs_scatter_pipe(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
                       uint32_t* __restrict__ vout, int64_t n, int shift, const uint32_t* __restrict__ offs, int ntiles)
 {
     extern __shared__ __align__(128) unsigned char rs_pipe_smem[];
-    RsPipe<K>& S = *reinterpret_cast<RsPipe<K>*>(rs_pipe_smem);
+    RsPipe<K, V>& S = *reinterpret_cast<RsPipe<K, V>*>(rs_pipe_smem);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nfull = (int)(n / RS_TILE);
-    constexpr unsigned TILE_BYTES = RS_TILE * (sizeof(K) + sizeof(uint32_t));
+    constexpr unsigned TILE_BYTES = RS_TILE * (sizeof(K) + (V ? sizeof(uint32_t) : 0));
     if (threadIdx.x == 0)
     {
         mbar_init(&S.full[0], 1);
@@ -428,7 +438,8 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
     {
         mbar_expect_tx(&S.full[0], TILE_BYTES);
         bulk_load(S.key[0], kin + (int64_t)tile * RS_TILE, RS_TILE * sizeof(K), &S.full[0]);
-        bulk_load(S.val[0], vin + (int64_t)tile * RS_TILE, RS_TILE * 4, &S.full[0]);
+        if constexpr (V)
+            bulk_load(S.val[0], vin + (int64_t)tile * RS_TILE, RS_TILE * 4, &S.full[0]);
     }
     uint32_t toff = tile < ntiles ? offs[(int64_t)threadIdx.x * ntiles + tile] : 0;
     unsigned parity = 0;  // bit st: phase of stage st's barrier
@@ -441,7 +452,8 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
         {
             mbar_expect_tx(&S.full[st ^ 1], TILE_BYTES);
             bulk_load(S.key[st ^ 1], kin + (int64_t)next * RS_TILE, RS_TILE * sizeof(K), &S.full[st ^ 1]);
-            bulk_load(S.val[st ^ 1], vin + (int64_t)next * RS_TILE, RS_TILE * 4, &S.full[st ^ 1]);
+            if constexpr (V)
+                bulk_load(S.val[st ^ 1], vin + (int64_t)next * RS_TILE, RS_TILE * 4, &S.full[st ^ 1]);
         }
         const uint32_t toff_next = next < ntiles ? offs[(int64_t)threadIdx.x * ntiles + next] : 0;
         S.toff[threadIdx.x] = toff;
@@ -451,7 +463,9 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
         const int64_t tbase = (int64_t)tile * RS_TILE;
         const int tn = (int)min((int64_t)RS_TILE, n - tbase);
         K* skey = S.key[st];
-        uint32_t* sval = S.val[st];
+        uint32_t* sval = nullptr;
+        if constexpr (V)
+            sval = S.val[st];
         bool ok = true;
         if (tile < nfull)
         {
@@ -462,7 +476,8 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
             for (int i = threadIdx.x; i < tn; i += RS_THREADS)
             {
                 skey[i] = kin[tbase + i];
-                sval[i] = vin[tbase + i];
+                if constexpr (V)
+                    sval[i] = vin[tbase + i];
             }
         if (__syncthreads_or(!ok))
         {
@@ -485,7 +500,8 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
             const int i = w * (RS_ROUNDS * 32) + r * 32 + lane;
             const bool valid = i < tn;
             key[r] = valid ? skey[i] : (K)0;
-            val[r] = valid ? sval[i] : 0u;
+            if constexpr (V)
+                val[r] = valid ? sval[i] : 0u;
             unsigned d = valid ? (unsigned)(key[r] >> shift) & 255u : 256u;
             unsigned peers = __match_any_sync(GD_FULL, d);
             unsigned c = valid ? S.wcnt[w][d] : 0;
@@ -537,7 +553,8 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
                 unsigned d = (unsigned)(key[r] >> shift) & 255u;
                 uint32_t pos = S.lstart[d] + S.wcnt[w][d] + ((rank2[r >> 1] >> (16 * (r & 1))) & 0xffffu);
                 skey[pos] = key[r];
-                sval[pos] = val[r];
+                if constexpr (V)
+                    sval[pos] = val[r];
             }
         }
         __syncthreads();
@@ -547,7 +564,8 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K>())
             unsigned d = (unsigned)(k >> shift) & 255u;
             uint32_t dest = S.toff[d] + (uint32_t)i - S.lstart[d];
             kout[dest] = k;
-            vout[dest] = sval[i];
+            if constexpr (V)
+                vout[dest] = sval[i];
         }
         // this stage is refilled by the bulk copy engine two tiles on: order these generic
         // accesses before it
@@ -638,6 +656,65 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
     return cur;
 }
 
+template <typename K>
+int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* scratch, cudaStream_t s)
+{
+    if (n <= 1 || end_bit <= begin_bit)
+        return 0;
+    int64_t tiles64 = gd_cdiv<int64_t>(n, RS_TILE);
+    if (tiles64 > (1 << 30) || n > 0xffffffffll)
+    {
+        gd_set_error("radix sort of %lld items exceeds 32-bit offsets", (long long)n);
+        return -1;
+    }
+    if (((uintptr_t)k0 & 15) || ((uintptr_t)k1 & 15))
+    {
+        gd_set_error("keys-only radix sort needs 16-byte aligned arrays");
+        return -1;
+    }
+    const int ntiles = (int)tiles64;
+    static int grids[GD_MAX_DEVICES] = {};
+    const int dv = gd_device();
+    if (dv < 0)
+    {
+        gd_set_error("radix sort: no usable current device");
+        return -1;
+    }
+    int& grid = grids[dv];
+    if (!grid)
+    {
+        GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter_pipe<K, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RsPipe<K, false>)));
+        int sms = 0, per = 0;
+        GD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dv));
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rs_scatter_pipe<K, false>, RS_THREADS,
+                                                              sizeof(RsPipe<K, false>)));
+        grid = sms * std::max(per, 1);
+    }
+    int64_t ncnt = (int64_t)ntiles * 256;
+    uint32_t* counts = (uint32_t*)scratch;
+    void* sscr = (void*)(((uintptr_t)(counts + ncnt) + 255) & ~(uintptr_t)255);
+    int cur = 0;
+    for (int b = begin_bit; b < end_bit; b += 8)
+    {
+        K* kin = cur ? k1 : k0;
+        K* kout = cur ? k0 : k1;
+        k_rs_hist<K><<<ntiles, RS_THREADS, 0, s>>>(kin, n, b, counts, ntiles);
+        GD_LAUNCHED(1);
+        if (exclusive_scan<uint32_t>(counts, counts, ncnt, (uint32_t*)nullptr, sscr, s))
+            return -1;
+        k_rs_scatter_pipe<K, false><<<std::min(ntiles, grid), RS_THREADS, sizeof(RsPipe<K, false>), s>>>(
+            kin, nullptr, kout, nullptr, n, b, counts, ntiles);
+        GD_LAUNCHED(1);
+        cur ^= 1;
+    }
+    GD_CUDA(cudaGetLastError());
+    if (radix_sort_wait_check(s))
+        return -1;
+    return cur;
+}
+
+template int radix_sort_keys<uint64_t>(uint64_t*, uint64_t*, int64_t, int, int, void*, cudaStream_t);
 template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, int64_t, int, int, void*,
                                         cudaStream_t);
 template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, int64_t, int, int, void*,

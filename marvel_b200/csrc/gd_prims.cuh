@@ -48,4 +48,8 @@ template <typename K>
 int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int begin_bit, int end_bit, void* scratch,
                      cudaStream_t s);
 
+// The same for keys alone (16-byte aligned k0 and k1).
+template <typename K>
+int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* scratch, cudaStream_t s);
+
 }  // namespace gd
