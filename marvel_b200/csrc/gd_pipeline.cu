@@ -285,8 +285,24 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
     int sort_bits = 8 * ((2 * Kmer + 7) / 8);  // mersort bytes (filter.c:713-716)
     if (sort_bits > (int)(8 * sizeof(K)))
         sort_bits = 8 * sizeof(K);
+    // with packed values the last pass writes the index arrays itself (masked slots, sorted to
+    // the end, included: the arrays hold every slot)
+    const bool fused = pbits >= 0 && nslots > 1;
+    RsFinal fin;
+    if (fused)
+    {
+        if (ensure(sl.code, (nslots + 1) * sizeof(K)) || ensure(sl.read, (nslots + 1) * 4) ||
+            ensure(sl.rpos, (nslots + 1) * 4))
+            return -1;
+        fin.kind = RsFinal::INDEX;
+        fin.a = sl.code.p;
+        fin.b = P<int32_t>(sl.read);
+        fin.c = P<int32_t>(sl.rpos);
+        fin.bits = pbits;
+        fin.kmer = Kmer;
+    }
     int which = radix_sort_pairs<K>(P<K>(c->k0), P<uint32_t>(c->v0), P<K>(c->k1), P<uint32_t>(c->v1), nslots, 0,
-                                    sort_bits, c->scratch.p, s);
+                                    sort_bits, c->scratch.p, s, fused ? &fin : nullptr);
     if (which < 0)
         return -1;
     K* skeys = which ? P<K>(c->k1) : P<K>(c->k0);
@@ -297,7 +313,9 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
     int64_t n = nslots - hmask;
     if (ensure(sl.code, (n + 1) * sizeof(K)) || ensure(sl.read, (n + 1) * 4) || ensure(sl.rpos, (n + 1) * 4))
         return -1;
-    if (pbits >= 0)
+    if (fused)
+        ;  // written by the sort's last pass
+    else if (pbits >= 0)
     {
         if (launch_unpack<K>(skeys, svals, n, pbits, Kmer, P<K>(sl.code), P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
             return -1;
@@ -730,18 +748,34 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     uint32_t *hdiag, *pflags, *ppos;  // pflags / ppos: free ping-pong halves
     if (hb.qbits > 0)
     {
-        // packed hits: keys alone through the passes, the B position riding below the key
-        int which = radix_sort_keys<uint64_t>(P<uint64_t>(c->hk0), P<uint64_t>(c->hk1), nhits, hb.qbits,
-                                              hb.qbits + hbits, c->scratch.p, s);
-        if (which < 0)
-            return -1;
-        uint64_t* packed = which ? P<uint64_t>(c->hk1) : P<uint64_t>(c->hk0);
-        hkey = which ? P<uint64_t>(c->hk0) : P<uint64_t>(c->hk1);
+        // packed hits: keys alone through the passes, the B position riding below the key; the
+        // last pass writes the key and diag arrays (with no pass to run, a separate unpack)
+        const int passes = (hbits + 7) / 8;
+        uint64_t* out = (passes & 1) ? P<uint64_t>(c->hk1) : P<uint64_t>(c->hk0);  // the last pass's target
+        uint64_t* in = (passes & 1) ? P<uint64_t>(c->hk0) : P<uint64_t>(c->hk1);   // and its source
         hdiag = P<uint32_t>(c->hd0);
-        if (launch_hit_unpack(packed, nhits, hb, hkey, hdiag, s))
-            return -1;
+        if (nhits > 1)
+        {
+            RsFinal fin;
+            fin.kind = RsFinal::HITS;
+            fin.a = out;
+            fin.b = (int32_t*)hdiag;
+            fin.bits = hb.qbits;
+            fin.pbits = hb.pbits;
+            if (radix_sort_keys<uint64_t>(P<uint64_t>(c->hk0), P<uint64_t>(c->hk1), nhits, hb.qbits,
+                                          hb.qbits + hbits, c->scratch.p, s, &fin) < 0)
+                return -1;
+            hkey = out;
+            ppos = (uint32_t*)in;
+        }
+        else
+        {
+            hkey = P<uint64_t>(c->hk1);
+            if (launch_hit_unpack(P<uint64_t>(c->hk0), nhits, hb, hkey, hdiag, s))
+                return -1;
+            ppos = (uint32_t*)P<uint64_t>(c->hk0);
+        }
         pflags = P<uint32_t>(c->hd1);
-        ppos = (uint32_t*)packed;
     }
     else
     {

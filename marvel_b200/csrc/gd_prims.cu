@@ -416,10 +416,11 @@ constexpr int rs_pipe_ctas()
 
 // Full tiles (all but possibly the last) arrive by bulk copy; a ragged last tile is read
 // with plain loads.  Requires 16-byte aligned kin and vin.  V = false: keys only.
-template <typename K, bool V = true>
+template <typename K, bool V = true, int F = RsFinal::NONE>
 __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
     k_rs_scatter_pipe(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
-                      uint32_t* __restrict__ vout, int64_t n, int shift, const uint32_t* __restrict__ offs, int ntiles)
+                      uint32_t* __restrict__ vout, int64_t n, int shift, const uint32_t* __restrict__ offs, int ntiles,
+                      RsFinal fin)
 {
     extern __shared__ __align__(128) unsigned char rs_pipe_smem[];
     RsPipe<K, V>& S = *reinterpret_cast<RsPipe<K, V>*>(rs_pipe_smem);
@@ -563,9 +564,26 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
             K k = skey[i];
             unsigned d = (unsigned)(k >> shift) & 255u;
             uint32_t dest = S.toff[d] + (uint32_t)i - S.lstart[d];
-            kout[dest] = k;
-            if constexpr (V)
-                vout[dest] = sval[i];
+            if constexpr (F == RsFinal::INDEX)
+            {
+                const uint32_t v = sval[i];
+                static_cast<K*>(fin.a)[dest] = k;
+                fin.b[dest] = (int32_t)(v >> fin.bits);
+                fin.c[dest] = (int32_t)(v & ((1u << fin.bits) - 1u)) + fin.kmer - 1;
+            }
+            else if constexpr (F == RsFinal::HITS)
+            {
+                const uint64_t hk = (uint64_t)k >> fin.bits;
+                const int bpos = (int)((uint64_t)k & ((1ull << fin.bits) - 1));
+                static_cast<uint64_t*>(fin.a)[dest] = hk;
+                fin.b[dest] = (int32_t)((int)(hk & ((1ull << fin.pbits) - 1)) - bpos);
+            }
+            else
+            {
+                kout[dest] = k;
+                if constexpr (V)
+                    vout[dest] = sval[i];
+            }
         }
         // this stage is refilled by the bulk copy engine two tiles on: order these generic
         // accesses before it
@@ -593,7 +611,7 @@ int radix_sort_wait_check(cudaStream_t s)
 
 template <typename K>
 int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int begin_bit, int end_bit, void* scratch,
-                     cudaStream_t s)
+                     cudaStream_t s, const RsFinal* fin)
 {
     if (n <= 1 || end_bit <= begin_bit)
         return 0;
@@ -618,6 +636,8 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
                                      (int)sizeof(RsTile<K>)));
         GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter_pipe<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(RsPipe<K>)));
+        GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter_pipe<K, true, RsFinal::INDEX>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RsPipe<K>)));
         int dev = 0, sms = 0, per = 0;
         GD_CUDA(cudaGetDevice(&dev));
         GD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -628,6 +648,11 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
     // the bulk copies need 16-byte aligned sources (tile starts are then aligned too)
     const bool pipe = ((uintptr_t)k0 & 15) == 0 && ((uintptr_t)k1 & 15) == 0 && ((uintptr_t)v0 & 15) == 0 &&
                       ((uintptr_t)v1 & 15) == 0;
+    if (fin && (fin->kind != RsFinal::INDEX || !pipe))
+    {
+        gd_set_error("radix sort: this final pass needs the pipelined kernel and an index target");
+        return -1;
+    }
     int64_t ncnt = (int64_t)ntiles * 256;
     uint32_t* counts = (uint32_t*)scratch;
     void* sscr = (void*)(((uintptr_t)(counts + ncnt) + 255) & ~(uintptr_t)255);
@@ -642,9 +667,12 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
         GD_LAUNCHED(1);
         if (exclusive_scan<uint32_t>(counts, counts, ncnt, (uint32_t*)nullptr, sscr, s))
             return -1;
-        if (pipe)
+        if (fin && b + 8 >= end_bit)
+            k_rs_scatter_pipe<K, true, RsFinal::INDEX><<<std::min(ntiles, pipe_grid), RS_THREADS, sizeof(RsPipe<K>),
+                                                         s>>>(kin, vin, kout, vout, n, b, counts, ntiles, *fin);
+        else if (pipe)
             k_rs_scatter_pipe<K><<<std::min(ntiles, pipe_grid), RS_THREADS, sizeof(RsPipe<K>), s>>>(
-                kin, vin, kout, vout, n, b, counts, ntiles);
+                kin, vin, kout, vout, n, b, counts, ntiles, RsFinal{});
         else
             k_rs_scatter<K><<<ntiles, RS_THREADS, sizeof(RsTile<K>), s>>>(kin, vin, kout, vout, n, b, counts, ntiles);
         GD_LAUNCHED(1);
@@ -657,7 +685,8 @@ int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int be
 }
 
 template <typename K>
-int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* scratch, cudaStream_t s)
+int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* scratch, cudaStream_t s,
+                    const RsFinal* fin)
 {
     if (n <= 1 || end_bit <= begin_bit)
         return 0;
@@ -672,6 +701,11 @@ int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* s
         gd_set_error("keys-only radix sort needs 16-byte aligned arrays");
         return -1;
     }
+    if (fin && fin->kind != RsFinal::HITS)
+    {
+        gd_set_error("keys-only radix sort: this final pass needs a hit target");
+        return -1;
+    }
     const int ntiles = (int)tiles64;
     static int grids[GD_MAX_DEVICES] = {};
     const int dv = gd_device();
@@ -684,6 +718,8 @@ int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* s
     if (!grid)
     {
         GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter_pipe<K, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RsPipe<K, false>)));
+        GD_CUDA(cudaFuncSetAttribute((const void*)k_rs_scatter_pipe<K, false, RsFinal::HITS>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RsPipe<K, false>)));
         int sms = 0, per = 0;
         GD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dv));
@@ -703,8 +739,13 @@ int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* s
         GD_LAUNCHED(1);
         if (exclusive_scan<uint32_t>(counts, counts, ncnt, (uint32_t*)nullptr, sscr, s))
             return -1;
-        k_rs_scatter_pipe<K, false><<<std::min(ntiles, grid), RS_THREADS, sizeof(RsPipe<K, false>), s>>>(
-            kin, nullptr, kout, nullptr, n, b, counts, ntiles);
+        if (fin && b + 8 >= end_bit)
+            k_rs_scatter_pipe<K, false, RsFinal::HITS><<<std::min(ntiles, grid), RS_THREADS,
+                                                         sizeof(RsPipe<K, false>), s>>>(kin, nullptr, kout, nullptr,
+                                                                                        n, b, counts, ntiles, *fin);
+        else
+            k_rs_scatter_pipe<K, false><<<std::min(ntiles, grid), RS_THREADS, sizeof(RsPipe<K, false>), s>>>(
+                kin, nullptr, kout, nullptr, n, b, counts, ntiles, RsFinal{});
         GD_LAUNCHED(1);
         cur ^= 1;
     }
@@ -714,10 +755,11 @@ int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* s
     return cur;
 }
 
-template int radix_sort_keys<uint64_t>(uint64_t*, uint64_t*, int64_t, int, int, void*, cudaStream_t);
+template int radix_sort_keys<uint64_t>(uint64_t*, uint64_t*, int64_t, int, int, void*, cudaStream_t,
+                                       const RsFinal*);
 template int radix_sort_pairs<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint32_t*, int64_t, int, int, void*,
-                                        cudaStream_t);
+                                        cudaStream_t, const RsFinal*);
 template int radix_sort_pairs<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, int64_t, int, int, void*,
-                                        cudaStream_t);
+                                        cudaStream_t, const RsFinal*);
 
 }  // namespace gd

@@ -34,6 +34,25 @@ inline size_t scan_scratch_bytes(int64_t n)
 template <typename T>
 int exclusive_scan(const T* in, T* out, int64_t n, T* total, void* scratch, cudaStream_t s);
 
+// What the last pass of a radix sort writes instead of the sorted arrays:
+//   INDEX: the k-mer index from (code, packed value = read << bits | first position):
+//          code[], read[] = v >> bits, rpos[] = (v & mask) + kmer - 1
+//   HITS:  the hit list from keys-only packed hits (key << bits | bpos): hkey[] = k >> bits,
+//          hdiag[] = apos - bpos with apos = hkey & ((1 << pbits) - 1)
+struct RsFinal
+{
+    enum Kind
+    {
+        NONE = 0,
+        INDEX = 1,
+        HITS = 2
+    } kind = NONE;
+    void* a = nullptr;       // code[] / hkey[]
+    int32_t* b = nullptr;    // read[] / hdiag[]
+    int32_t* c = nullptr;    // rpos[]
+    int bits = 0, pbits = 0, kmer = 0;
+};
+
 // Bytes of scratch a radix sort of n items needs (tile histograms + their scan).
 inline size_t radix_scratch_bytes(int64_t n)
 {
@@ -44,12 +63,15 @@ inline size_t radix_scratch_bytes(int64_t n)
 
 // Stable sort of (key, val) pairs by key bits [begin_bit, end_bit).  Ping-pongs between
 // (k0,v0) and (k1,v1); returns 0 if the result is in (k0,v0), 1 if in (k1,v1), -1 on error.
+// fin (optional): the last pass writes fin's arrays instead (the return value then only
+// says where the sorted pairs would have been; with fewer than 2 items nothing is written).
 template <typename K>
 int radix_sort_pairs(K* k0, uint32_t* v0, K* k1, uint32_t* v1, int64_t n, int begin_bit, int end_bit, void* scratch,
-                     cudaStream_t s);
+                     cudaStream_t s, const RsFinal* fin = nullptr);
 
 // The same for keys alone (16-byte aligned k0 and k1).
 template <typename K>
-int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* scratch, cudaStream_t s);
+int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* scratch, cudaStream_t s,
+                    const RsFinal* fin = nullptr);
 
 }  // namespace gd
