@@ -314,7 +314,9 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
     if (ensure(sl.code, (n + 1) * sizeof(K)) || ensure(sl.read, (n + 1) * 4) || ensure(sl.rpos, (n + 1) * 4))
         return -1;
     if (fused)
-        ;  // written by the sort's last pass
+    {
+        // the sort's last pass wrote the index arrays
+    }
     else if (pbits >= 0)
     {
         if (launch_unpack<K>(skeys, svals, n, pbits, Kmer, P<K>(sl.code), P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
