@@ -98,6 +98,15 @@ int64_t gd_get_kmers(gd_context* ctx, int slot, uint64_t* code, int32_t* read, i
  * Appends the overlaps it finds to the context's overlap buffer. */
 int gd_match_filter(gd_context* ctx, int bslot, int comp, int self);
 
+/* daligner's -b (BIASED, dalign/daligner.c:61,681-683): gd_sort_kmers then builds the
+ * frequency-weighted index of biased_tuple_thread (dalign/filter.c:492-633): per read a window
+ * of at most k bases, grown until its information (sum of ceil(-10000 log4 freq[base]))
+ * reaches 10000 k, kept when above 10000 (k - 2), coded with its bases at the top of the k-mer
+ * code.  The weights come from the frequencies of gd_new_align_spec (daligner gives the A
+ * block's, which is also the first block it indexes); they must lie in (0, 1].  Not
+ * available with variant 2.  Changing the flag drops the slots' indices. */
+int gd_set_biased(gd_context* ctx, int biased);
+
 /* daligner2 mode (the reference's dalign2/, modimizer seeds).  variant 1 = daligner (the
  * default), 2 = daligner2; hgap = daligner2's -H (HGAP_MIN, dalign2/daligner.c:29,570: pairs
  * whose reads are both shorter are skipped, shorter reads get no record of their own).

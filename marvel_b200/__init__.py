@@ -61,7 +61,8 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_timer_elapsed_ms", "gd_kernel_launches", "gd_local_alignment_batch_noalloc",
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
            "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge",
-           "gd_set_wave_limit", "gd_set_variant", "gd_match_filter2", "gd_test_handle_redundancies_d2"]
+           "gd_set_wave_limit", "gd_set_variant", "gd_match_filter2", "gd_test_handle_redundancies_d2",
+           "gd_set_biased"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -83,6 +84,7 @@ def lib():
     L.gd_set_globals.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64]
     L.gd_load_block.argtypes = [C.c_void_p, C.c_int, C.POINTER(GdBlock)]
     L.gd_set_variant.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.gd_set_biased.argtypes = [C.c_void_p, C.c_int]
     L.gd_match_filter2.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.gd_sort_kmers.argtypes = [C.c_void_p, C.c_int]
     L.gd_sort_kmers.restype = C.c_int64
@@ -237,6 +239,10 @@ class Context:
         rpos = np.zeros(max(n, 1), np.int32)
         k = _check(lib().gd_get_kmers(self.h, slot, code.ctypes.data, read.ctypes.data, rpos.ctypes.data, n))
         return code[:k], read[:k], rpos[:k]
+
+    def set_biased(self, biased=True):
+        """daligner's -b: frequency-weighted tuples in the index (weights from new_align_spec's freq)."""
+        _check(lib().gd_set_biased(self.h, int(bool(biased))))
 
     def set_variant(self, variant, hgap=0):
         """1 = daligner (default), 2 = daligner2 (modimizer seeds; hgap = its -H)."""

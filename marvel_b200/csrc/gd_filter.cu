@@ -5,6 +5,7 @@
 // over HBM-resident arrays: one thread per k-mer slot for extraction, one thread per index
 // entry for the join, with binary searches replacing the reference's merge cursors.
 #include "gd_filter.cuh"
+#include "gd_prims.cuh"
 
 namespace gd
 {
@@ -169,6 +170,228 @@ int launch_decode(const DevBlock& b, int kmer, const uint32_t* slots, int64_t n,
     if (n <= 0)
         return 0;
     k_decode<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(b, kmer, slots, n, read, rpos);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// ---- -b: frequency-weighted tuples ---------------------------------------------------
+
+constexpr int BT = 128;
+
+// The bases of one read, read forward through a cached aligned 8-byte word (the block
+// buffer has slack on both sides, so the word around any base is in bounds).
+struct BaseStream
+{
+    const uint8_t* s;
+    uintptr_t word;
+    uint64_t w;
+    __device__ __forceinline__ int at(int p)
+    {
+        const uintptr_t a = (uintptr_t)(s + p);
+        if ((a >> 3) != word)
+        {
+            word = a >> 3;
+            w = __ldg(reinterpret_cast<const unsigned long long*>(a & ~(uintptr_t)7));
+        }
+        return (int)(w >> (8 * (a & 7))) & 0xff;
+    }
+};
+
+// One scan of bases [p, q) of a read: the loop of biased_tuple_thread (dalign/filter.c:536-570
+// over a mask track's unmasked segment, :583-612 over a whole read), left at the first
+// iteration that starts at or after pend.  The window s[p-k+1..p] is the low 2k bits of c, so
+// the trim and the slide take the leaving base from c.  When growing runs into q the
+// untracked scan stops, the tracked one still tests the window (now s[q-k..q-1]) and keeps it
+// at position q; its trim is skipped there, as it cannot remove a base from a window below
+// norm when every weight is >= 0.
+template <typename F>
+__device__ __forceinline__ void bias_scan(BaseStream& bs, int p, int q, int pend, bool tracked, const BiasParams& bp,
+                                          uint64_t kmask, F&& keep)
+{
+    uint64_t c = 0;
+    int a = 0, k = 1;
+    while (p < q && p < pend)
+    {
+        int x = bs.at(p);
+        a += bp.w[x];
+        c = (c << 2) | (uint64_t)x;
+        bool cut = false;
+        while (a < bp.norm && k < bp.kmer)
+        {
+            if (++p >= q)
+            {
+                cut = true;
+                break;
+            }
+            k += 1;
+            x = bs.at(p);
+            a += bp.w[x];
+            c = (c << 2) | (uint64_t)x;
+        }
+        if (cut && !tracked)
+            return;
+        if (!cut)
+            while (true)
+            {
+                const int u = a - bp.w[(int)(c >> (2 * (k - 1))) & 3];
+                if (u < bp.norm)
+                    break;
+                a = u;
+                k -= 1;
+            }
+        if (a > bp.thresh)
+            keep(p, (c << (2 * (bp.kmer - k))) & kmask);
+        a -= bp.w[(int)(c >> (2 * (k - 1))) & 3];
+        p += 1;
+    }
+}
+
+// Chunks: chunk t of read r keeps the tuples at positions [t*BCHUNK, (t+1)*BCHUNK); a read has
+// rlen / BCHUNK + 1 of them (a tracked tuple can sit at rlen).
+//
+// A chunk's thread starts its scan of a segment that began before c0 - 3K afresh at
+// x = c0 - 3K (k = 1, nothing summed), and the tuples it keeps from c0 on are the reference's.
+// With weights >= 0, the window length at any kept-or-tested position p >= x + K - 1 is
+// min(K, shortest suffix ending at p that reaches norm), the same in both scans, and from a
+// position both scans test they go on alike.  A scan tests a position at least every K bases
+// (growing stops at length K).  Let p1 <= x + 2K - 2 be the fresh scan's first tested position
+// at or after x + K - 1.  If the true scan skips p1, it is growing a window [L, .] that is below
+// norm and shorter than K there; the fresh scan's window then always starts left of L (a
+// shortest suffix reaching norm, or K bases), so when the true scan next tests a position
+// r <= p1 + K - 1 -- its window reached norm, or K bases -- the fresh window ending at r
+// contains it and is tested too.  Both scans test r <= x + 3K - 3 < c0 with the same window.
+constexpr int BCHUNK = 512;
+
+__global__ void __launch_bounds__(BT) k_bias_nchunks(DevBlock b, uint32_t* nch)
+{
+    const int r = blockIdx.x * BT + threadIdx.x;
+    if (r < b.nreads)
+        nch[r] = (uint32_t)(b.rlen[r] / BCHUNK + 1);
+}
+
+// EMIT: count[] holds the chunks' output offsets
+template <typename K, bool EMIT>
+__global__ void __launch_bounds__(BT) k_bias(DevBlock b, const int64_t* __restrict__ mask_anno,
+                                            const int32_t* __restrict__ mask_data, BiasParams bp,
+                                            const uint32_t* __restrict__ cfirst, uint32_t nchunks,
+                                            uint32_t* __restrict__ count, K* __restrict__ keys,
+                                            uint32_t* __restrict__ vals, int32_t* __restrict__ eread,
+                                            int32_t* __restrict__ erpos, int pbits)
+{
+    const uint32_t i = blockIdx.x * BT + threadIdx.x;
+    if (i >= nchunks)
+        return;
+    int lo = 0, hi = b.nreads - 1;  // the read: largest r with cfirst[r] <= i
+    while (lo < hi)
+    {
+        const int md = (lo + hi + 1) >> 1;
+        if (cfirst[md] <= i)
+            lo = md;
+        else
+            hi = md - 1;
+    }
+    const int r = lo;
+    const int c0 = (int)(i - cfirst[r]) * BCHUNK, c1 = c0 + BCHUNK;
+    const int back = 3 * bp.kmer;
+    BaseStream bs{b.bases + b.boff[r], ~(uintptr_t)0, 0};
+    const int rlen = b.rlen[r];
+    const uint64_t kmask = bp.kmer >= 32 ? ~0ull : (1ull << (2 * bp.kmer)) - 1;
+    uint32_t n = EMIT ? count[i] : 0;
+    auto keep = [&](int p, uint64_t code) {
+        if (p < c0 || p >= c1)
+            return;
+        if constexpr (EMIT)
+        {
+            keys[n] = (K)code;
+            if (pbits >= 0)
+                vals[n] = ((uint32_t)r << pbits) | (uint32_t)p;
+            else
+            {
+                vals[n] = n;
+                eread[n] = r;
+                erpos[n] = p;
+            }
+        }
+        n += 1;
+    };
+    if (!mask_anno)
+    {
+        if (c0 < rlen)
+            bias_scan(bs, max(0, c0 - back), rlen, c1, false, bp, kmask, keep);
+    }
+    else
+    {
+        const int64_t f0 = mask_anno[r], f1 = mask_anno[r + 1];
+        for (int64_t j = f0; j <= f1; j += 2)
+        {
+            const int p = j == f0 ? 0 : mask_data[j - 1];
+            if (p >= c1)
+                break;
+            const int q = j == f1 ? rlen : mask_data[j];
+            if (p + bp.kmer <= q && q >= c0)
+                bias_scan(bs, max(p, c0 - back), q, c1, true, bp, kmask, keep);
+        }
+    }
+    if constexpr (!EMIT)
+        count[i] = n;
+}
+
+int bias_chunks(const DevBlock& b, uint32_t* cfirst, uint32_t* total, void* scratch, cudaStream_t s)
+{
+    if (b.nreads <= 0)
+        return 0;
+    k_bias_nchunks<<<gd_cdiv(b.nreads, BT), BT, 0, s>>>(b, cfirst);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return exclusive_scan<uint32_t>(cfirst, cfirst, b.nreads, total, scratch, s);
+}
+
+int launch_bias_count(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, const BiasParams& bp,
+                      const uint32_t* cfirst, uint32_t nchunks, uint32_t* count, cudaStream_t s)
+{
+    if (nchunks == 0)
+        return 0;
+    k_bias<uint32_t, false><<<gd_cdiv(nchunks, (uint32_t)BT), BT, 0, s>>>(b, mask_anno, mask_data, bp, cfirst, nchunks,
+                                                                          count, nullptr, nullptr, nullptr, nullptr, 0);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename K>
+int launch_bias_emit(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, const BiasParams& bp,
+                     const uint32_t* cfirst, uint32_t nchunks, const uint32_t* offs, K* keys, uint32_t* vals,
+                     int32_t* eread, int32_t* erpos, int pbits, cudaStream_t s)
+{
+    if (nchunks == 0)
+        return 0;
+    k_bias<K, true><<<gd_cdiv(nchunks, (uint32_t)BT), BT, 0, s>>>(b, mask_anno, mask_data, bp, cfirst, nchunks,
+                                                                  const_cast<uint32_t*>(offs), keys, vals, eread, erpos,
+                                                                  pbits);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+__global__ void __launch_bounds__(FT) k_gather_read_pos(const uint32_t* __restrict__ idx, int64_t n,
+                                                       const int32_t* __restrict__ eread,
+                                                       const int32_t* __restrict__ erpos, int32_t* read, int32_t* rpos)
+{
+    const int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t j = idx[i];
+    read[i] = eread[j];
+    rpos[i] = erpos[j];
+}
+
+int launch_gather_read_pos(const uint32_t* idx, int64_t n, const int32_t* eread, const int32_t* erpos, int32_t* read,
+                           int32_t* rpos, cudaStream_t s)
+{
+    if (n <= 0)
+        return 0;
+    k_gather_read_pos<<<(unsigned)gd_cdiv<int64_t>(n, FT), FT, 0, s>>>(idx, n, eread, erpos, read, rpos);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
@@ -676,6 +899,9 @@ int launch_complement(const DevBlock& src, uint8_t* dst_bases, const int64_t* an
                                   cudaStream_t);                                                                 \
     template int launch_decode<K>(const DevBlock&, int, const uint32_t*, int64_t, int32_t*, int32_t*,            \
                                   cudaStream_t);                                                                 \
+    template int launch_bias_emit<K>(const DevBlock&, const int64_t*, const int32_t*, const BiasParams&,         \
+                                     const uint32_t*, uint32_t, const uint32_t*, K*, uint32_t*, int32_t*,        \
+                                     int32_t*, int, cudaStream_t);                                               \
     template int launch_suppress_flags<K>(const K*, int64_t, int, uint32_t*, cudaStream_t);                      \
     template int launch_compact_index<K>(const K*, const int32_t*, const int32_t*, const uint32_t*,              \
                                          const uint32_t*, int64_t, K*, int32_t*, int32_t*, cudaStream_t);        \

@@ -25,6 +25,37 @@ template <typename K>
 int launch_decode(const DevBlock& b, int kmer, const uint32_t* slots, int64_t n, int32_t* read, int32_t* rpos,
                   cudaStream_t s);
 
+// daligner -b (biased_tuple_thread, dalign/filter.c:492-633, tables :718-733): per read, a
+// window of k <= K bases whose information (sum of w[base]) is grown to reach norm, trimmed
+// from the left while it stays at norm, kept when above thresh, then slid one base.
+struct BiasParams
+{
+    int w[4];    // ceil(-10000 log4 freq[base]), all >= 0
+    int norm;    // 10000 K
+    int thresh;  // 10000 (K - MAX_BIAS), MAX_BIAS = 2
+    int kmer;
+};
+
+// The scan works in chunks of positions (one thread each): cfirst[r] = the read's first chunk
+// (exclusive scan over the reads; *total = the number of chunks).
+int bias_chunks(const DevBlock& b, uint32_t* cfirst, uint32_t* total, void* scratch, cudaStream_t s);
+
+// Tuples each chunk keeps (count[chunk]).
+int launch_bias_count(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, const BiasParams& bp,
+                      const uint32_t* cfirst, uint32_t nchunks, uint32_t* count, cudaStream_t s);
+
+// The kept tuples at offs[chunk] (exclusive offsets), in (read, position) order: keys = K-mer
+// codes (the window's k bases at the top), vals = read << pbits | position with pbits >= 0,
+// else the entry index with (read, position) in eread/erpos.
+template <typename K>
+int launch_bias_emit(const DevBlock& b, const int64_t* mask_anno, const int32_t* mask_data, const BiasParams& bp,
+                     const uint32_t* cfirst, uint32_t nchunks, const uint32_t* offs, K* keys, uint32_t* vals,
+                     int32_t* eread, int32_t* erpos, int pbits, cudaStream_t s);
+
+// read[i] = eread[idx[i]], rpos[i] = erpos[idx[i]]
+int launch_gather_read_pos(const uint32_t* idx, int64_t n, const int32_t* eread, const int32_t* erpos, int32_t* read,
+                           int32_t* rpos, cudaStream_t s);
+
 // Keep flags for -t suppression: 1 where the entry's code run is shorter than t.
 template <typename K>
 int launch_suppress_flags(const K* code, int64_t n, int t, uint32_t* keep, cudaStream_t s);

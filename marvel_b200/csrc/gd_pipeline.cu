@@ -182,6 +182,9 @@ struct gd_context
     int agrid_w = 0;
     int test_narrow = 0;  // tests only: the main aligner pass with the 32-diagonal instance
     int variant = 1, hgap = 0;  // 2 = daligner2 (modimizer seeds, dalign2/), its -H
+    int biased = 0;             // daligner -b: frequency-weighted tuples
+    // -b: the reads' first chunks, tuples per chunk (then offsets), unpacked (read, position)
+    DevBuf bchunk, bcount, brp;
     DevBuf d2rd, d2rp, d2sgn, cnt2, hoff2, hk2, hd2, runstart, btable;
     int pcap = 32768, mcap = 1024, tcap = 1 << 17;
     int bvcap = 8192, btcap = 1024;  // daligner2 bridging scratch per warp (ints, trace values)
@@ -335,6 +338,123 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
     return n;
 }
 
+// -b weights from the frequencies of the align spec (Sort_Kmers, dalign/filter.c:718-733: the
+// reference takes them once, from the first block it indexes, daligner's A block, whose
+// frequencies are the ones New_Align_Spec gets).  The table is made on the host with the
+// reference's own double expression.
+static int bias_params(const gd_context* c, gd::BiasParams& bp)
+{
+    const double scale = -10000. / ::log(4.);
+    for (int i = 0; i < 4; i++)
+    {
+        if (!(c->freq[i] > 0.f && c->freq[i] <= 1.f))
+        {
+            gd_set_error("-b needs base frequencies in (0, 1], got %g for base %d", (double)c->freq[i], i);
+            return -1;
+        }
+        bp.w[i] = (int)::ceil(scale * ::log((double)c->freq[i]));  // the float widened, as in C
+    }
+    bp.norm = 10000 * c->kmer;
+    bp.thresh = 10000 * (c->kmer - 2);
+    bp.kmer = c->kmer;
+    return 0;
+}
+
+// Sort_Kmers with -b: the reads cut into chunks of positions, one scan per chunk counts its
+// tuples, a scan of the counts places them, a second scan writes them; then the sort and -t as
+// for the plain index.  Entries come out in (read, position) order before the sort, as the
+// reference's threads list them.
+template <typename K>
+static int64_t index_slot_bias_t(gd_context* c, Slot& sl)
+{
+    using namespace gd;
+    const int Kmer = c->kmer;
+    const int nr = sl.blk.nreads;
+    cudaStream_t s = c->s;
+    sl.nk = 0;
+    if (nr <= 0)
+        return 0;
+    BiasParams bp;
+    if (bias_params(c, bp))
+        return -1;
+    const int64_t* manno = sl.has_mask ? P<int64_t>(sl.manno) : nullptr;
+    const int32_t* mdata = sl.has_mask ? P<int32_t>(sl.mdata) : nullptr;
+    if (ensure(c->bchunk, (nr + 1) * 4) || ensure(c->misc, 64) ||
+        ensure(c->scratch, scan_scratch_bytes<uint32_t>(nr)))
+        return -1;
+    uint32_t* cfirst = P<uint32_t>(c->bchunk);
+    uint32_t* total = P<uint32_t>(c->misc);
+    uint32_t hn = 0;
+    if (bias_chunks(sl.blk, cfirst, total, c->scratch.p, s))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(&hn, total, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    const uint32_t nchunks = hn;
+    if (ensure(c->bcount, ((int64_t)nchunks + 1) * 4) || ensure(c->scratch, scan_scratch_bytes<uint32_t>(nchunks)))
+        return -1;
+    uint32_t* count = P<uint32_t>(c->bcount);
+    if (launch_bias_count(sl.blk, manno, mdata, bp, cfirst, nchunks, count, s) ||
+        exclusive_scan<uint32_t>(count, count, nchunks, total, c->scratch.p, s))
+        return -1;
+    GD_CUDA(cudaMemcpyAsync(&hn, total, 4, cudaMemcpyDeviceToHost, s));
+    GD_CUDA(cudaStreamSynchronize(s));
+    int64_t n = hn;
+    if (n == 0)
+        return 0;
+    // positions run to maxlen (a tracked tuple can sit at rlen)
+    const int pb = bits_for(std::max(sl.blk.maxlen, 1));
+    const int pbits = (bits_for(std::max(nr - 1, 1)) + pb <= 32) ? pb : -1;
+    if (ensure(c->k0, n * sizeof(K)) || ensure(c->k1, n * 8) || ensure(c->v0, n * 4) || ensure(c->v1, n * 4) ||
+        ensure(c->scratch, radix_scratch_bytes(n)) || ensure(sl.code, (n + 1) * sizeof(K)) ||
+        ensure(sl.read, (n + 1) * 4) || ensure(sl.rpos, (n + 1) * 4) || (pbits < 0 && ensure(c->brp, n * 8)))
+        return -1;
+    int32_t* eread = pbits < 0 ? P<int32_t>(c->brp) : nullptr;
+    int32_t* erpos = pbits < 0 ? eread + n : nullptr;
+    if (launch_bias_emit<K>(sl.blk, manno, mdata, bp, cfirst, nchunks, count, P<K>(c->k0), P<uint32_t>(c->v0), eread,
+                            erpos, pbits, s))
+        return -1;
+    int sort_bits = 8 * ((2 * Kmer + 7) / 8);  // mersort bytes (filter.c:713-716)
+    if (sort_bits > (int)(8 * sizeof(K)))
+        sort_bits = 8 * sizeof(K);
+    const bool fused = pbits >= 0 && n > 1;
+    RsFinal fin;
+    if (fused)
+    {
+        fin.kind = RsFinal::INDEX;
+        fin.a = sl.code.p;
+        fin.b = P<int32_t>(sl.read);
+        fin.c = P<int32_t>(sl.rpos);
+        fin.bits = pbits;
+        fin.kmer = 1;  // the value holds the position itself
+    }
+    int which = radix_sort_pairs<K>(P<K>(c->k0), P<uint32_t>(c->v0), P<K>(c->k1), P<uint32_t>(c->v1), n, 0,
+                                    sort_bits, c->scratch.p, s, fused ? &fin : nullptr);
+    if (which < 0)
+        return -1;
+    K* skeys = which ? P<K>(c->k1) : P<K>(c->k0);
+    uint32_t* svals = which ? P<uint32_t>(c->v1) : P<uint32_t>(c->v0);
+    if (fused)
+    {
+        // the sort's last pass wrote the index arrays
+    }
+    else if (pbits >= 0)
+    {
+        if (launch_unpack<K>(skeys, svals, n, pbits, 1, P<K>(sl.code), P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
+            return -1;
+    }
+    else
+    {
+        GD_CUDA(cudaMemcpyAsync(sl.code.p, skeys, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+        if (launch_gather_read_pos(svals, n, eread, erpos, P<int32_t>(sl.read), P<int32_t>(sl.rpos), s))
+            return -1;
+    }
+    if (suppress_index<K>(c, sl, n))
+        return -1;
+    GD_CUDA(cudaStreamSynchronize(s));
+    sl.nk = n;
+    return n;
+}
+
 // -t: drop codes occurring >= t times (compsize/compress_thread, filter.c:645-696 and
 // dalign2/filter.c:771-832); k0, k1 (2n int32), v0 and v1 hold at least n entries
 template <typename K>
@@ -448,10 +568,17 @@ static int tri_append(gd_context* c, unsigned ng)
 
 static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBits hb, int comp, int self);
 
-// bits of the B position when (bread, aread, apos, bpos) fits one 64-bit word, else 0
-static int hit_qbits(const gd::HitBits& hb, const Slot& B)
+// bits of a tuple position in a block: at most maxlen - 1, or maxlen with -b (a tuple that
+// growing pushed to the end of an unmasked segment, dalign/filter.c:545-551)
+static int pos_bits(const gd_context* c, const Slot& S)
 {
-    const int q = bits_for(std::max(B.blk.maxlen - 1, 1));
+    return bits_for(std::max(S.blk.maxlen - (c->biased ? 0 : 1), 1));
+}
+
+// bits of the B position when (bread, aread, apos, bpos) fits one 64-bit word, else 0
+static int hit_qbits(const gd_context* c, const gd::HitBits& hb, const Slot& B)
+{
+    const int q = pos_bits(c, B);
     return hb.pbits + hb.abits + hb.bbits + q <= 64 ? q : 0;
 }
 static int pair_cap(gd_context* c, int64_t na, int64_t nb, int same_index, int* limit_out);
@@ -587,7 +714,7 @@ static int match_emit_t(gd_context* c, Slot& A, Slot& B, int64_t na, uint64_t* d
         return -1;
     }
     HitBits hb;
-    hb.pbits = bits_for(std::max(A.blk.maxlen - 1, 1));
+    hb.pbits = pos_bits(c, A);
     hb.abits = bits_for(std::max(A.blk.nreads - 1, 1));
     hb.bbits = bits_for(std::max(B.blk.nreads - 1, 1));
     int hbits = hb.pbits + hb.abits + hb.bbits;
@@ -596,7 +723,7 @@ static int match_emit_t(gd_context* c, Slot& A, Slot& B, int64_t na, uint64_t* d
         gd_set_error("hit key needs %d bits (> 64): block too large for this build", hbits);
         return -1;
     }
-    hb.qbits = hit_qbits(hb, B);
+    hb.qbits = hit_qbits(c, hb, B);
     if (ensure(c->hk0, nhits * 8) || ensure(c->hk1, nhits * 8) || ensure(c->hd0, nhits * 4) ||
         ensure(c->hd1, nhits * 4) || ensure(c->scratch, radix_scratch_bytes(nhits)))
         return -1;
@@ -712,7 +839,7 @@ static int match_filter_d2_t(gd_context* c, int bslot, int cslot, int self)
         gd_set_error("hit key needs %d bits (> 64): block too large for this build", hb.pbits + hb.abits + hb.bbits);
         return -1;
     }
-    hb.qbits = hit_qbits(hb, B);
+    hb.qbits = hit_qbits(c, hb, B);
     if (ensure(c->hk0, nmax * 8 + 8) || ensure(c->hk1, nmax * 8 + 8) || ensure(c->hd0, nmax * 4 + 4) ||
         ensure(c->hd1, nmax * 4 + 4) || ensure(c->hk2, nc * 8 + 8) || ensure(c->hd2, nc * 4 + 4) ||
         ensure(c->scratch, radix_scratch_bytes(nmax)))
@@ -1417,6 +1544,9 @@ int64_t gd_sort_kmers(gd_context* c, int slot)
     int64_t n;
     if (c->variant == 2)
         n = c->kmer <= 15 ? index_slot_d2_t<uint32_t>(c, c->slot[slot]) : index_slot_d2_t<uint64_t>(c, c->slot[slot]);
+    else if (c->biased)
+        n = c->kmer <= 15 ? index_slot_bias_t<uint32_t>(c, c->slot[slot])
+                          : index_slot_bias_t<uint64_t>(c, c->slot[slot]);
     else
         n = c->kmer <= 15 ? index_slot_t<uint32_t>(c, c->slot[slot]) : index_slot_t<uint64_t>(c, c->slot[slot]);
     GD_CUDA(cudaEventRecord(c->ev1, c->s));
@@ -1472,11 +1602,29 @@ int gd_match_filter(gd_context* c, int bslot, int comp, int self)
                          : match_filter_t<uint64_t>(c, bslot, comp, self);
 }
 
+int gd_set_biased(gd_context* c, int biased)
+{
+    if (biased && c->variant == 2)
+    {
+        gd_set_error("daligner2 has no -b (biased tuples)");
+        return -1;
+    }
+    c->biased = biased != 0;
+    for (int i = 0; i < 3; i++)
+        c->slot[i].nk = -1;  // an index of the other kind must be rebuilt
+    return 0;
+}
+
 int gd_set_variant(gd_context* c, int variant, int hgap)
 {
     if (variant != 1 && variant != 2)
     {
         gd_set_error("variant must be 1 (daligner) or 2 (daligner2), got %d", variant);
+        return -1;
+    }
+    if (variant == 2 && c->biased)
+    {
+        gd_set_error("daligner2 has no -b (biased tuples)");
         return -1;
     }
     c->variant = variant;

@@ -2,8 +2,8 @@
  *
  * Same options, defaults, validation, output directories and .las names as MARVEL's
  * daligner (dalign/daligner.c:27-58, 615-1029); the filter and aligner run on the GPU
- * through include/gpudalign.h.  Not supported: -b (biased k-mer sampling) and -D (dynamic
- * mask server); both are rejected with a message.  -j is validated and otherwise unused.
+ * through include/gpudalign.h.  Not supported: -D (dynamic mask server), rejected with a
+ * message.  -j is validated and otherwise unused.
  */
 #include <errno.h>
 #include <getopt.h>
@@ -20,7 +20,7 @@
 static void usage(void)
 {
     fprintf(stderr, "usage:  \n");
-    fprintf(stderr, "daligner [-vAIOT] [-k<int(14)>] [-w<int(6)>] [-h<int(35)>] [-t<int>] [-M<int>]\n");
+    fprintf(stderr, "daligner [-vbAIOT] [-k<int(14)>] [-w<int(6)>] [-h<int(35)>] [-t<int>] [-M<int>]\n");
     fprintf(stderr, "         [-e<double(.70)] [-l<int(1000)>] [-s<int(100)>] [-H<int>] [-j<int>]\n");
     fprintf(stderr, "         [-m<track>]+ <subject:db|dam> <target:db|dam> ...\n");
     fprintf(stderr, "         [-r<int()1>]\n");
@@ -117,7 +117,7 @@ static void load(dz_block* b, const char* name, char** mask, int mtop, int kmer)
 
 int main(int argc, char* argv[])
 {
-    int VERBOSE = 0, SYMMETRIC = 1, IDENTITY = 0, ONLY_IDENTITY = 0, NO_TRACE_POINTS = 0;
+    int VERBOSE = 0, SYMMETRIC = 1, IDENTITY = 0, ONLY_IDENTITY = 0, NO_TRACE_POINTS = 0, BIASED = 0;
     int KMER_LEN = 14, HIT_MIN = 35, BIN_SHIFT = 6, MAX_REPS = 0, HGAP_MIN = 0, SPACING = 100, RUN_ID = 1;
     int MINOVER = 1000;
     double AVE_ERROR = .70;
@@ -132,9 +132,7 @@ int main(int argc, char* argv[])
         switch (c)
         {
         case 'v': VERBOSE = 1; break;
-        case 'b':
-            fprintf(stderr, "daligner: -b (biased k-mer sampling) is not supported by the GPU path\n");
-            exit(1);
+        case 'b': BIASED = 1; break;
         case 'T': NO_TRACE_POINTS = 1; break;
         case 'I': IDENTITY = 1; break;
         case 'O': IDENTITY = 1; ONLY_IDENTITY = 1; break;
@@ -223,6 +221,7 @@ int main(int argc, char* argv[])
     }
     GPU(gd_set_filter_params(ctx, KMER_LEN, BIN_SHIFT, MAX_REPS, HIT_MIN));
     GPU(gd_set_globals(ctx, MINOVER, IDENTITY, (uint64_t)MEM_LIMIT));
+    GPU(gd_set_biased(ctx, BIASED));
 
     const char* afile = argv[optind];
     dz_block A, B;

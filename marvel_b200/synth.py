@@ -31,6 +31,8 @@ class GenomeModel:
     tandem_period: tuple = (2, 201)
     diploid_snp: float = 0.0
     diploid_indel: float = 0.0
+    # background base probabilities (A, C, G, T); empty = uniform
+    base_probs: tuple = ()
 
 
 @dataclasses.dataclass(frozen=True)
@@ -92,7 +94,10 @@ def _mutate_indels(rng, seq, rate):
 
 def make_genome(model: GenomeModel, rng: np.random.Generator):
     """Returns a list of haplotype arrays (uint8 0..3)."""
-    g = rng.integers(0, 4, model.length, dtype=np.uint8)
+    if model.base_probs:
+        g = rng.choice(4, size=model.length, p=np.asarray(model.base_probs, float)).astype(np.uint8)
+    else:
+        g = rng.integers(0, 4, model.length, dtype=np.uint8)
     n = model.length
     # fixed repeat families: copies of one unit at a given divergence
     for copies, unit, div in model.repeats:
@@ -208,6 +213,19 @@ WORKLOADS = {
                      ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=11),
     "tiny_tandem": Workload("tiny_tandem", GenomeModel(80_000, tandem_frac=0.10, tandem_period=(2, 7)),
                             ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=13),
+    # AT-rich (A, T at 32 %): the frequency weights of daligner -b differ per base
+    "tiny_at": Workload("tiny_at", GenomeModel(60_000, base_probs=(0.32, 0.18, 0.18, 0.32)),
+                        ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=15),
+    "tiny_at_tandem": Workload("tiny_at_tandem",
+                               GenomeModel(80_000, tandem_frac=0.10, tandem_period=(2, 7),
+                                           base_probs=(0.32, 0.18, 0.18, 0.32)),
+                               ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=16),
+    # strongly skewed (A, T at 40 %) with 20 % tandem repeats: many short weighted windows and
+    # many unmasked segments
+    "tiny_skew_tandem": Workload("tiny_skew_tandem",
+                                 GenomeModel(80_000, tandem_frac=0.20, tandem_period=(2, 7),
+                                             base_probs=(0.40, 0.10, 0.10, 0.40)),
+                                 ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=17),
     "small": Workload("small", GenomeModel(200_000, repeats=((6, 3000, 0.015),)),
                       ReadModel(15, 6000, 3000, 1000, 20000, **PACBIO), seed=12),
     # reads of 30-150 kbp: a-positions beyond the 50,000-bp panels of the seed scan

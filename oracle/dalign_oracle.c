@@ -7,6 +7,7 @@
 #include "dalign_oracle.h"
 
 #include <limits.h>
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -89,12 +90,121 @@ static int64_t extract_kmers(const or_block* b, int K, KPos* list)
     return n;
 }
 
+/* daligner -b: frequency-weighted tuples (biased_tuple_thread, filter.c:492-633, with the
+ * tables of Sort_Kmers, filter.c:718-733).  A base x carries the information
+ * w[x] = ceil(-10000 log4 freq[x]); a window of k <= K bases is grown to the right while its
+ * information is below 10000 K (and k < K), trimmed from the left while what remains still
+ * reaches 10000 K, and kept when its information exceeds 10000 (K - 2), as a K-mer code with
+ * its k bases at the top and zeros below.  The window then slides one base (same length).
+ * The tables are made once, from the frequencies of the first block indexed: daligner's A
+ * block, whose frequencies are the ones New_Align_Spec receives. */
+typedef struct
+{
+    int w[5], norm, thresh, K; /* w[4] = 0: see bias_scan */
+    u64 kmask;
+} Bias;
+
+static void bias_tables(const float freq[4], int K, Bias* B)
+{
+    double scale = -10000. / log(4.);
+    for (int i = 0; i < 4; i++)
+        B->w[i] = (int)ceil(scale * log(freq[i]));
+    B->w[4] = 0;
+    B->norm = 10000 * K;
+    B->thresh = 10000 * (K - 2); /* MAX_BIAS = 2 (filter.c:18) */
+    B->K = K;
+    B->kmask = (K >= 32) ? ~0ull : ((1ull << (2 * K)) - 1);
+}
+
+/* One scan of read s from p: over [p, q) when the block has a mask track (tracked), else up
+ * to the read's 4 terminator.  The two loops differ where growing meets the end: untracked
+ * stops, tracked still tests the window s[q-k, q) and keeps it at position q
+ * (filter.c:545-551 against 591-592).  There the trim finds the window below 10000 K and
+ * stops at once; it would read the base after the segment only for a one-base window, which
+ * needs a frequency below 4^-K (the reference then reads past its table; w[4] = 0 here). */
+static int64_t bias_scan(const Bias* B, const uint8_t* s, int p, int q, int tracked, int read, KPos* list, int64_t n)
+{
+    u64 c = 0;
+    int a = 0, k = 1;
+    while (tracked ? p < q : s[p] != 4)
+    {
+        int x = s[p];
+        a += B->w[x];
+        c = (c << 2) | x;
+        while (a < B->norm && k < B->K)
+        {
+            p += 1;
+            if (tracked ? p >= q : s[p] == 4)
+            {
+                if (!tracked)
+                    return n;
+                break;
+            }
+            k += 1;
+            x = s[p];
+            a += B->w[x];
+            c = (c << 2) | x;
+        }
+        /* trim: the window's first base is s[p - k + 1] */
+        while (a - B->w[s[p - k + 1]] >= B->norm)
+        {
+            a -= B->w[s[p - k + 1]];
+            k -= 1;
+        }
+        if (a > B->thresh)
+        {
+            list[n].code = (c << (2 * (B->K - k))) & B->kmask;
+            list[n].read = read;
+            list[n].rpos = p;
+            n++;
+        }
+        p += 1;
+        a -= B->w[s[p - k]];
+    }
+    return n;
+}
+
+/* All reads in order; the untracked scan needs no segment test, a tracked segment needs
+ * K bases (filter.c:533). */
+static int64_t extract_biased(const or_block* b, const Bias* B, KPos* list)
+{
+    int64_t n = 0;
+    for (int i = 0; i < b->nreads; i++)
+    {
+        const uint8_t* s = b->bases + b->boff[i];
+        int rlen = b->rlen[i];
+        if (!b->mask_anno)
+        {
+            n = bias_scan(B, s, 0, rlen, 0, i, list, n);
+            continue;
+        }
+        int64_t f0 = b->mask_anno[i], f1 = b->mask_anno[i + 1];
+        for (int64_t a = f0; a <= f1; a += 2)
+        {
+            int p = (a == f0) ? 0 : b->mask_data[a - 1];
+            int q = (a == f1) ? rlen : b->mask_data[a];
+            if (p + B->K <= q)
+                n = bias_scan(B, s, p, q, 1, i, list, n);
+        }
+    }
+    return n;
+}
+
 static KPos* build_index(const or_block* b, const or_params* p, int64_t* len)
 {
     int K = p->kmer;
-    int64_t cap = b->totlen + 1;
+    /* a biased scan keeps at most one tuple per position, plus one per segment end */
+    int64_t cap = b->totlen + 1 + (p->biased ? b->nreads + (b->mask_anno ? b->mask_anno[b->nreads] : 0) : 0);
     KPos* list = (KPos*)malloc(sizeof(KPos) * (cap + 1));
-    int64_t n = extract_kmers(b, K, list);
+    int64_t n;
+    if (p->biased)
+    {
+        Bias B;
+        bias_tables(p->freq, K, &B);
+        n = extract_biased(b, &B, list);
+    }
+    else
+        n = extract_kmers(b, K, list);
     sort_kpos(list, n, (2 * K + 7) / 8); /* mersort bytes (filter.c:713-716) */
     list[n].code = 1ull << (2 * K);      /* Kpowr sentinel (filter.c:796) */
     if (p->suppress > 0 && n > 0)        /* -t: drop codes occurring >= t times (filter.c:645-696) */

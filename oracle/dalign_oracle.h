@@ -43,6 +43,7 @@ typedef struct
     float freq[4];                            /* A-block base frequencies */
     int32_t hgap;                             /* daligner2 -H (its HGAP_MIN is live) */
     int32_t variant;                          /* 1 = daligner, 2 = daligner2 (dalign2/) */
+    int32_t biased;                           /* daligner -b: frequency-weighted tuples */
 } or_params;
 
 typedef struct

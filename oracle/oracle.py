@@ -23,7 +23,7 @@ class or_params(C.Structure):
                 ("ave_corr", C.c_double), ("tspace", C.c_int32), ("minover", C.c_int32),
                 ("symmetric", C.c_int32), ("identity", C.c_int32), ("only_identity", C.c_int32),
                 ("no_trace", C.c_int32), ("mem_limit", C.c_uint64), ("freq", C.c_float * 4),
-                ("hgap", C.c_int32), ("variant", C.c_int32)]
+                ("hgap", C.c_int32), ("variant", C.c_int32), ("biased", C.c_int32)]
 
 
 class or_overlap(C.Structure):
@@ -100,11 +100,12 @@ class BlockRef:
 
 
 def make_params(freq, k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=32, symmetric=True, identity=False,
-                only_identity=False, no_trace=False, H=0, variant=1):
-    """variant 1 = daligner (dalign/), 2 = daligner2 (dalign2/, where -H is live)."""
+                only_identity=False, no_trace=False, H=0, variant=1, biased=False):
+    """variant 1 = daligner (dalign/), 2 = daligner2 (dalign2/, where -H is live); biased = daligner's -b."""
     p = or_params()
     p.hgap = int(H)
     p.variant = int(variant)
+    p.biased = int(biased)
     p.kmer, p.binshift, p.suppress, p.hitmin = k, w, t, h
     p.ave_corr = e
     p.tspace = s

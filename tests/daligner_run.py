@@ -12,7 +12,7 @@ from marvel_b200 import dazzdb
 
 def parse_flags(flags):
     o = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=None, A=False, I=False, O=False, T=False, r=1, m=[],
-             H=0)
+             H=0, b=False)
     for f in flags:
         c, v = f[1], f[2:]
         if c in "kwhtlsHr":
@@ -23,7 +23,7 @@ def parse_flags(flags):
             o["e"] = float(v)
         elif c == "m":
             o["m"].append(v)
-        elif c in "AIOT":
+        elif c in "AIOTb":
             o[c] = True
         elif c == "j":
             pass
@@ -100,7 +100,7 @@ def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1):
         import oracle
         p = oracle.make_params(A.freq, k=o["k"], w=o["w"], h=o["h"], t=o["t"], e=o["e"], l=o["l"], s=o["s"],
                                M=0, symmetric=symmetric, identity=o["I"], only_identity=o["O"], no_trace=o["T"],
-                               H=o["H"], variant=variant)
+                               H=o["H"], variant=variant, biased=o["b"])
         p.mem_limit = mem
         recs, traces, st = oracle.daligner(A, B, dazzdb.complement_block(B), p, self_cmp)
         if st["status"]:
@@ -112,6 +112,8 @@ def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1):
             ctx.set_wave_limit(wave_limit)
         if variant == 2:
             ctx.set_variant(2, o["H"])
+        if o["b"]:
+            ctx.set_biased(True)
         ctx.set_filter_params(o["k"], o["w"], o["t"], o["h"])
         ctx.new_align_spec(o["e"], o["s"], A.freq, symmetric, o["O"], o["T"])
         ctx.set_globals(2 * o["l"], o["I"] or o["O"], mem)

@@ -35,6 +35,13 @@ CASES = {
     # tandem repeats masked by the reference DBdust track (-mdust), blocks of ~0.4 Mbp
     "pair_dust": ("tiny_tandem", 1.0, 0.4, ["-mdust", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100"],
                   ["G.1", "G.2"]),
+    # -b: frequency-weighted tuples on an AT-rich genome, whole reads and (with a dust track)
+    # unmasked segments
+    "self_biased": ("tiny_at", 1.0, 200, ["-b", "-k14", "-w6", "-h35", "-e.70", "-l1000", "-s100"], ["G.1", "G.1"]),
+    "pair_dust_biased": ("tiny_at_tandem", 1.0, 0.4, ["-b", "-mdust", "-k14", "-w6", "-h35", "-e.70", "-l1000",
+                                                      "-s100"], ["G.1", "G.2"]),
+    "self_dust_biased_k12": ("tiny_skew_tandem", 1.0, 200, ["-b", "-mdust", "-k12", "-w6", "-h30", "-e.70", "-l800",
+                                                            "-s100"], ["G.1", "G.1"]),
 }
 DUST = os.path.join(ROOT, "oracle", "_ref", "DBdust")
 

@@ -27,7 +27,6 @@ def _copy_db(src, dst):
 @pytest.mark.parametrize("args,msg", [
     (["-j3", "G.1", "G.1"], "Must be a power of 2"),
     (["-e.4", "G.1", "G.1"], "Average correlation must be in [.5,1.)"),
-    (["-b", "G.1", "G.1"], "-b (biased k-mer sampling) is not supported"),
     (["-Dhost:1", "G.1", "G.1"], "-D (dynamic mask server) is not supported"),
     (["-x", "G.1", "G.1"], "Unsupported option"),
     (["G.1"], "at least one target and one subject block are required"),
