@@ -38,6 +38,18 @@ sys.path.insert(0, ROOT)
 from marvel_b200 import dazzdb, synth  # noqa: E402
 
 PARAMS = dict(k=14, w=6, h=35, t=0, e=0.70, l=1000, s=100, M=32)
+FLAGS = "-k14 -w6 -h35 -e.70 -l1000 -s100 -M32"
+BIASED = False  # --biased: daligner -b on both arms
+
+
+def flag_str():
+    return ("-b " if BIASED else "") + FLAGS
+
+
+def path_name():
+    return "daligner -b path" if BIASED else "plain daligner path"
+
+
 CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
 CPU_SAMPLE_SCALE = 0.2   # CPU baseline: the same genome/read model on a 1/5-size genome
 # k_align_pairs DRAM bytes (read + write) per wave cell, from the ncu capture of the cfg1
@@ -130,6 +142,7 @@ def run_gpu(args):
     ctx.set_filter_params(p["k"], p["w"], p["t"], p["h"])
     ctx.new_align_spec(p["e"], p["s"], A.freq)
     ctx.set_globals(2 * p["l"], False, p["M"] * 0x40000000)
+    ctx.set_biased(BIASED)
 
     def barrier():
         torch.cuda.synchronize()
@@ -274,7 +287,7 @@ def run_gpu(args):
         # 16 B per k-mer each (read+write key and value), as the reference's pass count
         idx_bytes = kmers * (8 + 1 + 4 * 16 + 12)
         out = {
-            "metric": "overlaps/s (plain daligner path, one block vs itself)",
+            "metric": f"overlaps/s ({path_name()}, one block vs itself)",
             "value": round(value, 1),
             "unit": "overlaps/s",
             "n_gpus": ws,
@@ -287,7 +300,7 @@ def run_gpu(args):
             "dtype": "u8/int32",
             "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": f"{args.workload}: " + WORKLOAD_DESC.get(args.workload, args.workload),
-                       "flags": "-k14 -w6 -h35 -e.70 -l1000 -s100 -M32", "block_reads": A.nreads,
+                       "flags": flag_str(), "block_reads": A.nreads,
                        "block_bases": int(A.totlen), "parallelism": f"dp{ws} (one block per GPU)",
                        "l2": "inputs larger than L2 (k-mer index > 1 GB)"},
             "records_per_step": recs // args.steps,
@@ -373,7 +386,8 @@ def run_reference_once(path, threads, h=35, prog="daligner"):
         cmd = [b, f"-T{threads}", "-Pd2out", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
         las = os.path.join(d, "d2out_00001", "W.1.W.1.las")
     else:
-        cmd = [b, f"-j{threads}", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
+        cmd = [b, f"-j{threads}"] + (["-b"] if BIASED else []) + ["-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000",
+                                                                  "-s100", name, name]
         las = os.path.join(d, "001_00001", "W.1.W.1.las")
     t = time.perf_counter()
     subprocess.run(cmd, cwd=d, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
@@ -435,12 +449,12 @@ def run_reference(args):
     v = n_tot / t_tot
     sample = (f"reference daligner -j{j} (host cores) on the {args.workload} model with a {CPU_SAMPLE_SCALE}x genome, "
               f"{n_tot // args.steps} overlaps per step")
-    out = {"impl": "reference", "metric": "overlaps/s (plain daligner path, one block vs itself)",
+    out = {"impl": "reference", "metric": f"overlaps/s ({path_name()}, one block vs itself)",
            "value": round(v, 1), "unit": "overlaps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(1e3 * t_tot / args.steps, 1), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded generator, no dataset)",
            "config": {"workload": f"{args.workload}: " + WORKLOAD_DESC.get(args.workload, args.workload),
-                      "flags": "-k14 -w6 -h35 -e.70 -l1000 -s100 -M32", "cpu_sample_scale": CPU_SAMPLE_SCALE},
+                      "flags": flag_str(), "cpu_sample_scale": CPU_SAMPLE_SCALE},
            "cpu_baseline": {"value": round(v, 1), "unit": "overlaps/s", "cores": j, "kind": "reference",
                             "sample": sample},
            "e2e": {"value": round(v, 1), "unit": "overlaps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -460,7 +474,13 @@ def main():
                     help="skip the learned-triage measurement (reported beside the exact path)")
     ap.add_argument("--no-d2", dest="d2", action="store_false",
                     help="skip the daligner2 (modimizer seeds) measurement (reported beside the exact path)")
+    ap.add_argument("--biased", action="store_true",
+                    help="daligner -b (frequency-weighted tuples) on both arms instead of the plain path")
     args = ap.parse_args()
+    global BIASED
+    BIASED = args.biased
+    if BIASED:
+        args.d2 = False  # daligner2 has no -b
     if args.impl == "reference":
         run_reference(args)
     else:
