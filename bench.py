@@ -307,6 +307,12 @@ def run_gpu(args):
             "stages_ms": {"index": round(idx_ms, 3), "merge_hitsort": round(sum(st["ms_merge"]), 3),
                           "seed_scan_align": round(align_ms, 3)},
             "gcups": round(gcups, 2) if gcups else None,
+            # per-stage rates of the last step (its stats): k-mers sorted, hits emitted and
+            # sorted, Local_Alignment calls
+            "rates": {"kmers_sorted_per_s": round(kmers / (idx_ms / 1e3), 1) if idx_ms > 0 else None,
+                      "hits_per_s": round(sum(st["hits"]) / (sum(st["ms_merge"]) / 1e3), 1)
+                      if sum(st["ms_merge"]) > 0 else None,
+                      "alignments_per_s": round(sum(st["seeds"]) / (align_ms / 1e3), 1) if align_ms > 0 else None},
             "roofline": {"bound": "issue", "kernel": "k_align_pairs", "achieved": round(achieved, 3),
                          "peak": round(issue_peak, 2), "unit": "T int lane-ops/s",
                          "frac": round(achieved / issue_peak, 4),

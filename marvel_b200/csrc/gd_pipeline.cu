@@ -286,6 +286,13 @@ static int64_t index_slot_t(gd_context* c, Slot& sl)
                           nmasked, pbits, s))
         return -1;
     int sort_bits = 8 * ((2 * Kmer + 7) / 8);  // mersort bytes (filter.c:713-716)
+    // A masked slot's key is all ones.  When the sorted bytes end at the code's top bit (k a
+    // multiple of 4) that ties with the poly-T code, and cutting the masked count off the end
+    // could then keep masked slots and drop real k-mers (the reference's own result there
+    // depends on its thread split: its pads sit at the end of each thread's part of the list).
+    // One more byte puts every masked slot behind every k-mer.
+    if (sl.has_mask && (2 * Kmer) % 8 == 0)
+        sort_bits += 8;
     if (sort_bits > (int)(8 * sizeof(K)))
         sort_bits = 8 * sizeof(K);
     // with packed values the last pass writes the index arrays itself (masked slots, sorted to

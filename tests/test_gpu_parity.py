@@ -72,6 +72,32 @@ def test_kmer_index_and_hits_match_oracle(mb, name, k):
     ctx.close()
 
 
+@pytest.mark.parametrize("k", [12, 16])
+def test_masked_index_keeps_poly_t(mb, k):
+    """k a multiple of 4 with a mask track: the masked slots' all-ones key must not take the
+    place of real poly-T k-mers (the oracle lists the unmasked k-mers only)."""
+    import oracle
+    d, _ = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    A.bases = A.bases.copy()
+    mask = []
+    for i in range(A.nreads):
+        o = int(A.boff[i]) + 1
+        if i % 3 == 0:
+            A.bases[o + 100:o + 140] = 3  # a poly-T run outside the masks
+        mask.append([(600, 700)] if i % 2 == 0 else [(int(A.rlen[i]) - 50, int(A.rlen[i]))])
+    A.mask = mask
+    p = oracle.make_params(A.freq, k=k)
+    ctx = _ctx(mb, A, k=k)
+    ctx.load_block(0, A)
+    n = ctx.sort_kmers(0)
+    gc, gr, gp = ctx.get_kmers(0, n)
+    oc, orr, op = oracle.sort_kmers(A, p)
+    assert (oc == (1 << (2 * k)) - 1).sum() > 1000
+    assert n == oc.size and (gc == oc).all() and (gr == orr).all() and (gp == op).all()
+    ctx.close()
+
+
 def test_masked_index_matches_oracle(mb):
     """-m track masking in tuple extraction (dalign/filter.c:428-470), masks mirrored for cB."""
     import oracle
