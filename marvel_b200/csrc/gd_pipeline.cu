@@ -140,6 +140,7 @@ struct Slot
     DevBuf bases, boff, rlen, manno, mdata;
     DevBlock blk{};
     int64_t totlen = 0, nslots = 0;
+    int64_t nmask = 0;  // ints of mask interval data
     int has_mask = 0, loaded = 0;
     DevBuf code, read, rpos;
     int64_t nk = -1;
@@ -384,6 +385,14 @@ static int64_t index_slot_bias_t(gd_context* c, Slot& sl)
     BiasParams bp;
     if (bias_params(c, bp))
         return -1;
+    // chunk counts, tuple counts and offsets are 32-bit: at most one tuple per position and
+    // one more per unmasked segment
+    if (sl.totlen + 2 * (int64_t)nr + (sl.has_mask ? sl.nmask : 0) > 0xffffffffll)
+    {
+        gd_set_error("-b index of a %lld-base block exceeds this build's 32-bit tuple offsets",
+                     (long long)sl.totlen);
+        return -1;
+    }
     const int64_t* manno = sl.has_mask ? P<int64_t>(sl.manno) : nullptr;
     const int32_t* mdata = sl.has_mask ? P<int32_t>(sl.mdata) : nullptr;
     if (ensure(c->bchunk, (nr + 1) * 4) || ensure(c->misc, 64) ||
@@ -1446,9 +1455,11 @@ int gd_load_block(gd_context* c, int slot, const gd_block* b)
     GD_CUDA(cudaMemcpyAsync(s.boff.p, b->boff, (b->nreads + 1) * 8, cudaMemcpyHostToDevice, c->s));
     GD_CUDA(cudaMemcpyAsync(s.rlen.p, b->rlen, b->nreads * 4, cudaMemcpyHostToDevice, c->s));
     s.has_mask = b->mask_anno != nullptr;
+    s.nmask = 0;
     if (s.has_mask)
     {
         int64_t nd = b->mask_anno[b->nreads];
+        s.nmask = nd;
         if (ensure(s.manno, (b->nreads + 1) * 8) || ensure(s.mdata, nd * 4 + 8))
             return -1;
         GD_CUDA(cudaMemcpyAsync(s.manno.p, b->mask_anno, (b->nreads + 1) * 8, cudaMemcpyHostToDevice, c->s));
@@ -1490,6 +1501,7 @@ int gd_complement_block(gd_context* c, int src, int dst)
     GD_CUDA(cudaMemcpyAsync(D.boff.p, S.boff.p, (n + 1) * 8, cudaMemcpyDeviceToDevice, c->s));
     GD_CUDA(cudaMemcpyAsync(D.rlen.p, S.rlen.p, n * 4, cudaMemcpyDeviceToDevice, c->s));
     D.has_mask = S.has_mask;
+    D.nmask = S.nmask;
     int32_t* mdst = nullptr;
     if (S.has_mask)
     {
