@@ -44,7 +44,7 @@ def build(verbose=False, force=False):
         cli_src = os.path.join(CSRC, "host", main)
         if force or _stale(cli, [cli_src, LIB, os.path.join(CSRC, "host", "dazz_db.c")]):
             cmd = ["gcc", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), "-o", cli, cli_src,
-                   os.path.join(CSRC, "host", "dazz_db.c"), "-L" + HERE, "-lgpudalign", "-Wl,-rpath,$ORIGIN"]
+                   os.path.join(CSRC, "host", "dazz_db.c"), "-L" + HERE, "-lgpudalign", "-lm", "-Wl,-rpath,$ORIGIN"]
             subprocess.run(cmd, check=True)
     return LIB
 

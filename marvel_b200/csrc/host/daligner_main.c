@@ -26,6 +26,114 @@ static void usage(void)
     fprintf(stderr, "         [-r<int()1>]\n");
 }
 
+/* Print_Number (db/DB.c:193-240): the number with its digits grouped by commas, right-aligned
+ * in width characters (0: no padding) */
+static void print_number(int64_t num, int width)
+{
+    char t[48];
+    long long n = (long long)num;
+    if (n < 1000ll)
+        snprintf(t, sizeof t, "%lld", n);
+    else if (n < 1000000ll)
+        snprintf(t, sizeof t, "%lld,%03lld", n / 1000ll, n % 1000ll);
+    else if (n < 1000000000ll)
+        snprintf(t, sizeof t, "%lld,%03lld,%03lld", n / 1000000ll, (n % 1000000ll) / 1000ll, n % 1000ll);
+    else
+        snprintf(t, sizeof t, "%lld,%03lld,%03lld,%03lld", n / 1000000000ll, (n % 1000000000ll) / 1000000ll,
+                 (n % 1000000ll) / 1000ll, n % 1000ll);
+    printf("%*s", width, t);
+}
+
+/* Sort_Kmers' report under -v and its memory warning (dalign/filter.c:754-759, 865-892):
+ * the k-mer slots of the block, the index left after masking and -t. */
+static void report_index(gd_context* ctx, int slot, const dz_block* b, int kmer, int suppress, int64_t mem_limit,
+                         int mem_physical, int verbose)
+{
+    const int64_t slots = b->boff[b->nreads] - (int64_t)kmer * b->nreads;
+    if (slots <= 0)
+        return;
+    gd_stats st;
+    gd_get_stats(ctx, &st);
+    const int64_t kmers = st.kmers[slot];
+    if (verbose)
+    {
+        printf("\n   Kmer count = ");
+        print_number(slots, 0);
+        printf("\n   Using %.2fGb of space\n", (1. * slots) / 33554432);
+        if (suppress > 0)
+        {
+            printf("   Revised kmer count = ");
+            print_number(kmers, 0);
+            printf("\n");
+        }
+        printf("   Index occupies %.2fGb\n", (1. * kmers) / 67108864);
+        fflush(stdout);
+    }
+    if (kmers > 0 && mem_limit > 0 && kmers > mem_limit / 64)
+    {
+        fprintf(stderr, "Warning: Block size too big, index occupies more than 1/4 of");
+        if (mem_physical)
+            fprintf(stderr, " physical memory (%.1fGb)\n", (1. * mem_limit) / 0x40000000ll);
+        else
+            fprintf(stderr, " desired memory allocation (%.1fGb)\n", (1. * mem_limit) / 0x40000000ll);
+        fflush(stderr);
+    }
+}
+
+/* Match_Filter's report under -v (dalign/filter.c:2058-2063, 2105-2106, 2158-2162, 2180-2189,
+ * 2388-2405): the pair cap, the hits, the Local_Alignment calls (seed hits) and the overlaps
+ * they added (confirmed hits).  same_index: A's index also served as B's. */
+static void report_match(gd_context* ctx, const char* aname, const char* bname, int comp, int same_index, int bslot,
+                         int64_t recs_before, const dz_block* a, const dz_block* b, int kmer, int64_t mem_limit)
+{
+    gd_stats st;
+    gd_get_stats(ctx, &st);
+    int64_t tb = 0;
+    const int64_t recs = gd_num_overlaps(ctx, &tb);
+    const int64_t alen = st.kmers[0], blen = st.kmers[bslot];
+    int64_t nhits = 0, nfilt = 0, ncheck = 0;
+    if (comp)
+        printf("\nComparing %s to c(%s)\n", aname, bname);
+    else
+        printf("\nComparing %s to %s\n", aname, bname);
+    if (alen > 0 && blen > 0)
+    {
+        printf("\n");
+        if (mem_limit > 0)
+            printf("   Capping mutual k-mer matches over %d (effectively -t%d)\n", st.limit[comp],
+                   (int)sqrt(1. * st.limit[comp]));
+        nhits = st.hits[comp];
+        printf("   Hit count = ");
+        print_number(nhits, 0);
+        if (same_index || nhits >= blen)
+            printf("\n   Highwater of %.2fGb space\n", (1. * (alen + 2 * nhits)) / 67108864);
+        else
+            printf("\n   Highwater of %.2fGb space\n", (1. * (alen + blen + nhits)) / 67108864);
+        if (nhits > 0)
+        {
+            nfilt = st.seeds[comp];
+            ncheck = recs - recs_before;
+        }
+    }
+    const double atot = (double)a->totlen, btot = (double)b->totlen;
+    int width = nhits <= 0 ? 1 : (int)log10((double)nhits) + 1;
+    width += (width - 1) / 3;
+    printf("\n     ");
+    print_number(nhits, width);
+    printf(" %d-mers (%e of matrix)\n     ", kmer, (1. * nhits / atot) / btot);
+    print_number(nfilt, width);
+    printf(" seed hits (%e of matrix)\n     ", (1. * nfilt / atot) / btot);
+    print_number(ncheck, width);
+    printf(" confirmed hits (%e of matrix)\n", (1. * ncheck / atot) / btot);
+    fflush(stdout);
+}
+
+static int64_t num_overlaps(gd_context* ctx)
+{
+    int64_t tb = 0;
+    return gd_num_overlaps(ctx, &tb);
+}
+
 static int64_t physical_memory(void)
 {
     long pages = sysconf(_SC_PHYS_PAGES), psz = sysconf(_SC_PAGESIZE);
@@ -121,7 +229,8 @@ int main(int argc, char* argv[])
     int KMER_LEN = 14, HIT_MIN = 35, BIN_SHIFT = 6, MAX_REPS = 0, HGAP_MIN = 0, SPACING = 100, RUN_ID = 1;
     int MINOVER = 1000;
     double AVE_ERROR = .70;
-    int64_t MEM_LIMIT = physical_memory();
+    const int64_t MEM_PHYSICAL_BYTES = physical_memory();
+    int64_t MEM_LIMIT = MEM_PHYSICAL_BYTES;
     int MTOP = 0, MMAX = 10;
     char** MASK = (char**)malloc(MMAX * sizeof(char*));
     int c;
@@ -213,6 +322,7 @@ int main(int argc, char* argv[])
     }
     MINOVER *= 2;
 
+    const int MEM_PHYSICAL = MEM_LIMIT == MEM_PHYSICAL_BYTES;
     gd_context* ctx = gd_create();
     if (!ctx)
     {
@@ -265,6 +375,7 @@ int main(int argc, char* argv[])
             if (VERBOSE)
                 printf("\nBuilding index for %s\n", aroot);
             GPU(gd_sort_kmers(ctx, 0));
+            report_index(ctx, 0, &A, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
         }
         if (strcmp(afile, bfile) != 0)
         {
@@ -277,32 +388,40 @@ int main(int argc, char* argv[])
             if (VERBOSE)
                 printf("\nBuilding index for %s\n", broot);
             GPU(gd_sort_kmers(ctx, 1));
+            report_index(ctx, 1, &B, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
+            int64_t r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 1, 0, 0));
+            if (VERBOSE)
+                report_match(ctx, aroot, broot, 0, 0, 1, r0, &A, &B, KMER_LEN, MEM_LIMIT);
             GPU(gd_complement_block(ctx, 1, 2));
             if (VERBOSE)
                 printf("\nBuilding index for c(%s)\n", broot);
             GPU(gd_sort_kmers(ctx, 2));
+            report_index(ctx, 2, &B, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
+            r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 2, 1, 0));
+            if (VERBOSE)
+                report_match(ctx, aroot, broot, 1, 0, 2, r0, &A, &B, KMER_LEN, MEM_LIMIT);
             int lastRead = (B.part < A.part) ? B.ufirst + B.nreads - 1 : A.ufirst + A.nreads - 1;
             GPU(gd_write_overlap_buffer(ctx, RUN_ID, aroot, broot, lastRead));
             dz_free(&B);
         }
         else
         {
+            int64_t r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 0, 0, 1));
+            if (VERBOSE)
+                report_match(ctx, aroot, aroot, 0, 1, 0, r0, &A, &A, KMER_LEN, MEM_LIMIT);
             GPU(gd_complement_block(ctx, 0, 2));
             if (VERBOSE)
                 printf("\nBuilding index for c(%s)\n", aroot);
             GPU(gd_sort_kmers(ctx, 2));
+            report_index(ctx, 2, &A, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
+            r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 2, 1, 1));
+            if (VERBOSE)
+                report_match(ctx, aroot, aroot, 1, 0, 2, r0, &A, &A, KMER_LEN, MEM_LIMIT);
             GPU(gd_write_overlap_buffer(ctx, RUN_ID, aroot, aroot, A.ufirst + A.nreads - 1));
-        }
-        if (VERBOSE)
-        {
-            gd_stats st;
-            gd_get_stats(ctx, &st);
-            printf("\n   %lld + %lld hits, %lld + %lld seed hits, %lld overlaps\n", (long long)st.hits[0],
-                   (long long)st.hits[1], (long long)st.seeds[0], (long long)st.seeds[1], (long long)st.records);
         }
         GPU(gd_reset_overlap_buffer(ctx));
     }

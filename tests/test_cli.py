@@ -49,6 +49,19 @@ def test_cli_matches_reference_golden(name, tmp_path):
         assert ok, f"{name} {n}: {msg}"
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["self_s200_t20", "pair_blocks", "self_asym_lowmem", "pair_dust_biased"])
+def test_cli_verbose_report_matches_reference(name, tmp_path):
+    """-v prints the reference's report (index sizes, pair cap, hit counts, seed and
+    confirmed hits) character for character (tests/golden/make_verbose_golden.py)."""
+    d, meta = load(name)
+    _copy_db(d, str(tmp_path))
+    r = _run(["-v", "-j4"] + meta["flags"] + meta["blocks"], str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    with open(os.path.join(d, "verbose.txt")) as f:
+        assert r.stdout == f.read()
+
+
 @pytest.mark.parametrize("args,msg", [
     (["-x", "G.1", "G.1"], "-x is an illegal option"),
     (["-e.5", "G.1", "G.1"], "Average correlation must be in [.7,1.)"),
