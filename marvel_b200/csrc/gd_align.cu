@@ -133,6 +133,38 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
     return y;
 }
 
+// The same from the 2-bit copies: A's base i at apk index ag + i, B's at bpk index bg + i; 16
+// bases per step (one funnel shift per sequence), the read ends found from the lengths
+// instead of the 4s: the extension stops at the first mismatch, the end of b (bend, also when
+// both end there) or the end of a (aend), as the 4s stop the byte loop.
+template <bool FWD>
+__device__ __forceinline__ int snake_pk(const uint32_t* __restrict__ apk, uint32_t ag,
+                                        const uint32_t* __restrict__ bpk, uint32_t bg, int y, int k, int alen,
+                                        int blen, bool& bend, bool& aend)
+{
+    int eb = FWD ? blen - y : y;  // bases left before the end of b / a in the direction of travel
+    int ea = FWD ? alen - (y + k) : y + k;
+    while (true)
+    {
+        const uint32_t sb = FWD ? bg + y : bg + y - 16, sa = FWD ? ag + y + k : ag + y + k - 16;
+        const uint32_t wb = __funnelshift_r(__ldg(bpk + (sb >> 4)), __ldg(bpk + (sb >> 4) + 1), 2 * (sb & 15));
+        const uint32_t wa = __funnelshift_r(__ldg(apk + (sa >> 4)), __ldg(apk + (sa >> 4) + 1), 2 * (sa & 15));
+        const uint32_t x = wa ^ wb;
+        // matching bases from the start of travel: low bits first forward, high bits first back
+        const int m = FWD ? (x ? (__ffs((int)x) - 1) >> 1 : 16) : (__clz((int)x) >> 1);
+        const int s = min(m, min(ea, eb));
+        if (s < 16)
+        {
+            bend = s == eb;
+            aend = !bend && s == ea;
+            return FWD ? y + s : y - s;
+        }
+        y += FWD ? 16 : -16;
+        ea -= 16;
+        eb -= 16;
+    }
+}
+
 // The trim test of forward_wave/reverse_wave (align.c:884-896): the newest 15 columns are
 // suffix-positive and so are the newest 30 (TABLE / SCORE built by set_table, align.c:196-210).
 __device__ __forceinline__ bool trim_ok(unsigned long long b, const int16_t* table, const int16_t* score)
@@ -159,8 +191,9 @@ __device__ __forceinline__ int peb_one(WarpCtx<RG>& w, int& npeb, int ptr, int d
 }
 
 // forward_wave (FWD) / reverse_wave (!FWD) restated, with lanes over diagonals.
-template <bool FWD, int RG>
-__device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0, int alen, int blen,
+template <bool FWD, int RG, bool PK>
+__device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0,
+                     const uint32_t* apk, uint32_t ag, const uint32_t* bpk, uint32_t bg, int alen, int blen,
                      int comp, LAPath* apath, LAPath* bpath, int* mind, int maxd, int mida, int minp, int maxp,
                      uint16_t* atrace, uint16_t* btrace)
 {
@@ -223,7 +256,8 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
             hb = peb_one(w, npeb, -1, k, 0, y);
         }
         bool bend, aend;
-        y = snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
+        y = PK ? snake_pk<FWD>(apk, ag, bpk, bg, y, k, alen, blen, bend, aend)
+               : snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
         if (bend)
         {
             more = 0;
@@ -291,7 +325,9 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
         if (!more)
         {
             const int besty = w.sm->besty;
-            if (__ldg(bs + besty) != 4 && __ldg(as + besta - besty) != 4)
+            // the best point is not at a read end (the bytes there are 4s)
+            if (PK ? (FWD ? (besty < blen && besta - besty < alen) : (besty > 0 && besta - besty > 0))
+                   : (__ldg(bs + besty) != 4 && __ldg(as + besta - besty) != 4))
                 more = 1;
             if (FWD ? (hgh >= aclip) : (low <= aclip))
             {
@@ -435,7 +471,8 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
                 hb = R.HB[prv][ks & RM];
                 y = (c - k) >> 1;
                 int y0 = y;
-                y = snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
+                y = PK ? snake_pk<FWD>(apk, ag, bpk, bg, y, k, alen, blen, bend, aend)
+               : snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
                 int L = FWD ? (y - y0) : (y0 - y);
                 b = (L >= 61) ? ~0ull : ((b << L) | ((1ull << L) - 1ull));
                 c = (y << 1) + k;
@@ -864,8 +901,9 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
 }
 
 // Local_Alignment from one seed (diag, anti) with lbord = hbord = -1 (align.c:1922-2060).
-template <int RG>
-__device__ void local_alignment(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq, const uint8_t* bseq, int alen,
+template <int RG, bool PK>
+__device__ void local_alignment(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq, const uint8_t* bseq,
+                                const uint32_t* apk, uint32_t ag, const uint32_t* bpk, uint32_t bg, int alen,
                                 int blen, int comp, int diag, int anti)
 {
     const int TS = P.tspace;
@@ -891,10 +929,12 @@ __device__ void local_alignment(WarpCtx<RG>& w, const AlignParams& P, const uint
         ap->diffs = bp->diffs = 0;
     }
     __syncwarp();
-    wave<true>(w, P, aseq, bseq, alen, blen, comp, ap, bp, &low, hgh, anti, minp, maxp, atrace, btrace);
+    wave<true, RG, PK>(w, P, aseq, bseq, apk, ag, bpk, bg, alen, blen, comp, ap, bp, &low, hgh, anti, minp, maxp,
+                       atrace, btrace);
     if (w.err)
         return;
-    wave<false>(w, P, aseq, bseq, alen, blen, comp, ap, bp, &low, low, anti, minp, maxp, atrace, btrace);
+    wave<false, RG, PK>(w, P, aseq, bseq, apk, ag, bpk, bg, alen, blen, comp, ap, bp, &low, low, anti, minp, maxp,
+                        atrace, btrace);
     if (w.err)
         return;
     if (comp && w.lane == 0)
@@ -1992,6 +2032,7 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
         const int alen = A.rlen[ar], blen = B.rlen[br];
         const uint8_t* aseq = A.bases + A.boff[ar];
         const uint8_t* bseq = B.bases + B.boff[br];
+        const uint32_t ag = PK_BIAS + (uint32_t)A.boff[ar], bg = PK_BIAS + (uint32_t)B.boff[br];
         if (D2 && alen < P.hgap && blen < P.hgap)
             continue;  // daligner2 -H: neither read is long enough (filter_reporter_cpu.c:156-162)
         const bool doA = !D2 || alen >= P.hgap;
@@ -2088,7 +2129,8 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
                         continue;
                     nseeds++;
                     int bpj = apj - dj;
-                    local_alignment(w, P, aseq, bseq, alen, blen, P.comp, dj, apj + bpj);
+                    local_alignment<RG, true>(w, P, aseq, bseq, A.pk, ag, B.pk, bg, alen, blen, P.comp, dj,
+                                              apj + bpj);
                     if (w.err)
                         break;
                     const LAPath apth = w.sm->ap;
@@ -2436,7 +2478,8 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32)
         w.item = sd;
         const uint8_t* aseq = abase + aoff[sd];
         const uint8_t* bseq = bbase + boff[sd];
-        local_alignment(w, P, aseq, bseq, alen[sd], blen[sd], P.comp, diag[sd], anti[sd]);
+        local_alignment<RING, false>(w, P, aseq, bseq, nullptr, 0, nullptr, 0, alen[sd], blen[sd], P.comp, diag[sd],
+                                     anti[sd]);
         if (w.err)
         {
             if (w.err == 2 && lane == 0)

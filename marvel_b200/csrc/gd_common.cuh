@@ -37,7 +37,13 @@ struct DevBlock
     int32_t nreads;
     int32_t maxlen;
     int32_t ufirst;
+    // the block's bases 2 bits each, 16 per word (base i at index PK_BIAS + i, a 4 packed as
+    // 0): the aligner's match extension reads 16 bases per word
+    const uint32_t* pk;
 };
+
+// index in DevBlock::pk of bases[0] (the byte buffer's slack before it plus its leading 4)
+constexpr int PK_BIAS = 33;
 
 // k-mer slots of a block: read r owns slots [kstart(r), kstart(r+1)), one per position p of
 // its last k-mer base (p >= k-1); slot kstart(r) + p - (k-1).  A block's reads are >= k long.

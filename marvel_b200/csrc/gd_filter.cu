@@ -849,6 +849,40 @@ int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits,
     return 0;
 }
 
+__global__ void __launch_bounds__(FT) k_pack2(const uint8_t* __restrict__ buf, int64_t nbytes, uint32_t* pk,
+                                             int64_t nwords)
+{
+    const int64_t i = (int64_t)blockIdx.x * FT + threadIdx.x;
+    if (i >= nwords)
+        return;
+    const int64_t o = 16 * i;
+    uint32_t w = 0;
+    if (o + 16 <= nbytes)
+    {
+        const uint4 v = *reinterpret_cast<const uint4*>(buf + o);
+        const uint32_t q[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                w |= ((q[j] >> (8 * t)) & 3u) << (2 * (4 * j + t));
+    }
+    else
+        for (int j = 0; j < 16 && o + j < nbytes; j++)
+            w |= (uint32_t)(buf[o + j] & 3) << (2 * j);
+    pk[i] = w;
+}
+
+int launch_pack2(const uint8_t* buf, int64_t nbytes, uint32_t* pk, int64_t nwords, cudaStream_t s)
+{
+    if (nwords <= 0)
+        return 0;
+    k_pack2<<<(unsigned)gd_cdiv<int64_t>(nwords, FT), FT, 0, s>>>(buf, nbytes, pk, nwords);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 __global__ void __launch_bounds__(FT) k_complement(DevBlock b, uint8_t* dst)
 {
     int r = blockIdx.x;

@@ -141,6 +141,10 @@ int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits,
                          HitBits hb, const int32_t* arlen, const int32_t* brlen, uint2* groups, uint32_t* cost,
                          uint32_t* idx, unsigned int* ngroups, cudaStream_t s);
 
+// DevBlock::pk from a block's byte buffer (buf 16-byte aligned): word i holds bytes
+// [16 i, 16 i + 16), byte j of them in bits 2j..2j+1 (low two bits: a 4 packs as 0)
+int launch_pack2(const uint8_t* buf, int64_t nbytes, uint32_t* pk, int64_t nwords, cudaStream_t s);
+
 // complement_DB (dalign/daligner.c:474-573) on the device: reverse-complement every read of
 // src into dst (same offsets, 4s kept), and mirror the mask intervals if there are any.
 int launch_complement(const DevBlock& src, uint8_t* dst_bases, const int64_t* anno, const int32_t* mdata,

@@ -137,7 +137,7 @@ int ensure_host(HostBuf& b, size_t bytes)
 
 struct Slot
 {
-    DevBuf bases, boff, rlen, manno, mdata;
+    DevBuf bases, boff, rlen, manno, mdata, pk;
     DevBlock blk{};
     int64_t totlen = 0, nslots = 0;
     int64_t nmask = 0;  // ints of mask interval data
@@ -1433,6 +1433,8 @@ int gd_set_globals(gd_context* c, int minover, int identity, uint64_t mem_limit)
     return 0;
 }
 
+static int pack_slot(gd_context* c, Slot& s, int64_t nbytes);
+
 int gd_load_block(gd_context* c, int slot, const gd_block* b)
 {
     if (slot < 0 || slot > 2)
@@ -1472,12 +1474,30 @@ int gd_load_block(gd_context* c, int slot, const gd_block* b)
     s.blk.nreads = b->nreads;
     s.blk.maxlen = b->maxlen;
     s.blk.ufirst = b->ufirst;
+    if (pack_slot(c, s, nb + 1 + 64))
+        return -1;
     s.totlen = b->totlen;
     s.nslots = nb - (int64_t)c->kmer * b->nreads;
     s.hrlen.assign(b->rlen, b->rlen + b->nreads);
     s.loaded = 1;
     s.nk = -1;
     GD_CUDA(cudaStreamSynchronize(c->s));
+    return 0;
+}
+
+// The 2-bit copy of a slot's byte buffer (its first nbytes) for the aligner: the buffer's
+// base index must fit 32 bits; one word more than the bytes cover, for the two-word reads
+static int pack_slot(gd_context* c, Slot& s, int64_t nbytes)
+{
+    const int64_t nwords = (nbytes + 15) / 16 + 1;
+    if (nbytes + 32 > 0xffffffffll)
+    {
+        gd_set_error("block of %lld bytes exceeds this build's 32-bit base index", (long long)nbytes);
+        return -1;
+    }
+    if (ensure(s.pk, nwords * 4) || gd::launch_pack2((const uint8_t*)s.bases.p, nbytes, P<uint32_t>(s.pk), nwords, c->s))
+        return -1;
+    s.blk.pk = P<uint32_t>(s.pk);
     return 0;
 }
 
@@ -1518,6 +1538,8 @@ int gd_complement_block(gd_context* c, int src, int dst)
     D.blk.rlen = P<int32_t>(D.rlen);
     if (gd::launch_complement(S.blk, (uint8_t*)D.bases.p + 33, S.has_mask ? P<int64_t>(S.manno) : nullptr,
                               S.has_mask ? P<int32_t>(S.mdata) : nullptr, mdst, c->s))
+        return -1;
+    if (pack_slot(c, D, nb + 1 + 64))
         return -1;
     D.totlen = S.totlen;
     D.nslots = S.nslots;
