@@ -554,8 +554,10 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
             // the records are enumerated with a prefix-max scan.
             int wv = valid ? (FWD ? c : -c) : INT_MIN;
             int wbest = FWD ? besta : -besta;
-            // the PATH_AVE and trim tests of every lane, in parallel with the reduction
-            const bool q1 = valid && __popcll(b & MASK61) >= PATH_AVE;
+            // the PATH_AVE and trim tests, in parallel with the reduction, of the lanes that can be
+            // records (above the best so far): only records read them, so the others skip the
+            // table lookups
+            const bool q1 = valid && wv > wbest && __popcll(b & MASK61) >= PATH_AVE;
             const bool q2 = q1 && trim_ok(b, P.table, P.score);
             int wmax = __reduce_max_sync(GD_FULL, wv);
             if (wmax > wbest)
