@@ -53,8 +53,8 @@ def path_name():
 CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
 CPU_SAMPLE_SCALE = 0.2   # CPU baseline: the same genome/read model on a 1/5-size genome
 # k_align_pairs DRAM bytes (read + write) per wave cell, from the ncu capture of the cfg1
-# N-orientation launch: 160.6 MB over 282 M cells
-ALIGN_DRAM_BYTES_PER_CELL = 160.6e6 / 282.0e6
+# N-orientation launch: 114.3 MB over 282 M cells
+ALIGN_DRAM_BYTES_PER_CELL = 114.3e6 / 282.0e6
 
 
 def make_db(workload, seed_offset=0, scale=1.0):
@@ -320,9 +320,9 @@ def run_gpu(args):
                          "traffic_source": "bytes per launch: dram read+write per wave cell of the cfg1 ncu capture "
                                            "(profiles/k_align_pairs_cfg1.md) x this launch's cells",
                          "peak_source": "derived: 148 SM x 128 lanes/clk x median SM clock under load",
-                         "issue_slots_busy": 0.727,
+                         "issue_slots_busy": 0.751,
                          "issue_source": "smsp__issue_active of the cfg1 ncu capture (profiles/k_align_pairs_cfg1.md): "
-                                         "the kernel issues on 73 % of cycles; a wave is ~11 diagonals wide, so a "
+                                         "the kernel issues on 75 % of cycles; a wave is ~11 diagonals wide, so a "
                                          "warp instruction carries about a third of a warp of cells"},
             "roofline_filter": {"bound": "hbm", "kernel": "k-mer index (extract + 4 LSD passes)",
                                 "achieved": round(idx_bytes / (idx_ms / 1e3) / 1e9, 1),
