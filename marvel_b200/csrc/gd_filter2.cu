@@ -326,12 +326,28 @@ __global__ void __launch_bounds__(F2T) k_d2_pair_count(const K* __restrict__ aco
         cnt_c[i] = n - fwd;
         run = arun_excl[i] + arun_flag[i] - 1;
     }
-    const unsigned long long key = act ? (unsigned long long)run : ~0ull;
-    const unsigned peers = __match_any_sync(GD_FULL, key);
-    unsigned long long tot = 0;
-    for (unsigned mm = peers; mm; mm &= mm - 1)
-        tot += __shfl_sync(peers, n, __ffs(mm) - 1);
-    if (act && (peers & lanemask_lt()) == 0 && tot)
+    // per-run sums over contiguous runs: each lane alone when every lane holds its own run,
+    // else a segmented shuffle sum added by each run's last lane
+    const int lane = threadIdx.x & 31;
+    const uint32_t rkey = act ? run : 0xffffffffu;
+    const uint32_t prev = __shfl_up_sync(GD_FULL, rkey, 1);
+    const unsigned heads = __ballot_sync(GD_FULL, lane == 0 || prev != rkey);
+    if (heads == GD_FULL)
+    {
+        if (act && n)
+            atomicAdd(&ctrun[run], (unsigned long long)n);
+        return;
+    }
+    const uint32_t next = __shfl_down_sync(GD_FULL, rkey, 1);
+    const int seg0 = 31 - __clz((int)(heads & (0xffffffffu >> (31 - lane))));
+    unsigned long long tot = n;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const unsigned long long t = __shfl_up_sync(GD_FULL, tot, o);
+        if (lane - o >= seg0)
+            tot += t;
+    }
+    if (act && (lane == 31 || next != rkey) && tot)
         atomicAdd(&ctrun[run], tot);
 }
 
