@@ -7,8 +7,9 @@ Match_Filter(A,cA), dalign/daligner.c:957-1012), on the bacterial-scale workload
 repeats (4.6 Mbp genome + 40 x 5 kbp repeats at 1.5% + 3 x 6 kbp at 0.2%, 25x PacBio-like
 reads, mean 10 kbp; k14 w6 h35 e.70 l1000 s100 M32), generated from a seed.
 
-  value  overlaps/s with the block resident in HBM (all device stages, overlaps brought
-         to host memory, device-timed with CUDA events on the library's stream)
+  value  overlaps/s with the block resident in HBM (all device stages up to the overlap
+         buffer sorted into .las order on the device; device-timed with CUDA events on the
+         library's stream; nothing crosses PCIe inside the timed region)
   e2e    the same through the C ABI from pinned host buffers: block H2D + pipeline +
          sorted overlap buffer D2H, device-timed
 
@@ -16,7 +17,9 @@ Multi-GPU: each rank compares its own block (seed + rank): weak scaling, no coll
 the data path; the job value is all ranks' overlaps over the slowest rank's time.
 
 --impl reference runs the reference daligner (built from source into oracle/_ref) on
-the host cores with a bounded sample of the same workload.
+the host cores (-j = the largest power of two <= cores) on the same block and flags, one
+whole block comparison per step; cpu_baseline on the GPU line is one such run plus a
+filter-only run, which split off the aligner's CPU time for its GCUPS.
 """
 from __future__ import annotations
 
@@ -42,8 +45,22 @@ FLAGS = "-k14 -w6 -h35 -e.70 -l1000 -s100 -M32"
 BIASED = False  # --biased: daligner -b on both arms
 
 
+# workloads whose comparison is block 1 against block 2 with mask tracks (-m), the rest are
+# one block against itself
+MASKS = {"cfg5": ["dust"]}
+WORKLOAD = "cfg2"
+
+
+def is_pair(workload=None):
+    return synth.WORKLOADS[workload or WORKLOAD].nblocks >= 2
+
+
 def flag_str():
-    return ("-b " if BIASED else "") + FLAGS
+    return ("-b " if BIASED else "") + "".join(f"-m{m} " for m in MASKS.get(WORKLOAD, [])) + FLAGS
+
+
+def comparison():
+    return "block 1 vs block 2" if is_pair() else "one block vs itself"
 
 
 def path_name():
@@ -51,7 +68,6 @@ def path_name():
 
 
 CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
-CPU_SAMPLE_SCALE = 0.2   # CPU baseline: the same genome/read model on a 1/5-size genome
 # k_align_pairs DRAM bytes (read + write) per wave cell, from the ncu capture of the cfg1
 # N-orientation launch: 114.3 MB over 282 M cells
 ALIGN_DRAM_BYTES_PER_CELL = 114.3e6 / 282.0e6
@@ -60,6 +76,36 @@ ALIGN_DRAM_BYTES_PER_CELL = 114.3e6 / 282.0e6
 def make_db(workload, seed_offset=0, scale=1.0):
     """Generates (or reuses) the DB of a workload; returns the path of block 1."""
     return synth.cached_db(workload, seed_offset, scale, CACHE)
+
+
+def dust_track(path, on_gpu):
+    """The dust track of the workload's DB (whole DB), made once: on the GPU arm by this
+    package's device DBdust, on the reference arm by the reference DBdust (the two write the
+    same bytes)."""
+    root = path.rsplit(".", 1)[0]
+    if os.path.exists(os.path.join(os.path.dirname(root), "." + os.path.basename(root) + ".dust.anno")):
+        return
+    if on_gpu:
+        from marvel_b200 import dbdust
+        dbdust.dust_db(root)
+    else:
+        subprocess.run([ref_binary("DBdust"), os.path.basename(root)], cwd=os.path.dirname(root), check=True,
+                       stdout=subprocess.DEVNULL)
+
+
+def load_blocks(workload, seed_offset=0):
+    """(A, B) of a workload: B is None for a block against itself; mask tracks loaded."""
+    path = make_db(workload, seed_offset)
+    masks = MASKS.get(workload, [])
+    if masks:
+        dust_track(path, True)
+    A = dazzdb.open_block(path)
+    B = dazzdb.open_block(path[:-2] + ".2") if is_pair(workload) else None
+    for m in masks:
+        for blk in (A, B):
+            if blk is not None:
+                dazzdb.load_track(blk, m)
+    return A, B
 
 
 class ClockSampler:
@@ -135,8 +181,8 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.synchronize()
 
-    path = make_db(args.workload, seed_offset=rank)
-    A = dazzdb.open_block(path)
+    A, B = load_blocks(args.workload, seed_offset=rank)
+    pair = B is not None
     ctx = mb.Context()
     p = PARAMS
     ctx.set_filter_params(p["k"], p["w"], p["t"], p["h"])
@@ -158,9 +204,11 @@ def run_gpu(args):
 
     # ---- device-resident timing
     ctx.load_block(0, A)
+    if pair:
+        ctx.load_block(1, B)
     for _ in range(args.warmup):  # the same work as a timed step, so that every buffer is allocated
         ctx.reset_overlap_buffer()
-        mb.run_loaded(ctx, True)
+        mb.run_loaded(ctx, not pair)
         ctx.sort_overlaps()
     barrier()
     l0 = mb.kernel_launches()
@@ -169,7 +217,7 @@ def run_gpu(args):
         for _ in range(args.steps):
             ctx.reset_overlap_buffer()
             ctx.timer_mark(0)
-            mb.run_loaded(ctx, True)
+            mb.run_loaded(ctx, not pair)
             ctx.sort_overlaps()   # the .las order, on the device
             ctx.timer_mark(1)
             times.append(ctx.timer_elapsed_ms())
@@ -183,10 +231,20 @@ def run_gpu(args):
     value = recs_all / (tot_ms_max / 1e3)
 
     # ---- end to end through the C ABI from pinned host buffers
-    pin_bases = torch.empty(A.bases.size, dtype=torch.uint8, pin_memory=True)
-    pin_bases.numpy()[:] = A.bases
-    Ap = dazzdb.Block(pin_bases.numpy(), A.boff, A.rlen, A.ufirst, A.part, A.freq, A.maxlen, A.totlen)
-    h2d = A.bases.size + A.boff.nbytes + A.rlen.nbytes
+    def pinned(X):
+        pin = torch.empty(X.bases.size, dtype=torch.uint8, pin_memory=True)
+        pin.numpy()[:] = X.bases
+        return pin, dazzdb.Block(pin.numpy(), X.boff, X.rlen, X.ufirst, X.part, X.freq, X.maxlen, X.totlen,
+                                 X.root, X.mask)
+    pin_a, Ap = pinned(A)
+    pin_b, Bp = pinned(B) if pair else (None, None)
+
+    def block_bytes(X):
+        n = X.bases.size + X.boff.nbytes + X.rlen.nbytes
+        if X.mask is not None:
+            n += 8 * (X.nreads + 1) + 8 * sum(len(iv) for iv in X.mask)
+        return n
+    h2d = block_bytes(A) + (block_bytes(B) if pair else 0)
     # result buffers in pinned host memory, sized from the device-resident runs
     nrec, ntb = ctx.sort_overlaps()
     pin_rec = torch.empty(int(nrec * 1.05 + 1024) * mb.OVL_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
@@ -197,7 +255,9 @@ def run_gpu(args):
         ctx.reset_overlap_buffer()
         ctx.timer_mark(0)
         ctx.load_block(0, Ap)
-        mb.run_loaded(ctx, True)
+        if pair:
+            ctx.load_block(1, Bp)
+        mb.run_loaded(ctx, not pair)
         r, tr = ctx.overlaps(out=outbuf)
         ctx.timer_mark(1)
         if i >= args.warmup:
@@ -217,7 +277,7 @@ def run_gpu(args):
         for i in range(1 + args.steps):
             ctx.reset_overlap_buffer()
             ctx.timer_mark(0)
-            mb.run_loaded(ctx, True)
+            mb.run_loaded(ctx, not pair)
             ctx.sort_overlaps()
             ctx.timer_mark(1)
             if i >= 1:
@@ -287,7 +347,7 @@ def run_gpu(args):
         # 16 B per k-mer each (read+write key and value), as the reference's pass count
         idx_bytes = kmers * (8 + 1 + 4 * 16 + 12)
         out = {
-            "metric": f"overlaps/s ({path_name()}, one block vs itself)",
+            "metric": f"overlaps/s ({path_name()}, {comparison()})",
             "value": round(value, 1),
             "unit": "overlaps/s",
             "n_gpus": ws,
@@ -299,10 +359,7 @@ def run_gpu(args):
             "vs_baseline": None,
             "dtype": "u8/int32",
             "data": "synthetic (seeded generator, no dataset)",
-            "config": {"workload": f"{args.workload}: " + WORKLOAD_DESC.get(args.workload, args.workload),
-                       "flags": flag_str(), "block_reads": A.nreads,
-                       "block_bases": int(A.totlen), "parallelism": f"dp{ws} (one block per GPU)",
-                       "l2": "inputs larger than L2 (k-mer index > 1 GB)"},
+            "config": bench_config(args, A, ws, B),
             "records_per_step": recs // args.steps,
             "stages_ms": {"index": round(idx_ms, 3), "merge_hitsort": round(sum(st["ms_merge"]), 3),
                           "seed_scan_align": round(align_ms, 3)},
@@ -337,14 +394,14 @@ def run_gpu(args):
             "clocks": clocks,
         }
         if args.cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline(args)
+            out["cpu_baseline"] = cpu_baseline(args, cells)
             if d2 is not None and ref_binary("daligner2"):
                 j = ref_threads()
-                n2, dt2 = run_reference_once(make_db(args.workload, scale=CPU_SAMPLE_SCALE), j, prog="daligner2")
+                n2, dt2 = run_reference_once(make_db(args.workload), j, prog="daligner2")
                 d2["cpu_baseline"] = {"value": round(n2 / dt2, 1), "unit": "overlaps/s", "cores": j,
                                       "kind": "reference",
-                                      "sample": f"reference daligner2 -T{j} on the {args.workload} model with a "
-                                                f"{CPU_SAMPLE_SCALE}x genome ({n2} overlaps, {dt2:.1f} s wall)"}
+                                      "sample": f"reference daligner2 -T{j} on the same block ({n2} overlaps, "
+                                                f"{dt2:.1f} s wall)"}
         print(json.dumps(out), flush=True)
     ctx.close()
     if ws > 1:
@@ -358,6 +415,10 @@ WORKLOAD_DESC = {
             "sd 5 kbp, 9/4.5/1.5% ins/del/sub; one block (~115 Mbp) vs itself",
     "cfg1": "1 Mbp genome, 20x, mean 8 kbp sd 4 kbp, 9/4.5/1.5% ins/del/sub; one block vs itself",
     "cfg3": "10 Mbp genome, 30x, mean 20 kbp sd 15 kbp (1-150 kbp), 3/5/2% ins/del/sub; one block vs itself",
+    "cfg4": "20 Mbp genome, 10% interspersed 1-8 kbp repeat families at 5-15% divergence, 30x, mean 10 kbp; "
+            "block 1 (200 Mbp) vs itself",
+    "cfg5": "200 Mbp diploid (0.5% SNP, 0.05% indel), 35% interspersed 1-10 kbp repeats at 5-15%, 2% tandem "
+            "repeats, 30x, mean 15 kbp; 400 Mbp block 1 vs 400 Mbp block 2 with -mdust",
 }
 
 
@@ -383,23 +444,31 @@ def ref_threads():
 
 
 def run_reference_once(path, threads, h=35, prog="daligner"):
-    """The reference daligner (or daligner2) on a block against itself; returns (records,
+    """The reference daligner (or daligner2) on the workload's comparison (a block against
+    itself, or block 1 against block 2 with its mask tracks); returns (records written,
     seconds).  With h=100000 no pair group reaches the aligner: the filter alone."""
     b = ref_binary(prog)
     d = os.path.dirname(path)
     name = os.path.basename(path)
+    bname = name[:-2] + ".2" if is_pair() else name
+    masks = [f"-m{m}" for m in MASKS.get(WORKLOAD, [])]
+    if masks:
+        dust_track(path, False)
     if prog == "daligner2":
         cmd = [b, f"-T{threads}", "-Pd2out", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
-        las = os.path.join(d, "d2out_00001", "W.1.W.1.las")
+        las = [os.path.join(d, "d2out_00001", "W.1.W.1.las")]
     else:
-        cmd = [b, f"-j{threads}"] + (["-b"] if BIASED else []) + ["-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000",
-                                                                  "-s100", name, name]
-        las = os.path.join(d, "001_00001", "W.1.W.1.las")
+        cmd = [b, f"-j{threads}"] + (["-b"] if BIASED else []) + masks + ["-M32", "-k14", "-w6", f"-h{h}", "-e.70",
+                                                                          "-l1000", "-s100", name, bname]
+        las = [os.path.join(d, "001_00001", "W.1.W.2.las"), os.path.join(d, "001_00002", "W.2.W.1.las")] \
+            if is_pair() else [os.path.join(d, "001_00001", "W.1.W.1.las")]
     t = time.perf_counter()
     subprocess.run(cmd, cwd=d, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     dt = time.perf_counter() - t
-    with open(las, "rb") as f:
-        n = int(np.frombuffer(f.read(8), "<i8")[0])
+    n = 0
+    for x in las:
+        with open(x, "rb") as f:
+            n += int(np.frombuffer(f.read(8), "<i8")[0])
     return n, dt
 
 
@@ -414,25 +483,60 @@ def cpu_model():
     return None
 
 
-def cpu_baseline(args):
-    path = make_db(args.workload, scale=CPU_SAMPLE_SCALE)
+def bench_config(args, A, ws, B=None):
+    """The workload both arms run (the same dict on both JSON lines)."""
+    out = {"workload": f"{args.workload}: " + WORKLOAD_DESC.get(args.workload, args.workload),
+           "flags": flag_str(), "block_reads": int(A.nreads), "block_bases": int(A.totlen),
+           "parallelism": f"dp{ws} (one block {'pair' if B is not None else ''} per rank)".replace("  ", " "),
+           "l2": "inputs larger than L2 (k-mer index > 1 GB)"}
+    if B is not None:
+        out["b_block_reads"] = int(B.nreads)
+        out["b_block_bases"] = int(B.totlen)
+    return out
+
+
+def pinned_cells(workload):
+    """The reference's own wave-cell count for the full block of a workload (its WAVE_STATS
+    counters), as recorded beside the parity digests; None when not recorded."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "config_digests.json")) as f:
+            rec = json.load(f).get(workload)
+    except OSError:
+        return None
+    if rec and rec.get("scale") == 1.0 and rec.get("seed_offset") == 0:
+        return rec.get("cells")
+    return None
+
+
+def cpu_baseline(args, cells=None):
+    """The reference daligner on the host cores, on the same block as the GPU arm: one full
+    run and one filter-only run (-h100000: no pair group reaches the aligner), so that the
+    aligner's CPU time and its GCUPS (the same wave cells the GPU counts, equal to the
+    reference's WAVE_STATS count) follow."""
+    path = make_db(args.workload)
     if ref_binary():
         j = ref_threads()
         n, dt = run_reference_once(path, j)
         _, df = run_reference_once(path, j, h=100000)
-        return {"value": round(n / dt, 1), "unit": "overlaps/s", "cores": j, "kind": "reference",
-                "sample": f"reference daligner -j{j} on the {args.workload} model with a {CPU_SAMPLE_SCALE}x genome "
-                          f"({n} overlaps, {dt:.1f} s wall)",
-                "filter_only_s": round(df, 2), "cpu_model": cpu_model()}
+        out = {"value": round(n / dt, 1), "unit": "overlaps/s", "cores": j, "kind": "reference",
+               "sample": f"reference daligner -j{j} on the same block as the GPU arm ({n} overlaps, {dt:.1f} s wall)",
+               "filter_only_s": round(df, 2), "cpu_model": cpu_model()}
+        if cells and dt > df:
+            out["align_s"] = round(dt - df, 2)
+            out["gcups"] = round(cells / (dt - df) / 1e9, 3)
+            out["gcups_source"] = ("wave cells of the block (the GPU's count, equal to the reference's WAVE_STATS "
+                                   "count) / (full run - filter-only run) wall time")
+        return out
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    A = dazzdb.open_block(path)
+    A, B = load_blocks(args.workload)
     p = oracle.make_params(A.freq)
     t = time.perf_counter()
-    recs, _, _ = oracle.daligner(A, A, dazzdb.complement_block(A), p, True)
+    Bx = A if B is None else B
+    recs, _, _ = oracle.daligner(A, Bx, dazzdb.complement_block(Bx), p, B is None)
     dt = time.perf_counter() - t
     return {"value": round(len(recs) / dt, 1), "unit": "overlaps/s", "cores": 1, "kind": "port",
-            "sample": f"C restatement, 1 thread, {args.workload} model with a {CPU_SAMPLE_SCALE}x genome"}
+            "sample": f"C restatement, 1 thread, on the same block as the GPU arm"}
 
 
 def run_reference(args):
@@ -443,7 +547,9 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/daligner was not built "
                           "(make -C oracle ref needs the reference sources)"}))
         return None
-    path = make_db(args.workload, scale=CPU_SAMPLE_SCALE)
+    path = make_db(args.workload)
+    A = dazzdb.open_block(path)
+    B = dazzdb.open_block(path[:-2] + ".2") if is_pair() else None
     j = ref_threads()
     for _ in range(args.warmup):
         run_reference_once(path, j)
@@ -453,17 +559,21 @@ def run_reference(args):
         n_tot += n
         t_tot += dt
     v = n_tot / t_tot
-    sample = (f"reference daligner -j{j} (host cores) on the {args.workload} model with a {CPU_SAMPLE_SCALE}x genome, "
+    sample = (f"reference daligner -j{j} (host cores, {cpu_model()}) on the same block as the GPU arm, "
               f"{n_tot // args.steps} overlaps per step")
-    out = {"impl": "reference", "metric": f"overlaps/s ({path_name()}, one block vs itself)",
+    out = {"impl": "reference", "metric": f"overlaps/s ({path_name()}, {comparison()})",
            "value": round(v, 1), "unit": "overlaps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(1e3 * t_tot / args.steps, 1), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic (seeded generator, no dataset)",
-           "config": {"workload": f"{args.workload}: " + WORKLOAD_DESC.get(args.workload, args.workload),
-                      "flags": flag_str(), "cpu_sample_scale": CPU_SAMPLE_SCALE},
+           "config": bench_config(args, A, ws, B),
            "cpu_baseline": {"value": round(v, 1), "unit": "overlaps/s", "cores": j, "kind": "reference",
                             "sample": sample},
            "e2e": {"value": round(v, 1), "unit": "overlaps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    cells = pinned_cells(args.workload)
+    if cells and not BIASED:
+        out["gcups_whole_run"] = round(cells / (t_tot / args.steps) / 1e9, 3)
+        out["gcups_note"] = ("the reference's WAVE_STATS wave cells of this block over the whole run's wall time "
+                             "(filter included); bench.py's GPU line splits the filter off")
     print(json.dumps(out), flush=True)
     return out
 
@@ -483,8 +593,11 @@ def main():
     ap.add_argument("--biased", action="store_true",
                     help="daligner -b (frequency-weighted tuples) on both arms instead of the plain path")
     args = ap.parse_args()
-    global BIASED
+    global BIASED, WORKLOAD
     BIASED = args.biased
+    WORKLOAD = args.workload
+    if is_pair():
+        args.d2 = False  # the daligner2 line is measured on the one-block workloads
     if BIASED:
         args.d2 = False  # daligner2 has no -b
     if args.impl == "reference":

@@ -61,6 +61,7 @@ typedef struct
     double ms_align[2];   /* device time of seed scan + alignment */
     int64_t skipped[2];   /* pair groups the learned triage skipped (0 with no model set) */
     int64_t wide[2];      /* pair groups whose band outgrew 128 diagonals (aligned by the wide kernel) */
+    int64_t reruns[2];    /* aligner re-runs after a scratch or output buffer was grown */
 } gd_stats;
 
 /* Context on the current CUDA device. */
@@ -163,6 +164,19 @@ int64_t gd_dust(gd_context* ctx, int slot, int window, double thresh, int mflag,
  * output must not change). */
 int gd_set_wave_limit(gd_context* ctx, int limit);
 
+/* Test hook, no counterpart in the reference: the aligner's starting capacities -- pebbles
+ * and pair-trace values per warp, paths per pair, overlap records and trace bytes per
+ * Match_Filter.  Each one the aligner outgrows is reported by the device, grown on the host
+ * and the alignment stage re-run (gd_stats.reruns); small values force that path, and the
+ * output must not change.  Values <= 0 keep the current capacity. */
+int gd_set_capacities(gd_context* ctx, int pebbles, int traces, int paths, int64_t records, int64_t trace_bytes);
+
+/* Test hook, no counterpart in the reference: one block of the radix sort's bounded wait on
+ * an mbarrier armed for a copy that is never issued (nothing is in flight), with polls
+ * tries; the wait must give up, raise the sort's wait flag and return, and the check every
+ * sort makes afterwards must report it (-1, gd_last_error set) and clear it. */
+int gd_test_wait_expiry(gd_context* ctx, int polls);
+
 /* LAsort (dalign/LAsort.c:65-90, 139-256) of one .las file on the device: writes out_path
  * with the records of in_path ordered by (aread, bread, abpos) -- ties, which the
  * reference's qsort leaves unordered, by (aepos, bbpos) and then file order -- each record's
@@ -213,10 +227,14 @@ int gd_local_alignment_batch(gd_context* ctx, const uint8_t* abases, int64_t ale
  * bytes before the first base and after the last 4); maxlen is the longest read among the
  * seeds; stream is a cudaStream_t (NULL = legacy default stream).  ctx must have had
  * gd_new_align_spec called (that call may allocate; do it during set-up).
- * Working memory is one file-scope device array of 2,359,552 bytes (16 warps, 8192
- * pebbles and 8192 trace-point slots per warp) that every GPU loading the library keeps
- * until exit; maxlen / tspace may be at most 1020 (reads up to 102,099 bp at trace
- * spacing 100), larger batches are rejected with an error.  The first call on a device looks up that array's device address
+ * Working memory is one file-scope device array of 17,301,760 bytes (16 warps, 65,536
+ * pebbles and 16,384 trace-point slots per warp) that every GPU loading the library keeps
+ * until exit; maxlen / tspace may be at most 2044 (reads up to 204,499 bp at trace
+ * spacing 100), larger batches are rejected up front with an error.  The pebbles bound the
+ * band: a wave over L bases of A whose band averages W diagonals needs up to about
+ * 2 * W * L / tspace of them (65,536 hold 150 kbp at W = 21, spacing 100); a seed that
+ * needs more fails the call with an error naming it, as does a seed whose trace is longer
+ * than trstride / 2.  The first call on a device looks up that array's device address
  * (cudaGetSymbolAddress) with the device current, so make the first call before any
  * stream capture.  Calls share the array: two calls that overlap on the GPU (different
  * streams or threads) race and must be serialised by the caller.  The call synchronizes

@@ -50,7 +50,8 @@ class GdStats(C.Structure):
     _fields_ = [("kmers", C.c_int64 * 3), ("hits", C.c_int64 * 2), ("groups", C.c_int64 * 2),
                 ("seeds", C.c_int64 * 2), ("cells", C.c_int64 * 2), ("records", C.c_int64),
                 ("limit", C.c_int32 * 2), ("ms_index", C.c_double * 3), ("ms_merge", C.c_double * 2),
-                ("ms_align", C.c_double * 2), ("skipped", C.c_int64 * 2), ("wide", C.c_int64 * 2)]
+                ("ms_align", C.c_double * 2), ("skipped", C.c_int64 * 2), ("wide", C.c_int64 * 2),
+                ("reruns", C.c_int64 * 2)]
 
 
 # exported symbols of include/gpudalign.h
@@ -62,7 +63,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
            "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge",
            "gd_set_wave_limit", "gd_set_variant", "gd_match_filter2", "gd_test_handle_redundancies_d2",
-           "gd_set_biased"]
+           "gd_set_biased", "gd_set_capacities", "gd_test_wait_expiry"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -104,6 +105,8 @@ def lib():
     L.gd_las_merge.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int, C.c_char_p]
     L.gd_las_merge.restype = C.c_int64
     L.gd_set_wave_limit.argtypes = [C.c_void_p, C.c_int]
+    L.gd_set_capacities.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64]
+    L.gd_test_wait_expiry.argtypes = [C.c_void_p, C.c_int]
     L.gd_dust.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_float),
                           C.c_void_p, C.c_void_p, C.c_int64]
     L.gd_dust.restype = C.c_int64
@@ -335,6 +338,18 @@ class Context:
     def set_wave_limit(self, limit):
         """Test hook: the widest band of the main aligner kernel, 128 (default) or 32."""
         _check(lib().gd_set_wave_limit(self.h, int(limit)))
+
+    def set_capacities(self, pebbles=0, traces=0, paths=0, records=0, trace_bytes=0):
+        """Test hook: the aligner's starting capacities (0 keeps one); outgrown ones are grown
+        and the alignment stage re-run."""
+        _check(lib().gd_set_capacities(self.h, int(pebbles), int(traces), int(paths), int(records),
+                                       int(trace_bytes)))
+
+    def test_wait_expiry(self, polls):
+        """Test hook: the radix sort's bounded mbarrier wait run out on a copy never issued;
+        returns (status of the sort's wait check, its error text)."""
+        rc = lib().gd_test_wait_expiry(self.h, int(polls))
+        return rc, (lib().gd_last_error() or b"").decode()
 
     def las_merge(self, in_paths, out_path):
         """LAmerge of .las files on the device; returns the number of records."""

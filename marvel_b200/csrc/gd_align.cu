@@ -2489,6 +2489,14 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32)
             continue;
         }
         LAPath a = w.sm->ap, b = w.sm->bp;
+        if (a.tlen > trstride / 2 || b.tlen > trstride / 2)
+        {
+            // the caller's trace stride cannot hold this seed's traces: an error, not a
+            // silently shortened trace
+            if (lane == 0)
+                gd_fail(st, GD_ERR_TRACE_STRIDE, sd, 2 * max(a.tlen, b.tlen));
+            continue;
+        }
         if (lane == 0)
         {
             int32_t* o = out12 + 12 * (size_t)sd;
@@ -2508,9 +2516,9 @@ __global__ void __launch_bounds__(ALIGN_WARPS * 32)
         }
         uint16_t* ta = tr + (size_t)sd * trstride;
         uint16_t* tb = ta + trstride / 2;
-        for (int i = lane; i < a.tlen && i < trstride / 2; i += 32)
+        for (int i = lane; i < a.tlen; i += 32)
             ta[i] = w.pts[a.toff + i];
-        for (int i = lane; i < b.tlen && i < trstride / 2; i += 32)
+        for (int i = lane; i < b.tlen; i += 32)
             tb[i] = w.pts[b.toff + i];
         __syncwarp();
     }

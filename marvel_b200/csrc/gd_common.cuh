@@ -89,6 +89,7 @@ enum
     GD_ERR_RING = 7,         // band left the ring window
     GD_ERR_BRIDGE = 8,       // daligner2: bridging scratch exhausted (info: ints needed)
     GD_ERR_TRACE8 = 9,       // daligner2: a trace value above 255 fails the 8-bit compression check
+    GD_ERR_TRACE_STRIDE = 10,  // Local_Alignment batch: a trace longer than half the caller's stride (info: stride needed)
 };
 
 __device__ __forceinline__ void gd_fail(DevStatus* st, int code, int where, int info)

@@ -18,13 +18,21 @@
 namespace
 {
 
-constexpr int NOALLOC_WARPS = 16;     // 4 CTAs of 4 warps
-constexpr int NOALLOC_PCAP = 8192;    // pebbles per warp and wave direction
-constexpr int NOALLOC_PTSCAP = 8192;  // trace-point slots per warp (uint16)
+// Two resources bound what one seed may need.  The trace-point slots bound the read length
+// up front (checked before launch).  The pebbles -- one per band diagonal each time the
+// wave's furthest point on that diagonal crosses an A or a B trace point -- depend on how
+// wide the band grows, which no caller knows in advance: a wave spanning L bases of A with
+// a band of W diagonals on average needs at most about 2 * W * L / tspace of them, so 65,536
+// hold a 150 kbp wave at spacing 100 whose band averages up to ~21 diagonals.  A seed that
+// needs more fails the call with GD_ERR_PEBBLES, nothing of that seed written; the
+// allocating entry point grows its arena instead.
+constexpr int NOALLOC_WARPS = 16;      // 4 CTAs of 4 warps
+constexpr int NOALLOC_PCAP = 65536;    // pebbles per warp (each wave of a seed starts it afresh)
+constexpr int NOALLOC_PTSCAP = 16384;  // trace-point slots per warp (uint16)
 constexpr size_t NOALLOC_STATUS = 256;
 constexpr size_t NOALLOC_PEB_BYTES = (size_t)NOALLOC_WARPS * NOALLOC_PCAP * sizeof(int4);
 constexpr size_t NOALLOC_PTS_BYTES = (size_t)NOALLOC_WARPS * NOALLOC_PTSCAP * sizeof(uint16_t);
-constexpr size_t NOALLOC_BYTES = NOALLOC_STATUS + NOALLOC_PEB_BYTES + NOALLOC_PTS_BYTES;  // 2,359,552 bytes
+constexpr size_t NOALLOC_BYTES = NOALLOC_STATUS + NOALLOC_PEB_BYTES + NOALLOC_PTS_BYTES;  // 17,301,760 bytes
 
 // The scratch.  Host code must not take its address directly: the name is only a host-side
 // stand-in; the device address comes from cudaGetSymbolAddress below.
@@ -129,11 +137,24 @@ extern "C" int gd_local_alignment_batch_noalloc(gd_context* ctx, const uint8_t* 
         gd_set_error("gd_local_alignment_batch_noalloc: %s", cudaGetErrorString(cudaGetLastError()));
         return -1;
     }
+    if (hs.code == GD_ERR_PEBBLES)
+    {
+        gd_set_error("gd_local_alignment_batch_noalloc: seed %d needs more than the %d pebbles per warp of the static "
+                     "scratch (its band is too wide for its length)",
+                     hs.where, NOALLOC_PCAP);
+        return -1;
+    }
+    if (hs.code == GD_ERR_TRACE_STRIDE)
+    {
+        gd_set_error("gd_local_alignment_batch_noalloc: seed %d has a trace longer than trstride / 2 (trstride %d, "
+                     "needs %d)",
+                     hs.where, trstride, hs.info);
+        return -1;
+    }
     if (hs.code)
     {
-        gd_set_error("gd_local_alignment_batch_noalloc: seed %d failed with code %d (info %d); the static scratch "
-                     "holds %d pebbles per warp",
-                     hs.where, hs.code, hs.info, NOALLOC_PCAP);
+        gd_set_error("gd_local_alignment_batch_noalloc: seed %d failed with code %d (info %d)", hs.where, hs.code,
+                     hs.info);
         return -1;
     }
     return 0;

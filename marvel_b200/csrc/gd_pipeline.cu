@@ -1024,8 +1024,11 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     int maxlen = std::max(A.blk.maxlen, B.blk.maxlen);
     int ptscap = 4 * (2 * (maxlen / c->tspace + 2)) + 32;
     int nbands = ap.maxdiag - ap.mindiag + 8;
-    for (int attempt = 0; attempt < 6; attempt++)
+    c->stats.reruns[oi] = 0;
+    for (int attempt = 0; attempt < 48; attempt++)
     {
+        if (attempt)
+            c->stats.reruns[oi]++;
         const int bvcap = ap.d2 ? c->bvcap : 0, btcap = ap.d2 ? c->btcap : 0;
         AlignScratch sc{};
         size_t need = align_scratch_bytes(nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
@@ -1443,12 +1446,42 @@ int gd_load_block(gd_context* c, int slot, const gd_block* b)
         return -1;
     }
     Slot& s = c->slot[slot];
+    if (!b->bases || !b->boff || !b->rlen || b->nreads < 0 || (b->mask_anno == nullptr) != (b->mask_data == nullptr))
+    {
+        gd_set_error("gd_load_block: bases, boff and rlen are required (mask_anno and mask_data together)");
+        return -1;
+    }
     int64_t nb = b->boff[b->nreads];  // bytes after bases[-1], through the last 4
     for (int i = 0; i < b->nreads; i++)
         if (b->rlen[i] < c->kmer)
         {
             gd_set_error("Block contains reads < %dbp long !  Run DBsplit.", c->kmer);
             return -1;
+        }
+    // the kernels index the block by these offsets: read i ends with a 4 right before read i+1
+    if (b->nreads > 0 && b->boff[0] != 0)
+    {
+        gd_set_error("gd_load_block: read 0 must start at offset 0 (boff[0] = %lld)", (long long)b->boff[0]);
+        return -1;
+    }
+    for (int i = 0; i < b->nreads; i++)
+        if (b->boff[i + 1] != b->boff[i] + b->rlen[i] + 1 || b->rlen[i] > b->maxlen)
+        {
+            gd_set_error("gd_load_block: read %d is not laid out as Read_All_Sequences leaves it (boff %lld, rlen %d, "
+                         "next boff %lld, maxlen %d)",
+                         i, (long long)b->boff[i], b->rlen[i], (long long)b->boff[i + 1], b->maxlen);
+            return -1;
+        }
+    if (b->mask_anno)
+        for (int i = 0; i < b->nreads; i++)
+        {
+            const int64_t lo = b->mask_anno[i], hi = b->mask_anno[i + 1];
+            if (lo < 0 || hi < lo || ((hi - lo) & 1))
+            {
+                gd_set_error("gd_load_block: mask intervals of read %d are malformed (anno %lld .. %lld)", i,
+                             (long long)lo, (long long)hi);
+                return -1;
+            }
         }
     if (ensure(s.bases, nb + 1 + 64) || ensure(s.boff, (b->nreads + 1) * 8) || ensure(s.rlen, b->nreads * 4 + 4))
         return -1;
@@ -2237,6 +2270,33 @@ int gd_set_wave_limit(gd_context* c, int limit)
     }
     c->test_narrow = limit == gd::TEST_RING;
     return 0;
+}
+
+int gd_set_capacities(gd_context* c, int pebbles, int traces, int paths, int64_t records, int64_t trace_bytes)
+{
+    if (pebbles > 0)
+        c->pcap = pebbles;
+    if (traces > 0)
+        c->tcap = traces;
+    if (paths > 0)
+        c->mcap = paths;
+    if (records > 0)
+        c->rcap = (uint64_t)records;
+    if (trace_bytes > 0)
+        c->tbcap = (uint64_t)trace_bytes;
+    return 0;
+}
+
+int gd_test_wait_expiry(gd_context* c, int polls)
+{
+    if (polls < 1)
+    {
+        gd_set_error("gd_test_wait_expiry: polls must be positive");
+        return -2;
+    }
+    if (gd::radix_sort_test_wait_expiry(polls, c->s))
+        return -2;
+    return gd::radix_sort_wait_check(c->s);
 }
 
 int gd_get_stats(gd_context* c, gd_stats* st)

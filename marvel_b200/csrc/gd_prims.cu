@@ -358,10 +358,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
 }
 
 // bounded wait for the phase with the given parity; false if the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int polls = 1 << 22)
 {
     const uint32_t a = smem_addr(bar);
-    for (int it = 0; it < (1 << 22); it++)
+    for (int it = 0; it < polls; it++)
     {
         uint32_t done;
         asm volatile(
@@ -591,6 +591,37 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
         __syncthreads();
         toff = toff_next;
     }
+}
+
+// Test of the wait's expiry path: an mbarrier armed for 16 bytes that no copy will bring
+// (none is issued, so nothing is in flight when the block leaves), waited on with a short
+// limit; the expiry raises the same flag a stalled tile copy raises.
+__global__ void k_test_wait_expiry(int polls)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0)
+    {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        mbar_expect_tx(&bar, 16);
+    __syncthreads();
+    const bool ok = mbar_wait(&bar, 0, polls);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0)
+        atomicExch(&g_rs_wait_failed, 1);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar)) : "memory");
+}
+
+int radix_sort_test_wait_expiry(int polls, cudaStream_t s)
+{
+    k_test_wait_expiry<<<1, 32, 0, s>>>(polls);
+    GD_LAUNCHED(1);
+    GD_CUDA(cudaGetLastError());
+    return 0;
 }
 
 int radix_sort_wait_check(cudaStream_t s)

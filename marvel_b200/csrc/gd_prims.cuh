@@ -74,4 +74,11 @@ template <typename K>
 int radix_sort_keys(K* k0, K* k1, int64_t n, int begin_bit, int end_bit, void* scratch, cudaStream_t s,
                     const RsFinal* fin = nullptr);
 
+// 0, or -1 with the error set when a sort's bounded tile-copy wait ran out since the last
+// check (the flag is cleared); synchronizes s.
+int radix_sort_wait_check(cudaStream_t s);
+
+// Test hook: the wait's expiry path on an mbarrier no copy completes (see gd_test_wait_expiry).
+int radix_sort_test_wait_expiry(int polls, cudaStream_t s);
+
 }  // namespace gd

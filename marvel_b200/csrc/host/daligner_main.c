@@ -15,6 +15,7 @@
 #include <unistd.h>
 
 #include "dazz_db.h"
+#include "gd_report.h"
 #include "gpudalign.h"
 
 static void usage(void)
@@ -24,108 +25,6 @@ static void usage(void)
     fprintf(stderr, "         [-e<double(.70)] [-l<int(1000)>] [-s<int(100)>] [-H<int>] [-j<int>]\n");
     fprintf(stderr, "         [-m<track>]+ <subject:db|dam> <target:db|dam> ...\n");
     fprintf(stderr, "         [-r<int()1>]\n");
-}
-
-/* Print_Number (db/DB.c:193-240): the number with its digits grouped by commas, right-aligned
- * in width characters (0: no padding) */
-static void print_number(int64_t num, int width)
-{
-    char t[48];
-    long long n = (long long)num;
-    if (n < 1000ll)
-        snprintf(t, sizeof t, "%lld", n);
-    else if (n < 1000000ll)
-        snprintf(t, sizeof t, "%lld,%03lld", n / 1000ll, n % 1000ll);
-    else if (n < 1000000000ll)
-        snprintf(t, sizeof t, "%lld,%03lld,%03lld", n / 1000000ll, (n % 1000000ll) / 1000ll, n % 1000ll);
-    else
-        snprintf(t, sizeof t, "%lld,%03lld,%03lld,%03lld", n / 1000000000ll, (n % 1000000000ll) / 1000000ll,
-                 (n % 1000000ll) / 1000ll, n % 1000ll);
-    printf("%*s", width, t);
-}
-
-/* Sort_Kmers' report under -v and its memory warning (dalign/filter.c:754-759, 865-892):
- * the k-mer slots of the block, the index left after masking and -t. */
-static void report_index(gd_context* ctx, int slot, const dz_block* b, int kmer, int suppress, int64_t mem_limit,
-                         int mem_physical, int verbose)
-{
-    const int64_t slots = b->boff[b->nreads] - (int64_t)kmer * b->nreads;
-    if (slots <= 0)
-        return;
-    gd_stats st;
-    gd_get_stats(ctx, &st);
-    const int64_t kmers = st.kmers[slot];
-    if (verbose)
-    {
-        printf("\n   Kmer count = ");
-        print_number(slots, 0);
-        printf("\n   Using %.2fGb of space\n", (1. * slots) / 33554432);
-        if (suppress > 0)
-        {
-            printf("   Revised kmer count = ");
-            print_number(kmers, 0);
-            printf("\n");
-        }
-        printf("   Index occupies %.2fGb\n", (1. * kmers) / 67108864);
-        fflush(stdout);
-    }
-    if (kmers > 0 && mem_limit > 0 && kmers > mem_limit / 64)
-    {
-        fprintf(stderr, "Warning: Block size too big, index occupies more than 1/4 of");
-        if (mem_physical)
-            fprintf(stderr, " physical memory (%.1fGb)\n", (1. * mem_limit) / 0x40000000ll);
-        else
-            fprintf(stderr, " desired memory allocation (%.1fGb)\n", (1. * mem_limit) / 0x40000000ll);
-        fflush(stderr);
-    }
-}
-
-/* Match_Filter's report under -v (dalign/filter.c:2058-2063, 2105-2106, 2158-2162, 2180-2189,
- * 2388-2405): the pair cap, the hits, the Local_Alignment calls (seed hits) and the overlaps
- * they added (confirmed hits).  same_index: A's index also served as B's. */
-static void report_match(gd_context* ctx, const char* aname, const char* bname, int comp, int same_index, int bslot,
-                         int64_t recs_before, const dz_block* a, const dz_block* b, int kmer, int64_t mem_limit)
-{
-    gd_stats st;
-    gd_get_stats(ctx, &st);
-    int64_t tb = 0;
-    const int64_t recs = gd_num_overlaps(ctx, &tb);
-    const int64_t alen = st.kmers[0], blen = st.kmers[bslot];
-    int64_t nhits = 0, nfilt = 0, ncheck = 0;
-    if (comp)
-        printf("\nComparing %s to c(%s)\n", aname, bname);
-    else
-        printf("\nComparing %s to %s\n", aname, bname);
-    if (alen > 0 && blen > 0)
-    {
-        printf("\n");
-        if (mem_limit > 0)
-            printf("   Capping mutual k-mer matches over %d (effectively -t%d)\n", st.limit[comp],
-                   (int)sqrt(1. * st.limit[comp]));
-        nhits = st.hits[comp];
-        printf("   Hit count = ");
-        print_number(nhits, 0);
-        if (same_index || nhits >= blen)
-            printf("\n   Highwater of %.2fGb space\n", (1. * (alen + 2 * nhits)) / 67108864);
-        else
-            printf("\n   Highwater of %.2fGb space\n", (1. * (alen + blen + nhits)) / 67108864);
-        if (nhits > 0)
-        {
-            nfilt = st.seeds[comp];
-            ncheck = recs - recs_before;
-        }
-    }
-    const double atot = (double)a->totlen, btot = (double)b->totlen;
-    int width = nhits <= 0 ? 1 : (int)log10((double)nhits) + 1;
-    width += (width - 1) / 3;
-    printf("\n     ");
-    print_number(nhits, width);
-    printf(" %d-mers (%e of matrix)\n     ", kmer, (1. * nhits / atot) / btot);
-    print_number(nfilt, width);
-    printf(" seed hits (%e of matrix)\n     ", (1. * nfilt / atot) / btot);
-    print_number(ncheck, width);
-    printf(" confirmed hits (%e of matrix)\n", (1. * ncheck / atot) / btot);
-    fflush(stdout);
 }
 
 static int64_t num_overlaps(gd_context* ctx)
@@ -213,6 +112,7 @@ static void load(dz_block* b, const char* name, char** mask, int mtop, int kmer)
         if (dz_add_mask(b, mask[i], err, sizeof err))
         {
             printf("[ERROR] - Unable to load track %s!\n", mask[i]);
+            fprintf(stderr, "daligner: %s\n", err);
             exit(1);
         }
     for (int i = 0; i < b->nreads; i++)
@@ -323,6 +223,11 @@ int main(int argc, char* argv[])
     MINOVER *= 2;
 
     const int MEM_PHYSICAL = MEM_LIMIT == MEM_PHYSICAL_BYTES;
+    /* the subject block is read before the device is touched: a malformed DB or track is
+       reported (exit 1) on any machine */
+    const char* afile = argv[optind];
+    dz_block A, B;
+    load(&A, afile, MASK, MTOP, KMER_LEN);
     gd_context* ctx = gd_create();
     if (!ctx)
     {
@@ -333,9 +238,6 @@ int main(int argc, char* argv[])
     GPU(gd_set_globals(ctx, MINOVER, IDENTITY, (uint64_t)MEM_LIMIT));
     GPU(gd_set_biased(ctx, BIASED));
 
-    const char* afile = argv[optind];
-    dz_block A, B;
-    load(&A, afile, MASK, MTOP, KMER_LEN);
     char aroot[1024], broot[1024];
     root_of(afile, aroot, sizeof aroot);
     optind++;
@@ -375,7 +277,7 @@ int main(int argc, char* argv[])
             if (VERBOSE)
                 printf("\nBuilding index for %s\n", aroot);
             GPU(gd_sort_kmers(ctx, 0));
-            report_index(ctx, 0, &A, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
+            gd_report_index(ctx, 0, A.boff[A.nreads] - (int64_t)KMER_LEN * A.nreads, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
         }
         if (strcmp(afile, bfile) != 0)
         {
@@ -388,20 +290,20 @@ int main(int argc, char* argv[])
             if (VERBOSE)
                 printf("\nBuilding index for %s\n", broot);
             GPU(gd_sort_kmers(ctx, 1));
-            report_index(ctx, 1, &B, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
+            gd_report_index(ctx, 1, B.boff[B.nreads] - (int64_t)KMER_LEN * B.nreads, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
             int64_t r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 1, 0, 0));
             if (VERBOSE)
-                report_match(ctx, aroot, broot, 0, 0, 1, r0, &A, &B, KMER_LEN, MEM_LIMIT);
+                gd_report_match(ctx, aroot, broot, 0, 0, 1, r0, (double)A.totlen, (double)B.totlen, KMER_LEN, MEM_LIMIT);
             GPU(gd_complement_block(ctx, 1, 2));
             if (VERBOSE)
                 printf("\nBuilding index for c(%s)\n", broot);
             GPU(gd_sort_kmers(ctx, 2));
-            report_index(ctx, 2, &B, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
+            gd_report_index(ctx, 2, B.boff[B.nreads] - (int64_t)KMER_LEN * B.nreads, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
             r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 2, 1, 0));
             if (VERBOSE)
-                report_match(ctx, aroot, broot, 1, 0, 2, r0, &A, &B, KMER_LEN, MEM_LIMIT);
+                gd_report_match(ctx, aroot, broot, 1, 0, 2, r0, (double)A.totlen, (double)B.totlen, KMER_LEN, MEM_LIMIT);
             int lastRead = (B.part < A.part) ? B.ufirst + B.nreads - 1 : A.ufirst + A.nreads - 1;
             GPU(gd_write_overlap_buffer(ctx, RUN_ID, aroot, broot, lastRead));
             dz_free(&B);
@@ -411,16 +313,16 @@ int main(int argc, char* argv[])
             int64_t r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 0, 0, 1));
             if (VERBOSE)
-                report_match(ctx, aroot, aroot, 0, 1, 0, r0, &A, &A, KMER_LEN, MEM_LIMIT);
+                gd_report_match(ctx, aroot, aroot, 0, 1, 0, r0, (double)A.totlen, (double)A.totlen, KMER_LEN, MEM_LIMIT);
             GPU(gd_complement_block(ctx, 0, 2));
             if (VERBOSE)
                 printf("\nBuilding index for c(%s)\n", aroot);
             GPU(gd_sort_kmers(ctx, 2));
-            report_index(ctx, 2, &A, KMER_LEN, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
+            gd_report_index(ctx, 2, A.boff[A.nreads] - (int64_t)KMER_LEN * A.nreads, MAX_REPS, MEM_LIMIT, MEM_PHYSICAL, VERBOSE);
             r0 = num_overlaps(ctx);
             GPU(gd_match_filter(ctx, 2, 1, 1));
             if (VERBOSE)
-                report_match(ctx, aroot, aroot, 1, 0, 2, r0, &A, &A, KMER_LEN, MEM_LIMIT);
+                gd_report_match(ctx, aroot, aroot, 1, 0, 2, r0, (double)A.totlen, (double)A.totlen, KMER_LEN, MEM_LIMIT);
             GPU(gd_write_overlap_buffer(ctx, RUN_ID, aroot, aroot, A.ufirst + A.nreads - 1));
         }
         GPU(gd_reset_overlap_buffer(ctx));

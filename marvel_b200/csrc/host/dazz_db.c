@@ -289,6 +289,12 @@ static int read_track_file(dz_block* b, const char* track, int64_t** anno_out, i
     }
     {
         int64_t off = anno[0];
+        /* byte offsets of (begin, end) int pairs: non-decreasing, whole pairs per read */
+        for (int i = 0; i < n; i++)
+            if (anno[i + 1] < anno[i] || (anno[i + 1] - anno[i]) % 8 != 0)
+                goto junk;
+        if (off < 0)
+            goto junk;
         for (int i = 0; i <= n; i++)
             anno[i] = (anno[i] - off) / 4; /* bytes -> ints (dalign/daligner.c:425-428) */
         int64_t cnt = anno[n];

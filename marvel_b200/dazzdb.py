@@ -299,3 +299,81 @@ def las_equal(path_a, path_b, key="overlap", pad=False):
     onlya = [k for k in ka if k not in sb]
     onlyb = [k for k in kb if k not in sa]
     return False, f"{len(onlya)} records only in {path_a}, {len(onlyb)} only in {path_b}; first: {onlya[:1]} vs {onlyb[:1]}"
+
+
+def read_las_arrays(path):
+    """Like read_las, as flat arrays for large files: (tspace, records of LAS_REC_DTYPE,
+    trace bytes as stored, byte offset of each record's trace in them)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    novl = int(np.frombuffer(data[0:8], "<i8")[0])
+    tspace = int(np.frombuffer(data[8:12], "<i4")[0])
+    tbytes = 1 if tspace <= 125 else 2
+    offs = np.empty(novl, np.int64)
+    off = 12
+    from_bytes = int.from_bytes
+    for i in range(novl):
+        offs[i] = off
+        off += 40 + from_bytes(data[off:off + 4], "little", signed=True) * tbytes
+    assert off == len(data), (off, len(data))
+    raw = np.frombuffer(data, np.uint8)
+    recs = raw[offs[:, None] + np.arange(40)].copy().view(LAS_REC_DTYPE).reshape(novl)
+    nb = recs["tlen"].astype(np.int64) * tbytes
+    toff = np.zeros(novl, np.int64)
+    if novl:
+        toff[1:] = np.cumsum(nb)[:-1]
+    idx = np.repeat(offs + 40 - toff, nb) + np.arange(int(nb.sum()), dtype=np.int64)
+    return tspace, recs, raw[idx].copy(), toff
+
+
+def las_digest(recs, trace_bytes, toff, tbytes=1):
+    """Order-free SHA-256 of an overlap set: every record's nine fields (tlen, diffs, abpos,
+    bbpos, aepos, bepos, flags, aread, bread -- the pad word is left out, it is uninitialised
+    in daligner's files) and its trace bytes, over the records sorted by all of them.  Two
+    .las files (or a file and an in-memory buffer) have equal digests exactly when they hold
+    the same records, whatever the order among tied sort keys.  recs: any structured array
+    with those fields; toff: each record's byte offset into trace_bytes.  Returns
+    (hex digest, record count)."""
+    import hashlib
+    names = ("tlen", "diffs", "abpos", "bbpos", "aepos", "bepos", "flags", "aread", "bread")
+    n = int(recs.size)
+    fixed = np.empty((n, 9), np.int64)
+    for j, f in enumerate(names):
+        fixed[:, j] = recs[f]
+    # primary key first: aread, bread, flags, abpos, aepos, bbpos, bepos, diffs, tlen
+    keyorder = (7, 8, 6, 2, 4, 3, 5, 1, 0)
+    order = np.lexsort(tuple(fixed[:, j] for j in reversed(keyorder)))
+    fixed = fixed[order]
+    toff = np.asarray(toff, np.int64)[order]
+    nb = fixed[:, 0] * tbytes
+    tb = np.asarray(trace_bytes, np.uint8)
+
+    def trace_of(i):
+        return tb[toff[i]:toff[i] + nb[i]].tobytes()
+    # records whose nine fields all tie are ordered by their trace bytes
+    if n > 1:
+        same = np.all(fixed[1:] == fixed[:-1], axis=1)
+        i = 0
+        tied = np.nonzero(same)[0]
+        while i < tied.size:
+            j = i
+            while j + 1 < tied.size and tied[j + 1] == tied[j] + 1:
+                j += 1
+            lo, hi = int(tied[i]), int(tied[j]) + 2
+            sub = sorted(range(lo, hi), key=trace_of)
+            order_sub = np.asarray(sub, np.int64)
+            toff[lo:hi] = toff[order_sub]
+            i = j + 1
+    h = hashlib.sha256()
+    h.update(fixed.astype("<i4").tobytes())
+    ends = np.cumsum(nb)
+    idx = np.repeat(toff - (ends - nb), nb) + np.arange(int(nb.sum()), dtype=np.int64)
+    h.update(tb[idx].tobytes())
+    return h.hexdigest(), n
+
+
+def las_file_digest(path):
+    """las_digest of a .las file: (tspace, hex digest, record count)."""
+    tspace, recs, tb, toff = read_las_arrays(path)
+    d, n = las_digest(recs, tb, toff, 1 if tspace <= 125 else 2)
+    return tspace, d, n

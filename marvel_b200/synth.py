@@ -54,6 +54,11 @@ class Workload:
     genome: GenomeModel
     reads: ReadModel
     seed: int
+    # DB blocks (DBsplit -s<block_mbp>); 0 = the whole DB in one block.  nblocks > 0 generates
+    # only the reads of the first nblocks blocks: the reads come in random genome order, so
+    # these are exactly the first blocks of the full-coverage DB.
+    block_mbp: float = 0
+    nblocks: int = 0
 
 
 def _mutate_subs(rng, seq, rate):
@@ -172,14 +177,16 @@ def _apply_errors(rng, tmpl, rm: ReadModel):
     return res
 
 
-def make_reads(haps, rm: ReadModel, rng: np.random.Generator):
-    """Returns a list of uint8 reads (0..3)."""
+def make_reads(haps, rm: ReadModel, rng: np.random.Generator, max_bases: int = 0):
+    """Returns a list of uint8 reads (0..3); max_bases > 0 stops once the reads hold that
+    many bases (the same reads, in the same order, as the start of the full set)."""
     glen = haps[0].size
     mu, sigma = _lognormal_params(rm.mean_len, rm.sd_len)
     reads = []
     target = rm.coverage * glen
     total = 0
-    while total < target:
+    nbases = 0
+    while total < target and (max_bases <= 0 or nbases < max_bases):
         L = int(np.clip(np.round(rng.lognormal(mu, sigma)), rm.min_len, min(rm.max_len, glen)))
         h = haps[int(rng.integers(0, len(haps)))]
         L = min(L, h.size)
@@ -192,6 +199,7 @@ def make_reads(haps, rm: ReadModel, rng: np.random.Generator):
             continue
         reads.append(r)
         total += L
+        nbases += r.size
     return reads
 
 
@@ -208,6 +216,18 @@ WORKLOADS = {
     "cfg3": Workload("cfg3", GenomeModel(10_000_000),
                      ReadModel(30, 20000, 15000, 1000, 150000, p_ins=0.03, p_del=0.05, p_sub=0.02,
                                homopolymer_del_bias=3.0), seed=3),
+    # learned-triage evaluation: 20 Mbp with 10 % interspersed repeat families of 1-8 kbp at
+    # 5-15 % divergence, 30x PacBio-like reads, blocks of 200 Mbp (3 blocks)
+    "cfg4": Workload("cfg4", GenomeModel(20_000_000, interspersed_frac=0.10, interspersed_len=(1000, 8001),
+                                         interspersed_div=(0.05, 0.15)),
+                     ReadModel(30, 10000, 5000, 1000, 60000, **PACBIO), seed=4, block_mbp=200),
+    # large block pair: 200 Mbp diploid (0.5 % SNPs, 0.05 % short indels between the haplotypes),
+    # 35 % interspersed repeat families of 1-10 kbp at 5-15 % divergence, 2 % tandem repeats of
+    # period 2-200, 30x PacBio-like reads with mean 15 kbp; blocks of 400 Mbp, the first two
+    "cfg5": Workload("cfg5", GenomeModel(200_000_000, interspersed_frac=0.35, interspersed_len=(1000, 10001),
+                                         interspersed_div=(0.05, 0.15), tandem_frac=0.02, tandem_period=(2, 201),
+                                         diploid_snp=0.005, diploid_indel=0.0005),
+                     ReadModel(30, 15000, 7500, 1000, 100000, **PACBIO), seed=5, block_mbp=400, nblocks=2),
     # small cases for tests
     "tiny": Workload("tiny", GenomeModel(60_000),
                      ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=11),
@@ -243,7 +263,8 @@ def generate(w: Workload | str, scale: float = 1.0):
     if scale != 1.0:
         gm = dataclasses.replace(gm, length=max(20000, int(gm.length * scale)))
     haps = make_genome(gm, rng)
-    reads = make_reads(haps, w.reads, rng)
+    max_bases = int(w.nblocks * w.block_mbp * 1e6) if w.nblocks > 0 else 0
+    reads = make_reads(haps, w.reads, rng, max_bases)
     return reads, haps
 
 
@@ -257,8 +278,9 @@ def write_fasta(path, reads, width=0):
 
 
 def cached_db(workload: str, seed_offset: int = 0, scale: float = 1.0, cache: str | None = None):
-    """Writes (once) a one-block DB of a workload -- seed shifted by 1000 * seed_offset, genome
-    and repeat counts scaled by scale -- under cache and returns the path of block 1."""
+    """Writes (once) the DB of a workload -- seed shifted by 1000 * seed_offset, genome, repeat
+    counts and block size scaled by scale -- under cache and returns the path of block 1
+    (block n is the same path with its last number replaced)."""
     import os
     import tempfile
     from . import dazzdb
@@ -276,7 +298,8 @@ def cached_db(workload: str, seed_offset: int = 0, scale: float = 1.0, cache: st
         reads, _ = generate(w)
         tmp = d + f".tmp{os.getpid()}"
         os.makedirs(tmp, exist_ok=True)
-        dazzdb.write_db(os.path.join(tmp, "W"), reads, 100000)   # a single block
+        # a single block unless the workload is split (DBsplit -s<block_mbp>)
+        dazzdb.write_db(os.path.join(tmp, "W"), reads, w.block_mbp * scale if w.block_mbp else 100000)
         try:
             os.rename(tmp, d)
         except OSError:   # another process finished first

@@ -29,7 +29,10 @@ import numpy as np
 from . import TRI_NF, TRI_NPARAM, Context, _check, lib, run_loaded
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_MODEL = os.path.join(HERE, "models", "triage_cfg2.npz")
+DEFAULT_MODEL = os.path.join(HERE, "models", "triage_cfg12.npz")
+# the training blocks of the default model: the CPU-runnable and the bacterial-scale
+# workloads' models on other seeds than the benchmark's (seed offset 0), about 10^7 groups
+TRAIN_SPECS = (("cfg2", 1), ("cfg2", 2), ("cfg1", 1), ("cfg1", 2), ("cfg1", 3), ("cfg1", 4))
 
 
 @dataclass
@@ -136,27 +139,45 @@ def fit(ctx: Context, feat, records, *, recall=0.999, holdout=0.25, seed=1, **kw
 
 
 def train_on_workload(workload: str, seed_offset: int, out: str, recall: float = 0.999, epochs: int = 25,
-                      scale: float = 1.0):
+                      scale: float = 1.0, batch: int = 8192):
     """Collects the groups of one synthetic block compared with itself (bench's generator,
     another seed than the benchmark's), trains on the device and writes the model file."""
+    return train_on_workloads(((workload, seed_offset),), out, recall, epochs, scale, batch)
+
+
+def train_on_workloads(specs, out: str, recall: float = 0.999, epochs: int = 25, scale: float = 1.0,
+                       batch: int = 8192):
+    """Collects the groups of synthetic blocks, each compared with itself -- specs lists
+    (workload, seed offset) pairs, seed offsets other than the benchmark's 0 -- trains on
+    the device with mini-batches of batch groups and writes the model file and a .json
+    record of the training."""
     import json
     import time
 
     from . import daligner_block, dazzdb, synth
 
-    A = dazzdb.open_block(synth.cached_db(workload, seed_offset, scale))
     ctx = Context()
-    ctx.triage_reset()
-    ctx.triage_collect(True)
-    daligner_block(ctx, A)
-    ctx.triage_collect(False)
-    feat, rec, cells = ctx.triage_groups()
+    feats, recs = [], []
+    for workload, seed_offset in specs:
+        A = dazzdb.open_block(synth.cached_db(workload, seed_offset, scale))
+        ctx.triage_reset()
+        ctx.triage_collect(True)
+        daligner_block(ctx, A)
+        ctx.triage_collect(False)
+        feat, rec, _ = ctx.triage_groups()
+        feats.append(feat)
+        recs.append(rec)
+    feat = np.concatenate(feats)
+    rec = np.concatenate(recs)
     t0 = time.perf_counter()
-    model, info = fit(ctx, feat, rec, recall=recall, epochs=epochs)
+    model, info = fit(ctx, feat, rec, recall=recall, epochs=epochs, batch=batch)
     info["train_s"] = round(time.perf_counter() - t0, 2)
     info["groups"] = int(len(rec))
     info["positive_groups"] = int((rec > 0).sum())
-    info["trained_on"] = f"{workload} genome, seed offset {seed_offset}, scale {scale}"
+    info["batch"] = batch
+    info["epochs"] = epochs
+    info["trained_on"] = ", ".join(f"{w} genome seed offset {o}" for w, o in specs) + f" (scale {scale}); the "
+    info["trained_on"] += "benchmark's blocks are seed offset 0"
     ctx.close()
     model.save(out)
     with open(os.path.splitext(out)[0] + ".json", "w") as f:
@@ -165,18 +186,19 @@ def train_on_workload(workload: str, seed_offset: int, out: str, recall: float =
 
 
 def main(argv=None):
-    """python -m marvel_b200.triage train [--workload cfg2] [--seed-offset 1] [--out PATH]"""
+    """python -m marvel_b200.triage train [--workload cfg2:1 ...] [--batch 8192] [--out PATH]"""
     import argparse
     p = argparse.ArgumentParser(prog="marvel_b200.triage")
     p.add_argument("cmd", choices=["train"])
-    p.add_argument("--workload", default="cfg2")
-    p.add_argument("--seed-offset", type=int, default=1)
+    p.add_argument("--workload", action="append", help="workload:seed_offset (repeatable); default: TRAIN_SPECS")
     p.add_argument("--scale", type=float, default=1.0)
     p.add_argument("--recall", type=float, default=0.999)
     p.add_argument("--epochs", type=int, default=25)
+    p.add_argument("--batch", type=int, default=8192)
     p.add_argument("--out", default=DEFAULT_MODEL)
     a = p.parse_args(argv)
-    model, info = train_on_workload(a.workload, a.seed_offset, a.out, a.recall, a.epochs, a.scale)
+    specs = [(w.split(":")[0], int(w.split(":")[1])) for w in a.workload] if a.workload else TRAIN_SPECS
+    model, info = train_on_workloads(specs, a.out, a.recall, a.epochs, a.scale, a.batch)
     print(f"threshold {model.threshold:.4g}; calibration {info['calibration']}; {info['train_s']} s")
     return 0
 

@@ -76,10 +76,11 @@ def write_las(path, recs, traces, tspace):
             f.write(np.asarray(t).astype("<u1" if tb == 1 else "<u2").tobytes())
 
 
-def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1):
+def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1, ctx_hook=None, stats_out=None):
     """Runs `daligner flags blocks[0] blocks[1]` (variant 2: `daligner2 -Pout ...`) with impl in
     {"oracle", "gpu"}; returns the paths.  wave_limit (gpu only) sets the widest band of the
-    main aligner kernel (test hook)."""
+    main aligner kernel (test hook); ctx_hook (gpu only) is called with the new context;
+    stats_out (gpu only), a dict, receives the context's statistics after the run."""
     o = parse_flags(flags)
     aname, bname = blocks
     A = dazzdb.open_block(os.path.join(dbdir, aname))
@@ -110,6 +111,8 @@ def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1):
         ctx = mb.Context()
         if wave_limit is not None:
             ctx.set_wave_limit(wave_limit)
+        if ctx_hook is not None:
+            ctx_hook(ctx)
         if variant == 2:
             ctx.set_variant(2, o["H"])
         if o["b"]:
@@ -125,6 +128,8 @@ def run(dbdir, flags, blocks, outdir, impl, wave_limit=None, variant=1):
         else:
             mb.run_loaded(ctx, self_cmp)
         r, tr = ctx.overlaps()
+        if stats_out is not None:
+            stats_out.update(ctx.stats())
         ctx.close()
         tb = 1 if tspace <= 125 else 2
         recs = r

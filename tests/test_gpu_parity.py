@@ -248,33 +248,31 @@ def test_size_independent_properties_cfg2(mb, tmp_path):
         assert int(x["tlen"]) == 2 * npts
 
 
-@pytest.mark.parametrize("name", ["self_default", "pair_blocks", "self_s200_t20"])
-def test_compute_trace_pts_matches_oracle(mb, name):
+@pytest.mark.parametrize("name", cases())
+def test_compute_trace_pts_matches_reference(mb, name):
     """Compute_Trace_PTS (dalign/align.c:5286-5397) on the device: exact diffs of every
-    record of a reference .las file, against the oracle's restatement of iter_np."""
-    import oracle
+    record of every reference .las file of the goldens, against the diffs the reference's
+    own Compute_Trace_PTS computes (tests/golden/trace_pts.npz, from
+    tests/golden/make_trace_pts_golden.py).  The whole DB sits in one slot, its complement
+    in another."""
+    fx = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "trace_pts.npz"))
     d, meta = load(name)
-    aname, bname = meta["blocks"]
-    A = dazzdb.open_block(os.path.join(d, aname))
-    B = dazzdb.open_block(os.path.join(d, bname))
-    Bc = dazzdb.complement_block(B)
-    ts, recs, traces = dazzdb.read_las(os.path.join(d, meta["las"][0]))
-    tb = 1 if ts <= 125 else 2
-    rec = np.zeros(recs.size, mb.OVL_DTYPE)
-    for f in ("tlen", "diffs", "abpos", "bbpos", "aepos", "bepos", "flags", "aread", "bread"):
-        rec[f] = recs[f]
-    offs = np.cumsum([0] + [t.size * tb for t in traces])
-    rec["toff"] = offs[:-1]
-    tr = np.concatenate([t.view(np.uint8) if tb == 2 else t for t in traces]) if traces else np.zeros(1, np.uint8)
+    G = dazzdb.open_block(os.path.join(d, "G"))
     ctx = mb.Context()
-    ctx.new_align_spec(0.70, ts, A.freq)
-    ctx.load_block(0, A)
-    ctx.load_block(1, B)
-    ctx.complement_block(1, 2)
-    g = ctx.compute_trace_pts(rec, tr, 0, 1, 2)
+    for las in meta["las"]:
+        ts, recs, traces = dazzdb.read_las(os.path.join(d, las))
+        tb = 1 if ts <= 125 else 2
+        rec = np.zeros(recs.size, mb.OVL_DTYPE)
+        for f in ("tlen", "diffs", "abpos", "bbpos", "aepos", "bepos", "flags", "aread", "bread"):
+            rec[f] = recs[f]
+        offs = np.cumsum([0] + [t.size * tb for t in traces])
+        rec["toff"] = offs[:-1]
+        tr = np.concatenate([t.view(np.uint8) if tb == 2 else t for t in traces]) if traces else np.zeros(1, np.uint8)
+        ctx.new_align_spec(0.70, ts, G.freq)
+        ctx.load_block(0, G)
+        ctx.complement_block(0, 2)
+        g = ctx.compute_trace_pts(rec, tr, 0, 0, 2)
+        want = fx[f"{name}/{las}"]
+        bad = np.nonzero(g != want)[0]
+        assert bad.size == 0, (las, int(bad[0]), int(g[bad[0]]), int(want[bad[0]]))
     ctx.close()
-    for i in range(recs.size):
-        r = recs[i]
-        bb = (Bc if r["flags"] & 1 else B).read(int(r["bread"]) - B.ufirst)
-        o = oracle.trace_pts_diffs(A.read(int(r["aread"]) - A.ufirst), bb, r, traces[i], ts)
-        assert int(g[i]) == o, (i, int(g[i]), o)

@@ -78,3 +78,48 @@ def test_oracle_d2_bridging_matches_reference():
             assert all(np.array_equal(x, y) for (_, x), (_, y) in zip(gb, eb)), i
         bridged += dbc.was_bridged(c, (ea, eb))
     assert bridged >= len(cases) // 2
+
+
+def _trace_pts_fixture():
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "trace_pts.npz"))
+
+
+@pytest.mark.parametrize("name", cases())
+def test_oracle_trace_pts_matches_reference_compute_trace_pts(name):
+    """The restatement of Compute_Trace_PTS / iter_np (dalign/align.c:4556-4917, 5286-5397)
+    gives, on every record of every golden .las file, the diffs the reference's own
+    Compute_Trace_PTS computes (tests/golden/make_trace_pts_golden.py)."""
+    import oracle
+    fx = _trace_pts_fixture()
+    d, meta = load(name)
+    G = dazzdb.open_block(os.path.join(d, "G"))
+    Gc = dazzdb.complement_block(G)
+    for las in meta["las"]:
+        ts, recs, traces = dazzdb.read_las(os.path.join(d, las))
+        want = fx[f"{name}/{las}"]
+        assert want.size == recs.size
+        for i in range(recs.size):
+            r = recs[i]
+            bb = (Gc if r["flags"] & 1 else G).read(int(r["bread"]) - G.ufirst)
+            got = oracle.trace_pts_diffs(G.read(int(r["aread"]) - G.ufirst), bb, r, traces[i], ts)
+            assert got == int(want[i]), (las, i, got, int(want[i]))
+
+
+def test_oracle_matches_reference_on_full_cfg1_block():
+    """The restatement on the whole cfg1 block (1 Mbp genome, 20x; regenerated from its seed)
+    gives the records the reference daligner writes for it (digest of the reference's
+    .las, tests/golden/config_digests.json) and the reference's wave-cell count."""
+    import json
+    import oracle
+    from marvel_b200 import synth
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "config_digests.json")) as f:
+        want = json.load(f)["cfg1"]
+    A = dazzdb.open_block(synth.cached_db(want["workload"], want["seed_offset"], want["scale"]))
+    recs, traces, st = oracle.daligner(A, A, dazzdb.complement_block(A), oracle.make_params(A.freq), True)
+    toff = np.zeros(len(traces), np.int64)
+    if len(traces):
+        toff[1:] = np.cumsum([t.size for t in traces])[:-1]
+    tb = np.concatenate(traces).astype(np.uint8) if traces else np.zeros(0, np.uint8)
+    digest, n = dazzdb.las_digest(recs, tb, toff, 1)
+    assert n == want["novl"] and digest == want["sha256"]
+    assert st["cells"] == want["cells"]
