@@ -189,6 +189,8 @@ def run_gpu(args):
     ctx.new_align_spec(p["e"], p["s"], A.freq)
     ctx.set_globals(2 * p["l"], False, p["M"] * 0x40000000)
     ctx.set_biased(BIASED)
+    if args.schedule:
+        ctx.set_align_schedule([int(x) for x in args.schedule.split(",")])
 
     def barrier():
         torch.cuda.synchronize()
@@ -206,6 +208,10 @@ def run_gpu(args):
     ctx.load_block(0, A)
     if pair:
         ctx.load_block(1, B)
+    tuned = None
+    if args.autotune:
+        from marvel_b200 import autotune
+        tuned = autotune.tune(ctx, A, B)
     for _ in range(args.warmup):  # the same work as a timed step, so that every buffer is allocated
         ctx.reset_overlap_buffer()
         mb.run_loaded(ctx, not pair)
@@ -270,10 +276,24 @@ def run_gpu(args):
     # ---- learned triage (beside the exact path): the shipped model, trained on another genome
     tri = None
     from marvel_b200 import triage as mtri
-    if args.triage and os.path.exists(mtri.DEFAULT_MODEL):
-        model = mtri.TriageModel.load(mtri.DEFAULT_MODEL)
+    model_path = args.triage_model or mtri.DEFAULT_MODEL
+    if args.triage and os.path.exists(model_path):
+        model = mtri.TriageModel.load(model_path)
+        # one untimed plain run with collection: how the wave cells split between groups that
+        # yield records and groups that do not (the most any triage can skip), and the
+        # model's choices on those groups
+        ctx.triage_reset()
+        ctx.triage_collect(True)
+        ctx.reset_overlap_buffer()
+        mb.run_loaded(ctx, not pair)
+        ctx.triage_collect(False)
+        gfeat, grec, gcells = ctx.triage_groups()
+        ctx.triage_reset()
+        gprob = ctx.mlp_forward(model.params, gfeat)
+        gev = mtri.evaluate(gprob, grec, gcells, model.threshold)
+        dead = float(gcells[grec == 0].sum()) / max(float(gcells.sum()), 1.0)
         ctx.triage_set_model(model.params, model.threshold)
-        ttimes, trecs, tskip, tgroups = [], 0, 0, 0
+        ttimes, trecs, tskip, tgroups, talign = [], 0, 0, 0, 0.0
         for i in range(1 + args.steps):
             ctx.reset_overlap_buffer()
             ctx.timer_mark(0)
@@ -286,6 +306,7 @@ def run_gpu(args):
                 trecs += tst["records"]
                 tskip += sum(tst["skipped"])
                 tgroups += sum(tst["groups"])
+                talign += sum(tst["ms_align"])
         ctx.triage_set_model(None)
         barrier()
         t_ms_max, = reduce([sum(ttimes)], torch.distributed.ReduceOp.MAX if ws > 1 else None)
@@ -294,8 +315,12 @@ def run_gpu(args):
                "ms_per_step": round(t_ms_max / args.steps, 3),
                "record_recall": round(trecs / recs, 5) if recs else None,
                "groups_skipped": round(tskip / tgroups, 4) if tgroups else None,
-               "model": os.path.relpath(mtri.DEFAULT_MODEL, ROOT) + " (trained on the GPU on another genome of "
-                        "this workload's model, seed offset 1)",
+               "seed_scan_align_ms": round(talign / args.steps, 3),
+               "cells_skipped": round(gev["cells_skipped"], 4),
+               "cells_in_groups_without_records": round(dead, 4),
+               "bound": "skipping every group without records (and no other) would leave "
+                        f"{1 - dead:.3f} of the wave cells: at most {1 / max(1 - dead, 1e-9):.2f}x on the aligner",
+               "model": os.path.relpath(model_path, ROOT) + " (" + model_trained_on(model_path) + ")",
                "note": "records are a subset of the exact path's; recall < 1, so not the headline"}
     # ---- daligner2 (modimizer seeds) on the same resident block, beside the headline path
     d2 = None
@@ -389,6 +414,10 @@ def run_gpu(args):
             "e2e": {"value": round(e2e, 1), "unit": "overlaps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
+            "align_schedule": ("one launch per length class, alen+blen edges " + args.schedule) if args.schedule
+            else (f"autotuned: {tuned['chosen']}" if tuned
+                  else "one persistent launch, pair groups longest first from a device queue"),
+            "autotune": tuned,
             "triage": tri,
             "daligner2": d2,
             "clocks": clocks,
@@ -420,6 +449,14 @@ WORKLOAD_DESC = {
     "cfg5": "200 Mbp diploid (0.5% SNP, 0.05% indel), 35% interspersed 1-10 kbp repeats at 5-15%, 2% tandem "
             "repeats, 30x, mean 15 kbp; 400 Mbp block 1 vs 400 Mbp block 2 with -mdust",
 }
+
+
+def model_trained_on(model_path):
+    try:
+        with open(os.path.splitext(model_path)[0] + ".json") as f:
+            return "trained on the GPU on " + json.load(f)["trained_on"]
+    except (OSError, KeyError, ValueError):
+        return "trained on the GPU"
 
 
 def load_peaks():
@@ -588,6 +625,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-triage", dest="triage", action="store_false",
                     help="skip the learned-triage measurement (reported beside the exact path)")
+    ap.add_argument("--triage-model", default=None, help="model file (default: the shipped model)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="time the aligner schedules on the block first and run the fastest (marvel_b200.autotune)")
+    ap.add_argument("--schedule", default="",
+                    help="alen+blen edges (bp, comma-separated): one aligner launch per length class instead of "
+                         "the one persistent launch (a comparison schedule)")
     ap.add_argument("--no-d2", dest="d2", action="store_false",
                     help="skip the daligner2 (modimizer seeds) measurement (reported beside the exact path)")
     ap.add_argument("--biased", action="store_true",

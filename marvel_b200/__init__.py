@@ -63,7 +63,7 @@ SYMBOLS = ["gd_create", "gd_destroy", "gd_last_error", "gd_set_filter_params", "
            "gd_compute_trace_pts", "gd_triage_collect", "gd_triage_get_groups", "gd_triage_reset",
            "gd_triage_set_model", "gd_mlp_init", "gd_mlp_forward", "gd_mlp_grad", "gd_mlp_train", "gd_sort_overlaps", "gd_las_sort", "gd_dust", "gd_las_merge",
            "gd_set_wave_limit", "gd_set_variant", "gd_match_filter2", "gd_test_handle_redundancies_d2",
-           "gd_set_biased", "gd_set_capacities", "gd_test_wait_expiry"]
+           "gd_set_biased", "gd_set_capacities", "gd_test_wait_expiry", "gd_set_align_schedule"]
 
 TRI_NF = 12        # features per pair group
 TRI_NPARAM = 5081  # model parameter vector (gd_triage_set_model)
@@ -107,6 +107,7 @@ def lib():
     L.gd_set_wave_limit.argtypes = [C.c_void_p, C.c_int]
     L.gd_set_capacities.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64]
     L.gd_test_wait_expiry.argtypes = [C.c_void_p, C.c_int]
+    L.gd_set_align_schedule.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.gd_dust.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_float),
                           C.c_void_p, C.c_void_p, C.c_int64]
     L.gd_dust.restype = C.c_int64
@@ -344,6 +345,18 @@ class Context:
         and the alignment stage re-run."""
         _check(lib().gd_set_capacities(self.h, int(pebbles), int(traces), int(paths), int(records),
                                        int(trace_bytes)))
+
+    def set_align_schedule(self, edges=(), kinds=None):
+        """() = one persistent aligner launch over all pair groups (default); else one launch
+        per length class split at these alen + blen edges (bp); kinds (one per class, longest
+        first): 0 = the 128-diagonal warp instance, 1 = the 512-diagonal instance."""
+        e = np.ascontiguousarray(edges, np.int32)
+        k = None if kinds is None else np.ascontiguousarray(kinds, np.int32)
+        if k is not None and k.size != e.size + 1:
+            raise ValueError("one instance kind per length class (len(edges) + 1)")
+        self._sched = (e, k)   # keep the arrays alive for the call
+        _check(lib().gd_set_align_schedule(self.h, int(e.size), e.ctypes.data if e.size else None,
+                                           k.ctypes.data if k is not None else None))
 
     def test_wait_expiry(self, polls):
         """Test hook: the radix sort's bounded mbarrier wait run out on a copy never issued;

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -182,6 +183,10 @@ struct gd_context
     DevBuf ascr_w, wide;  // the wide aligner instance's scratch, and its group list + count
     int agrid_w = 0;
     int test_narrow = 0;  // tests only: the main aligner pass with the 32-diagonal instance
+    // aligner schedule: empty = every pair group in one persistent launch (longest first from
+    // the device queue); else one launch per length class, split at these alen + blen edges
+    std::vector<int32_t> sched_edges;
+    std::vector<int32_t> sched_kind;  // per length class (longest first): 0 = RING instance, 1 = WIDE_RING
     int variant = 1, hgap = 0;  // 2 = daligner2 (modimizer seeds, dalign2/), its -H
     int biased = 0;             // daligner -b: frequency-weighted tuples
     // -b: the reads' first chunks, tuples per chunk (then offsets), unpacked (read, position)
@@ -966,6 +971,25 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     if (gw < 0)
         return -1;
     uint32_t* order = gw ? P<uint32_t>(c->gidx2) : P<uint32_t>(c->gidx);
+    // per-length-class launches (the comparison schedule): each class is a contiguous range of
+    // the cost-sorted order, found from the sorted keys ~(alen + blen)
+    std::vector<unsigned> bucket{0u};
+    if (!c->sched_edges.empty() && ng > 0)
+    {
+        std::vector<uint32_t> keys(ng);
+        GD_CUDA(cudaMemcpyAsync(keys.data(), gw ? P<uint32_t>(c->gcost2) : P<uint32_t>(c->gcost), (size_t)ng * 4,
+                                cudaMemcpyDeviceToHost, s));
+        GD_CUDA(cudaStreamSynchronize(s));
+        std::vector<int32_t> edges = c->sched_edges;
+        std::sort(edges.begin(), edges.end(), std::greater<int32_t>());
+        for (int32_t e : edges)
+        {
+            unsigned p = (unsigned)(std::upper_bound(keys.begin(), keys.end(), ~(uint32_t)e) - keys.begin());
+            if (p > bucket.back() && p < ng)
+                bucket.push_back(p);
+        }
+    }
+    bucket.push_back(ng);
     // learned triage: group features, MLP, skip flags (one launch)
     const uint8_t* skip = nullptr;
     unsigned* d_nskip = P<unsigned>(c->misc) + 32;
@@ -1051,10 +1075,37 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
         GD_CUDA(cudaMemsetAsync(d_nwide, 0, 4, s));
         AlignOut out{P<OutRec>(c->outrec), P<uint8_t>(c->outtr), P<unsigned long long>(c->counters), c->rcap,
                      c->tbcap, skip, c->tri_collect ? P<uint2>(c->tri_gstat) : nullptr, wide_list, d_nwide};
+        // a length class the schedule gives to the wide instance runs there directly, with the
+        // wide instance's scratch
+        bool any_wide = false;
+        for (size_t b = 0; b + 1 < bucket.size(); b++)
+            any_wide |= b < c->sched_kind.size() && c->sched_kind[b] == 1;
+        AlignScratch scw0{};
+        if (any_wide)
+        {
+            const size_t need_w =
+                align_scratch_bytes(nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
+            if (ensure(c->ascr_w, need_w))
+                return -1;
+            align_scratch_carve(&scw0, c->ascr_w.p, nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap,
+                                btcap);
+            GD_CUDA(cudaMemsetAsync(scw0.bands, 0, (size_t)nwarps_w * 3 * nbands * 4, s));
+        }
         GD_CUDA(cudaEventRecord(c->ev0, s));
-        if (launch_align_pairs(A.blk, B.blk, hkey, hdiag, P<uint2>(c->groups), order, ng, ap, sc, out,
-                               P<unsigned>(c->queue), P<DevStatus>(c->status), c->agrid, s, 0))
-            return -1;
+        for (size_t b = 0; b + 1 < bucket.size(); b++)
+        {
+            const bool wide_class = b < c->sched_kind.size() && c->sched_kind[b] == 1;
+            AlignOut o2 = out;
+            if (wide_class)
+            {
+                o2.wide_list = nullptr;
+                o2.nwide = nullptr;
+            }
+            if (launch_align_pairs(A.blk, B.blk, hkey, hdiag, P<uint2>(c->groups), order + bucket[b],
+                                   bucket[b + 1] - bucket[b], ap, wide_class ? scw0 : sc, o2, P<unsigned>(c->queue),
+                                   P<DevStatus>(c->status), wide_class ? c->agrid_w : c->agrid, s, wide_class))
+                return -1;
+        }
         // pair groups whose band outgrew the main instance: the wide one, appending to the same
         // output with its own scratch (a band wider than WIDE_RING is an error there)
         unsigned nwide = 0;
@@ -2284,6 +2335,26 @@ int gd_set_capacities(gd_context* c, int pebbles, int traces, int paths, int64_t
         c->rcap = (uint64_t)records;
     if (trace_bytes > 0)
         c->tbcap = (uint64_t)trace_bytes;
+    return 0;
+}
+
+int gd_set_align_schedule(gd_context* c, int nedges, const int32_t* edges, const int32_t* kind)
+{
+    if (nedges < 0 || (nedges > 0 && !edges))
+    {
+        gd_set_error("gd_set_align_schedule: bad edge list");
+        return -1;
+    }
+    for (int i = 0; kind && i <= nedges; i++)
+        if (kind[i] != 0 && kind[i] != 1)
+        {
+            gd_set_error("gd_set_align_schedule: instance %d of class %d is neither 0 nor 1", kind[i], i);
+            return -1;
+        }
+    c->sched_edges.assign(edges, edges + nedges);
+    c->sched_kind.clear();
+    if (nedges > 0 && kind)
+        c->sched_kind.assign(kind, kind + nedges + 1);
     return 0;
 }
 

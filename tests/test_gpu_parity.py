@@ -276,3 +276,16 @@ def test_compute_trace_pts_matches_reference(mb, name):
         bad = np.nonzero(g != want)[0]
         assert bad.size == 0, (las, int(bad[0]), int(g[bad[0]]), int(want[bad[0]]))
     ctx.close()
+
+
+@pytest.mark.parametrize("name,kinds", [("self_long_panels", None), ("self_default", None),
+                                        ("self_long_panels", [1, 1, 0, 0, 0]), ("self_default", [0, 0, 1, 0, 1])])
+def test_length_class_schedule_gives_the_same_output(mb, name, kinds, tmp_path):
+    """One aligner launch per length class (gd_set_align_schedule) instead of the one
+    persistent launch, some classes on the wide instance: the same .las files."""
+    d, meta = load(name)
+    names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "gpu",
+                             ctx_hook=lambda ctx: ctx.set_align_schedule([8000, 20000, 60000, 150000], kinds))
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
+        assert ok, f"{name} {n}: {msg}"
