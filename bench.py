@@ -45,10 +45,13 @@ FLAGS = "-k14 -w6 -h35 -e.70 -l1000 -s100 -M32"
 BIASED = False  # --biased: daligner -b on both arms
 
 
-# workloads whose comparison is block 1 against block 2 with mask tracks (-m), the rest are
-# one block against itself
-MASKS = {"cfg5": ["dust"]}
+# a workload with two blocks generated compares block 1 against block 2, the rest one block
+# against itself; synth.Workload.masks names the tracks daligner masks with (-m)
 WORKLOAD = "cfg2"
+
+
+def masks_of(workload=None):
+    return list(synth.WORKLOADS[workload or WORKLOAD].masks)
 
 
 def is_pair(workload=None):
@@ -56,7 +59,7 @@ def is_pair(workload=None):
 
 
 def flag_str():
-    return ("-b " if BIASED else "") + "".join(f"-m{m} " for m in MASKS.get(WORKLOAD, [])) + FLAGS
+    return ("-b " if BIASED else "") + "".join(f"-m{m} " for m in masks_of()) + FLAGS
 
 
 def comparison():
@@ -78,34 +81,20 @@ def make_db(workload, seed_offset=0, scale=1.0):
     return synth.cached_db(workload, seed_offset, scale, CACHE)
 
 
-def dust_track(path, on_gpu):
-    """The dust track of the workload's DB (whole DB), made once: on the GPU arm by this
-    package's device DBdust, on the reference arm by the reference DBdust (the two write the
-    same bytes)."""
+def dust_track(path):
+    """The dust track of the workload's DB (whole DB) for the reference arm, made once by the
+    reference DBdust unless the GPU arm's device DBdust already wrote it (the same bytes)."""
     root = path.rsplit(".", 1)[0]
     if os.path.exists(os.path.join(os.path.dirname(root), "." + os.path.basename(root) + ".dust.anno")):
         return
-    if on_gpu:
-        from marvel_b200 import dbdust
-        dbdust.dust_db(root)
-    else:
-        subprocess.run([ref_binary("DBdust"), os.path.basename(root)], cwd=os.path.dirname(root), check=True,
-                       stdout=subprocess.DEVNULL)
+    subprocess.run([ref_binary("DBdust"), os.path.basename(root)], cwd=os.path.dirname(root), check=True,
+                   stdout=subprocess.DEVNULL)
 
 
 def load_blocks(workload, seed_offset=0):
     """(A, B) of a workload: B is None for a block against itself; mask tracks loaded."""
-    path = make_db(workload, seed_offset)
-    masks = MASKS.get(workload, [])
-    if masks:
-        dust_track(path, True)
-    A = dazzdb.open_block(path)
-    B = dazzdb.open_block(path[:-2] + ".2") if is_pair(workload) else None
-    for m in masks:
-        for blk in (A, B):
-            if blk is not None:
-                dazzdb.load_track(blk, m)
-    return A, B
+    from marvel_b200 import workloads
+    return workloads.blocks(workload, seed_offset, 1.0, CACHE)
 
 
 class ClockSampler:
@@ -488,9 +477,9 @@ def run_reference_once(path, threads, h=35, prog="daligner"):
     d = os.path.dirname(path)
     name = os.path.basename(path)
     bname = name[:-2] + ".2" if is_pair() else name
-    masks = [f"-m{m}" for m in MASKS.get(WORKLOAD, [])]
+    masks = [f"-m{m}" for m in masks_of()]
     if masks:
-        dust_track(path, False)
+        dust_track(path)
     if prog == "daligner2":
         cmd = [b, f"-T{threads}", "-Pd2out", "-M32", "-k14", "-w6", f"-h{h}", "-e.70", "-l1000", "-s100", name, name]
         las = [os.path.join(d, "d2out_00001", "W.1.W.1.las")]

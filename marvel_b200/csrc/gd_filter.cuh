@@ -135,11 +135,39 @@ int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread
 int launch_hit_unpack(const uint64_t* packed, int64_t n, HitBits hb, uint64_t* hkey, uint32_t* hdiag, cudaStream_t s);
 
 // Pair groups of the sorted hits: start flags, then (start, end) of groups with >= minhit hits.
+// With band_need > 0 a group is also dropped when no two adjacent diagonal bands (diag >>
+// binshift) hold band_need of its hits: a band score adds at most k per hit
+// (dalign/filter.c:1757-1766) and a seed needs two adjacent bands to reach h (:1776-1781), so
+// such a group can fire no Local_Alignment and yields nothing -- the seed scan would only
+// have scanned it.  band_need = ceil(h / k); 0 keeps every group with >= minhit hits.
 int launch_pair_flags(const uint64_t* hkey, int64_t n, int pbits, uint32_t* flags, cudaStream_t s);
 int launch_pair_scatter(const uint32_t* flags, const uint32_t* pos, int64_t n, uint32_t* starts, cudaStream_t s);
 int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* hkey,
-                         HitBits hb, const int32_t* arlen, const int32_t* brlen, uint2* groups, uint32_t* cost,
-                         uint32_t* idx, unsigned int* ngroups, cudaStream_t s);
+                         const uint32_t* hdiag, int binshift, int band_need, HitBits hb, const int32_t* arlen,
+                         const int32_t* brlen, uint2* groups, uint32_t* cost, uint32_t* idx, unsigned int* ngroups,
+                         cudaStream_t s);
+
+// The band test above for one group [s, e) of hdiag (groups longer than 32 hits pass).
+__device__ __forceinline__ bool group_can_fire(const uint32_t* __restrict__ hdiag, uint32_t s, uint32_t e,
+                                               int binshift, int need)
+{
+    if (need <= 0 || e - s > 32)
+        return true;
+    for (uint32_t i = s; i < e; i++)
+    {
+        const int d = ((int)__ldg(hdiag + i)) >> binshift;
+        int lo = 0, hi = 0;  // hits in bands {d - 1, d} and {d, d + 1}
+        for (uint32_t j = s; j < e; j++)
+        {
+            const int x = ((int)__ldg(hdiag + j)) >> binshift;
+            lo += (x == d) | (x == d - 1);
+            hi += (x == d) | (x == d + 1);
+        }
+        if (lo >= need || hi >= need)
+            return true;
+    }
+    return false;
+}
 
 // DevBlock::pk from a block's byte buffer (buf 16-byte aligned): word i holds bytes
 // [16 i, 16 i + 16), byte j of them in bits 2j..2j+1 (low two bits: a 4 packs as 0)

@@ -955,10 +955,35 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
         ensure(c->gcost2, (size_t)nst * 4 + 8) || ensure(c->gidx2, (size_t)nst * 4 + 8))
         return -1;
     unsigned* d_ng = P<unsigned>(c->misc) + 28;
-    if (launch_pair_scatter(pflags, ppos, nhits, P<uint32_t>(c->starts), s) ||
-        launch_select_groups(P<uint32_t>(c->starts), nst, nhits, (c->hitmin - 1) / c->kmer + 1, hkey, hb,
-                             P<int32_t>(A.rlen), P<int32_t>(B.rlen), P<uint2>(c->groups), P<uint32_t>(c->gcost),
-                             P<uint32_t>(c->gidx), d_ng, s))
+    // with the learned triage on (or its features collected), group selection and the triage
+    // are one kernel: features, MLP and skip flag per kept group as it is selected
+    const bool triage = c->tri_on || c->tri_collect;
+    unsigned* d_nskip = P<unsigned>(c->misc) + 32;
+    if (triage)
+    {
+        if (ensure(c->tri_skip, (size_t)nst + 8) || ensure(c->tri_gstat, (size_t)nst * 8 + 8) ||
+            (c->tri_collect && ensure(c->tri_feat, (size_t)nst * TRI_NF * 4 + 64)))
+            return -1;
+        GD_CUDA(cudaMemsetAsync(d_nskip, 0, 4, s));
+    }
+    if (launch_pair_scatter(pflags, ppos, nhits, P<uint32_t>(c->starts), s))
+        return -1;
+    // daligner's seed test needs ceil(h/k) hits in two adjacent bands: groups without them are
+    // dropped here, exactly (daligner2's report keeps its own selection)
+    const int minhit = (c->hitmin - 1) / c->kmer + 1;
+    const int band_need = c->variant == 1 ? minhit : 0;
+    if (triage
+            ? launch_select_groups_triage(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, band_need, hb,
+                                          A.blk, B.blk, comp, c->minover, c->binshift,
+                                          A.has_mask ? P<int64_t>(A.manno) : nullptr,
+                                          A.has_mask ? P<int32_t>(A.mdata) : nullptr,
+                                          c->tri_on ? P<float>(c->tri_params) : nullptr, c->tri_thr,
+                                          c->tri_collect ? P<float>(c->tri_feat) : nullptr, P<uint2>(c->groups),
+                                          P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), P<uint8_t>(c->tri_skip), d_ng,
+                                          d_nskip, s)
+            : launch_select_groups(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, c->binshift, band_need,
+                                   hb, P<int32_t>(A.rlen), P<int32_t>(B.rlen), P<uint2>(c->groups),
+                                   P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), d_ng, s))
         return -1;
     unsigned ng = 0;
     GD_CUDA(cudaMemcpyAsync(&ng, d_ng, 4, cudaMemcpyDeviceToHost, s));
@@ -990,21 +1015,10 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
         }
     }
     bucket.push_back(ng);
-    // learned triage: group features, MLP, skip flags (one launch)
+    // the learned triage's skip flags came with the groups
     const uint8_t* skip = nullptr;
-    unsigned* d_nskip = P<unsigned>(c->misc) + 32;
-    if ((c->tri_on || c->tri_collect) && ng > 0)
+    if (triage && ng > 0)
     {
-        if (ensure(c->tri_skip, ng) || ensure(c->tri_gstat, (size_t)ng * 8) ||
-            (c->tri_collect && ensure(c->tri_feat, (size_t)ng * TRI_NF * 4)))
-            return -1;
-        GD_CUDA(cudaMemsetAsync(d_nskip, 0, 4, s));
-        if (launch_triage_groups(hkey, hdiag, P<uint2>(c->groups), ng, hb, A.blk, B.blk, comp, c->minover, c->binshift,
-                                 A.has_mask ? P<int64_t>(A.manno) : nullptr, A.has_mask ? P<int32_t>(A.mdata) : nullptr,
-                                 c->tri_on ? P<float>(c->tri_params) : nullptr, c->tri_thr,
-                                 c->tri_collect ? P<float>(c->tri_feat) : nullptr, P<uint8_t>(c->tri_skip),
-                                 d_nskip, s))
-            return -1;
         if (c->tri_on)
             skip = P<uint8_t>(c->tri_skip);
         if (c->tri_collect)

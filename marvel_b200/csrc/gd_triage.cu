@@ -381,52 +381,82 @@ __global__ void __launch_bounds__(MT) k_mlp_forward(const float* __restrict__ P,
     }
 }
 
-// Features, MLP and skip flags of the pair groups inside Match_Filter: one thread per group
-// computes its features, the warps run the MLP over the tile on tensor cores.  feat
-// (optional) receives the raw features; with P == nullptr only features are computed.
-__global__ void __launch_bounds__(MT) k_triage_groups(const uint64_t* __restrict__ hkey,
-                                                     const uint32_t* __restrict__ hdiag,
-                                                     const uint2* __restrict__ groups, unsigned ng, HitBits hb,
-                                                     DevBlock A, DevBlock B, int comp, int minover, int binshift,
-                                                     const int64_t* __restrict__ anno, const int32_t* __restrict__ mdata,
-                                                     const float* __restrict__ P, float thr, float* feat,
-                                                     uint8_t* skip, unsigned* nskip)
+// Pair-group selection fused with the triage (report_thread's minhit test,
+// dalign/filter.c:1699-1709, and the learned triage in one pass): each thread takes one run
+// start of the sorted hits, keeps the run when it has >= minhit hits, computes the kept
+// group's features from its hits, the CTA's warps run the MLP over the tile's 128 rows on
+// tensor cores, and the kept groups are written out (range, cost key, index) with their
+// skip flag (p < thr) and, when feat is given, their raw features.  With P == nullptr only
+// features are computed (collection).
+__global__ void __launch_bounds__(MT) k_select_groups_triage(
+    const uint32_t* __restrict__ starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* __restrict__ hkey,
+    const uint32_t* __restrict__ hdiag, int band_need, HitBits hb, DevBlock A, DevBlock B, int comp, int minover,
+    int binshift, const int64_t* __restrict__ anno, const int32_t* __restrict__ mdata, const float* __restrict__ P,
+    float thr, float* feat, uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
+    unsigned* nskip)
 {
     extern __shared__ __align__(16) unsigned char infer_smem_t[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(infer_smem_t);
     if (P)
         infer_load_weights(S, P);
     __syncthreads();
-    const unsigned ntiles = (ng + IR - 1) / IR;
+    const int64_t ntiles = (nstarts + IR - 1) / IR;
     unsigned cnt = 0;
-    for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        const unsigned g = tile * IR + threadIdx.x;
+        const int64_t g = tile * IR + threadIdx.x;
+        bool take = false;
+        uint32_t st = 0, en = 0, c = 0;
         float f[TRI_NF];
 #pragma unroll
         for (int j = 0; j < TRI_NF; j++)
             f[j] = 0.f;
-        if (g < ng)
+        if (g < nstarts)
         {
-            group_features(hkey, hdiag, groups[g], hb, A, B, comp, minover, binshift, anno, mdata, f);
+            st = starts[g];
+            en = (g + 1 < nstarts) ? starts[g + 1] : (uint32_t)nhits;
+            take = (int64_t)(en - st) >= minhit && group_can_fire(hdiag, st, en, binshift, band_need);
+            if (take)
+            {
+                const uint64_t k = hkey[st];
+                const int ar = (int)((k >> hb.pbits) & ((1ull << hb.abits) - 1));
+                const int br = (int)(k >> (hb.pbits + hb.abits));
+                c = (uint32_t)(A.rlen[ar] + B.rlen[br]);
+                group_features(hkey, hdiag, make_uint2(st, en), hb, A, B, comp, minover, binshift, anno, mdata, f);
+            }
+        }
+        bool drop = false;
+        if (P)
+        {
+            infer_put_row(S, threadIdx.x, f, take);
+            __syncthreads();
+            infer_rows(S);
+            __syncthreads();
+            drop = take && 1.f / (1.f + __expf(-S.z[threadIdx.x])) < thr;
+            __syncthreads();  // S.X and S.z are rewritten by the next tile
+        }
+        // compaction: a slot per kept group, one atomic per warp
+        const unsigned m = __ballot_sync(GD_FULL, take);
+        unsigned base = 0;
+        if (m)
+        {
+            if (lane_id() == 0)
+                base = atomicAdd(ngroups, (unsigned)__popc(m));
+            base = __shfl_sync(GD_FULL, base, 0);
+        }
+        if (take)
+        {
+            const unsigned slot = base + __popc(m & lanemask_lt());
+            groups[slot] = make_uint2(st, en);
+            cost[slot] = ~c;  // ascending sort of ~cost = longest pairs first
+            idx[slot] = slot;
+            skip[slot] = drop ? 1 : 0;
+            cnt += drop;
             if (feat)
 #pragma unroll
                 for (int j = 0; j < TRI_NF; j++)
-                    feat[(size_t)g * TRI_NF + j] = f[j];
+                    feat[(size_t)slot * TRI_NF + j] = f[j];
         }
-        if (!P)
-            continue;
-        infer_put_row(S, threadIdx.x, f, g < ng);
-        __syncthreads();
-        infer_rows(S);
-        __syncthreads();
-        if (g < ng)
-        {
-            bool drop = 1.f / (1.f + __expf(-S.z[threadIdx.x])) < thr;
-            skip[g] = drop ? 1 : 0;
-            cnt += drop;
-        }
-        __syncthreads();
     }
     if (P)
     {
@@ -604,9 +634,9 @@ static int infer_grid(int64_t ntiles)
         int dev = 0, nsm = 0, per = 0;
         GD_CUDA(cudaGetDevice(&dev));
         GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        GD_CUDA(cudaFuncSetAttribute((const void*)k_triage_groups, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        GD_CUDA(cudaFuncSetAttribute((const void*)k_select_groups_triage, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(InferSmem)));
-        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_triage_groups, MT, sizeof(InferSmem)));
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_select_groups_triage, MT, sizeof(InferSmem)));
         blocks = nsm * std::max(per, 1);
     }
     return (int)std::min<int64_t>(ntiles, blocks);
@@ -662,18 +692,25 @@ int launch_adam(float* params, const float* grad, float* m, float* v, int step, 
     return 0;
 }
 
-int launch_triage_groups(const uint64_t* hkey, const uint32_t* hdiag, const uint2* groups, unsigned ng, HitBits hb,
-                         const DevBlock& A, const DevBlock& B, int comp, int minover, int binshift,
-                         const int64_t* amask_anno, const int32_t* amask_data, const float* params, float threshold,
-                         float* feat, uint8_t* skip, unsigned* nskip, cudaStream_t s)
+int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit,
+                                const uint64_t* hkey, const uint32_t* hdiag, int band_need, HitBits hb,
+                                const DevBlock& A,
+                                const DevBlock& B, int comp, int minover, int binshift, const int64_t* amask_anno,
+                                const int32_t* amask_data, const float* params, float threshold, float* feat,
+                                uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
+                                unsigned* nskip, cudaStream_t s)
 {
-    if (ng == 0)
+    GD_CUDA(cudaMemsetAsync(ngroups, 0, sizeof(unsigned), s));
+    if (nstarts <= 0)
         return 0;
-    int grid = infer_grid((ng + IR - 1) / IR);
+    int grid = infer_grid((nstarts + IR - 1) / IR);
     if (grid <= 0)
         return -1;
-    k_triage_groups<<<grid, MT, sizeof(InferSmem), s>>>(hkey, hdiag, groups, ng, hb, A, B, comp, minover, binshift,
-                                                      amask_anno, amask_data, params, threshold, feat, skip, nskip);
+    k_select_groups_triage<<<grid, MT, sizeof(InferSmem), s>>>(starts, nstarts, nhits, minhit, hkey, hdiag, band_need,
+                                                             hb, A, B,
+                                                             comp, minover, binshift, amask_anno, amask_data, params,
+                                                             threshold, feat, groups, cost, idx, skip, ngroups,
+                                                             nskip);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;

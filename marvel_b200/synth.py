@@ -59,6 +59,8 @@ class Workload:
     # these are exactly the first blocks of the full-coverage DB.
     block_mbp: float = 0
     nblocks: int = 0
+    # interval tracks daligner masks with (-m), made by DBdust on the whole DB
+    masks: tuple = ()
 
 
 def _mutate_subs(rng, seq, rate):
@@ -227,7 +229,8 @@ WORKLOADS = {
     "cfg5": Workload("cfg5", GenomeModel(200_000_000, interspersed_frac=0.35, interspersed_len=(1000, 10001),
                                          interspersed_div=(0.05, 0.15), tandem_frac=0.02, tandem_period=(2, 201),
                                          diploid_snp=0.005, diploid_indel=0.0005),
-                     ReadModel(30, 15000, 7500, 1000, 100000, **PACBIO), seed=5, block_mbp=400, nblocks=2),
+                     ReadModel(30, 15000, 7500, 1000, 100000, **PACBIO), seed=5, block_mbp=400, nblocks=2,
+                     masks=("dust",)),
     # small cases for tests
     "tiny": Workload("tiny", GenomeModel(60_000),
                      ReadModel(12, 4000, 2000, 1000, 12000, **PACBIO), seed=11),

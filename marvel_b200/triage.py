@@ -185,11 +185,44 @@ def train_on_workloads(specs, out: str, recall: float = 0.999, epochs: int = 25,
     return model, info
 
 
+def calibrate_on_workload(model_path: str, workload: str, seed_offset: int, out: str, recall: float = 0.999):
+    """Keeps a model's weights and re-calibrates its threshold on the pair groups of another
+    genome of a workload's model (seed offset other than the benchmark's 0): the largest
+    threshold whose skipped groups hold at most 1 - recall of that genome's records.  Writes
+    the model file and a .json record."""
+    import json
+
+    from . import daligner_block, workloads
+
+    model = TriageModel.load(model_path)
+    A, B = workloads.blocks(workload, seed_offset)
+    ctx = Context()
+    ctx.triage_reset()
+    ctx.triage_collect(True)
+    daligner_block(ctx, A, B)
+    ctx.triage_collect(False)
+    feat, rec, cells = ctx.triage_groups()
+    prob = ctx.mlp_forward(model.params, feat)
+    ctx.close()
+    thr = calibrate(prob, rec, recall)
+    cal = TriageModel(model.params, thr, recall)
+    cal.save(out)
+    info = {"weights": os.path.basename(model_path), "calibrated_on": f"{workload} genome seed offset {seed_offset}",
+            "groups": int(len(rec)), "positive_groups": int((rec > 0).sum()), "threshold": thr,
+            "at_threshold": evaluate(prob, rec, cells, thr),
+            "at_training_threshold": evaluate(prob, rec, cells, model.threshold)}
+    with open(os.path.splitext(out)[0] + ".json", "w") as f:
+        json.dump(info, f, indent=1)
+    return cal, info
+
+
 def main(argv=None):
-    """python -m marvel_b200.triage train [--workload cfg2:1 ...] [--batch 8192] [--out PATH]"""
+    """python -m marvel_b200.triage train [--workload cfg2:1 ...] [--batch 8192] [--out PATH]
+    python -m marvel_b200.triage calibrate --model PATH --workload cfg5:1 [--recall 0.999] --out PATH"""
     import argparse
     p = argparse.ArgumentParser(prog="marvel_b200.triage")
-    p.add_argument("cmd", choices=["train"])
+    p.add_argument("cmd", choices=["train", "calibrate"])
+    p.add_argument("--model", default=DEFAULT_MODEL, help="calibrate: the model whose weights are kept")
     p.add_argument("--workload", action="append", help="workload:seed_offset (repeatable); default: TRAIN_SPECS")
     p.add_argument("--scale", type=float, default=1.0)
     p.add_argument("--recall", type=float, default=0.999)
@@ -198,6 +231,13 @@ def main(argv=None):
     p.add_argument("--out", default=DEFAULT_MODEL)
     a = p.parse_args(argv)
     specs = [(w.split(":")[0], int(w.split(":")[1])) for w in a.workload] if a.workload else TRAIN_SPECS
+    if a.cmd == "calibrate":
+        if len(specs) != 1 or not a.workload:
+            p.error("calibrate takes one --workload NAME:SEED_OFFSET")
+        cal, info = calibrate_on_workload(a.model, specs[0][0], specs[0][1], a.out, a.recall)
+        print(f"threshold {cal.threshold:.4g}; {info['at_threshold']}; at the training threshold "
+              f"{info['at_training_threshold']}")
+        return 0
     model, info = train_on_workloads(specs, a.out, a.recall, a.epochs, a.scale, a.batch)
     print(f"threshold {model.threshold:.4g}; calibration {info['calibration']}; {info['train_s']} s")
     return 0
