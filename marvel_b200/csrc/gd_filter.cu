@@ -814,8 +814,8 @@ int launch_pair_scatter(const uint32_t* flags, const uint32_t* pos, int64_t n, u
 
 __global__ void __launch_bounds__(FT) k_select_groups(const uint32_t* __restrict__ starts, int64_t nstarts,
                                                      int64_t nhits, int minhit, const uint64_t* __restrict__ hkey,
-                                                     const uint32_t* __restrict__ hdiag, int binshift, int band_need,
-                                                     HitBits hb, const int32_t* __restrict__ arlen,
+                                                     const uint32_t* __restrict__ hdiag, int binshift, int kmer,
+                                                     int hitmin, HitBits hb, const int32_t* __restrict__ arlen,
                                                      const int32_t* __restrict__ brlen, uint2* groups, uint32_t* cost,
                                                      uint32_t* idx, unsigned int* ngroups)
 {
@@ -826,7 +826,7 @@ __global__ void __launch_bounds__(FT) k_select_groups(const uint32_t* __restrict
     {
         s = starts[g];
         e = (g + 1 < nstarts) ? starts[g + 1] : (uint32_t)nhits;
-        take = (int64_t)(e - s) >= minhit && group_can_fire(hdiag, s, e, binshift, band_need);
+        take = (int64_t)(e - s) >= minhit && group_can_fire(hkey, hdiag, s, e, hb.pbits, binshift, kmer, hitmin, minhit);
         if (take)
         {
             uint64_t k = hkey[s];
@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(FT) k_select_groups(const uint32_t* __restrict
 }
 
 int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* hkey,
-                         const uint32_t* hdiag, int binshift, int band_need, HitBits hb, const int32_t* arlen,
+                         const uint32_t* hdiag, int binshift, int kmer, int hitmin, HitBits hb, const int32_t* arlen,
                          const int32_t* brlen, uint2* groups, uint32_t* cost, uint32_t* idx, unsigned int* ngroups,
                          cudaStream_t s)
 {
@@ -861,7 +861,7 @@ int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits,
     if (nstarts <= 0)
         return 0;
     k_select_groups<<<(unsigned)gd_cdiv<int64_t>(nstarts, FT), FT, 0, s>>>(
-        starts, nstarts, nhits, minhit, hkey, hdiag, binshift, band_need, hb, arlen, brlen, groups, cost, idx, ngroups);
+        starts, nstarts, nhits, minhit, hkey, hdiag, binshift, kmer, hitmin, hb, arlen, brlen, groups, cost, idx, ngroups);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;

@@ -135,36 +135,80 @@ int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread
 int launch_hit_unpack(const uint64_t* packed, int64_t n, HitBits hb, uint64_t* hkey, uint32_t* hdiag, cudaStream_t s);
 
 // Pair groups of the sorted hits: start flags, then (start, end) of groups with >= minhit hits.
-// With band_need > 0 a group is also dropped when no two adjacent diagonal bands (diag >>
-// binshift) hold band_need of its hits: a band score adds at most k per hit
-// (dalign/filter.c:1757-1766) and a seed needs two adjacent bands to reach h (:1776-1781), so
-// such a group can fire no Local_Alignment and yields nothing -- the seed scan would only
-// have scanned it.  band_need = ceil(h / k); 0 keeps every group with >= minhit hits.
+// With hitmin > 0 a group of at most 32 hits is also dropped when the seed scan would find no
+// candidate seed in it (group_can_fire): such a group fires no Local_Alignment and yields
+// nothing, the scan would only have read its hits.  hitmin = 0 keeps every group with >=
+// minhit hits.
 int launch_pair_flags(const uint64_t* hkey, int64_t n, int pbits, uint32_t* flags, cudaStream_t s);
 int launch_pair_scatter(const uint32_t* flags, const uint32_t* pos, int64_t n, uint32_t* starts, cudaStream_t s);
 int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* hkey,
-                         const uint32_t* hdiag, int binshift, int band_need, HitBits hb, const int32_t* arlen,
+                         const uint32_t* hdiag, int binshift, int kmer, int hitmin, HitBits hb, const int32_t* arlen,
                          const int32_t* brlen, uint2* groups, uint32_t* cost, uint32_t* idx, unsigned int* ngroups,
                          cudaStream_t s);
 
-// The band test above for one group [s, e) of hdiag (groups longer than 32 hits pass).
-__device__ __forceinline__ bool group_can_fire(const uint32_t* __restrict__ hdiag, uint32_t s, uint32_t e,
-                                               int binshift, int need)
+// the seed scan's panels: a-position windows of 50,000 overlapping by 10,000 (filter.c:1717-1745)
+constexpr int GD_PANEL_SIZE = 50000;
+constexpr int GD_PANEL_OVERLAP = 10000;
+
+// Whether the seed scan of report_thread (dalign/filter.c:1717-1781) finds a candidate seed in
+// the group [s, e) of the sorted hits: per panel (a panel with fewer than minhit hits is
+// skipped), each diagonal band (diag >> binshift) scores the sum over its hits of min(k,
+// apos - the band's previous apos in the panel, 0 for its first), and a hit is a candidate when
+// its band and a neighbouring band together reach hitmin.  The same panel bounds and sums as
+// k_align_pairs forms; a group without a candidate aligns nothing.  Groups of more than 32
+// hits are passed without the test.
+__device__ __forceinline__ bool group_can_fire(const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
+                                               uint32_t s, uint32_t e, int pbits, int binshift, int kmer, int hitmin,
+                                               int minhit)
 {
-    if (need <= 0 || e - s > 32)
+    const int n = (int)(e - s);
+    if (hitmin <= 0 || n > 32)
         return true;
-    for (uint32_t i = s; i < e; i++)
+    int ap[32], bd[32], dl[32];
+    const uint64_t pm = (1ull << pbits) - 1;
+    for (int i = 0; i < n; i++)
     {
-        const int d = ((int)__ldg(hdiag + i)) >> binshift;
-        int lo = 0, hi = 0;  // hits in bands {d - 1, d} and {d, d + 1}
-        for (uint32_t j = s; j < e; j++)
+        ap[i] = (int)(__ldg(hkey + s + i) & pm);
+        bd[i] = ((int)__ldg(hdiag + s + i)) >> binshift;
+    }
+    int nidx = 0, amark2 = 0;
+    while (nidx < n)
+    {
+        const int amark = amark2 + GD_PANEL_SIZE;
+        amark2 = amark - GD_PANEL_OVERLAP;
+        const int lidx = nidx;
+        int q = lidx;
+        while (q < n && ap[q] <= amark)
+            q++;
+        const int nend = q < n ? q + 1 : n;
+        int h2 = lidx;
+        while (h2 < nend && ap[h2] <= amark2)
+            h2++;
+        if (nend - lidx >= minhit)
         {
-            const int x = ((int)__ldg(hdiag + j)) >> binshift;
-            lo += (x == d) | (x == d - 1);
-            hi += (x == d) | (x == d + 1);
+            // each hit's contribution to its band's score in this panel
+            for (int j = lidx; j < nend; j++)
+            {
+                int prev = 0;
+                for (int i = lidx; i < j; i++)
+                    if (bd[i] == bd[j])
+                        prev = ap[i];
+                dl[j] = (ap[j] - prev >= kmer) ? kmer : ap[j] - prev;
+            }
+            for (int i = lidx; i < nend; i++)
+            {
+                int sc0 = 0, up = 0, dn = 0;  // scores of bands bd[i], bd[i] + 1, bd[i] - 1
+                for (int j = lidx; j < nend; j++)
+                {
+                    sc0 += bd[j] == bd[i] ? dl[j] : 0;
+                    up += bd[j] == bd[i] + 1 ? dl[j] : 0;
+                    dn += bd[j] == bd[i] - 1 ? dl[j] : 0;
+                }
+                if (sc0 + up >= hitmin || sc0 + dn >= hitmin)
+                    return true;
+            }
         }
-        if (lo >= need || hi >= need)
-            return true;
+        nidx = h2;
     }
     return false;
 }

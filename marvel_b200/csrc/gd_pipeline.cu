@@ -968,12 +968,13 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     }
     if (launch_pair_scatter(pflags, ppos, nhits, P<uint32_t>(c->starts), s))
         return -1;
-    // daligner's seed test needs ceil(h/k) hits in two adjacent bands: groups without them are
-    // dropped here, exactly (daligner2's report keeps its own selection)
+    // groups in which daligner's seed scan would find no candidate are dropped here, exactly
+    // (daligner2's report keeps its own selection)
     const int minhit = (c->hitmin - 1) / c->kmer + 1;
-    const int band_need = c->variant == 1 ? minhit : 0;
+    const int seed_test = c->variant == 1 ? c->hitmin : 0;
     if (triage
-            ? launch_select_groups_triage(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, band_need, hb,
+            ? launch_select_groups_triage(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, c->kmer, seed_test,
+                                          hb,
                                           A.blk, B.blk, comp, c->minover, c->binshift,
                                           A.has_mask ? P<int64_t>(A.manno) : nullptr,
                                           A.has_mask ? P<int32_t>(A.mdata) : nullptr,
@@ -981,8 +982,8 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
                                           c->tri_collect ? P<float>(c->tri_feat) : nullptr, P<uint2>(c->groups),
                                           P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), P<uint8_t>(c->tri_skip), d_ng,
                                           d_nskip, s)
-            : launch_select_groups(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, c->binshift, band_need,
-                                   hb, P<int32_t>(A.rlen), P<int32_t>(B.rlen), P<uint2>(c->groups),
+            : launch_select_groups(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, c->binshift, c->kmer,
+                                   seed_test, hb, P<int32_t>(A.rlen), P<int32_t>(B.rlen), P<uint2>(c->groups),
                                    P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), d_ng, s))
         return -1;
     unsigned ng = 0;

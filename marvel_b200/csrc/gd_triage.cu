@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(MT) k_mlp_forward(const float* __restrict__ P,
 // features are computed (collection).
 __global__ void __launch_bounds__(MT) k_select_groups_triage(
     const uint32_t* __restrict__ starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* __restrict__ hkey,
-    const uint32_t* __restrict__ hdiag, int band_need, HitBits hb, DevBlock A, DevBlock B, int comp, int minover,
+    const uint32_t* __restrict__ hdiag, int kmer, int hitmin, HitBits hb, DevBlock A, DevBlock B, int comp, int minover,
     int binshift, const int64_t* __restrict__ anno, const int32_t* __restrict__ mdata, const float* __restrict__ P,
     float thr, float* feat, uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
     unsigned* nskip)
@@ -415,7 +415,8 @@ __global__ void __launch_bounds__(MT) k_select_groups_triage(
         {
             st = starts[g];
             en = (g + 1 < nstarts) ? starts[g + 1] : (uint32_t)nhits;
-            take = (int64_t)(en - st) >= minhit && group_can_fire(hdiag, st, en, binshift, band_need);
+            take = (int64_t)(en - st) >= minhit &&
+                   group_can_fire(hkey, hdiag, st, en, hb.pbits, binshift, kmer, hitmin, minhit);
             if (take)
             {
                 const uint64_t k = hkey[st];
@@ -693,7 +694,7 @@ int launch_adam(float* params, const float* grad, float* m, float* v, int step, 
 }
 
 int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit,
-                                const uint64_t* hkey, const uint32_t* hdiag, int band_need, HitBits hb,
+                                const uint64_t* hkey, const uint32_t* hdiag, int kmer, int hitmin, HitBits hb,
                                 const DevBlock& A,
                                 const DevBlock& B, int comp, int minover, int binshift, const int64_t* amask_anno,
                                 const int32_t* amask_data, const float* params, float threshold, float* feat,
@@ -706,7 +707,7 @@ int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t
     int grid = infer_grid((nstarts + IR - 1) / IR);
     if (grid <= 0)
         return -1;
-    k_select_groups_triage<<<grid, MT, sizeof(InferSmem), s>>>(starts, nstarts, nhits, minhit, hkey, hdiag, band_need,
+    k_select_groups_triage<<<grid, MT, sizeof(InferSmem), s>>>(starts, nstarts, nhits, minhit, hkey, hdiag, kmer, hitmin,
                                                              hb, A, B,
                                                              comp, minover, binshift, amask_anno, amask_data, params,
                                                              threshold, feat, groups, cost, idx, skip, ngroups,

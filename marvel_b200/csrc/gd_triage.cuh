@@ -21,12 +21,13 @@ constexpr int TRI_OFF_B3 = TRI_OFF_W3 + TRI_H;
 constexpr int TRI_NPARAM = TRI_OFF_B3 + 1;  // 5081, of which 5057 trained
 
 // Pair-group selection (runs of >= minhit hits from the run starts of the sorted hits) fused
-// with the triage (band_need as for launch_select_groups): per kept group its range, cost key
+// with the triage (kmer, hitmin: the seed test as for launch_select_groups): per kept group its
+// range, cost key
 // ~(alen + blen), index, the features
 // (into feat, when given) and with params != nullptr the MLP's verdict skip[g] = p <
 // threshold (nskip += #skipped).  One persistent launch, 128 run starts per tile.
 int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit,
-                                const uint64_t* hkey, const uint32_t* hdiag, int band_need, HitBits hb,
+                                const uint64_t* hkey, const uint32_t* hdiag, int kmer, int hitmin, HitBits hb,
                                 const DevBlock& A,
                                 const DevBlock& B, int comp, int minover, int binshift, const int64_t* amask_anno,
                                 const int32_t* amask_data, const float* params, float threshold, float* feat,
