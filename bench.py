@@ -265,7 +265,7 @@ def run_gpu(args):
     # ---- learned triage (beside the exact path): the shipped model, trained on another genome
     tri = None
     from marvel_b200 import triage as mtri
-    model_path = args.triage_model or mtri.DEFAULT_MODEL
+    model_path = args.triage_model or mtri.model_for(args.workload)
     if args.triage and os.path.exists(model_path):
         model = mtri.TriageModel.load(model_path)
         # one untimed plain run with collection: how the wave cells split between groups that

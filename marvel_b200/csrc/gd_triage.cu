@@ -382,12 +382,62 @@ __global__ void __launch_bounds__(MT) k_mlp_forward(const float* __restrict__ P,
 }
 
 // Pair-group selection fused with the triage (report_thread's minhit test,
-// dalign/filter.c:1699-1709, and the learned triage in one pass): each thread takes one run
-// start of the sorted hits, keeps the run when it has >= minhit hits, computes the kept
-// group's features from its hits, the CTA's warps run the MLP over the tile's 128 rows on
-// tensor cores, and the kept groups are written out (range, cost key, index) with their
-// skip flag (p < thr) and, when feat is given, their raw features.  With P == nullptr only
-// features are computed (collection).
+// dalign/filter.c:1699-1709, the seed-candidate test, and the learned triage in one pass):
+// each thread takes one run start of the sorted hits and keeps the run when it has >= minhit
+// hits and a candidate seed; a kept group's features are computed from its hits and staged in
+// shared memory with its range; whenever a tile of run starts would overflow the 128 staged
+// rows (and at the end) the CTA's warps run the MLP over the staged rows on tensor cores and
+// the groups are written out (range, cost key, index) with their skip flag (p < thr) and,
+// when feat is given, their raw features.  Staging keeps the MLP to kept groups only, however
+// sparse they are among the run starts.  With P == nullptr only features are computed.
+struct SelStage
+{
+    uint32_t st[IR], en[IR], c[IR];
+    float f[IR][TRI_NF];
+    int woff[MT / 32];
+};
+
+constexpr size_t SEL_SMEM = (sizeof(InferSmem) + 15) / 16 * 16 + sizeof(SelStage);
+
+__device__ void sel_flush(InferSmem& S, SelStage& G, int nrows, const float* __restrict__ P, float thr, float* feat,
+                          uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
+                          unsigned& cnt)
+{
+    const int r = threadIdx.x;
+    const bool mine = r < nrows;
+    bool drop = false;
+    if (P)
+    {
+        infer_put_row(S, r, G.f[r], mine);
+        __syncthreads();
+        infer_rows(S);
+        __syncthreads();
+        drop = mine && 1.f / (1.f + __expf(-S.z[r])) < thr;
+    }
+    const unsigned m = __ballot_sync(GD_FULL, mine);
+    unsigned base = 0;
+    if (m)
+    {
+        if (lane_id() == 0)
+            base = atomicAdd(ngroups, (unsigned)__popc(m));
+        base = __shfl_sync(GD_FULL, base, 0);
+    }
+    if (mine)
+    {
+        const unsigned slot = base + __popc(m & lanemask_lt());
+        groups[slot] = make_uint2(G.st[r], G.en[r]);
+        cost[slot] = ~G.c[r];  // ascending sort of ~cost = longest pairs first
+        idx[slot] = slot;
+        skip[slot] = drop ? 1 : 0;
+        cnt += drop;
+        if (feat)
+#pragma unroll
+            for (int j = 0; j < TRI_NF; j++)
+                feat[(size_t)slot * TRI_NF + j] = G.f[r][j];
+    }
+    __syncthreads();  // the staging rows and S.X / S.z are rewritten next
+}
+
 __global__ void __launch_bounds__(MT) k_select_groups_triage(
     const uint32_t* __restrict__ starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* __restrict__ hkey,
     const uint32_t* __restrict__ hdiag, int kmer, int hitmin, HitBits hb, DevBlock A, DevBlock B, int comp, int minover,
@@ -397,11 +447,14 @@ __global__ void __launch_bounds__(MT) k_select_groups_triage(
 {
     extern __shared__ __align__(16) unsigned char infer_smem_t[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(infer_smem_t);
+    SelStage& G = *reinterpret_cast<SelStage*>(infer_smem_t + (sizeof(InferSmem) + 15) / 16 * 16);
     if (P)
         infer_load_weights(S, P);
     __syncthreads();
     const int64_t ntiles = (nstarts + IR - 1) / IR;
+    const int w = threadIdx.x >> 5;
     unsigned cnt = 0;
+    int rows = 0;  // staged rows (the same in every thread)
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
         const int64_t g = tile * IR + threadIdx.x;
@@ -426,39 +479,40 @@ __global__ void __launch_bounds__(MT) k_select_groups_triage(
                 group_features(hkey, hdiag, make_uint2(st, en), hb, A, B, comp, minover, binshift, anno, mdata, f);
             }
         }
-        bool drop = false;
-        if (P)
-        {
-            infer_put_row(S, threadIdx.x, f, take);
-            __syncthreads();
-            infer_rows(S);
-            __syncthreads();
-            drop = take && 1.f / (1.f + __expf(-S.z[threadIdx.x])) < thr;
-            __syncthreads();  // S.X and S.z are rewritten by the next tile
-        }
-        // compaction: a slot per kept group, one atomic per warp
+        // the tile's kept groups, in thread order, behind the rows already staged
         const unsigned m = __ballot_sync(GD_FULL, take);
-        unsigned base = 0;
-        if (m)
+        if (lane_id() == 0)
+            G.woff[w] = __popc(m);
+        __syncthreads();
+        int before = 0, ntake = 0;
+#pragma unroll
+        for (int i = 0; i < MT / 32; i++)
         {
-            if (lane_id() == 0)
-                base = atomicAdd(ngroups, (unsigned)__popc(m));
-            base = __shfl_sync(GD_FULL, base, 0);
+            const int cw = G.woff[i];
+            before += i < w ? cw : 0;
+            ntake += cw;
+        }
+        __syncthreads();
+        if (rows + ntake > IR)
+        {
+            sel_flush(S, G, rows, P, thr, feat, groups, cost, idx, skip, ngroups, cnt);
+            rows = 0;
         }
         if (take)
         {
-            const unsigned slot = base + __popc(m & lanemask_lt());
-            groups[slot] = make_uint2(st, en);
-            cost[slot] = ~c;  // ascending sort of ~cost = longest pairs first
-            idx[slot] = slot;
-            skip[slot] = drop ? 1 : 0;
-            cnt += drop;
-            if (feat)
+            const int r = rows + before + __popc(m & lanemask_lt());
+            G.st[r] = st;
+            G.en[r] = en;
+            G.c[r] = c;
 #pragma unroll
-                for (int j = 0; j < TRI_NF; j++)
-                    feat[(size_t)slot * TRI_NF + j] = f[j];
+            for (int j = 0; j < TRI_NF; j++)
+                G.f[r][j] = f[j];
         }
+        rows += ntake;
+        __syncthreads();
     }
+    if (rows > 0)
+        sel_flush(S, G, rows, P, thr, feat, groups, cost, idx, skip, ngroups, cnt);
     if (P)
     {
         for (int o = 16; o; o >>= 1)
@@ -636,8 +690,8 @@ static int infer_grid(int64_t ntiles)
         GD_CUDA(cudaGetDevice(&dev));
         GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         GD_CUDA(cudaFuncSetAttribute((const void*)k_select_groups_triage, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(InferSmem)));
-        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_select_groups_triage, MT, sizeof(InferSmem)));
+                                     (int)SEL_SMEM));
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_select_groups_triage, MT, SEL_SMEM));
         blocks = nsm * std::max(per, 1);
     }
     return (int)std::min<int64_t>(ntiles, blocks);
@@ -707,7 +761,7 @@ int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t
     int grid = infer_grid((nstarts + IR - 1) / IR);
     if (grid <= 0)
         return -1;
-    k_select_groups_triage<<<grid, MT, sizeof(InferSmem), s>>>(starts, nstarts, nhits, minhit, hkey, hdiag, kmer, hitmin,
+    k_select_groups_triage<<<grid, MT, SEL_SMEM, s>>>(starts, nstarts, nhits, minhit, hkey, hdiag, kmer, hitmin,
                                                              hb, A, B,
                                                              comp, minover, binshift, amask_anno, amask_data, params,
                                                              threshold, feat, groups, cost, idx, skip, ngroups,

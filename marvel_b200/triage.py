@@ -50,6 +50,14 @@ class TriageModel:
         return TriageModel(np.asarray(z["params"], np.float32), float(z["threshold"]), float(z["recall"]))
 
 
+def model_for(workload: str) -> str:
+    """The shipped model for a workload: the default weights with the threshold calibrated on
+    another genome of that workload's model when such a file exists (triage_cfg12_cal_<w>.npz),
+    else the default model."""
+    cal = os.path.join(HERE, "models", f"triage_cfg12_cal_{workload}.npz")
+    return cal if os.path.exists(cal) else DEFAULT_MODEL
+
+
 def mlp_init(feat: np.ndarray, seed: int = 1) -> np.ndarray:
     """Feature scales from feat and seeded He-uniform weights (gd_mlp_init)."""
     feat = np.ascontiguousarray(feat, np.float32).reshape(-1, TRI_NF)
