@@ -172,6 +172,7 @@ def run_gpu(args):
 
     A, B = load_blocks(args.workload, seed_offset=rank)
     pair = B is not None
+    free0, total_mem = torch.cuda.mem_get_info()
     ctx = mb.Context()
     p = PARAMS
     ctx.set_filter_params(p["k"], p["w"], p["t"], p["h"])
@@ -220,6 +221,8 @@ def run_gpu(args):
     barrier()
     launches = mb.kernel_launches() - l0
     st = ctx.stats()
+    # device memory the library holds after the steps (its buffers are grown once and kept)
+    held = free0 - torch.cuda.mem_get_info()[0]
     tot_ms = sum(times)
     tot_ms_max, = reduce([tot_ms], torch.distributed.ReduceOp.MAX if ws > 1 else None)
     recs_all, = reduce([float(recs)], torch.distributed.ReduceOp.SUM if ws > 1 else None)
@@ -403,6 +406,8 @@ def run_gpu(args):
             "e2e": {"value": round(e2e, 1), "unit": "overlaps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
+            "device_gb_held": round(held / 1e9, 2),
+            "device_gb_total": round(total_mem / 1e9, 1),
             "align_schedule": ("one launch per length class, alen+blen edges " + args.schedule) if args.schedule
             else (f"autotuned: {tuned['chosen']}" if tuned
                   else "one persistent launch, pair groups longest first from a device queue"),
