@@ -72,8 +72,11 @@ def path_name():
 
 CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
 # k_align_pairs DRAM bytes (read + write) per wave cell, from the ncu capture of the cfg1
-# N-orientation launch: 114.3 MB over 282 M cells
-ALIGN_DRAM_BYTES_PER_CELL = 114.3e6 / 282.0e6
+# N-orientation launch (profiles/k_align_pairs_cfg1.md): 90.1 MB over 282 M cells
+ALIGN_DRAM_BYTES_PER_CELL = 90.1e6 / 282.0e6
+# k-mer index build DRAM bytes per k-mer (extraction + 4 LSD passes), from the ncu capture of
+# the cfg1 index (profiles/filter_kernels_cfg1.md): 1,731 MB over 21.08 M k-mers
+INDEX_DRAM_BYTES_PER_KMER = 1731.2e6 / 21082465
 
 
 def make_db(workload, seed_offset=0, scale=1.0):
@@ -394,7 +397,7 @@ def run_gpu(args):
                          "traffic_source": "bytes per launch: dram read+write per wave cell of the cfg1 ncu capture "
                                            "(profiles/k_align_pairs_cfg1.md) x this launch's cells",
                          "peak_source": "derived: 148 SM x 128 lanes/clk x median SM clock under load",
-                         "issue_slots_busy": 0.751,
+                         "issue_slots_busy": 0.755,
                          "issue_source": "smsp__issue_active of the cfg1 ncu capture (profiles/k_align_pairs_cfg1.md): "
                                          "the kernel issues on 75 % of cycles; a wave is ~11 diagonals wide, so a "
                                          "warp instruction carries about a third of a warp of cells"},
@@ -402,7 +405,10 @@ def run_gpu(args):
                                 "achieved": round(idx_bytes / (idx_ms / 1e3) / 1e9, 1),
                                 "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                                 "frac": round(idx_bytes / (idx_ms / 1e3) / 1e9 / peaks.get("hbm_gbs", 6650.0), 4),
-                                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                                "traffic": int(INDEX_DRAM_BYTES_PER_KMER * kmers),
+                                "traffic_source": "dram read+write per k-mer of the cfg1 index build's ncu capture "
+                                                  "(profiles/filter_kernels_cfg1.md) x this step's k-mers",
+                                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
             "e2e": {"value": round(e2e, 1), "unit": "overlaps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),

@@ -479,19 +479,19 @@ __global__ void __launch_bounds__(MT) k_select_groups_triage(
                 group_features(hkey, hdiag, make_uint2(st, en), hb, A, B, comp, minover, binshift, anno, mdata, f);
             }
         }
+        // most tiles keep no group: one barrier tells, and they cost nothing more
+        const int ntake = __syncthreads_count(take);
+        if (ntake == 0)
+            continue;
         // the tile's kept groups, in thread order, behind the rows already staged
         const unsigned m = __ballot_sync(GD_FULL, take);
         if (lane_id() == 0)
             G.woff[w] = __popc(m);
         __syncthreads();
-        int before = 0, ntake = 0;
+        int before = 0;
 #pragma unroll
         for (int i = 0; i < MT / 32; i++)
-        {
-            const int cw = G.woff[i];
-            before += i < w ? cw : 0;
-            ntake += cw;
-        }
+            before += i < w ? G.woff[i] : 0;
         __syncthreads();
         if (rows + ntake > IR)
         {
