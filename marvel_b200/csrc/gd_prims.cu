@@ -402,6 +402,7 @@ struct RsPipe : RsPipeVals<V>
 {
     K key[2][RS_TILE];
     uint32_t wcnt[RS_WARPS][256];
+    uint32_t lstart[256];
     uint32_t toff[256];
     uint32_t wsum[RS_WARPS];
     uint64_t full[2];
