@@ -517,14 +517,14 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
             __syncwarp();
         }
         __syncthreads();
-        // per digit (one per thread): the run length in this tile, its start among the tile's
-        // runs (a scan over the digits), then each warp's start inside the tile folded into
-        // wcnt and the tile's start subtracted from the digit's global offset, so that the
-        // re-order and the write-out below each read one table entry per item
         uint32_t tot = 0;
 #pragma unroll
         for (int i = 0; i < RS_WARPS; i++)
-            tot += S.wcnt[i][threadIdx.x];
+        {
+            uint32_t t = S.wcnt[i][threadIdx.x];
+            S.wcnt[i][threadIdx.x] = tot;
+            tot += t;
+        }
         {
             uint32_t x = tot;
 #pragma unroll
@@ -541,15 +541,7 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
 #pragma unroll
             for (int i = 0; i < RS_WARPS; i++)
                 wo += i < w ? S.wsum[i] : 0;
-            uint32_t run = wo + x - tot;  // the digit's run start in the re-ordered tile
-            S.toff[threadIdx.x] -= run;   // global position of tile slot i of the run: toff + i
-#pragma unroll
-            for (int i = 0; i < RS_WARPS; i++)
-            {
-                uint32_t t = S.wcnt[i][threadIdx.x];
-                S.wcnt[i][threadIdx.x] = run;
-                run += t;
-            }
+            S.lstart[threadIdx.x] = wo + x - tot;
         }
         __syncthreads();
         // the stage's tile is in registers: re-order it in place
@@ -560,7 +552,7 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
             if (i < tn)
             {
                 unsigned d = (unsigned)(key[r] >> shift) & 255u;
-                uint32_t pos = S.wcnt[w][d] + ((rank2[r >> 1] >> (16 * (r & 1))) & 0xffffu);
+                uint32_t pos = S.lstart[d] + S.wcnt[w][d] + ((rank2[r >> 1] >> (16 * (r & 1))) & 0xffffu);
                 skey[pos] = key[r];
                 if constexpr (V)
                     sval[pos] = val[r];
@@ -571,7 +563,7 @@ __global__ void __launch_bounds__(RS_THREADS, rs_pipe_ctas<K, V>())
         {
             K k = skey[i];
             unsigned d = (unsigned)(k >> shift) & 255u;
-            uint32_t dest = S.toff[d] + (uint32_t)i;
+            uint32_t dest = S.toff[d] + (uint32_t)i - S.lstart[d];
             if constexpr (F == RsFinal::INDEX)
             {
                 const uint32_t v = sval[i];
