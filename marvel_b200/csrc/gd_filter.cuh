@@ -164,6 +164,23 @@ __device__ __forceinline__ bool group_can_fire(const uint64_t* __restrict__ hkey
     const int n = (int)(e - s);
     if (hitmin <= 0 || n > 32)
         return true;
+    // a band scores at most k per hit, so a candidate needs minhit hits in its band and a
+    // neighbouring one: most groups (hits on unrelated diagonals) fail this count at once
+    bool maybe = false;
+    for (int i = 0; i < n && !maybe; i++)
+    {
+        const int d = ((int)__ldg(hdiag + s + i)) >> binshift;
+        int lo = 0, hi = 0;  // hits in bands {d - 1, d} and {d, d + 1}
+        for (int j = 0; j < n; j++)
+        {
+            const int x = ((int)__ldg(hdiag + s + j)) >> binshift;
+            lo += (x == d) | (x == d - 1);
+            hi += (x == d) | (x == d + 1);
+        }
+        maybe = lo >= minhit || hi >= minhit;
+    }
+    if (!maybe)
+        return false;
     int ap[32], bd[32], dl[32];
     const uint64_t pm = (1ull << pbits) - 1;
     for (int i = 0; i < n; i++)
