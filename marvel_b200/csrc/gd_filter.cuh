@@ -135,7 +135,7 @@ int launch_emit(const int32_t* aread, const int32_t* arpos, const int32_t* bread
 int launch_hit_unpack(const uint64_t* packed, int64_t n, HitBits hb, uint64_t* hkey, uint32_t* hdiag, cudaStream_t s);
 
 // Pair groups of the sorted hits: start flags, then (start, end) of groups with >= minhit hits.
-// With hitmin > 0 a group of at most 32 hits is also dropped when the seed scan would find no
+// With hitmin > 0 a group of at most GD_FIRE_TEST_MAX hits is also dropped when the seed scan would find no
 // candidate seed in it (group_can_fire): such a group fires no Local_Alignment and yields
 // nothing, the scan would only have read its hits.  hitmin = 0 keeps every group with >=
 // minhit hits.
@@ -146,6 +146,10 @@ int launch_select_groups(const uint32_t* starts, int64_t nstarts, int64_t nhits,
                          const int32_t* brlen, uint2* groups, uint32_t* cost, uint32_t* idx, unsigned int* ngroups,
                          cudaStream_t s);
 
+// groups longer than this pass selection untested (the test is quadratic in the hits, and a
+// thread's long group would hold up its warp); nearly all groups without a candidate are shorter
+constexpr int GD_FIRE_TEST_MAX = 16;
+
 // the seed scan's panels: a-position windows of 50,000 overlapping by 10,000 (filter.c:1717-1745)
 constexpr int GD_PANEL_SIZE = 50000;
 constexpr int GD_PANEL_OVERLAP = 10000;
@@ -155,14 +159,14 @@ constexpr int GD_PANEL_OVERLAP = 10000;
 // skipped), each diagonal band (diag >> binshift) scores the sum over its hits of min(k,
 // apos - the band's previous apos in the panel, 0 for its first), and a hit is a candidate when
 // its band and a neighbouring band together reach hitmin.  The same panel bounds and sums as
-// k_align_pairs forms; a group without a candidate aligns nothing.  Groups of more than 32
-// hits are passed without the test.
+// k_align_pairs forms; a group without a candidate aligns nothing.  Groups of more than
+// GD_FIRE_TEST_MAX hits are passed without the test.
 __device__ __forceinline__ bool group_can_fire(const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
                                                uint32_t s, uint32_t e, int pbits, int binshift, int kmer, int hitmin,
                                                int minhit)
 {
     const int n = (int)(e - s);
-    if (hitmin <= 0 || n > 32)
+    if (hitmin <= 0 || n > GD_FIRE_TEST_MAX)
         return true;
     // a band scores at most k per hit, so a candidate needs minhit hits in its band and a
     // neighbouring one: most groups (hits on unrelated diagonals) fail this count at once
@@ -181,7 +185,7 @@ __device__ __forceinline__ bool group_can_fire(const uint64_t* __restrict__ hkey
     }
     if (!maybe)
         return false;
-    int ap[32], bd[32], dl[32];
+    int ap[GD_FIRE_TEST_MAX], bd[GD_FIRE_TEST_MAX], dl[GD_FIRE_TEST_MAX];
     const uint64_t pm = (1ull << pbits) - 1;
     for (int i = 0; i < n; i++)
     {

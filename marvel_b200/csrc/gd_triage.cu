@@ -383,137 +383,152 @@ __global__ void __launch_bounds__(MT) k_mlp_forward(const float* __restrict__ P,
 
 // Pair-group selection fused with the triage (report_thread's minhit test,
 // dalign/filter.c:1699-1709, the seed-candidate test, and the learned triage in one pass):
-// each thread takes one run start of the sorted hits and keeps the run when it has >= minhit
-// hits and a candidate seed; a kept group's features are computed from its hits and staged in
-// shared memory with its range; whenever a tile of run starts would overflow the 128 staged
-// rows (and at the end) the CTA's warps run the MLP over the staged rows on tensor cores and
-// the groups are written out (range, cost key, index) with their skip flag (p < thr) and,
-// when feat is given, their raw features.  Staging keeps the MLP to kept groups only, however
-// sparse they are among the run starts.  With P == nullptr only features are computed.
+// each thread tests SEL_U run starts of a tile of SEL_U * 128; a kept group's range and cost
+// key are appended to a ring of staged rows in shared memory; after each tile, while 128 rows
+// are staged, the CTA computes their features from their hits (a thread per row), runs the
+// MLP over them on tensor cores and writes the groups out (range, cost key, index) with their
+// skip flag (p < thr) and, when feat is given, their raw features; the last rows are flushed
+// at the end.  Staging keeps the MLP to kept groups only and one barrier per tile of run
+// starts.  With P == nullptr only features are computed.
+constexpr int SEL_U = 4;                 // run starts per thread per tile
+constexpr int SEL_CAP = IR * (SEL_U + 1);  // staged rows: a tile's worth behind < 128 waiting
+
 struct SelStage
 {
-    uint32_t st[IR], en[IR], c[IR];
-    float f[IR][TRI_NF];
-    int woff[MT / 32];
+    uint32_t st[SEL_CAP], en[SEL_CAP], c[SEL_CAP];
+    unsigned n;  // rows staged
 };
 
 constexpr size_t SEL_SMEM = (sizeof(InferSmem) + 15) / 16 * 16 + sizeof(SelStage);
 
-__device__ void sel_flush(InferSmem& S, SelStage& G, int nrows, const float* __restrict__ P, float thr, float* feat,
-                          uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
-                          unsigned& cnt)
+struct SelArgs
+{
+    const uint64_t* hkey;
+    const uint32_t* hdiag;
+    HitBits hb;
+    DevBlock A, B;
+    int comp, minover, binshift;
+    const int64_t* anno;
+    const int32_t* mdata;
+    const float* P;
+    float thr;
+    float* feat;
+    uint2* groups;
+    uint32_t* cost;
+    uint32_t* idx;
+    uint8_t* skip;
+    unsigned* ngroups;
+};
+
+// rows head .. head + nrows - 1 of the ring (nrows <= 128): features, MLP, output
+__device__ void sel_flush(InferSmem& S, SelStage& G, int head, int nrows, const SelArgs& a, unsigned& cnt)
 {
     const int r = threadIdx.x;
     const bool mine = r < nrows;
-    bool drop = false;
-    if (P)
+    const int q = (head + r) % SEL_CAP;
+    float f[TRI_NF];
+#pragma unroll
+    for (int j = 0; j < TRI_NF; j++)
+        f[j] = 0.f;
+    uint32_t st = 0, en = 0, c = 0;
+    if (mine)
     {
-        infer_put_row(S, r, G.f[r], mine);
+        st = G.st[q];
+        en = G.en[q];
+        c = G.c[q];
+        group_features(a.hkey, a.hdiag, make_uint2(st, en), a.hb, a.A, a.B, a.comp, a.minover, a.binshift, a.anno,
+                       a.mdata, f);
+    }
+    bool drop = false;
+    if (a.P)
+    {
+        infer_put_row(S, r, f, mine);
         __syncthreads();
         infer_rows(S);
         __syncthreads();
-        drop = mine && 1.f / (1.f + __expf(-S.z[r])) < thr;
+        drop = mine && 1.f / (1.f + __expf(-S.z[r])) < a.thr;
     }
     const unsigned m = __ballot_sync(GD_FULL, mine);
     unsigned base = 0;
     if (m)
     {
         if (lane_id() == 0)
-            base = atomicAdd(ngroups, (unsigned)__popc(m));
+            base = atomicAdd(a.ngroups, (unsigned)__popc(m));
         base = __shfl_sync(GD_FULL, base, 0);
     }
     if (mine)
     {
         const unsigned slot = base + __popc(m & lanemask_lt());
-        groups[slot] = make_uint2(G.st[r], G.en[r]);
-        cost[slot] = ~G.c[r];  // ascending sort of ~cost = longest pairs first
-        idx[slot] = slot;
-        skip[slot] = drop ? 1 : 0;
+        a.groups[slot] = make_uint2(st, en);
+        a.cost[slot] = ~c;  // ascending sort of ~cost = longest pairs first
+        a.idx[slot] = slot;
+        a.skip[slot] = drop ? 1 : 0;
         cnt += drop;
-        if (feat)
+        if (a.feat)
 #pragma unroll
             for (int j = 0; j < TRI_NF; j++)
-                feat[(size_t)slot * TRI_NF + j] = G.f[r][j];
+                a.feat[(size_t)slot * TRI_NF + j] = f[j];
     }
-    __syncthreads();  // the staging rows and S.X / S.z are rewritten next
+    __syncthreads();  // S.X / S.z are rewritten by the next flush
 }
 
-__global__ void __launch_bounds__(MT) k_select_groups_triage(
-    const uint32_t* __restrict__ starts, int64_t nstarts, int64_t nhits, int minhit, const uint64_t* __restrict__ hkey,
-    const uint32_t* __restrict__ hdiag, int kmer, int hitmin, HitBits hb, DevBlock A, DevBlock B, int comp, int minover,
-    int binshift, const int64_t* __restrict__ anno, const int32_t* __restrict__ mdata, const float* __restrict__ P,
-    float thr, float* feat, uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
-    unsigned* nskip)
+__global__ void __launch_bounds__(MT) k_select_groups_triage(const uint32_t* __restrict__ starts, int64_t nstarts,
+                                                           int64_t nhits, int minhit, int kmer, int hitmin, SelArgs a,
+                                                           unsigned* nskip)
 {
     extern __shared__ __align__(16) unsigned char infer_smem_t[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(infer_smem_t);
     SelStage& G = *reinterpret_cast<SelStage*>(infer_smem_t + (sizeof(InferSmem) + 15) / 16 * 16);
-    if (P)
-        infer_load_weights(S, P);
+    if (a.P)
+        infer_load_weights(S, a.P);
+    if (threadIdx.x == 0)
+        G.n = 0;
     __syncthreads();
-    const int64_t ntiles = (nstarts + IR - 1) / IR;
-    const int w = threadIdx.x >> 5;
+    const int64_t per = (int64_t)IR * SEL_U;
+    const int64_t ntiles = (nstarts + per - 1) / per;
     unsigned cnt = 0;
-    int rows = 0;  // staged rows (the same in every thread)
+    int head = 0;  // first staged row of the ring (the same in every thread)
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        const int64_t g = tile * IR + threadIdx.x;
-        bool take = false;
-        uint32_t st = 0, en = 0, c = 0;
-        float f[TRI_NF];
 #pragma unroll
-        for (int j = 0; j < TRI_NF; j++)
-            f[j] = 0.f;
-        if (g < nstarts)
+        for (int u = 0; u < SEL_U; u++)
         {
-            st = starts[g];
-            en = (g + 1 < nstarts) ? starts[g + 1] : (uint32_t)nhits;
-            take = (int64_t)(en - st) >= minhit &&
-                   group_can_fire(hkey, hdiag, st, en, hb.pbits, binshift, kmer, hitmin, minhit);
-            if (take)
+            const int64_t g = tile * per + (int64_t)u * IR + threadIdx.x;
+            if (g >= nstarts)
+                continue;
+            const uint32_t st = starts[g];
+            const uint32_t en = (g + 1 < nstarts) ? starts[g + 1] : (uint32_t)nhits;
+            if ((int64_t)(en - st) >= minhit &&
+                group_can_fire(a.hkey, a.hdiag, st, en, a.hb.pbits, a.binshift, kmer, hitmin, minhit))
             {
-                const uint64_t k = hkey[st];
-                const int ar = (int)((k >> hb.pbits) & ((1ull << hb.abits) - 1));
-                const int br = (int)(k >> (hb.pbits + hb.abits));
-                c = (uint32_t)(A.rlen[ar] + B.rlen[br]);
-                group_features(hkey, hdiag, make_uint2(st, en), hb, A, B, comp, minover, binshift, anno, mdata, f);
+                const uint64_t k = a.hkey[st];
+                const int ar = (int)((k >> a.hb.pbits) & ((1ull << a.hb.abits) - 1));
+                const int br = (int)(k >> (a.hb.pbits + a.hb.abits));
+                const int q = (head + (int)atomicAdd(&G.n, 1u)) % SEL_CAP;
+                G.st[q] = st;
+                G.en[q] = en;
+                G.c[q] = (uint32_t)(a.A.rlen[ar] + a.B.rlen[br]);
             }
         }
-        // most tiles keep no group: one barrier tells, and they cost nothing more
-        const int ntake = __syncthreads_count(take);
-        if (ntake == 0)
-            continue;
-        // the tile's kept groups, in thread order, behind the rows already staged
-        const unsigned m = __ballot_sync(GD_FULL, take);
-        if (lane_id() == 0)
-            G.woff[w] = __popc(m);
         __syncthreads();
-        int before = 0;
-#pragma unroll
-        for (int i = 0; i < MT / 32; i++)
-            before += i < w ? G.woff[i] : 0;
-        __syncthreads();
-        if (rows + ntake > IR)
+        int n = (int)G.n;
+        if (n >= IR)
         {
-            sel_flush(S, G, rows, P, thr, feat, groups, cost, idx, skip, ngroups, cnt);
-            rows = 0;
+            while (n >= IR)
+            {
+                sel_flush(S, G, head, IR, a, cnt);
+                head = (head + IR) % SEL_CAP;
+                n -= IR;
+            }
+            if (threadIdx.x == 0)
+                G.n = (unsigned)n;
         }
-        if (take)
-        {
-            const int r = rows + before + __popc(m & lanemask_lt());
-            G.st[r] = st;
-            G.en[r] = en;
-            G.c[r] = c;
-#pragma unroll
-            for (int j = 0; j < TRI_NF; j++)
-                G.f[r][j] = f[j];
-        }
-        rows += ntake;
         __syncthreads();
     }
-    if (rows > 0)
-        sel_flush(S, G, rows, P, thr, feat, groups, cost, idx, skip, ngroups, cnt);
-    if (P)
+    const int n = (int)G.n;
+    if (n > 0)
+        sel_flush(S, G, head, n, a, cnt);
+    if (a.P)
     {
         for (int o = 16; o; o >>= 1)
             cnt += __shfl_xor_sync(GD_FULL, cnt, o);
@@ -749,23 +764,20 @@ int launch_adam(float* params, const float* grad, float* m, float* v, int step, 
 
 int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit,
                                 const uint64_t* hkey, const uint32_t* hdiag, int kmer, int hitmin, HitBits hb,
-                                const DevBlock& A,
-                                const DevBlock& B, int comp, int minover, int binshift, const int64_t* amask_anno,
-                                const int32_t* amask_data, const float* params, float threshold, float* feat,
-                                uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
-                                unsigned* nskip, cudaStream_t s)
+                                const DevBlock& A, const DevBlock& B, int comp, int minover, int binshift,
+                                const int64_t* amask_anno, const int32_t* amask_data, const float* params,
+                                float threshold, float* feat, uint2* groups, uint32_t* cost, uint32_t* idx,
+                                uint8_t* skip, unsigned* ngroups, unsigned* nskip, cudaStream_t s)
 {
     GD_CUDA(cudaMemsetAsync(ngroups, 0, sizeof(unsigned), s));
     if (nstarts <= 0)
         return 0;
-    int grid = infer_grid((nstarts + IR - 1) / IR);
+    int grid = infer_grid((nstarts + (int64_t)IR * SEL_U - 1) / ((int64_t)IR * SEL_U));
     if (grid <= 0)
         return -1;
-    k_select_groups_triage<<<grid, MT, SEL_SMEM, s>>>(starts, nstarts, nhits, minhit, hkey, hdiag, kmer, hitmin,
-                                                             hb, A, B,
-                                                             comp, minover, binshift, amask_anno, amask_data, params,
-                                                             threshold, feat, groups, cost, idx, skip, ngroups,
-                                                             nskip);
+    SelArgs a{hkey, hdiag, hb, A, B, comp, minover, binshift, amask_anno, amask_data, params, threshold, feat,
+              groups, cost, idx, skip, ngroups};
+    k_select_groups_triage<<<grid, MT, SEL_SMEM, s>>>(starts, nstarts, nhits, minhit, kmer, hitmin, a, nskip);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;
