@@ -835,17 +835,28 @@ __global__ void __launch_bounds__(FT) k_select_groups(const uint32_t* __restrict
             c = (uint32_t)(arlen[ar] + brlen[br]);
         }
     }
-    unsigned m = __ballot_sync(GD_FULL, take);
-    unsigned base = 0;
-    if (m)
+    // slots for the block's kept groups: one atomic per block (a per-warp atomic on the one
+    // counter serialised millions of times on the large block pairs)
+    __shared__ unsigned wn[FT / 32];
+    __shared__ unsigned bbase;
+    const unsigned m = __ballot_sync(GD_FULL, take);
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 0)
+        wn[w] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0)
     {
-        if (lane_id() == 0)
-            base = atomicAdd(ngroups, (unsigned)__popc(m));
-        base = __shfl_sync(GD_FULL, base, 0);
+        unsigned tot = 0;
+        for (int i = 0; i < FT / 32; i++)
+            tot += wn[i];
+        bbase = tot ? atomicAdd(ngroups, tot) : 0u;
     }
+    __syncthreads();
     if (take)
     {
-        unsigned slot = base + __popc(m & lanemask_lt());
+        unsigned slot = bbase + __popc(m & lanemask_lt());
+        for (int i = 0; i < w; i++)
+            slot += wn[i];
         groups[slot] = make_uint2(s, e);
         cost[slot] = ~c;  // ascending sort of ~cost = longest pairs first
         idx[slot] = slot;

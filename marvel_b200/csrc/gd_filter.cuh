@@ -1,5 +1,6 @@
 // gd_filter.cuh -- device kernels of the k-mer filter (dalign/filter.c restated for sm_100a).
 #pragma once
+#include <climits>
 #include "gd_common.cuh"
 
 namespace gd
@@ -169,19 +170,25 @@ __device__ __forceinline__ bool group_can_fire(const uint64_t* __restrict__ hkey
     if (hitmin <= 0 || n > GD_FIRE_TEST_MAX)
         return true;
     // a band scores at most k per hit, so a candidate needs minhit hits in its band and a
-    // neighbouring one: most groups (hits on unrelated diagonals) fail this count at once
+    // neighbouring one: most groups (hits on unrelated diagonals) fail this count at once.
+    // The bands sit in registers (absent hits hold a band no hit can be next to).
+    int band[GD_FIRE_TEST_MAX];
+#pragma unroll
+    for (int i = 0; i < GD_FIRE_TEST_MAX; i++)
+        band[i] = i < n ? ((int)__ldg(hdiag + s + i)) >> binshift : INT_MIN / 2;
     bool maybe = false;
-    for (int i = 0; i < n && !maybe; i++)
+#pragma unroll
+    for (int i = 0; i < GD_FIRE_TEST_MAX; i++)
     {
-        const int d = ((int)__ldg(hdiag + s + i)) >> binshift;
+        const int d = band[i];
         int lo = 0, hi = 0;  // hits in bands {d - 1, d} and {d, d + 1}
-        for (int j = 0; j < n; j++)
+#pragma unroll
+        for (int j = 0; j < GD_FIRE_TEST_MAX; j++)
         {
-            const int x = ((int)__ldg(hdiag + s + j)) >> binshift;
-            lo += (x == d) | (x == d - 1);
-            hi += (x == d) | (x == d + 1);
+            lo += (band[j] == d) | (band[j] == d - 1);
+            hi += (band[j] == d) | (band[j] == d + 1);
         }
-        maybe = lo >= minhit || hi >= minhit;
+        maybe |= i < n && (lo >= minhit || hi >= minhit);
     }
     if (!maybe)
         return false;
