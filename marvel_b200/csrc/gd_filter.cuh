@@ -170,25 +170,21 @@ __device__ __forceinline__ bool group_can_fire(const uint64_t* __restrict__ hkey
     if (hitmin <= 0 || n > GD_FIRE_TEST_MAX)
         return true;
     // a band scores at most k per hit, so a candidate needs minhit hits in its band and a
-    // neighbouring one: most groups (hits on unrelated diagonals) fail this count at once.
-    // The bands sit in registers (absent hits hold a band no hit can be next to).
-    int band[GD_FIRE_TEST_MAX];
-#pragma unroll
-    for (int i = 0; i < GD_FIRE_TEST_MAX; i++)
-        band[i] = i < n ? ((int)__ldg(hdiag + s + i)) >> binshift : INT_MIN / 2;
+    // neighbouring one: most groups (hits on unrelated diagonals) fail this count at once
+    // (a loop over the few hits, left at the first band that passes: a fully unrolled count
+    // over GD_FIRE_TEST_MAX slots in registers made the selection kernels 2-3x slower)
     bool maybe = false;
-#pragma unroll
-    for (int i = 0; i < GD_FIRE_TEST_MAX; i++)
+    for (int i = 0; i < n && !maybe; i++)
     {
-        const int d = band[i];
+        const int d = ((int)__ldg(hdiag + s + i)) >> binshift;
         int lo = 0, hi = 0;  // hits in bands {d - 1, d} and {d, d + 1}
-#pragma unroll
-        for (int j = 0; j < GD_FIRE_TEST_MAX; j++)
+        for (int j = 0; j < n; j++)
         {
-            lo += (band[j] == d) | (band[j] == d - 1);
-            hi += (band[j] == d) | (band[j] == d + 1);
+            const int x = ((int)__ldg(hdiag + s + j)) >> binshift;
+            lo += (x == d) | (x == d - 1);
+            hi += (x == d) | (x == d + 1);
         }
-        maybe |= i < n && (lo >= minhit || hi >= minhit);
+        maybe = lo >= minhit || hi >= minhit;
     }
     if (!maybe)
         return false;
