@@ -182,8 +182,9 @@ def run_gpu(args):
     ctx.new_align_spec(p["e"], p["s"], A.freq)
     ctx.set_globals(2 * p["l"], False, p["M"] * 0x40000000)
     ctx.set_biased(BIASED)
-    if args.schedule:
-        ctx.set_align_schedule([int(x) for x in args.schedule.split(",")])
+    if args.schedule or args.kinds:
+        ctx.set_align_schedule([int(x) for x in args.schedule.split(",") if x],
+                               [int(x) for x in args.kinds.split(",")] if args.kinds else None)
 
     def barrier():
         torch.cuda.synchronize()
@@ -414,9 +415,10 @@ def run_gpu(args):
             "gpu_launches": int(launches),
             "device_gb_held": round(held / 1e9, 2),
             "device_gb_total": round(total_mem / 1e9, 1),
-            "align_schedule": ("one launch per length class, alen+blen edges " + args.schedule) if args.schedule
-            else (f"autotuned: {tuned['chosen']}" if tuned
-                  else "one persistent launch, pair groups longest first from a device queue"),
+            "align_schedule": (("one launch per length class, alen+blen edges " + args.schedule) if args.schedule
+                               else (f"autotuned: {tuned['chosen']}" if tuned
+                                     else "one persistent launch, pair groups longest first from a device queue"))
+            + (f"; instances {args.kinds} (0 warp, 1 wide, 2 duo)" if args.kinds else ""),
             "autotune": tuned,
             "triage": tri,
             "daligner2": d2,
@@ -631,6 +633,9 @@ def main():
     ap.add_argument("--schedule", default="",
                     help="alen+blen edges (bp, comma-separated): one aligner launch per length class instead of "
                          "the one persistent launch (a comparison schedule)")
+    ap.add_argument("--kinds", default="",
+                    help="the aligner instance of each length class (comma-separated, longest class first; one "
+                         "entry without --schedule): 0 warp, 1 wide, 2 duo")
     ap.add_argument("--no-d2", dest="d2", action="store_false",
                     help="skip the daligner2 (modimizer seeds) measurement (reported beside the exact path)")
     ap.add_argument("--biased", action="store_true",

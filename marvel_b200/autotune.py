@@ -10,8 +10,10 @@ keeps the fastest:
   of the block's pair lengths);
 * per length class, the kernel instance: a warp per alignment with 128-diagonal wave rings
   (4 warps per CTA, 6 CTAs per SM; a group whose band outgrows 128 diagonals is redone by the
-  wide instance) or the wide instance (512-diagonal rings, one warp per CTA), which takes such
-  groups in one pass.
+  wide instance), the wide instance (512-diagonal rings, one warp per CTA), which takes such
+  groups in one pass, or the duo instance (two 16-lane teams per warp, each on its own pair
+  group with 64-diagonal rings), which keeps twice the lanes busy on the narrow bands most
+  waves have.
 
 Candidates are timed on the loaded blocks (the aligner's device time of both orientations,
 gd_stats.ms_align, best of `repeats` runs).  The radix sorts have no choice here: their
@@ -39,13 +41,19 @@ def length_edges(A, B=None, nclasses=3):
 
 
 def candidates(edges):
-    """(name, edges, kinds) schedules to time: the persistent launch, the per-class launches
-    on the warp instance, and the per-class launches with the longest class (and the two
-    longest) on the wide instance."""
+    """(name, edges, kinds) schedules to time: the persistent launch on the warp and on the duo
+    instance; the per-class launches on either; the per-class launches with the longest class
+    (and the two longest) on the wide instance and the rest on the warp or the duo instance;
+    and the longest class on the warp instance with the rest on the duo instance."""
     n = len(edges) + 1
-    out = [("persistent", [], None), ("per-class", list(edges), [0] * n)]
+    e = list(edges)
+    out = [("persistent, warp instance", [], [0]), ("persistent, duo instance", [], [2]),
+           ("per-class, warp instance", e, [0] * n), ("per-class, duo instance", e, [2] * n)]
     for w in range(1, min(2, n - 1) + 1):
-        out.append((f"per-class, longest {w} on the wide instance", list(edges), [1] * w + [0] * (n - w)))
+        out.append((f"per-class, longest {w} on the wide instance, the rest warp", e, [1] * w + [0] * (n - w)))
+        out.append((f"per-class, longest {w} on the wide instance, the rest duo", e, [1] * w + [2] * (n - w)))
+    if n > 1:
+        out.append(("per-class, longest on the warp instance, the rest duo", e, [0] + [2] * (n - 1)))
     return out
 
 

@@ -35,15 +35,23 @@ namespace gd
 #define WAVE_LAG 30
 #define PANEL_SIZE 50000
 #define PANEL_OVERLAP 10000
-#define RM (RG - 1)  // ring index mask of the instance (RG diagonals)
+#define RM (ring_of<RG>() - 1)  // ring index mask of the instance
 #define SENT4 0x0404040404040404ull
+
+// An instance id RG is its ring size (diagonals per wave ring), with bit 16 set for the duo
+// instance's half-warp teams.
+template <int RG>
+constexpr int ring_of()
+{
+    return RG & 0xffff;
+}
 
 // wave vectors: [dif & 1] holds wave dif, so a wave reads the previous one while it writes
 template <int RG>
 struct WaveSmem
 {
-    unsigned long long T[2][RG];
-    int V[2][RG], HA[2][RG], HB[2][RG], NA[2][RG], NB[2][RG];
+    unsigned long long T[2][ring_of<RG>()];
+    int V[2][ring_of<RG>()], HA[2][ring_of<RG>()], HB[2][ring_of<RG>()], NA[2][ring_of<RG>()], NB[2][ring_of<RG>()];
 };
 
 struct LAPath
@@ -62,6 +70,14 @@ struct WarpSmem
     int besty;    // y of the best anti-diagonal
 };
 
+// The lanes that align one pair group together: a whole warp, or in the duo instance a
+// half-warp team of 16 (two pair groups per warp).
+template <int RG>
+constexpr int team_width()
+{
+    return (RG >> 16) ? 16 : 32;
+}
+
 template <int RG>
 struct WarpCtx
 {
@@ -71,11 +87,94 @@ struct WarpCtx
     uint16_t* pts;
     int ptscap;
     DevStatus* st;
-    int lane;
+    int lane;        // lane within the team
     int err;         // 1: failed (status set); 2: the band outgrew this instance (the caller decides)
     int item;
     unsigned cells;  // wave cells of the current pair group (or seed)
+    unsigned tmask;  // the team's lanes in the warp (half-warp teams only)
+    int tbase;       // the team's first lane in the warp (half-warp teams only)
 };
+
+// Warp collectives over a team: the whole warp (constant masks, as plain warp code) or a
+// half-warp (its mask; ballots and match masks shifted to the team's 16 bits).
+template <int RG>
+__device__ __forceinline__ unsigned tmask(const WarpCtx<RG>& w)
+{
+    if constexpr (team_width<RG>() == 32)
+        return GD_FULL;
+    else
+        return w.tmask;
+}
+
+template <int RG>
+__device__ __forceinline__ unsigned tballot(const WarpCtx<RG>& w, bool p)
+{
+    if constexpr (team_width<RG>() == 32)
+        return __ballot_sync(GD_FULL, p);
+    else
+        return (__ballot_sync(w.tmask, p) >> w.tbase) & 0xffffu;
+}
+
+template <int RG>
+__device__ __forceinline__ bool tany(const WarpCtx<RG>& w, bool p)
+{
+    return __any_sync(tmask(w), p);
+}
+
+template <int RG, typename T>
+__device__ __forceinline__ T tshfl(const WarpCtx<RG>& w, T v, int src)
+{
+    return __shfl_sync(tmask(w), v, src, team_width<RG>());
+}
+
+template <int RG, typename T>
+__device__ __forceinline__ T tshfl_up(const WarpCtx<RG>& w, T v, int o)
+{
+    return __shfl_up_sync(tmask(w), v, o, team_width<RG>());
+}
+
+template <int RG>
+__device__ __forceinline__ int tmax(const WarpCtx<RG>& w, int v)
+{
+    return __reduce_max_sync(tmask(w), v);
+}
+
+template <int RG>
+__device__ __forceinline__ int tmin(const WarpCtx<RG>& w, int v)
+{
+    return __reduce_min_sync(tmask(w), v);
+}
+
+template <int RG>
+__device__ __forceinline__ int tadd(const WarpCtx<RG>& w, int v)
+{
+    return __reduce_add_sync(tmask(w), v);
+}
+
+template <int RG>
+__device__ __forceinline__ unsigned tmatch(const WarpCtx<RG>& w, unsigned v)
+{
+    if constexpr (team_width<RG>() == 32)
+        return __match_any_sync(GD_FULL, v);
+    else
+        return (__match_any_sync(w.tmask, v) >> w.tbase) & 0xffffu;
+}
+
+template <int RG>
+__device__ __forceinline__ void tsync(const WarpCtx<RG>& w)
+{
+    __syncwarp(tmask(w));
+}
+
+// lanes of the team below this one
+template <int RG>
+__device__ __forceinline__ unsigned tlt(const WarpCtx<RG>& w)
+{
+    if constexpr (team_width<RG>() == 32)
+        return lanemask_lt();
+    else
+        return (1u << w.lane) - 1u;
+}
 
 __device__ __forceinline__ unsigned ld4u(const uint8_t* p)
 {
@@ -86,8 +185,7 @@ __device__ __forceinline__ unsigned ld4u(const uint8_t* p)
 
 // Extend the match on diagonal k from b-position y forward (FWD) or backward.
 // Returns the new y; sets bend/aend like the reference's snake loop (align.c:798-824).
-template <bool FWD>
-__device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, int y, int k, int lim, bool& bend,
+__device__ __forceinline__ int snake(const bool FWD, const uint8_t* aseq, const uint8_t* bseq, int y, int k, int lim, bool& bend,
                                      bool& aend)
 {
     if (FWD)
@@ -137,8 +235,7 @@ __device__ __forceinline__ int snake(const uint8_t* aseq, const uint8_t* bseq, i
 // bases per step (one funnel shift per sequence), the read ends found from the lengths
 // instead of the 4s: the extension stops at the first mismatch, the end of b (bend, also when
 // both end there) or the end of a (aend), as the 4s stop the byte loop.
-template <bool FWD>
-__device__ __forceinline__ int snake_pk(const uint32_t* __restrict__ apk, uint32_t ag,
+__device__ __forceinline__ int snake_pk(const bool FWD, const uint32_t* __restrict__ apk, uint32_t ag,
                                         const uint32_t* __restrict__ bpk, uint32_t bg, int y, int k, int alen,
                                         int blen, bool& bend, bool& aend)
 {
@@ -190,27 +287,37 @@ __device__ __forceinline__ int peb_one(WarpCtx<RG>& w, int& npeb, int ptr, int d
     return idx;
 }
 
-// forward_wave (FWD) / reverse_wave (!FWD) restated, with lanes over diagonals.
-template <bool FWD, int RG, bool PK>
-__device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0,
-                     const uint32_t* apk, uint32_t ag, const uint32_t* bpk, uint32_t bg, int alen, int blen,
-                     int comp, LAPath* apath, LAPath* bpath, int* mind, int maxd, int mida, int minp, int maxp,
-                     uint16_t* atrace, uint16_t* btrace)
+// The wave's state between waves (forward_wave / reverse_wave's loop-carried locals).
+struct WaveVars
+{
+    int hgh, low, dif, more, aclip, bclip, besta, lasta, npeb;
+};
+
+// forward_wave (FWD) / reverse_wave (!FWD) restated, with lanes over diagonals, in three
+// parts so that a caller can run it a wave at a time: wave_begin (the 0-wave from the seed
+// point), wave_step (one wave; false when the wave loop ends, or on an error in w.err) and
+// wave_end (the trace points of both paths from the pebble chains).
+template <int RG, bool PK>
+__device__ __forceinline__ void wave_begin(const bool FWD, WarpCtx<RG>& w, WaveVars& wvars, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0,
+    const uint32_t* apk, uint32_t ag, const uint32_t* bpk, uint32_t bg, int alen, int blen, int comp, int low0, int maxd, int mida)
 {
     WaveSmem<RG>& R = w.sm->ws;
     const int lane = w.lane;
     const int TS = P.tspace;
     const int S = FWD ? 1 : -1;
     const int VNONE = FWD ? -1 : INT_MAX;
-    int hgh = maxd, low = *mind, dif = 0;
     const int boff = comp ? blen % TS : 0;
+    int* const trim = w.sm->trim;
+    int* const clipm = w.sm->clipm;
+    const uint8_t* as = FWD ? aseq0 : aseq0 - 1;
+    const uint8_t* bs = FWD ? bseq0 : bseq0 - 1;
+    (void)S; (void)VNONE; (void)boff; (void)as; (void)bs; (void)trim; (void)clipm; (void)R; (void)TS; (void)lane;
+    int hgh = maxd, low = low0, dif = 0;
     int more = 1;
     int aclip = FWD ? INT_MAX : -INT_MAX;
     int bclip = FWD ? -INT_MAX : INT_MAX;
     int besta, lasta;
     besta = lasta = mida;
-    int* const trim = w.sm->trim;  // [0] a-diag, [1] y, [2] diffs, [3] A head, [4] B head
-    int* const clipm = w.sm->clipm;  // [0] M count (-1: none), [1] a-diag, [2] y, [3] diffs, [4] A head, [5] B head
     if (lane == 0)
     {
         trim[0] = mida;
@@ -222,15 +329,13 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
         w.sm->besty = (mida - hgh) >> 1;
     }
     int npeb = 0;
-    // the reverse wave compares the bases just before the point (align.c:1117-1118)
-    const uint8_t* as = FWD ? aseq0 : aseq0 - 1;
-    const uint8_t* bs = FWD ? bseq0 : bseq0 - 1;
 
     if (low != hgh)
     {
         if (lane == 0)
             gd_fail(w.st, GD_ERR_BAND_WIDTH, w.item, -1);
         w.err = 1;
+        wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
         return;
     }
 
@@ -256,8 +361,8 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
             hb = peb_one(w, npeb, -1, k, 0, y);
         }
         bool bend, aend;
-        y = PK ? snake_pk<FWD>(apk, ag, bpk, bg, y, k, alen, blen, bend, aend)
-               : snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
+        y = PK ? snake_pk(FWD, apk, ag, bpk, bg, y, k, alen, blen, bend, aend)
+               : snake(FWD, aseq0, bseq0, y, k, blen + 16, bend, aend);
         if (bend)
         {
             more = 0;
@@ -316,10 +421,13 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
             R.NA[0][k & RM] = na;
             R.NB[0][k & RM] = nb;
         }
-        __syncwarp();
+        tsync(w);
     }
     if (w.err)
+    {
+        wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
         return;
+    }
 
     auto clip_block = [&]() {
         if (!more)
@@ -345,7 +453,7 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
                     clipm[4] = R.HA[dif & 1][aclip & RM];
                     clipm[5] = R.HB[dif & 1][aclip & RM];
                 }
-                __syncwarp();
+                tsync(w);
             }
             if (FWD ? (low <= bclip) : (hgh >= bclip))
             {
@@ -363,217 +471,319 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
                     clipm[4] = R.HA[dif & 1][bclip & RM];
                     clipm[5] = R.HB[dif & 1][bclip & RM];
                 }
-                __syncwarp();
+                tsync(w);
             }
             aclip = FWD ? INT_MAX : -INT_MAX;
             bclip = FWD ? -INT_MAX : INT_MAX;
         }
     };
     clip_block();
+    wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
+}
 
-    const unsigned lt = lanemask_lt();
-    const int PATH_AVE = P.ave_path;
-
-    // ---- successive waves
-    while (more && (FWD ? (lasta >= besta - TRIM_MLAG) : (lasta <= besta + TRIM_MLAG)))
-    {
-        // widen the band by one each side (align.c:636-745).  Diagonals outside the previous
-        // band read as VNONE and new end diagonals take their inner neighbour's NA/NB: the
-        // reference writes those values into its vectors first, here they are read that way.
-        const int olow = low, ohgh = hgh;
-        if (olow > ohgh)  // every diagonal fell WAVE_LAG behind: the reference would read stale vectors
+template <int RG, bool PK>
+__device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVars& wvars, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0,
+    const uint32_t* apk, uint32_t ag, const uint32_t* bpk, uint32_t bg, int alen, int blen, int comp, int minp, int maxp)
+{
+    WaveSmem<RG>& R = w.sm->ws;
+    const int lane = w.lane;
+    const int TS = P.tspace;
+    const int S = FWD ? 1 : -1;
+    const int VNONE = FWD ? -1 : INT_MAX;
+    const int boff = comp ? blen % TS : 0;
+    int* const trim = w.sm->trim;
+    int* const clipm = w.sm->clipm;
+    const uint8_t* as = FWD ? aseq0 : aseq0 - 1;
+    const uint8_t* bs = FWD ? bseq0 : bseq0 - 1;
+    (void)S; (void)VNONE; (void)boff; (void)as; (void)bs; (void)trim; (void)clipm; (void)R; (void)TS; (void)lane;
+    int hgh = wvars.hgh, low = wvars.low, dif = wvars.dif, more = wvars.more;
+    int aclip = wvars.aclip, bclip = wvars.bclip, besta = wvars.besta, lasta = wvars.lasta, npeb = wvars.npeb;
+    auto clip_block = [&]() {
+        if (!more)
         {
-            if (lane == 0)
-                gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
-            w.err = 1;
-            return;
-        }
-        low -= 1;
-        hgh += 1;
-        if (low < minp)
-            low += 1;
-        if (hgh > maxp)
-            hgh -= 1;
-        dif += 1;
-        if (dif > alen + blen + 2)  // the edit distance cannot exceed alen + blen
-        {
-            if (lane == 0)
-                gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
-            w.err = 1;
-            return;
-        }
-        const int width = hgh - low + 1;
-        if ((unsigned)(width - 1) >= (unsigned)RG)  // empty, or wider than this instance
-        {
-            if (width > RG)
-                w.err = 2;  // a wider instance may take this pair (the caller decides)
-            else
+            const int besty = w.sm->besty;
+            // the best point is not at a read end (the bytes there are 4s)
+            if (PK ? (FWD ? (besty < blen && besta - besty < alen) : (besty > 0 && besta - besty > 0))
+                   : (__ldg(bs + besty) != 4 && __ldg(as + besta - besty) != 4))
+                more = 1;
+            if (FWD ? (hgh >= aclip) : (low <= aclip))
             {
-                if (lane == 0)
-                    gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, width);
-                w.err = 1;
-            }
-            return;
-        }
-        const int nch = (width + 31) >> 5;
-        const int hgh0 = hgh, low0 = low;
-        const int cur = dif & 1, prv = cur ^ 1;
-        int c0 = 0;  // chunk 0's new V, for the WAVE_LAG test
-#pragma unroll
-        for (int ch = 0; ch < RG / 32; ch++)
-        {
-            if (ch >= nch)
-                break;
-            const int p = ch * 32 + lane;
-            const bool valid = p < width;
-            const int k = FWD ? hgh - p : low + p;
-            int c = 0, y = 0, ha = 0, hb = 0, na = 0, nb = 0;
-            unsigned long long b = 0;
-            bool bend = false, aend = false;
-            if (valid)
-            {
-                // choose the furthest of the three predecessors (align.c:748-797)
-                const int kP = k + S, kN = k - S;
-                int vP = (kP >= olow && kP <= ohgh) ? R.V[prv][kP & RM] : VNONE;
-                int vC = (k >= olow && k <= ohgh) ? R.V[prv][k & RM] : VNONE;
-                int vN = (kN >= olow && kN <= ohgh) ? R.V[prv][kN & RM] : VNONE;
-                int wP = FWD ? vP : -vP, wC = FWD ? vC : -vC, wN = FWD ? vN : -vN;
-                int ks, vs, step;
-                if (wC < wN)
+                if (FWD)
+                    hgh = aclip - 1;
+                else
+                    low = aclip + 1;
+                int Mc = __popcll(R.T[dif & 1][aclip & RM] & MASK61);
+                if (lane == 0 && clipm[0] <= Mc)
                 {
-                    if (wN < wP)
-                    {
-                        ks = k + S;
-                        vs = vP;
-                    }
-                    else
-                    {
-                        ks = k - S;
-                        vs = vN;
-                    }
-                    step = 1;
+                    clipm[0] = Mc;
+                    clipm[1] = R.V[dif & 1][aclip & RM];
+                    clipm[2] = (clipm[1] - aclip) / 2;
+                    clipm[3] = dif;
+                    clipm[4] = R.HA[dif & 1][aclip & RM];
+                    clipm[5] = R.HB[dif & 1][aclip & RM];
                 }
-                else if (wC < wP)
+                tsync(w);
+            }
+            if (FWD ? (low <= bclip) : (hgh >= bclip))
+            {
+                if (FWD)
+                    low = bclip + 1;
+                else
+                    hgh = bclip - 1;
+                int Mc = __popcll(R.T[dif & 1][bclip & RM] & MASK61);
+                if (lane == 0 && clipm[0] <= Mc)
+                {
+                    clipm[0] = Mc;
+                    clipm[1] = R.V[dif & 1][bclip & RM];
+                    clipm[2] = (clipm[1] - bclip) / 2;
+                    clipm[3] = dif;
+                    clipm[4] = R.HA[dif & 1][bclip & RM];
+                    clipm[5] = R.HB[dif & 1][bclip & RM];
+                }
+                tsync(w);
+            }
+            aclip = FWD ? INT_MAX : -INT_MAX;
+            bclip = FWD ? -INT_MAX : INT_MAX;
+        }
+    };
+
+    const unsigned lt = tlt(w);
+    const int PATH_AVE = P.ave_path;
+    if (!(more && (FWD ? (lasta >= besta - TRIM_MLAG) : (lasta <= besta + TRIM_MLAG))))
+        return false;
+    // widen the band by one each side (align.c:636-745).  Diagonals outside the previous
+    // band read as VNONE and new end diagonals take their inner neighbour's NA/NB: the
+    // reference writes those values into its vectors first, here they are read that way.
+    const int olow = low, ohgh = hgh;
+    if (olow > ohgh)  // every diagonal fell WAVE_LAG behind: the reference would read stale vectors
+    {
+        if (lane == 0)
+            gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
+        w.err = 1;
+        wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
+        return false;
+    }
+    low -= 1;
+    hgh += 1;
+    if (low < minp)
+        low += 1;
+    if (hgh > maxp)
+        hgh -= 1;
+    dif += 1;
+    if (dif > alen + blen + 2)  // the edit distance cannot exceed alen + blen
+    {
+        if (lane == 0)
+            gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
+        w.err = 1;
+        wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
+        return false;
+    }
+    const int width = hgh - low + 1;
+    if ((unsigned)(width - 1) >= (unsigned)ring_of<RG>())  // empty, or wider than this instance
+    {
+        if (width > ring_of<RG>())
+            w.err = 2;  // a wider instance may take this pair (the caller decides)
+        else
+        {
+            if (lane == 0)
+                gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, width);
+            w.err = 1;
+        }
+        wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
+        return false;
+    }
+    constexpr int TW = team_width<RG>();
+    const int nch = (width + TW - 1) / TW;
+    const int hgh0 = hgh, low0 = low;
+    const int cur = dif & 1, prv = cur ^ 1;
+    int c0 = 0;  // chunk 0's new V, for the WAVE_LAG test
+#pragma unroll
+    for (int ch = 0; ch < ring_of<RG>() / TW; ch++)
+    {
+        if (ch >= nch)
+            break;
+        const int p = ch * TW + lane;
+        const bool valid = p < width;
+        const int k = FWD ? hgh - p : low + p;
+        int c = 0, y = 0, ha = 0, hb = 0, na = 0, nb = 0;
+        unsigned long long b = 0;
+        bool bend = false, aend = false;
+        if (valid)
+        {
+            // choose the furthest of the three predecessors (align.c:748-797)
+            const int kP = k + S, kN = k - S;
+            int vP = (kP >= olow && kP <= ohgh) ? R.V[prv][kP & RM] : VNONE;
+            int vC = (k >= olow && k <= ohgh) ? R.V[prv][k & RM] : VNONE;
+            int vN = (kN >= olow && kN <= ohgh) ? R.V[prv][kN & RM] : VNONE;
+            int wP = FWD ? vP : -vP, wC = FWD ? vC : -vC, wN = FWD ? vN : -vN;
+            int ks, vs, step;
+            if (wC < wN)
+            {
+                if (wN < wP)
                 {
                     ks = k + S;
                     vs = vP;
-                    step = 1;
                 }
                 else
                 {
-                    ks = k;
-                    vs = vC;
-                    step = 2;
+                    ks = k - S;
+                    vs = vN;
                 }
-                c = vs + S * step;
-                b = R.T[prv][ks & RM] << 1;
-                ha = R.HA[prv][ks & RM];
-                hb = R.HB[prv][ks & RM];
-                y = (c - k) >> 1;
-                int y0 = y;
-                y = PK ? snake_pk<FWD>(apk, ag, bpk, bg, y, k, alen, blen, bend, aend)
-               : snake<FWD>(aseq0, bseq0, y, k, blen + 16, bend, aend);
-                int L = FWD ? (y - y0) : (y0 - y);
-                b = (L >= 61) ? ~0ull : ((b << L) | ((1ull << L) - 1ull));
-                c = (y << 1) + k;
-                const int kn = k < olow ? olow : (k > ohgh ? ohgh : k);
-                na = R.NA[prv][kn & RM];
-                nb = R.NB[prv][kn & RM];
+                step = 1;
             }
-            // trace points of A and B crossed by this extension (align.c:826-878)
-            while (true)
+            else if (wC < wP)
             {
-                bool needA = valid && (FWD ? (y + k >= na) : (y + k <= na));
-                bool needB = valid && (FWD ? (y >= nb) : (y <= nb));
-                if (!__any_sync(GD_FULL, needA || needB))
-                    break;
-                bool cA = needA && (FWD ? (w.peb[ha].w < na) : (w.peb[ha].w > na));
-                bool cB = needB && (FWD ? (w.peb[hb].w < nb) : (w.peb[hb].w > nb));
-                unsigned ma = __ballot_sync(GD_FULL, cA), mbb = __ballot_sync(GD_FULL, cB);
-                if (ma | mbb)
+                ks = k + S;
+                vs = vP;
+                step = 1;
+            }
+            else
+            {
+                ks = k;
+                vs = vC;
+                step = 2;
+            }
+            c = vs + S * step;
+            b = R.T[prv][ks & RM] << 1;
+            ha = R.HA[prv][ks & RM];
+            hb = R.HB[prv][ks & RM];
+            y = (c - k) >> 1;
+            int y0 = y;
+            y = PK ? snake_pk(FWD, apk, ag, bpk, bg, y, k, alen, blen, bend, aend)
+           : snake(FWD, aseq0, bseq0, y, k, blen + 16, bend, aend);
+            int L = FWD ? (y - y0) : (y0 - y);
+            b = (L >= 61) ? ~0ull : ((b << L) | ((1ull << L) - 1ull));
+            c = (y << 1) + k;
+            const int kn = k < olow ? olow : (k > ohgh ? ohgh : k);
+            na = R.NA[prv][kn & RM];
+            nb = R.NB[prv][kn & RM];
+        }
+        // trace points of A and B crossed by this extension (align.c:826-878)
+        while (true)
+        {
+            bool needA = valid && (FWD ? (y + k >= na) : (y + k <= na));
+            bool needB = valid && (FWD ? (y >= nb) : (y <= nb));
+            if (!tany(w, needA || needB))
+                break;
+            bool cA = needA && (FWD ? (w.peb[ha].w < na) : (w.peb[ha].w > na));
+            bool cB = needB && (FWD ? (w.peb[hb].w < nb) : (w.peb[hb].w > nb));
+            unsigned ma = tballot(w, cA), mbb = tballot(w, cB);
+            if (ma | mbb)
+            {
+                int base = npeb;
+                npeb += __popc(ma) + __popc(mbb);
+                if (npeb > w.pcap)
                 {
-                    int base = npeb;
-                    npeb += __popc(ma) + __popc(mbb);
-                    if (npeb > w.pcap)
-                    {
-                        if (lane == 0)
-                            gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
-                        w.err = 1;
-                        return;
-                    }
-                    if (cA)
-                    {
-                        int idx = base + __popc(ma & lt);
-                        w.peb[idx] = make_int4(ha, k, dif, na);
-                        ha = idx;
-                    }
-                    if (cB)
-                    {
-                        int idx = base + __popc(ma) + __popc(mbb & lt);
-                        w.peb[idx] = make_int4(hb, k, dif, nb);
-                        hb = idx;
-                    }
+                    if (lane == 0)
+                        gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
+                    w.err = 1;
+                    wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
+                    return false;
                 }
-                if (needA)
-                    na += FWD ? TS : -TS;
-                if (needB)
-                    nb += FWD ? TS : -TS;
+                if (cA)
+                {
+                    int idx = base + __popc(ma & lt);
+                    w.peb[idx] = make_int4(ha, k, dif, na);
+                    ha = idx;
+                }
+                if (cB)
+                {
+                    int idx = base + __popc(ma) + __popc(mbb & lt);
+                    w.peb[idx] = make_int4(hb, k, dif, nb);
+                    hb = idx;
+                }
             }
-            if (ch == 0)
-                c0 = c;
-            if (valid)
-            {
-                R.V[cur][k & RM] = c;
-                R.T[cur][k & RM] = b;
-                R.HA[cur][k & RM] = ha;
-                R.HB[cur][k & RM] = hb;
-                R.NA[cur][k & RM] = na;
-                R.NB[cur][k & RM] = nb;
-            }
+            if (needA)
+                na += FWD ? TS : -TS;
+            if (needB)
+                nb += FWD ? TS : -TS;
+        }
+        if (ch == 0)
+            c0 = c;
+        if (valid)
+        {
+            R.V[cur][k & RM] = c;
+            R.T[cur][k & RM] = b;
+            R.HA[cur][k & RM] = ha;
+            R.HB[cur][k & RM] = hb;
+            R.NA[cur][k & RM] = na;
+            R.NB[cur][k & RM] = nb;
+        }
 
-            // clip bookkeeping: bclip = first B-end in scan order, aclip = last A-end
-            unsigned bm = __ballot_sync(GD_FULL, valid && bend);
-            if (bm)
-            {
-                int pb = ch * 32 + __ffs(bm) - 1;
-                int kb = FWD ? hgh - pb : low + pb;
-                bclip = FWD ? max(bclip, kb) : min(bclip, kb);
-                more = 0;
-            }
-            unsigned amk = __ballot_sync(GD_FULL, valid && aend);
-            if (amk)
-            {
-                int pa = ch * 32 + 31 - __clz(amk);
-                aclip = FWD ? hgh - pa : low + pa;
-                more = 0;
-            }
+        // clip bookkeeping: bclip = first B-end in scan order, aclip = last A-end
+        unsigned bm = tballot(w, valid && bend);
+        if (bm)
+        {
+            int pb = ch * TW + __ffs(bm) - 1;
+            int kb = FWD ? hgh - pb : low + pb;
+            bclip = FWD ? max(bclip, kb) : min(bclip, kb);
+            more = 0;
+        }
+        unsigned amk = tballot(w, valid && aend);
+        if (amk)
+        {
+            int pa = ch * TW + 31 - __clz(amk);
+            aclip = FWD ? hgh - pa : low + pa;
+            more = 0;
+        }
 
-            // best point: every new maximum in scan order is a record (align.c:880-897).  The
-            // last record is the first lane holding the chunk maximum; when it also passes the
-            // PATH_AVE and trim-table tests it decides besta, lasta and trim at once, otherwise
-            // the records are enumerated with a prefix-max scan.
-            int wv = valid ? (FWD ? c : -c) : INT_MIN;
-            int wbest = FWD ? besta : -besta;
-            // the PATH_AVE and trim tests, in parallel with the reduction, of the lanes that can be
-            // records (above the best so far): only records read them, so the others skip the
-            // table lookups
-            const bool q1 = valid && wv > wbest && __popcll(b & MASK61) >= PATH_AVE;
-            const bool q2 = q1 && trim_ok(b, P.table, P.score);
-            int wmax = __reduce_max_sync(GD_FULL, wv);
-            if (wmax > wbest)
+        // best point: every new maximum in scan order is a record (align.c:880-897).  The
+        // last record is the first lane holding the chunk maximum; when it also passes the
+        // PATH_AVE and trim-table tests it decides besta, lasta and trim at once, otherwise
+        // the records are enumerated with a prefix-max scan.
+        int wv = valid ? (FWD ? c : -c) : INT_MIN;
+        int wbest = FWD ? besta : -besta;
+        // the PATH_AVE and trim tests, in parallel with the reduction, of the lanes that can be
+        // records (above the best so far): only records read them, so the others skip the
+        // table lookups
+        const bool q1 = valid && wv > wbest && __popcll(b & MASK61) >= PATH_AVE;
+        const bool q2 = q1 && trim_ok(b, P.table, P.score);
+        int wmax = tmax(w, wv);
+        if (wmax > wbest)
+        {
+            int jm = __ffs(tballot(w, wv == wmax)) - 1;
+            const unsigned mq1 = tballot(w, q1), mq2 = tballot(w, q2);
+            besta = tshfl(w, c, jm);
+            if (lane == jm)
+                w.sm->besty = y;
+            bool p1j = (mq1 >> jm) & 1;
+            bool p2j = (mq2 >> jm) & 1;
+            if (p1j)
+                lasta = besta;
+            if (p2j)
             {
-                int jm = __ffs(__ballot_sync(GD_FULL, wv == wmax)) - 1;
-                const unsigned mq1 = __ballot_sync(GD_FULL, q1), mq2 = __ballot_sync(GD_FULL, q2);
-                besta = __shfl_sync(GD_FULL, c, jm);
                 if (lane == jm)
-                    w.sm->besty = y;
-                bool p1j = (mq1 >> jm) & 1;
-                bool p2j = (mq2 >> jm) & 1;
-                if (p1j)
-                    lasta = besta;
-                if (p2j)
                 {
-                    if (lane == jm)
+                    trim[0] = c;
+                    trim[1] = y;
+                    trim[2] = dif;
+                    trim[3] = ha;
+                    trim[4] = hb;
+                }
+            }
+            else
+            {
+                // prefix max over the lanes before jm only (records lie before the maximum)
+                int incl = wv;
+                for (int o = 1; o < jm; o <<= 1)
+                {
+                    int t = tshfl_up(w, incl, o);
+                    if (lane >= o)
+                        incl = max(incl, t);
+                }
+                int excl = tshfl_up(w, incl, 1);
+                if (lane == 0)
+                    excl = INT_MIN;
+                bool rec = valid && wv > max(wbest, excl) && lane < jm;
+                unsigned mrec = tballot(w, rec);
+                unsigned m1 = mrec & mq1;
+                if (m1 && !p1j)
+                    lasta = tshfl(w, c, 31 - __clz(m1));
+                unsigned m2 = mrec & mq2;
+                if (m2)
+                {
+                    int j2 = 31 - __clz(m2);
+                    if (lane == j2)
                     {
                         trim[0] = c;
                         trim[1] = y;
@@ -582,72 +792,409 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
                         trim[4] = hb;
                     }
                 }
-                else
-                {
-                    // prefix max over the lanes before jm only (records lie before the maximum)
-                    int incl = wv;
-                    for (int o = 1; o < jm; o <<= 1)
-                    {
-                        int t = __shfl_up_sync(GD_FULL, incl, o);
-                        if (lane >= o)
-                            incl = max(incl, t);
-                    }
-                    int excl = __shfl_up_sync(GD_FULL, incl, 1);
-                    if (lane == 0)
-                        excl = INT_MIN;
-                    bool rec = valid && wv > max(wbest, excl) && lane < jm;
-                    unsigned mrec = __ballot_sync(GD_FULL, rec);
-                    unsigned m1 = mrec & mq1;
-                    if (m1 && !p1j)
-                        lasta = __shfl_sync(GD_FULL, c, 31 - __clz(m1));
-                    unsigned m2 = mrec & mq2;
-                    if (m2)
-                    {
-                        int j2 = 31 - __clz(m2);
-                        if (lane == j2)
-                        {
-                            trim[0] = c;
-                            trim[1] = y;
-                            trim[2] = dif;
-                            trim[3] = ha;
-                            trim[4] = hb;
-                        }
-                    }
-                }
-                __syncwarp();  // a later chunk's best point and trim point overwrite these
+            }
+            tsync(w);  // a later chunk's best point and trim point overwrite these
+        }
+    }
+    tsync(w);
+    clip_block();
+
+    // drop diagonals more than WAVE_LAG behind the best (align.c:946-955), from this
+    // wave's ring; k runs monotonically with the lane position
+    {
+        const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
+        const int hw = FWD ? hgh0 : low0;  // wave origin before clipping
+        int nl = INT_MAX, nh = INT_MIN;
+#pragma unroll
+        for (int ch = 0; ch < ring_of<RG>() / TW; ch++)
+        {
+            if (ch >= nch)
+                break;
+            int p = ch * TW + lane;
+            int k = FWD ? hw - p : hw + p;
+            bool good = p < width && k >= low && k <= hgh;
+            if (good)
+            {
+                const int v = ch == 0 ? c0 : R.V[cur][k & RM];
+                good = FWD ? (v >= n) : (v <= n);
+            }
+            unsigned gm = tballot(w, good);
+            if (gm)
+            {
+                int pf = ch * TW + __ffs(gm) - 1, pl = ch * TW + 31 - __clz(gm);
+                int k1 = FWD ? hw - pf : hw + pf, k2 = FWD ? hw - pl : hw + pl;
+                nl = min(nl, min(k1, k2));
+                nh = max(nh, max(k1, k2));
             }
         }
-        __syncwarp();
-        clip_block();
-
-        // drop diagonals more than WAVE_LAG behind the best (align.c:946-955), from this
-        // wave's ring; k runs monotonically with the lane position
+        if (nh != INT_MIN)
         {
-            const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
-            const int hw = FWD ? hgh0 : low0;  // wave origin before clipping
-            int nl = INT_MAX, nh = INT_MIN;
+            hgh = nh;
+            low = nl;
+        }
+        else
+            hgh = low - 1;
+    }
+    w.cells += hgh - low + 1;
+    wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
+    return true;
+}
+
+// One wave of both teams of a duo warp at once: wave_step's work, for each team on its own
+// diagonals, with every instruction run by all 32 lanes.  Every collective is whole-warp (a
+// team reads its half of a ballot, shuffles within its 16 lanes, reduces by a 16-lane
+// butterfly) and every branch around one is taken when either team needs it, with the
+// team's own effects predicated, so that the two teams' waves share each issue slot instead
+// of taking turns.  go: this team is in a wave.  Returns whether the team's wave loop goes on
+// (false: it ended, or an error in w.err); a team that was not in a wave keeps its state.
+__device__ __forceinline__ bool wave_step_duo(bool go, const bool FWD, WarpCtx<DUO>& w, WaveVars& wvars,
+                                              const AlignParams& P, const uint32_t* apk, uint32_t ag,
+                                              const uint32_t* bpk, uint32_t bg, int alen, int blen, int minp,
+                                              int maxp)
+{
+    constexpr int RG = DUO;
+    constexpr int TW = 16;
+    constexpr int NR = ring_of<RG>();
+    WaveSmem<RG>& R = w.sm->ws;
+    const int lane = w.lane;
+    const int tb = w.tbase;
+    const int TS = P.tspace;
+    const int S = FWD ? 1 : -1;
+    const int VNONE = FWD ? -1 : INT_MAX;
+    int* const trim = w.sm->trim;
+    int* const clipm = w.sm->clipm;
+    int hgh = wvars.hgh, low = wvars.low, dif = wvars.dif, more = wvars.more;
+    int aclip = wvars.aclip, bclip = wvars.bclip, besta = wvars.besta, lasta = wvars.lasta, npeb = wvars.npeb;
+    const int PATH_AVE = P.ave_path;
+    auto half = [&](bool p) { return (__ballot_sync(GD_FULL, p) >> tb) & 0xffffu; };
+
+    go = go && more && (FWD ? (lasta >= besta - TRIM_MLAG) : (lasta <= besta + TRIM_MLAG));
+    if (!__any_sync(GD_FULL, go))
+        return false;
+    // widen the band by one each side (align.c:636-745); the checks of wave_step
+    const int olow = low, ohgh = hgh;
+    if (go && olow > ohgh)
+    {
+        if (lane == 0)
+            gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
+        w.err = 1;
+        go = false;
+    }
+    if (go)
+    {
+        low -= 1;
+        hgh += 1;
+        if (low < minp)
+            low += 1;
+        if (hgh > maxp)
+            hgh -= 1;
+        dif += 1;
+        if (dif > alen + blen + 2)
+        {
+            if (lane == 0)
+                gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, dif);
+            w.err = 1;
+            go = false;
+        }
+    }
+    int width = go ? hgh - low + 1 : 0;
+    if (go && (unsigned)(width - 1) >= (unsigned)NR)
+    {
+        if (width > NR)
+            w.err = 2;
+        else
+        {
+            if (lane == 0)
+                gd_fail(w.st, GD_ERR_EMPTY_BAND, w.item, width);
+            w.err = 1;
+        }
+        go = false;
+        width = 0;
+    }
+    const int nch = (width + TW - 1) / TW;
+    const int nchw = max(nch, __shfl_xor_sync(GD_FULL, nch, 16));  // chunks of the wider team
+    const int hgh0 = hgh, low0 = low;
+    const int cur = dif & 1, prv = cur ^ 1;
+    const unsigned lt = (1u << lane) - 1u;
+    int c0 = 0;
 #pragma unroll
-            for (int ch = 0; ch < RG / 32; ch++)
+    for (int ch = 0; ch < NR / TW; ch++)
+    {
+        if (ch >= nchw)
+            break;
+        const int p = ch * TW + lane;
+        const bool valid = p < width;
+        const int k = FWD ? hgh - p : low + p;
+        int c = 0, y = 0, ha = 0, hb = 0, na = 0, nb = 0;
+        unsigned long long b = 0;
+        bool bend = false, aend = false;
+        if (valid)
+        {
+            // choose the furthest of the three predecessors (align.c:748-797)
+            const int kP = k + S, kN = k - S;
+            int vP = (kP >= olow && kP <= ohgh) ? R.V[prv][kP & RM] : VNONE;
+            int vC = (k >= olow && k <= ohgh) ? R.V[prv][k & RM] : VNONE;
+            int vN = (kN >= olow && kN <= ohgh) ? R.V[prv][kN & RM] : VNONE;
+            int wP = FWD ? vP : -vP, wC = FWD ? vC : -vC, wN = FWD ? vN : -vN;
+            int ks, vs, step;
+            if (wC < wN)
             {
-                if (ch >= nch)
-                    break;
-                int p = ch * 32 + lane;
-                int k = FWD ? hw - p : hw + p;
-                bool good = p < width && k >= low && k <= hgh;
-                if (good)
+                if (wN < wP)
                 {
-                    const int v = ch == 0 ? c0 : R.V[cur][k & RM];
-                    good = FWD ? (v >= n) : (v <= n);
+                    ks = k + S;
+                    vs = vP;
                 }
-                unsigned gm = __ballot_sync(GD_FULL, good);
-                if (gm)
+                else
                 {
-                    int pf = ch * 32 + __ffs(gm) - 1, pl = ch * 32 + 31 - __clz(gm);
-                    int k1 = FWD ? hw - pf : hw + pf, k2 = FWD ? hw - pl : hw + pl;
-                    nl = min(nl, min(k1, k2));
-                    nh = max(nh, max(k1, k2));
+                    ks = k - S;
+                    vs = vN;
+                }
+                step = 1;
+            }
+            else if (wC < wP)
+            {
+                ks = k + S;
+                vs = vP;
+                step = 1;
+            }
+            else
+            {
+                ks = k;
+                vs = vC;
+                step = 2;
+            }
+            c = vs + S * step;
+            b = R.T[prv][ks & RM] << 1;
+            ha = R.HA[prv][ks & RM];
+            hb = R.HB[prv][ks & RM];
+            y = (c - k) >> 1;
+            const int y0 = y;
+            y = snake_pk(FWD, apk, ag, bpk, bg, y, k, alen, blen, bend, aend);
+            const int L = FWD ? (y - y0) : (y0 - y);
+            b = (L >= 61) ? ~0ull : ((b << L) | ((1ull << L) - 1ull));
+            c = (y << 1) + k;
+            const int kn = k < olow ? olow : (k > ohgh ? ohgh : k);
+            na = R.NA[prv][kn & RM];
+            nb = R.NB[prv][kn & RM];
+        }
+        // trace points of A and B crossed by this extension (align.c:826-878)
+        while (true)
+        {
+            const bool needA = valid && go && (FWD ? (y + k >= na) : (y + k <= na));
+            const bool needB = valid && go && (FWD ? (y >= nb) : (y <= nb));
+            if (!__any_sync(GD_FULL, needA || needB))
+                break;
+            const bool cA = needA && (FWD ? (w.peb[ha].w < na) : (w.peb[ha].w > na));
+            const bool cB = needB && (FWD ? (w.peb[hb].w < nb) : (w.peb[hb].w > nb));
+            const unsigned ma = half(cA), mbb = half(cB);
+            if (ma | mbb)
+            {
+                const int base = npeb;
+                npeb += __popc(ma) + __popc(mbb);
+                if (npeb > w.pcap)
+                {
+                    if (lane == 0)
+                        gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
+                    w.err = 1;
+                    go = false;  // the team stops here; its lanes only join the warp's collectives
+                }
+                else
+                {
+                    if (cA)
+                    {
+                        const int idx = base + __popc(ma & lt);
+                        w.peb[idx] = make_int4(ha, k, dif, na);
+                        ha = idx;
+                    }
+                    if (cB)
+                    {
+                        const int idx = base + __popc(ma) + __popc(mbb & lt);
+                        w.peb[idx] = make_int4(hb, k, dif, nb);
+                        hb = idx;
+                    }
                 }
             }
+            if (needA)
+                na += FWD ? TS : -TS;
+            if (needB)
+                nb += FWD ? TS : -TS;
+        }
+        const bool live = valid && go;
+        if (ch == 0)
+            c0 = c;
+        if (live)
+        {
+            R.V[cur][k & RM] = c;
+            R.T[cur][k & RM] = b;
+            R.HA[cur][k & RM] = ha;
+            R.HB[cur][k & RM] = hb;
+            R.NA[cur][k & RM] = na;
+            R.NB[cur][k & RM] = nb;
+        }
+
+        // clip bookkeeping: bclip = first B-end in scan order, aclip = last A-end
+        const unsigned bm = half(live && bend);
+        if (bm)
+        {
+            const int pb = ch * TW + __ffs(bm) - 1;
+            const int kb = FWD ? hgh - pb : low + pb;
+            bclip = FWD ? max(bclip, kb) : min(bclip, kb);
+            more = 0;
+        }
+        const unsigned amk = half(live && aend);
+        if (amk)
+        {
+            const int pa = ch * TW + 31 - __clz(amk);
+            aclip = FWD ? hgh - pa : low + pa;
+            more = 0;
+        }
+
+        // best point: the records of wave_step, per team
+        const int wv = live ? (FWD ? c : -c) : INT_MIN;
+        const int wbest = FWD ? besta : -besta;
+        const bool q1 = live && wv > wbest && __popcll(b & MASK61) >= PATH_AVE;
+        const bool q2 = q1 && trim_ok(b, P.table, P.score);
+        int wmax = wv;
+#pragma unroll
+        for (int o = 8; o >= 1; o >>= 1)
+            wmax = max(wmax, __shfl_xor_sync(GD_FULL, wmax, o, 16));
+        const bool recT = go && wmax > wbest;
+        if (__any_sync(GD_FULL, recT))
+        {
+            const int jm = __ffs(half(wv == wmax)) - 1;
+            const unsigned mq1 = half(q1), mq2 = half(q2);
+            const int cj = __shfl_sync(GD_FULL, c, jm, 16);
+            const bool p1j = (mq1 >> jm) & 1;
+            const bool p2j = (mq2 >> jm) & 1;
+            if (recT)
+            {
+                besta = cj;
+                if (lane == jm)
+                    w.sm->besty = y;
+                if (p1j)
+                    lasta = besta;
+                if (p2j && lane == jm)
+                {
+                    trim[0] = c;
+                    trim[1] = y;
+                    trim[2] = dif;
+                    trim[3] = ha;
+                    trim[4] = hb;
+                }
+            }
+            // the records before jm, when the maximum itself does not settle the trim point
+            const bool scan = recT && !p2j;
+            if (__any_sync(GD_FULL, scan))
+            {
+                const int js = scan ? jm : 0;
+                const int jmw = max(js, __shfl_xor_sync(GD_FULL, js, 16));
+                int incl = wv;
+                for (int o = 1; o < jmw; o <<= 1)  // lanes at or past a team's jm are not read
+                {
+                    const int t = __shfl_up_sync(GD_FULL, incl, o, 16);
+                    if (lane >= o)
+                        incl = max(incl, t);
+                }
+                int excl = __shfl_up_sync(GD_FULL, incl, 1, 16);
+                if (lane == 0)
+                    excl = INT_MIN;
+                const bool rec = scan && live && wv > max(wbest, excl) && lane < jm;
+                const unsigned mrec = half(rec);
+                const unsigned m1 = mrec & mq1;
+                const int c1 = __shfl_sync(GD_FULL, c, m1 ? 31 - __clz(m1) : 0, 16);
+                if (scan && m1 && !p1j)
+                    lasta = c1;
+                const unsigned m2 = mrec & mq2;
+                if (scan && m2)
+                {
+                    const int j2 = 31 - __clz(m2);
+                    if (lane == j2)
+                    {
+                        trim[0] = c;
+                        trim[1] = y;
+                        trim[2] = dif;
+                        trim[3] = ha;
+                        trim[4] = hb;
+                    }
+                }
+            }
+            __syncwarp();  // a later chunk's best point and trim point overwrite these
+        }
+    }
+    __syncwarp();
+    // clip_block of wave_step (lane 0 alone writes and reads the clip fallback)
+    if (go && !more)
+    {
+        const int besty = w.sm->besty;
+        if (FWD ? (besty < blen && besta - besty < alen) : (besty > 0 && besta - besty > 0))
+            more = 1;
+        if (FWD ? (hgh >= aclip) : (low <= aclip))
+        {
+            if (FWD)
+                hgh = aclip - 1;
+            else
+                low = aclip + 1;
+            const int Mc = __popcll(R.T[dif & 1][aclip & RM] & MASK61);
+            if (lane == 0 && clipm[0] <= Mc)
+            {
+                clipm[0] = Mc;
+                clipm[1] = R.V[dif & 1][aclip & RM];
+                clipm[2] = (clipm[1] - aclip) / 2;
+                clipm[3] = dif;
+                clipm[4] = R.HA[dif & 1][aclip & RM];
+                clipm[5] = R.HB[dif & 1][aclip & RM];
+            }
+        }
+        if (FWD ? (low <= bclip) : (hgh >= bclip))
+        {
+            if (FWD)
+                low = bclip + 1;
+            else
+                hgh = bclip - 1;
+            const int Mc = __popcll(R.T[dif & 1][bclip & RM] & MASK61);
+            if (lane == 0 && clipm[0] <= Mc)
+            {
+                clipm[0] = Mc;
+                clipm[1] = R.V[dif & 1][bclip & RM];
+                clipm[2] = (clipm[1] - bclip) / 2;
+                clipm[3] = dif;
+                clipm[4] = R.HA[dif & 1][bclip & RM];
+                clipm[5] = R.HB[dif & 1][bclip & RM];
+            }
+        }
+        aclip = FWD ? INT_MAX : -INT_MAX;
+        bclip = FWD ? -INT_MAX : INT_MAX;
+    }
+
+    // drop diagonals more than WAVE_LAG behind the best (align.c:946-955)
+    {
+        const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
+        const int hw = FWD ? hgh0 : low0;
+        int nl = INT_MAX, nh = INT_MIN;
+#pragma unroll
+        for (int ch = 0; ch < NR / TW; ch++)
+        {
+            if (ch >= nchw)
+                break;
+            const int p = ch * TW + lane;
+            const int k = FWD ? hw - p : hw + p;
+            bool good = go && p < width && k >= low && k <= hgh;
+            if (good)
+            {
+                const int v = ch == 0 ? c0 : R.V[cur][k & RM];
+                good = FWD ? (v >= n) : (v <= n);
+            }
+            const unsigned gm = half(good);
+            if (gm)
+            {
+                const int pf = ch * TW + __ffs(gm) - 1, pl = ch * TW + 31 - __clz(gm);
+                const int k1 = FWD ? hw - pf : hw + pf, k2 = FWD ? hw - pl : hw + pl;
+                nl = min(nl, min(k1, k2));
+                nh = max(nh, max(k1, k2));
+            }
+        }
+        if (go)
+        {
             if (nh != INT_MIN)
             {
                 hgh = nh;
@@ -655,12 +1202,40 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
             }
             else
                 hgh = low - 1;
+            w.cells += hgh - low + 1;
         }
-        w.cells += hgh - low + 1;
     }
+    wvars.hgh = hgh;
+    wvars.low = low;
+    wvars.dif = dif;
+    wvars.more = more;
+    wvars.aclip = aclip;
+    wvars.bclip = bclip;
+    wvars.besta = besta;
+    wvars.lasta = lasta;
+    wvars.npeb = npeb;
+    return go;
+}
 
+template <int RG, bool PK>
+__device__ __forceinline__ void wave_end(const bool FWD, WarpCtx<RG>& w, WaveVars& wvars, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0,
+    const uint32_t* apk, uint32_t ag, const uint32_t* bpk, uint32_t bg, int alen, int blen, int comp, LAPath* apath, LAPath* bpath, int* mind, int mida,
+    uint16_t* atrace, uint16_t* btrace)
+{
+    WaveSmem<RG>& R = w.sm->ws;
+    const int lane = w.lane;
+    const int TS = P.tspace;
+    const int S = FWD ? 1 : -1;
+    const int VNONE = FWD ? -1 : INT_MAX;
+    const int boff = comp ? blen % TS : 0;
+    int* const trim = w.sm->trim;
+    int* const clipm = w.sm->clipm;
+    const uint8_t* as = FWD ? aseq0 : aseq0 - 1;
+    const uint8_t* bs = FWD ? bseq0 : bseq0 - 1;
+    (void)S; (void)VNONE; (void)boff; (void)as; (void)bs; (void)trim; (void)clipm; (void)R; (void)TS; (void)lane;
+    int low = wvars.low;
     // ---- trace points of both paths from the pebble chains (align.c:970-1106, 1710-1902)
-    __syncwarp();
+    tsync(w);
     if (lane == 0)
     {
         int4* cells = w.peb;
@@ -897,9 +1472,27 @@ __device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0,
             bpath->toff = (int)(btrace + btlen - w.pts);
         }
     }
-    __syncwarp();
+    tsync(w);
     if (FWD)
         *mind = w.sm->span_lo;
+}
+
+template <bool FWD, int RG, bool PK>
+__device__ void wave(WarpCtx<RG>& w, const AlignParams& P, const uint8_t* aseq0, const uint8_t* bseq0,
+                     const uint32_t* apk, uint32_t ag, const uint32_t* bpk, uint32_t bg, int alen, int blen,
+                     int comp, LAPath* apath, LAPath* bpath, int* mind, int maxd, int mida, int minp, int maxp,
+                     uint16_t* atrace, uint16_t* btrace)
+{
+    WaveVars v;
+    wave_begin<RG, PK>(FWD, w, v, P, aseq0, bseq0, apk, ag, bpk, bg, alen, blen, comp, *mind, maxd, mida);
+    if (w.err)
+        return;
+    while (wave_step<RG, PK>(FWD, w, v, P, aseq0, bseq0, apk, ag, bpk, bg, alen, blen, comp, minp, maxp))
+        ;
+    if (w.err)
+        return;
+    wave_end<RG, PK>(FWD, w, v, P, aseq0, bseq0, apk, ag, bpk, bg, alen, blen, comp, apath, bpath, mind, mida, atrace,
+                          btrace);
 }
 
 // Local_Alignment from one seed (diag, anti) with lbord = hbord = -1 (align.c:1922-2060).
@@ -930,7 +1523,7 @@ __device__ void local_alignment(WarpCtx<RG>& w, const AlignParams& P, const uint
         ap->tlen = bp->tlen = 0;
         ap->diffs = bp->diffs = 0;
     }
-    __syncwarp();
+    tsync(w);
     wave<true, RG, PK>(w, P, aseq, bseq, apk, ag, bpk, bg, alen, blen, comp, ap, bp, &low, hgh, anti, minp, maxp,
                        atrace, btrace);
     if (w.err)
@@ -955,7 +1548,7 @@ __device__ void local_alignment(WarpCtx<RG>& w, const AlignParams& P, const uint
             j += 2;
         }
     }
-    __syncwarp();
+    tsync(w);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1899,7 +2492,7 @@ __device__ void store_path(WarpCtx<RG>& w, const LAPath& lp, MPath* dst, PairBuf
         pb.err = 1;
         return;
     }
-    for (int i = w.lane; i < lp.tlen; i += 32)
+    for (int i = w.lane; i < lp.tlen; i += team_width<RG>())
         pb.tb[pb.ttop + i] = w.pts[lp.toff + i];
     if (w.lane == 0)
     {
@@ -1931,8 +2524,8 @@ __device__ void emit_paths(WarpCtx<RG>& w, const AlignParams& P, const MPath* m,
         r0 = atomicAdd(&out.counters[0], (unsigned long long)n);
         t0 = atomicAdd(&out.counters[1], (unsigned long long)tlen_tot * tbytes);
     }
-    r0 = __shfl_sync(GD_FULL, r0, 0);
-    t0 = __shfl_sync(GD_FULL, t0, 0);
+    r0 = tshfl(w, r0, 0);
+    t0 = tshfl(w, t0, 0);
     if (r0 + n > out.rcap || t0 + (unsigned long long)tlen_tot * tbytes > out.tcap)
         return;  // the host sees the counters past capacity and re-runs with more room
     unsigned long long toff = t0;
@@ -1956,11 +2549,12 @@ __device__ void emit_paths(WarpCtx<RG>& w, const AlignParams& P, const MPath* m,
             out.rec[r0 + i] = o;
         }
         const uint16_t* src = tb + m[i].toff;
+        constexpr int TW = team_width<RG>();
         if (P.trace8)
-            for (int j = w.lane; j < tl; j += 32)
+            for (int j = w.lane; j < tl; j += TW)
                 out.trace[toff + j] = (uint8_t)src[j];  // Compress_TraceTo8 (align.c:3352-3360)
         else
-            for (int j = w.lane; j < tl; j += 32)
+            for (int j = w.lane; j < tl; j += TW)
             {
                 out.trace[toff + 2 * j] = (uint8_t)(src[j] & 0xff);
                 out.trace[toff + 2 * j + 1] = (uint8_t)(src[j] >> 8);
@@ -2244,7 +2838,7 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
             if (!out.wide_list)
             {
                 if (lane == 0)
-                    gd_fail(st, GD_ERR_BAND_WIDTH, w.item, RG);
+                    gd_fail(st, GD_ERR_BAND_WIDTH, w.item, ring_of<RG>());
                 break;
             }
             // the band outgrew this instance: the group goes to the wide instance as if this
@@ -2297,6 +2891,462 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
         tcells += w.cells;
         tseeds += nseeds;
         __syncwarp();
+    }
+    if (lane == 0)
+    {
+        atomicAdd(&out.counters[2], tcells);
+        atomicAdd(&out.counters[3], tseeds);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// The duo instance: two pair groups per warp, one per half-warp team of 16 lanes.
+//
+// Most waves are narrow (a few to 20 diagonals), so a warp with lanes over diagonals leaves
+// most of its lanes idle; two teams of 16 keep them busy.  Each team runs its pair group as
+// a state machine: the warp takes one wave step of every team that is in a wave (the teams
+// run the same instructions on their own data, in either direction), then lets each team
+// that left its wave do everything up to its next wave -- the end of the wave, the next
+// seed, the next panel or pair group -- on its own.  Records, cells and seeds are those of
+// k_align_pairs: the per-team work is the same code at team width.  A group whose band
+// outgrows 128 diagonals goes to the wide list.
+// ------------------------------------------------------------------------------------------
+enum DuoState : int
+{
+    D_NEXT,    // take the next pair group from the queue
+    D_PANEL,   // the next panel of the group: its band scores
+    D_SEEDS,   // the next seed of the panel that passes the lasta test
+    D_BEGIN,   // the 0-wave of the forward (then reverse) wave from the seed
+    D_WAVE,    // one wave per warp step
+    D_WAVED,   // the wave ended: its trace points, the reverse wave, the path's bookkeeping
+    D_FINISH,  // the group ended: band resets, Handle_Redundancies, the records
+    D_DONE
+};
+
+#ifndef GD_DUO_MINB
+#define GD_DUO_MINB 7  // CTAs per SM the duo instance is compiled for (shared memory allows 7)
+#endif
+
+__global__ void __launch_bounds__(DUO_WARPS * 32, GD_DUO_MINB)
+    k_align_duo(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
+                const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
+                AlignScratch sc, AlignOut out, unsigned* queue, DevStatus* st)
+{
+    constexpr int RG = DUO;
+    constexpr int TW = team_width<RG>();
+    __shared__ WarpSmem<RG> smem[DUO_WARPS][2];
+    const int wlane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int team = wlane >> 4;
+    const int gt = (blockIdx.x * DUO_WARPS + wib) * 2 + team;  // the team's scratch slot
+    if ((blockIdx.x * DUO_WARPS + wib) * 2 >= sc.nwarps)
+        return;
+    WarpCtx<RG> w;
+    w.sm = &smem[wib][team];
+    w.peb = sc.peb + (size_t)gt * sc.pcap;
+    w.pcap = sc.pcap;
+    w.pts = sc.pts + (size_t)gt * sc.ptscap;
+    w.ptscap = sc.ptscap;
+    w.st = st;
+    w.lane = wlane & 15;
+    w.tbase = team * 16;
+    w.tmask = 0xffffu << w.tbase;
+    w.err = 0;
+    w.cells = 0;
+    w.item = 0;
+    const int lane = w.lane;
+    MPath* amatch = sc.match + (size_t)gt * 2 * sc.mcap;
+    MPath* bmatch = amatch + sc.mcap;
+    uint16_t* tbuf = sc.tbuf + (size_t)gt * sc.tcap;
+    int* score = sc.bands + (size_t)gt * 3 * sc.nbands - (P.mindiag - 2);
+    int* lastp = score + sc.nbands;
+    int* lasta = lastp + sc.nbands;
+    const int K = P.kmer, BS = P.binshift, TS = P.tspace;
+    const int minhit = (P.hitmin - 1) / K + 1;
+    const unsigned lt = tlt(w);
+    unsigned long long tcells = 0, tseeds = 0;
+
+    // the team's pair group, panel and seed
+    int state = D_NEXT;
+    unsigned item = 0, nseeds = 0;
+    int s = 0, e = 0, ar = 0, br = 0, alen = 0, blen = 0;
+    bool doA = false, doB = false;
+    const uint8_t* aseq = nullptr;
+    const uint8_t* bseq = nullptr;
+    uint32_t ag = 0, bg = 0;
+    PairBuf pb;
+    pb.am = amatch;
+    pb.bm = bmatch;
+    pb.tb = tbuf;
+    pb.tcap = sc.tcap;
+    pb.ttop = 0;
+    pb.err = 0;
+    int novla = 0, novlb = 0, tlo = INT_MAX, thi = INT_MIN;
+    int nidx = 0, amark2 = 0, lidx = 0, nend = 0, h2 = 0, base = 0;
+    unsigned cm = 0;
+    // the alignment: its direction, seed, and wave state
+    bool fwd = true;
+    int dj = 0, anti = 0, low = 0, minp = 0, maxp = 0, maxtp = 0;
+    WaveVars wv{};
+
+    while (true)
+    {
+        const bool act = state == D_WAVE;
+        if (__any_sync(GD_FULL, act))
+        {
+            const bool cont = wave_step_duo(act, fwd, w, wv, P, A.pk, ag, B.pk, bg, alen, blen, minp, maxp);
+            if (act && !cont)
+                state = D_WAVED;
+        }
+        // everything up to the team's next wave
+        while (state != D_WAVE && state != D_DONE)
+        {
+            if (state == D_NEXT)
+            {
+                unsigned g = 0;
+                if (lane == 0)
+                    g = atomicAdd(queue, 1u);
+                g = tshfl(w, g, 0);
+                if (g >= ngroups || st->code != 0)
+                {
+                    state = D_DONE;
+                    break;
+                }
+                item = order[g];
+                if (out.skip && out.skip[item])
+                    continue;
+                const uint2 grp = groups[item];
+                s = (int)grp.x;
+                e = (int)grp.y;
+                w.item = (int)item;
+                w.cells = 0;
+                nseeds = 0;
+                const uint64_t k0 = hkey[s];
+                ar = (int)((k0 >> P.hb.pbits) & ((1ull << P.hb.abits) - 1));
+                br = (int)(k0 >> (P.hb.pbits + P.hb.abits));
+                alen = A.rlen[ar];
+                blen = B.rlen[br];
+                aseq = A.bases + A.boff[ar];
+                bseq = B.bases + B.boff[br];
+                ag = PK_BIAS + (uint32_t)A.boff[ar];
+                bg = PK_BIAS + (uint32_t)B.boff[br];
+                doA = true;
+                doB = P.symmetric && (ar != br || !P.self || !P.comp);
+                pb.ttop = 0;
+                pb.err = 0;
+                novla = novlb = 0;
+                tlo = INT_MAX;
+                thi = INT_MIN;
+                nidx = s;
+                amark2 = 0;
+                state = D_PANEL;
+            }
+            else if (state == D_PANEL)
+            {
+                if (!(nidx < e && !w.err && !pb.err))
+                {
+                    state = D_FINISH;
+                    continue;
+                }
+                const int amark = amark2 + PANEL_SIZE;
+                amark2 = amark - PANEL_OVERLAP;
+                lidx = nidx;
+                const int q = first_above(hkey, lidx, e, amark, P.hb);
+                nend = (q < e) ? q + 1 : e;
+                h2 = first_above(hkey, lidx, nend, amark2, P.hb);
+                if (nend - lidx < minhit)
+                {
+                    nidx = h2;
+                    continue;
+                }
+                // panel band scores (filter.c:1754-1766)
+                for (int b0 = lidx; b0 < nend; b0 += TW)
+                {
+                    const int i = b0 + lane;
+                    const bool valid = i < nend;
+                    int ap = 0, dg = 0;
+                    if (valid)
+                    {
+                        ap = hit_apos(hkey[i], P.hb);
+                        dg = ((int)hdiag[i]) >> BS;
+                    }
+                    const unsigned key = valid ? (unsigned)dg : (0x80000000u | (unsigned)lane);
+                    const unsigned peers = tmatch(w, key);
+                    const unsigned lower = peers & lt;
+                    const int src = lower ? 31 - __clz(lower) : lane;
+                    const int prevap = tshfl(w, ap, src);
+                    int delta = 0;
+                    if (valid)
+                    {
+                        const int prev = lower ? prevap : lastp[dg];
+                        delta = (ap - prev >= K) ? K : ap - prev;
+                    }
+                    unsigned todo = tballot(w, valid);
+                    while (todo)
+                    {
+                        const int leader = __ffs(todo) - 1;
+                        const unsigned grpm = tshfl(w, peers, leader);
+                        const int sum = tadd(w, ((grpm >> lane) & 1) ? delta : 0);
+                        const int last = 31 - __clz(grpm);
+                        const int lastap = tshfl(w, ap, last);
+                        const int gdg = tshfl(w, dg, leader);
+                        if (lane == 0)
+                        {
+                            score[gdg] += sum;
+                            lastp[gdg] = lastap;
+                        }
+                        todo &= ~grpm;
+                    }
+                    tsync(w);
+                }
+                base = lidx - TW;
+                cm = 0;
+                state = D_SEEDS;
+            }
+            else if (state == D_SEEDS)
+            {
+                // seeds in hit order (filter.c:1776-1893)
+                if (w.err || pb.err || (cm == 0 && base + TW >= nend))
+                {
+                    // reset the panel's band scores (filter.c:1895-1899)
+                    for (int i = lidx + lane; i < nend; i += TW)
+                    {
+                        const int dg = ((int)hdiag[i]) >> BS;
+                        score[dg] = 0;
+                        lastp[dg] = 0;
+                    }
+                    tsync(w);
+                    nidx = h2;
+                    state = D_PANEL;
+                    continue;
+                }
+                if (cm == 0)
+                {
+                    base += TW;
+                    const int i = base + lane;
+                    bool cand = false;
+                    if (i < nend)
+                    {
+                        const int dg = ((int)hdiag[i]) >> BS;
+                        const int sc0 = score[dg];
+                        cand = (sc0 + score[dg + 1] >= P.hitmin) || (sc0 + score[dg - 1] >= P.hitmin);
+                    }
+                    cm = tballot(w, cand);
+                    continue;
+                }
+                const int j = __ffs(cm) - 1;
+                cm &= cm - 1;
+                const int apj = hit_apos(hkey[base + j], P.hb);
+                dj = (int)hdiag[base + j];
+                if (!(apj > lasta[dj >> BS]))
+                    continue;
+                nseeds++;
+                // Local_Alignment from (dj, apj + bpj) with lbord = hbord = -1 (align.c:1922-2060)
+                anti = 2 * apj - dj;
+                maxtp = 2 * (max(alen, blen) / TS + 2);
+                if (4 * maxtp + 16 > w.ptscap)
+                {
+                    if (lane == 0)
+                        gd_fail(w.st, GD_ERR_TRACE, w.item, maxtp);
+                    w.err = 1;
+                    continue;
+                }
+                low = dj;
+                const bool selfie = (aseq == bseq);
+                minp = (selfie && dj >= 0) ? 1 : -INT_MAX;
+                maxp = (selfie && dj <= 0) ? -1 : INT_MAX;
+                if (lane == 0)
+                {
+                    w.sm->ap.tlen = w.sm->bp.tlen = 0;
+                    w.sm->ap.diffs = w.sm->bp.diffs = 0;
+                }
+                tsync(w);
+                fwd = true;
+                state = D_BEGIN;
+            }
+            else if (state == D_BEGIN)
+            {
+                wave_begin<RG, true>(fwd, w, wv, P, aseq, bseq, A.pk, ag, B.pk, bg, alen, blen, P.comp, low, low, anti);
+                state = w.err ? D_SEEDS : D_WAVE;
+            }
+            else if (state == D_WAVED)
+            {
+                if (w.err)
+                {
+                    state = D_SEEDS;
+                    continue;
+                }
+                uint16_t* atrace = w.pts + maxtp;
+                uint16_t* btrace = atrace + 2 * maxtp;
+                wave_end<RG, true>(fwd, w, wv, P, aseq, bseq, A.pk, ag, B.pk, bg, alen, blen, P.comp, &w.sm->ap,
+                                   &w.sm->bp, &low, anti, atrace, btrace);
+                if (fwd)
+                {
+                    fwd = false;
+                    state = D_BEGIN;
+                    continue;
+                }
+                if (P.comp && lane == 0)
+                {
+                    uint16_t* tr = w.pts + w.sm->bp.toff;
+                    int i = w.sm->bp.tlen - 2, jj = 0;
+                    while (jj < i)
+                    {
+                        uint16_t t = tr[i];
+                        tr[i] = tr[jj];
+                        tr[jj] = t;
+                        t = tr[i + 1];
+                        tr[i + 1] = tr[jj + 1];
+                        tr[jj + 1] = t;
+                        i -= 2;
+                        jj += 2;
+                    }
+                }
+                tsync(w);
+                state = D_SEEDS;
+                const LAPath apth = w.sm->ap;
+                const LAPath bpth = w.sm->bp;
+                // Diagonal_Span (filter.c:1568-1599) of the A path, then widen lasta
+                int lo, hi;
+                {
+                    const uint16_t* points = w.pts + apth.toff;
+                    int dd = apth.abpos - apth.bbpos, dlo = dd, dhi = dd;
+                    dd = apth.aepos - apth.bepos;
+                    if (dd < dlo)
+                        dlo = dd;
+                    else if (dd > dhi)
+                        dhi = dd;
+                    dd = (apth.abpos / TS) * TS - apth.bbpos;
+                    const int tl = apth.tlen - 2;
+                    for (int b0 = 1; b0 < tl; b0 += 2 * TW)
+                    {
+                        const int idx = b0 + 2 * lane;
+                        int x = (idx < tl) ? (TS - (int)points[idx]) : 0;
+#pragma unroll
+                        for (int o = 1; o < TW; o <<= 1)
+                        {
+                            const int t = tshfl_up(w, x, o);
+                            if (lane >= o)
+                                x += t;
+                        }
+                        const int val = dd + x;
+                        dlo = min(dlo, tmin(w, (idx < tl) ? val : INT_MAX));
+                        dhi = max(dhi, tmax(w, (idx < tl) ? val : INT_MIN));
+                        dd = tshfl(w, val, TW - 1);
+                    }
+                    lo = (dlo >> BS) - 1;
+                    hi = (dhi >> BS) + 1;
+                }
+                const int dgj = dj >> BS;
+                if (dgj < lo)
+                    lo = dgj;
+                else if (dgj > hi)
+                    hi = dgj;
+                // the reference's band arrays end one band past each side (filter.c:2296-2311)
+                lo = max(lo, P.mindiag - 1);
+                hi = min(hi, P.maxdiag + 1);
+                const int ae = apth.aepos;
+                for (int dd2 = lo + lane; dd2 <= hi; dd2 += TW)
+                    if (ae > lasta[dd2])
+                        lasta[dd2] = ae;
+                tlo = min(tlo, lo);
+                thi = max(thi, hi);
+                tsync(w);
+                if ((apth.aepos - apth.abpos) + (apth.bepos - apth.bbpos) >= P.minover)
+                {
+                    if ((doA && novla >= sc.mcap) || (doB && novlb >= sc.mcap))
+                    {
+                        if (lane == 0)
+                            gd_fail(st, GD_ERR_MATCHES, w.item, sc.mcap);
+                        w.err = 1;
+                        continue;
+                    }
+                    if (doA)
+                    {
+                        store_path(w, apth, amatch + novla, pb);
+                        novla++;
+                    }
+                    if (doB)
+                    {
+                        store_path(w, bpth, bmatch + novlb, pb);
+                        novlb++;
+                    }
+                    tsync(w);
+                    if (pb.err)
+                    {
+                        if (lane == 0)
+                            gd_fail(st, GD_ERR_TRACE, w.item, sc.tcap);
+                        w.err = 1;
+                    }
+                }
+            }
+            else  // D_FINISH
+            {
+                // reset lasta (filter.c:1902-1920): every band this pair raised
+                if (tlo <= thi)
+                    for (int dd2 = tlo + lane; dd2 <= thi; dd2 += TW)
+                        lasta[dd2] = 0;
+                if (nidx < e)  // aborted pair: clear score/lastp of all its hits
+                    for (int i = s + lane; i < e; i += TW)
+                    {
+                        const int dg = ((int)hdiag[i]) >> BS;
+                        score[dg] = 0;
+                        lastp[dg] = 0;
+                    }
+                tsync(w);
+                if (w.err == 2)
+                {
+                    if (!out.wide_list)
+                    {
+                        if (lane == 0)
+                            gd_fail(st, GD_ERR_BAND_WIDTH, w.item, ring_of<RG>());
+                        state = D_DONE;
+                        break;
+                    }
+                    // the band outgrew this instance: the group goes to the wide instance as if
+                    // this team had never seen it (its band arrays are clean again)
+                    if (lane == 0)
+                        out.wide_list[atomicAdd(out.nwide, 1u)] = item;
+                    w.err = 0;
+                    tsync(w);
+                    state = D_NEXT;
+                    continue;
+                }
+                if (w.err)
+                {
+                    state = D_DONE;
+                    break;
+                }
+                // merge redundant paths (filter.c:1922-1938), lane 0
+                if (lane == 0)
+                {
+                    if (novla > 1)
+                    {
+                        if (novlb > 1)
+                            novla = novlb = handle_redundancies(amatch, novla, bmatch, pb, TS, P.comp);
+                        else
+                            novla = handle_redundancies(amatch, novla, nullptr, pb, TS, P.comp);
+                    }
+                    else if (novlb > 1)
+                        novlb = handle_redundancies(bmatch, novlb, nullptr, pb, TS, P.comp);
+                    if (pb.err)
+                        gd_fail(st, GD_ERR_TRACE, w.item, sc.tcap);
+                }
+                novla = tshfl(w, novla, 0);
+                novlb = tshfl(w, novlb, 0);
+                tsync(w);
+                emit_paths(w, P, amatch, novla, tbuf, ar + A.ufirst, br + B.ufirst, out);
+                emit_paths(w, P, bmatch, novlb, tbuf, br + B.ufirst, ar + A.ufirst, out);
+                if (out.gstat && lane == 0)
+                    out.gstat[item] = make_uint2((unsigned)(novla + novlb), w.cells);
+                tcells += w.cells;
+                tseeds += nseeds;
+                tsync(w);
+                state = D_NEXT;
+            }
+        }
+        if (__all_sync(GD_FULL, state == D_DONE))
+            break;
     }
     if (lane == 0)
     {
@@ -2403,9 +3453,11 @@ int align_grid(int* grid_out, int wide)
     int dev = 0, nsm = 0, per = 0;
     GD_CUDA(cudaGetDevice(&dev));
     GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    if (wide)
+    if (wide == 1)
         GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_align_pairs<WIDE_RING>,
                                                               warps_of<WIDE_RING>() * 32, 0));
+    else if (wide == 2)
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_align_duo, DUO_WARPS * 32, 0));
     else  // the narrow instances (RING, TEST_RING) have the same shape
         GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_align_pairs<RING>, ALIGN_WARPS * 32, 0));
     if (per < 1)
@@ -2416,7 +3468,12 @@ int align_grid(int* grid_out, int wide)
 
 int align_warps_per_cta(int wide)
 {
-    return wide ? warps_of<WIDE_RING>() : ALIGN_WARPS;
+    return wide == 1 ? warps_of<WIDE_RING>() : (wide == 2 ? DUO_WARPS : ALIGN_WARPS);
+}
+
+int align_slots_per_warp(int wide)
+{
+    return wide == 2 ? 2 : 1;
 }
 
 int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hkey, const uint32_t* hdiag,
@@ -2426,16 +3483,18 @@ int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hke
     GD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned), s));
     if (ngroups == 0)
         return 0;
-    if (p.d2)
+    if (wide == 2 && !p.d2 && !p.test_narrow)
+        k_align_duo<<<grid, DUO_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p, sc, out, queue, st);
+    else if (p.d2)
     {
-        if (wide)
+        if (wide == 1)
             k_align_pairs<WIDE_RING, true><<<grid, warps_of<WIDE_RING>() * 32, 0, s>>>(A, B, hkey, hdiag, groups, order,
                                                                                       ngroups, p, sc, out, queue, st);
         else
             k_align_pairs<RING, true><<<grid, ALIGN_WARPS * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups, p,
                                                                         sc, out, queue, st);
     }
-    else if (wide)
+    else if (wide == 1)
         k_align_pairs<WIDE_RING><<<grid, warps_of<WIDE_RING>() * 32, 0, s>>>(A, B, hkey, hdiag, groups, order, ngroups,
                                                                             p, sc, out, queue, st);
     else if (p.test_narrow)

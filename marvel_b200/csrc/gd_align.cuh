@@ -17,6 +17,12 @@ constexpr int RING = 128;           // wave-vector rings per warp, one for the p
 constexpr int WIDE_RING = 512;      // the same for the wide instance, for pair groups whose band outgrows RING
 constexpr int TEST_RING = 32;       // a narrow instance for tests only: most groups then go to the wide one
 constexpr int ALIGN_WARPS = 4;      // warps per CTA of the aligner (the wide instance: 1)
+constexpr int DUO = (1 << 16) | 128; // the two-teams-per-warp instance: its id carries the team split
+                                     // (bit 16: half-warp teams of 16 lanes) and the ring (128 per team)
+#ifndef GD_DUO_WARPS
+#define GD_DUO_WARPS 2
+#endif
+constexpr int DUO_WARPS = GD_DUO_WARPS;  // warps per CTA of the duo instance
 constexpr int TRIM_TABLE = 1 << 15; // TRIM_MASK + 1 (dalign/align.c:154)
 
 // One path as Local_Alignment returns it (dalign/align.h:76-83); trace is an offset into
@@ -85,7 +91,12 @@ size_t align_scratch_bytes(int nwarps, int pcap, int ptscap, int mcap, int tcap,
 void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int ptscap, int mcap, int tcap, int nbands,
                          int bvcap = 0, int btcap = 0);
 
-// Persistent seed-scan + alignment over the ordered pair groups.
+// Persistent seed-scan + alignment over the ordered pair groups on one instance (wide): 0 the
+// warp instance (RING), 1 the wide instance (WIDE_RING, one warp per CTA), 2 the duo instance
+// (two half-warp teams per warp, 128-diagonal rings each; sc holds a slot per team,
+// align_slots_per_warp).  The
+// duo instance aligns daligner's report; daligner2's (p.d2) and the tests' narrow instance
+// (p.test_narrow) take the warp instance in its place.
 int launch_align_pairs(const DevBlock& A, const DevBlock& B, const uint64_t* hkey, const uint32_t* hdiag,
                        const uint2* groups, const uint32_t* order, unsigned ngroups, AlignParams p, AlignScratch sc,
                        AlignOut out, unsigned* queue, DevStatus* st, int grid, cudaStream_t s, int wide = 0);
@@ -103,8 +114,10 @@ int launch_test_hr_d2(const uint8_t* aseq, const uint8_t* bseq, int alen, int bl
                       int hasB, const int32_t* hdr, MPath* paths, uint16_t* tbuf, int ttop, int tcap, int* vec,
                       int vcap, uint16_t* btr, int btcap, int32_t* out_hdr, int* out_n, cudaStream_t s);
 
-// CTAs for a persistent launch of the narrow (wide = 0) or wide instance, and its warps per CTA
+// CTAs for a persistent launch of an instance (wide as in launch_align_pairs), its warps per CTA
 int align_grid(int* grid_out, int wide = 0);
 int align_warps_per_cta(int wide);
+// scratch slots per warp of an instance: 2 for the duo instance, else 1
+int align_slots_per_warp(int wide);
 
 }  // namespace gd

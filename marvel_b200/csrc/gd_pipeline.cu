@@ -182,6 +182,8 @@ struct gd_context
     int agrid = 0;
     DevBuf ascr_w, wide;  // the wide aligner instance's scratch, and its group list + count
     int agrid_w = 0;
+    DevBuf ascr_d;        // the duo instance's scratch
+    int agrid_d = 0;
     int test_narrow = 0;  // tests only: the main aligner pass with the 32-diagonal instance
     // aligner schedule: empty = every pair group in one persistent launch (longest first from
     // the device queue); else one launch per length class, split at these alen + blen edges
@@ -1000,6 +1002,7 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     // per-length-class launches (the comparison schedule): each class is a contiguous range of
     // the cost-sorted order, found from the sorted keys ~(alen + blen)
     std::vector<unsigned> bucket{0u};
+    std::vector<int> bclass{0};  // the length class of each bucket (empty classes have none)
     if (!c->sched_edges.empty() && ng > 0)
     {
         std::vector<uint32_t> keys(ng);
@@ -1008,11 +1011,18 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
         GD_CUDA(cudaStreamSynchronize(s));
         std::vector<int32_t> edges = c->sched_edges;
         std::sort(edges.begin(), edges.end(), std::greater<int32_t>());
-        for (int32_t e : edges)
+        for (size_t i = 0; i < edges.size(); i++)
         {
-            unsigned p = (unsigned)(std::upper_bound(keys.begin(), keys.end(), ~(uint32_t)e) - keys.begin());
-            if (p > bucket.back() && p < ng)
+            unsigned p = (unsigned)(std::upper_bound(keys.begin(), keys.end(), ~(uint32_t)edges[i]) - keys.begin());
+            if (p >= ng)
+                break;
+            if (p > bucket.back())
+            {
                 bucket.push_back(p);
+                bclass.push_back((int)i + 1);
+            }
+            else
+                bclass.back() = (int)i + 1;  // the classes before this edge are empty
         }
     }
     bucket.push_back(ng);
@@ -1056,28 +1066,42 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     ap.test_narrow = c->test_narrow;
     ap.d2 = c->variant == 2;
     ap.hgap = c->hgap;
-    if ((!c->agrid && align_grid(&c->agrid, 0)) || (!c->agrid_w && align_grid(&c->agrid_w, 1)))
+    if ((!c->agrid && align_grid(&c->agrid, 0)) || (!c->agrid_w && align_grid(&c->agrid_w, 1)) ||
+        (!c->agrid_d && align_grid(&c->agrid_d, 2)))
         return -1;
-    int nwarps = c->agrid * ALIGN_WARPS;
     const int nwarps_w = c->agrid_w * align_warps_per_cta(1);
     int maxlen = std::max(A.blk.maxlen, B.blk.maxlen);
     int ptscap = 4 * (2 * (maxlen / c->tspace + 2)) + 32;
     int nbands = ap.maxdiag - ap.mindiag + 8;
+    // the instance of each length class (0 warp, 1 wide, 2 duo); daligner2's report has no duo
+    // instance and takes the warp instance there
+    std::vector<int> kind(bucket.size() - 1, 0);
+    for (size_t b = 0; b < kind.size(); b++)
+        if ((size_t)bclass[b] < c->sched_kind.size())
+            kind[b] = (c->sched_kind[bclass[b]] == 2 && ap.d2) ? 0 : c->sched_kind[bclass[b]];
+    DevBuf* const kbuf[3] = {&c->ascr, &c->ascr_w, &c->ascr_d};
+    const int kgrid[3] = {c->agrid, c->agrid_w, c->agrid_d};
     c->stats.reruns[oi] = 0;
     for (int attempt = 0; attempt < 48; attempt++)
     {
         if (attempt)
             c->stats.reruns[oi]++;
         const int bvcap = ap.d2 ? c->bvcap : 0, btcap = ap.d2 ? c->btcap : 0;
-        AlignScratch sc{};
-        size_t need = align_scratch_bytes(nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
-        if (ensure(c->ascr, need))
-            return -1;
-        align_scratch_carve(&sc, c->ascr.p, nwarps, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
-        // the band arrays (score, lastp, lasta per warp) start at zero on every launch: their
+        // each instance in use gets its scratch: a slot per warp (per team of the duo instance).
+        // The band arrays (score, lastp, lasta per slot) start at zero on every launch: their
         // place in the scratch moves with maxlen and the capacities, so an earlier launch's
         // clean-up does not cover them
-        GD_CUDA(cudaMemsetAsync(sc.bands, 0, (size_t)nwarps * 3 * nbands * 4, s));
+        AlignScratch ks[3]{};
+        for (int k = 0; k < 3; k++)
+        {
+            if (std::find(kind.begin(), kind.end(), k) == kind.end())
+                continue;
+            const int slots = kgrid[k] * align_warps_per_cta(k) * align_slots_per_warp(k);
+            if (ensure(*kbuf[k], align_scratch_bytes(slots, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap)))
+                return -1;
+            align_scratch_carve(&ks[k], kbuf[k]->p, slots, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
+            GD_CUDA(cudaMemsetAsync(ks[k].bands, 0, (size_t)slots * 3 * nbands * 4, s));
+        }
         if (ensure(c->outrec, c->rcap * sizeof(OutRec)) || ensure(c->outtr, c->tbcap) ||
             ensure(c->counters, 8 * 8) || ensure(c->status, sizeof(DevStatus)) || ensure(c->queue, 16))
             return -1;
@@ -1090,35 +1114,19 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
         GD_CUDA(cudaMemsetAsync(d_nwide, 0, 4, s));
         AlignOut out{P<OutRec>(c->outrec), P<uint8_t>(c->outtr), P<unsigned long long>(c->counters), c->rcap,
                      c->tbcap, skip, c->tri_collect ? P<uint2>(c->tri_gstat) : nullptr, wide_list, d_nwide};
-        // a length class the schedule gives to the wide instance runs there directly, with the
-        // wide instance's scratch
-        bool any_wide = false;
-        for (size_t b = 0; b + 1 < bucket.size(); b++)
-            any_wide |= b < c->sched_kind.size() && c->sched_kind[b] == 1;
-        AlignScratch scw0{};
-        if (any_wide)
-        {
-            const size_t need_w =
-                align_scratch_bytes(nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap, btcap);
-            if (ensure(c->ascr_w, need_w))
-                return -1;
-            align_scratch_carve(&scw0, c->ascr_w.p, nwarps_w, c->pcap, ptscap, c->mcap, c->tcap, nbands, bvcap,
-                                btcap);
-            GD_CUDA(cudaMemsetAsync(scw0.bands, 0, (size_t)nwarps_w * 3 * nbands * 4, s));
-        }
         GD_CUDA(cudaEventRecord(c->ev0, s));
-        for (size_t b = 0; b + 1 < bucket.size(); b++)
+        for (size_t b = 0; b < kind.size(); b++)
         {
-            const bool wide_class = b < c->sched_kind.size() && c->sched_kind[b] == 1;
+            // a class on the wide instance has no wider one to hand groups to
             AlignOut o2 = out;
-            if (wide_class)
+            if (kind[b] == 1)
             {
                 o2.wide_list = nullptr;
                 o2.nwide = nullptr;
             }
             if (launch_align_pairs(A.blk, B.blk, hkey, hdiag, P<uint2>(c->groups), order + bucket[b],
-                                   bucket[b + 1] - bucket[b], ap, wide_class ? scw0 : sc, o2, P<unsigned>(c->queue),
-                                   P<DevStatus>(c->status), wide_class ? c->agrid_w : c->agrid, s, wide_class))
+                                   bucket[b + 1] - bucket[b], ap, ks[kind[b]], o2, P<unsigned>(c->queue),
+                                   P<DevStatus>(c->status), kgrid[kind[b]], s, kind[b]))
                 return -1;
         }
         // pair groups whose band outgrew the main instance: the wide one, appending to the same
@@ -1433,7 +1441,7 @@ void gd_destroy(gd_context* c)
                       &c->tri_gstat, &c->tri_misc, &c->tri_x, &c->tri_y, &c->tri_perm, &c->tri_grad, &c->tri_m,
                       &c->tri_v, &c->tri_loss, &c->tri_w, &c->acc_rec, &c->acc_tr, &c->srt_rec, &c->srt_tr,
                       &c->okey0, &c->okey1, &c->oval0, &c->oval1, &c->olen, &c->las_raw, &c->las_off,
-                      &c->las_rec, &c->las_out, &c->ascr_w, &c->wide};
+                      &c->las_rec, &c->las_out, &c->ascr_w, &c->wide, &c->ascr_d};
     for (DevBuf* b : bufs)
         release(*b);
     for (HostBuf* h : {&c->h_rec, &c->h_tr})
@@ -2361,14 +2369,14 @@ int gd_set_align_schedule(gd_context* c, int nedges, const int32_t* edges, const
         return -1;
     }
     for (int i = 0; kind && i <= nedges; i++)
-        if (kind[i] != 0 && kind[i] != 1)
+        if (kind[i] < 0 || kind[i] > 2)
         {
-            gd_set_error("gd_set_align_schedule: instance %d of class %d is neither 0 nor 1", kind[i], i);
+            gd_set_error("gd_set_align_schedule: instance %d of class %d is not 0, 1 or 2", kind[i], i);
             return -1;
         }
     c->sched_edges.assign(edges, edges + nedges);
     c->sched_kind.clear();
-    if (nedges > 0 && kind)
+    if (kind)
         c->sched_kind.assign(kind, kind + nedges + 1);
     return 0;
 }

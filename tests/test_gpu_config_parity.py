@@ -6,7 +6,8 @@ uses); tests/golden/config_digests.json holds, per block, what the reference dal
 for it (record count, trace spacing and the order-free SHA-256 of its .las records, from
 tests/golden/make_config_digests.py) and the reference's own wave-cell count (its
 WAVE_STATS counters, -j1).  Bit-exact: every field of every record but the pad word, and
-every trace byte; the cell count exactly."""
+every trace byte; the cell count exactly.  Both on the default aligner schedule and with every
+pair group on the duo instance."""
 import json
 import os
 
@@ -40,8 +41,9 @@ def _sorted_like_write_overlap_buffer(recs):
     return bool((lead >= 0).all())
 
 
+@pytest.mark.parametrize("kinds", [None, [2]], ids=["warp", "duo"])
 @pytest.mark.parametrize("name", sorted(DIGESTS))
-def test_full_block_equals_reference(mb, name):
+def test_full_block_equals_reference(mb, name, kinds):
     want = DIGESTS[name]
     path = synth.cached_db(want["workload"], want["seed_offset"], want["scale"])
     A = dazzdb.open_block(path)
@@ -57,6 +59,8 @@ def test_full_block_equals_reference(mb, name):
             if blk is not None:
                 dazzdb.load_track(blk, m)
     ctx = mb.Context()
+    if kinds is not None:
+        ctx.set_align_schedule([], kinds)
     recs, tr = mb.daligner_block(ctx, A, B, k=14, w=6, h=35, e=0.70, l=1000, s=100, M=32)
     st = ctx.stats()
     ctx.close()

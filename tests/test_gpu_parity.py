@@ -278,8 +278,23 @@ def test_compute_trace_pts_matches_reference(mb, name):
     ctx.close()
 
 
+@pytest.mark.parametrize("name", cases())
+def test_duo_instance_matches_reference_golden(mb, name, tmp_path):
+    """Every pair group on the duo instance (two 16-lane teams per warp, each with its own
+    pair group, 64-diagonal rings; wider bands go to the wide instance): the reference's
+    .las files."""
+    d, meta = load(name)
+    names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "gpu",
+                             ctx_hook=lambda ctx: ctx.set_align_schedule([], [2]))
+    assert sorted(names) == sorted(meta["las"])
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
+        assert ok, f"{name} {n}: {msg}"
+
+
 @pytest.mark.parametrize("name,kinds", [("self_long_panels", None), ("self_default", None),
-                                        ("self_long_panels", [1, 1, 0, 0, 0]), ("self_default", [0, 0, 1, 0, 1])])
+                                        ("self_long_panels", [1, 1, 0, 0, 0]), ("self_default", [0, 0, 1, 0, 1]),
+                                        ("self_long_panels", [1, 2, 0, 2, 2]), ("self_default", [2, 0, 2, 1, 2])])
 def test_length_class_schedule_gives_the_same_output(mb, name, kinds, tmp_path):
     """One aligner launch per length class (gd_set_align_schedule) instead of the one
     persistent launch, some classes on the wide instance: the same .las files."""
