@@ -2572,8 +2572,12 @@ constexpr int warps_of()
 // D2: daligner2's report (dalign2/filter_reporter_cpu.c) -- its -H, its rule for the B-side
 // record of a read against itself, its Handle_Redundancies; a separate instance, so that
 // daligner's keeps its code layout.
+#ifndef GD_ALIGN_MINB
+#define GD_ALIGN_MINB 6  // CTAs per SM the warp instance is compiled for (80 registers; 7, at 72, spills and runs 9 % slower)
+#endif
+
 template <int RG, bool D2 = false>
-__global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : 6)
+__global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : GD_ALIGN_MINB)
     k_align_pairs(DevBlock A, DevBlock B, const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag,
                   const uint2* __restrict__ groups, const uint32_t* __restrict__ order, unsigned ngroups, AlignParams P,
                   AlignScratch sc, AlignOut out, unsigned* queue, DevStatus* st)
