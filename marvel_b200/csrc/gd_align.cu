@@ -18,7 +18,10 @@
 // Instances by ring size: RING (128 diagonals, 4 warps per CTA) aligns every pair group; a
 // group whose band grows wider is abandoned there (nothing emitted, its counts dropped) and
 // listed for the WIDE_RING instance (512 diagonals, 1 warp per CTA), which aligns it from
-// scratch.  TEST_RING (32) replaces RING in tests so that most groups take that route.
+// scratch.  TEST_RING (32) replaces RING in tests so that most groups take that route.  The
+// duo instance (k_align_duo, DUO) splits each warp into two 16-lane teams with 128-diagonal
+// rings each, one pair group per team; the wave functions are written over a team (WarpCtx
+// with team collectives), and wave_step_duo runs both teams' waves in lockstep.
 #include "gd_align.cuh"
 
 #include <climits>
