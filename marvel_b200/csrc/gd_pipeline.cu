@@ -957,8 +957,8 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
         ensure(c->gcost2, (size_t)nst * 4 + 8) || ensure(c->gidx2, (size_t)nst * 4 + 8))
         return -1;
     unsigned* d_ng = P<unsigned>(c->misc) + 28;
-    // with the learned triage on (or its features collected), group selection and the triage
-    // are one kernel: features, MLP and skip flag per kept group as it is selected
+    // with the learned triage on (or its features collected), the kept groups' features, MLP
+    // and skip flags follow selection
     const bool triage = c->tri_on || c->tri_collect;
     unsigned* d_nskip = P<unsigned>(c->misc) + 32;
     if (triage)
@@ -974,24 +974,20 @@ static int align_hits(gd_context* c, Slot& A, Slot& B, uint64_t nhits, gd::HitBi
     // (daligner2's report keeps its own selection)
     const int minhit = (c->hitmin - 1) / c->kmer + 1;
     const int seed_test = c->variant == 1 ? c->hitmin : 0;
-    if (triage
-            ? launch_select_groups_triage(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, c->kmer, seed_test,
-                                          hb,
-                                          A.blk, B.blk, comp, c->minover, c->binshift,
-                                          A.has_mask ? P<int64_t>(A.manno) : nullptr,
-                                          A.has_mask ? P<int32_t>(A.mdata) : nullptr,
-                                          c->tri_on ? P<float>(c->tri_params) : nullptr, c->tri_thr,
-                                          c->tri_collect ? P<float>(c->tri_feat) : nullptr, P<uint2>(c->groups),
-                                          P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), P<uint8_t>(c->tri_skip), d_ng,
-                                          d_nskip, s)
-            : launch_select_groups(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, c->binshift, c->kmer,
-                                   seed_test, hb, P<int32_t>(A.rlen), P<int32_t>(B.rlen), P<uint2>(c->groups),
-                                   P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), d_ng, s))
+    if (launch_select_groups(P<uint32_t>(c->starts), nst, nhits, minhit, hkey, hdiag, c->binshift, c->kmer, seed_test,
+                             hb, P<int32_t>(A.rlen), P<int32_t>(B.rlen), P<uint2>(c->groups), P<uint32_t>(c->gcost),
+                             P<uint32_t>(c->gidx), d_ng, s))
         return -1;
     unsigned ng = 0;
     GD_CUDA(cudaMemcpyAsync(&ng, d_ng, 4, cudaMemcpyDeviceToHost, s));
     GD_CUDA(cudaStreamSynchronize(s));
     c->stats.groups[oi] = ng;
+    if (triage &&
+        launch_triage_groups(P<uint2>(c->groups), ng, hkey, hdiag, hb, A.blk, B.blk, comp, c->minover, c->binshift,
+                             A.has_mask ? P<int64_t>(A.manno) : nullptr, A.has_mask ? P<int32_t>(A.mdata) : nullptr,
+                             c->tri_on ? P<float>(c->tri_params) : nullptr, c->tri_thr,
+                             c->tri_collect ? P<float>(c->tri_feat) : nullptr, P<uint8_t>(c->tri_skip), d_nskip, s))
+        return -1;
     if (ensure(c->scratch, std::max(c->scratch.n, radix_scratch_bytes(ng) + 4096)))
         return -1;
     int gw = radix_sort_pairs<uint32_t>(P<uint32_t>(c->gcost), P<uint32_t>(c->gidx), P<uint32_t>(c->gcost2),

@@ -74,6 +74,74 @@ __device__ void group_features(const uint64_t* __restrict__ hkey, const uint32_t
     f[11] = masked;
 }
 
+// group_features with a warp's lanes over the group's hits (every lane returns the features).
+// The diagonal sums are integer sums, exact in any order, so the result equals
+// group_features' wherever its double sums are exact (below 2^53).
+__device__ void group_features_warp(const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag, uint2 gr,
+                                    const HitBits& hb, const DevBlock& A, const DevBlock& B, int comp, int minover,
+                                    int binshift, const int64_t* __restrict__ anno, const int32_t* __restrict__ mdata,
+                                    float f[TRI_NF])
+{
+    const int lane = lane_id();
+    int s = (int)gr.x, e = (int)gr.y, n = e - s;
+    uint64_t k0 = hkey[s];
+    int ar = (int)((k0 >> hb.pbits) & ((1ull << hb.abits) - 1));
+    int br = (int)(k0 >> (hb.pbits + hb.abits));
+    float alen = (float)A.rlen[ar], blen = (float)B.rlen[br];
+    uint64_t pmask = (1ull << hb.pbits) - 1;
+    int amin = (int)(k0 & pmask), amax = (int)(hkey[e - 1] & pmask);
+    long long isum = 0;
+    unsigned long long isq = 0;
+    int dmin = INT_MAX, dmax = INT_MIN;
+    for (int i = s + lane; i < e; i += 32)
+    {
+        int d = (int)hdiag[i];
+        isum += d;
+        isq += (unsigned long long)((long long)d * d);
+        dmin = min(dmin, d);
+        dmax = max(dmax, d);
+    }
+    for (int o = 16; o; o >>= 1)
+    {
+        isum += __shfl_xor_sync(GD_FULL, isum, o);
+        isq += __shfl_xor_sync(GD_FULL, isq, o);
+    }
+    dmin = __reduce_min_sync(GD_FULL, dmin);
+    dmax = __reduce_max_sync(GD_FULL, dmax);
+    double sum = (double)isum, sq = (double)isq;
+    double mean = sum / n, var = fmax(sq / n - mean * mean, 0.0);
+    int band = 1 << binshift, near = 0;
+    for (int i = s + lane; i < e; i += 32)
+        near += fabs((double)(int)hdiag[i] - mean) <= band;
+    near = __reduce_add_sync(GD_FULL, near);
+    double ovl = fmin((double)alen, (double)blen + mean) - fmax(0.0, mean);
+    float masked = 0.f;
+    if (anno)
+    {
+        long long mb = 0;
+        for (int64_t j = anno[ar] + 2 * lane; j < anno[ar + 1]; j += 64)
+            mb += mdata[j + 1] - mdata[j];
+        for (int o = 16; o; o >>= 1)
+            mb += __shfl_xor_sync(GD_FULL, mb, o);
+        masked = (float)mb / alen;
+    }
+    f[0] = log2f((float)n);
+    f[1] = log2f(alen);
+    f[2] = log2f(blen);
+    f[3] = (float)(amax - amin) / alen;
+    f[4] = log2f(1.f + (float)(dmax - dmin));
+    f[5] = (float)(mean / alen);
+    f[6] = log2f(1.f + (float)sqrt(var));
+    f[7] = (float)(ovl / (2.0 * minover));
+    f[8] = 64.f * n / (float)(amax - amin + 1);
+    f[9] = (float)near / n;
+    f[10] = (float)comp;
+    f[11] = masked;
+}
+
+// groups of more hits than this get their features from a whole warp (group_features_warp)
+constexpr int TRI_WARP_FEATURES = 32;
+
 // ------------------------------------------------------------------------------------------
 // MLP on tensor cores
 // ------------------------------------------------------------------------------------------
@@ -381,27 +449,14 @@ __global__ void __launch_bounds__(MT) k_mlp_forward(const float* __restrict__ P,
     }
 }
 
-// Pair-group selection fused with the triage (report_thread's minhit test,
-// dalign/filter.c:1699-1709, the seed-candidate test, and the learned triage in one pass):
-// each thread tests SEL_U run starts of a tile of SEL_U * 128; a kept group's range and cost
-// key are appended to a ring of staged rows in shared memory; after each tile, while 128 rows
-// are staged, the CTA computes their features from their hits (a thread per row), runs the
-// MLP over them on tensor cores and writes the groups out (range, cost key, index) with their
-// skip flag (p < thr) and, when feat is given, their raw features; the last rows are flushed
-// at the end.  Staging keeps the MLP to kept groups only and one barrier per tile of run
-// starts.  With P == nullptr only features are computed.
-constexpr int SEL_U = 4;                 // run starts per thread per tile
-constexpr int SEL_CAP = IR * (SEL_U + 1);  // staged rows: a tile's worth behind < 128 waiting
-
-struct SelStage
-{
-    uint32_t st[SEL_CAP], en[SEL_CAP], c[SEL_CAP];
-    unsigned n;  // rows staged
-};
-
-constexpr size_t SEL_SMEM = (sizeof(InferSmem) + 15) / 16 * 16 + sizeof(SelStage);
-
-struct SelArgs
+// The learned triage of the pair groups that selection kept (groups[0, ng), after
+// k_select_groups): a CTA per tile of IR groups -- each group's features (a thread per short
+// group, the lanes of its warp together over a long one), the MLP over the tile on tensor
+// cores, the skip flag (p < thr) at the group's slot and, when feat is given, its raw
+// features.  With P == nullptr only the features are computed.  Selection keeps its own
+// full-occupancy kernel: the MLP's shared memory would hold the selection's latency-bound
+// candidate tests to a third of the resident warps.
+struct TriArgs
 {
     const uint64_t* hkey;
     const uint32_t* hdiag;
@@ -413,121 +468,67 @@ struct SelArgs
     const float* P;
     float thr;
     float* feat;
-    uint2* groups;
-    uint32_t* cost;
-    uint32_t* idx;
+    const uint2* groups;
     uint8_t* skip;
-    unsigned* ngroups;
 };
 
-// rows head .. head + nrows - 1 of the ring (nrows <= 128): features, MLP, output
-__device__ void sel_flush(InferSmem& S, SelStage& G, int head, int nrows, const SelArgs& a, unsigned& cnt)
-{
-    const int r = threadIdx.x;
-    const bool mine = r < nrows;
-    const int q = (head + r) % SEL_CAP;
-    float f[TRI_NF];
-#pragma unroll
-    for (int j = 0; j < TRI_NF; j++)
-        f[j] = 0.f;
-    uint32_t st = 0, en = 0, c = 0;
-    if (mine)
-    {
-        st = G.st[q];
-        en = G.en[q];
-        c = G.c[q];
-        group_features(a.hkey, a.hdiag, make_uint2(st, en), a.hb, a.A, a.B, a.comp, a.minover, a.binshift, a.anno,
-                       a.mdata, f);
-    }
-    bool drop = false;
-    if (a.P)
-    {
-        infer_put_row(S, r, f, mine);
-        __syncthreads();
-        infer_rows(S);
-        __syncthreads();
-        drop = mine && 1.f / (1.f + __expf(-S.z[r])) < a.thr;
-    }
-    const unsigned m = __ballot_sync(GD_FULL, mine);
-    unsigned base = 0;
-    if (m)
-    {
-        if (lane_id() == 0)
-            base = atomicAdd(a.ngroups, (unsigned)__popc(m));
-        base = __shfl_sync(GD_FULL, base, 0);
-    }
-    if (mine)
-    {
-        const unsigned slot = base + __popc(m & lanemask_lt());
-        a.groups[slot] = make_uint2(st, en);
-        a.cost[slot] = ~c;  // ascending sort of ~cost = longest pairs first
-        a.idx[slot] = slot;
-        a.skip[slot] = drop ? 1 : 0;
-        cnt += drop;
-        if (a.feat)
-#pragma unroll
-            for (int j = 0; j < TRI_NF; j++)
-                a.feat[(size_t)slot * TRI_NF + j] = f[j];
-    }
-    __syncthreads();  // S.X / S.z are rewritten by the next flush
-}
-
-__global__ void __launch_bounds__(MT) k_select_groups_triage(const uint32_t* __restrict__ starts, int64_t nstarts,
-                                                           int64_t nhits, int minhit, int kmer, int hitmin, SelArgs a,
-                                                           unsigned* nskip)
+__global__ void __launch_bounds__(MT) k_triage_groups(unsigned ng, TriArgs a, unsigned* nskip)
 {
     extern __shared__ __align__(16) unsigned char infer_smem_t[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(infer_smem_t);
-    SelStage& G = *reinterpret_cast<SelStage*>(infer_smem_t + (sizeof(InferSmem) + 15) / 16 * 16);
     if (a.P)
         infer_load_weights(S, a.P);
-    if (threadIdx.x == 0)
-        G.n = 0;
     __syncthreads();
-    const int64_t per = (int64_t)IR * SEL_U;
-    const int64_t ntiles = (nstarts + per - 1) / per;
     unsigned cnt = 0;
-    int head = 0;  // first staged row of the ring (the same in every thread)
+    const int64_t ntiles = ((int64_t)ng + IR - 1) / IR;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
+        const int r = threadIdx.x;
+        const int64_t slot = tile * IR + r;
+        const bool mine = slot < (int64_t)ng;
+        float f[TRI_NF];
 #pragma unroll
-        for (int u = 0; u < SEL_U; u++)
+        for (int j = 0; j < TRI_NF; j++)
+            f[j] = 0.f;
+        const uint2 gr = mine ? a.groups[slot] : make_uint2(0u, 0u);
+        if (mine && gr.y - gr.x <= TRI_WARP_FEATURES)
+            group_features(a.hkey, a.hdiag, gr, a.hb, a.A, a.B, a.comp, a.minover, a.binshift, a.anno, a.mdata, f);
+        // a long group is walked by its warp's lanes together, not by one thread while the CTA
+        // waits for it at the next barrier
+        unsigned big = __ballot_sync(GD_FULL, mine && gr.y - gr.x > TRI_WARP_FEATURES);
+        while (big)
         {
-            const int64_t g = tile * per + (int64_t)u * IR + threadIdx.x;
-            if (g >= nstarts)
-                continue;
-            const uint32_t st = starts[g];
-            const uint32_t en = (g + 1 < nstarts) ? starts[g + 1] : (uint32_t)nhits;
-            if ((int64_t)(en - st) >= minhit &&
-                group_can_fire(a.hkey, a.hdiag, st, en, a.hb.pbits, a.binshift, kmer, hitmin, minhit))
-            {
-                const uint64_t k = a.hkey[st];
-                const int ar = (int)((k >> a.hb.pbits) & ((1ull << a.hb.abits) - 1));
-                const int br = (int)(k >> (a.hb.pbits + a.hb.abits));
-                const int q = (head + (int)atomicAdd(&G.n, 1u)) % SEL_CAP;
-                G.st[q] = st;
-                G.en[q] = en;
-                G.c[q] = (uint32_t)(a.A.rlen[ar] + a.B.rlen[br]);
-            }
+            const int j = __ffs(big) - 1;
+            big &= big - 1;
+            const uint2 gj = make_uint2(__shfl_sync(GD_FULL, gr.x, j), __shfl_sync(GD_FULL, gr.y, j));
+            float fj[TRI_NF];
+            group_features_warp(a.hkey, a.hdiag, gj, a.hb, a.A, a.B, a.comp, a.minover, a.binshift, a.anno, a.mdata,
+                                fj);
+            if (lane_id() == j)
+#pragma unroll
+                for (int k = 0; k < TRI_NF; k++)
+                    f[k] = fj[k];
         }
-        __syncthreads();
-        int n = (int)G.n;
-        if (n >= IR)
+        bool drop = false;
+        if (a.P)
         {
-            while (n >= IR)
-            {
-                sel_flush(S, G, head, IR, a, cnt);
-                head = (head + IR) % SEL_CAP;
-                n -= IR;
-            }
-            if (threadIdx.x == 0)
-                G.n = (unsigned)n;
+            infer_put_row(S, r, f, mine);
+            __syncthreads();
+            infer_rows(S);
+            __syncthreads();
+            drop = mine && 1.f / (1.f + __expf(-S.z[r])) < a.thr;
         }
-        __syncthreads();
+        if (mine)
+        {
+            a.skip[slot] = drop ? 1 : 0;
+            cnt += drop;
+            if (a.feat)
+#pragma unroll
+                for (int j = 0; j < TRI_NF; j++)
+                    a.feat[slot * TRI_NF + j] = f[j];
+        }
+        __syncthreads();  // S.X / S.z are rewritten by the next tile
     }
-    const int n = (int)G.n;
-    if (n > 0)
-        sel_flush(S, G, head, n, a, cnt);
     if (a.P)
     {
         for (int o = 16; o; o >>= 1)
@@ -704,9 +705,9 @@ static int infer_grid(int64_t ntiles)
         int dev = 0, nsm = 0, per = 0;
         GD_CUDA(cudaGetDevice(&dev));
         GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        GD_CUDA(cudaFuncSetAttribute((const void*)k_select_groups_triage, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)SEL_SMEM));
-        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_select_groups_triage, MT, SEL_SMEM));
+        GD_CUDA(cudaFuncSetAttribute((const void*)k_triage_groups, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(InferSmem)));
+        GD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_triage_groups, MT, sizeof(InferSmem)));
         blocks = nsm * std::max(per, 1);
     }
     return (int)std::min<int64_t>(ntiles, blocks);
@@ -762,22 +763,19 @@ int launch_adam(float* params, const float* grad, float* m, float* v, int step, 
     return 0;
 }
 
-int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit,
-                                const uint64_t* hkey, const uint32_t* hdiag, int kmer, int hitmin, HitBits hb,
-                                const DevBlock& A, const DevBlock& B, int comp, int minover, int binshift,
-                                const int64_t* amask_anno, const int32_t* amask_data, const float* params,
-                                float threshold, float* feat, uint2* groups, uint32_t* cost, uint32_t* idx,
-                                uint8_t* skip, unsigned* ngroups, unsigned* nskip, cudaStream_t s)
+int launch_triage_groups(const uint2* groups, unsigned ng, const uint64_t* hkey, const uint32_t* hdiag, HitBits hb,
+                         const DevBlock& A, const DevBlock& B, int comp, int minover, int binshift,
+                         const int64_t* amask_anno, const int32_t* amask_data, const float* params, float threshold,
+                         float* feat, uint8_t* skip, unsigned* nskip, cudaStream_t s)
 {
-    GD_CUDA(cudaMemsetAsync(ngroups, 0, sizeof(unsigned), s));
-    if (nstarts <= 0)
+    if (ng == 0)
         return 0;
-    int grid = infer_grid((nstarts + (int64_t)IR * SEL_U - 1) / ((int64_t)IR * SEL_U));
+    int grid = infer_grid(((int64_t)ng + IR - 1) / IR);
     if (grid <= 0)
         return -1;
-    SelArgs a{hkey, hdiag, hb, A, B, comp, minover, binshift, amask_anno, amask_data, params, threshold, feat,
-              groups, cost, idx, skip, ngroups};
-    k_select_groups_triage<<<grid, MT, SEL_SMEM, s>>>(starts, nstarts, nhits, minhit, kmer, hitmin, a, nskip);
+    TriArgs a{hkey, hdiag, hb, A, B, comp, minover, binshift, amask_anno, amask_data, params, threshold, feat, groups,
+              skip};
+    k_triage_groups<<<grid, MT, sizeof(InferSmem), s>>>(ng, a, nskip);
     GD_LAUNCHED(1);
     GD_CUDA(cudaGetLastError());
     return 0;

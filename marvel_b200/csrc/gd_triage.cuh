@@ -20,19 +20,13 @@ constexpr int TRI_OFF_W3 = TRI_OFF_B2 + TRI_H;
 constexpr int TRI_OFF_B3 = TRI_OFF_W3 + TRI_H;
 constexpr int TRI_NPARAM = TRI_OFF_B3 + 1;  // 5081, of which 5057 trained
 
-// Pair-group selection (runs of >= minhit hits from the run starts of the sorted hits) fused
-// with the triage (kmer, hitmin: the seed test as for launch_select_groups): per kept group its
-// range, cost key
-// ~(alen + blen), index, the features
-// (into feat, when given) and with params != nullptr the MLP's verdict skip[g] = p <
-// threshold (nskip += #skipped).  One persistent launch, 128 run starts per tile.
-int launch_select_groups_triage(const uint32_t* starts, int64_t nstarts, int64_t nhits, int minhit,
-                                const uint64_t* hkey, const uint32_t* hdiag, int kmer, int hitmin, HitBits hb,
-                                const DevBlock& A,
-                                const DevBlock& B, int comp, int minover, int binshift, const int64_t* amask_anno,
-                                const int32_t* amask_data, const float* params, float threshold, float* feat,
-                                uint2* groups, uint32_t* cost, uint32_t* idx, uint8_t* skip, unsigned* ngroups,
-                                unsigned* nskip, cudaStream_t s);
+// The learned triage of the ng pair groups selection kept (groups[0, ng), each a hit range):
+// per group its features (into feat, when given, at the group's slot) and with params !=
+// nullptr the MLP's verdict skip[g] = p < threshold (nskip += #skipped).
+int launch_triage_groups(const uint2* groups, unsigned ng, const uint64_t* hkey, const uint32_t* hdiag, HitBits hb,
+                         const DevBlock& A, const DevBlock& B, int comp, int minover, int binshift,
+                         const int64_t* amask_anno, const int32_t* amask_data, const float* params, float threshold,
+                         float* feat, uint8_t* skip, unsigned* nskip, cudaStream_t s);
 
 // p[i] = sigmoid(MLP(x[i])) for n rows of TRI_NF features.
 int launch_mlp_forward(const float* params, const float* x, int64_t n, float* p, cudaStream_t s);

@@ -138,3 +138,61 @@ def test_triage_keeps_recall_and_saves_cells(mb):
     pb = mb.Context().mlp_forward(model.params, featb)
     ev = triage.evaluate(pb, recb, cellsb, model.threshold)
     assert abs(ev["groups_skipped"] * featb.shape[0] - sum(st["skipped"])) <= 0.001 * featb.shape[0] + 2
+
+
+def _features_f64(hits, rlen_a, rlen_b, binshift, minover, minhit, comp):
+    """The 12 features of every pair group of >= minhit hits, restated in float64 from the
+    sorted hit list (rows diag, apos, aread, bread): {(n, alen, blen): [feature rows]}."""
+    d, ap, ar, br = (hits[:, i].astype(np.int64) for i in range(4))
+    cut = np.flatnonzero((np.diff(ar) != 0) | (np.diff(br) != 0)) + 1
+    starts = np.concatenate([[0], cut])
+    ends = np.concatenate([cut, [d.size]])
+    out = {}
+    for s, e in zip(starts, ends):
+        n = e - s
+        if n < minhit:
+            continue
+        dd = d[s:e].astype(np.float64)
+        alen, blen = float(rlen_a[ar[s]]), float(rlen_b[br[s]])
+        mean = dd.sum() / n
+        var = max((dd * dd).sum() / n - mean * mean, 0.0)
+        near = np.count_nonzero(np.abs(dd - mean) <= (1 << binshift))
+        ovl = min(alen, blen + mean) - max(0.0, mean)
+        span = float(ap[e - 1] - ap[s])
+        f = [np.log2(n), np.log2(alen), np.log2(blen), span / alen, np.log2(1 + d[s:e].max() - d[s:e].min()),
+             mean / alen, np.log2(1 + np.sqrt(var)), ovl / (2.0 * minover), 64.0 * n / (span + 1), near / n,
+             float(comp), 0.0]
+        out.setdefault((n, int(alen), int(blen)), []).append(np.array(f))
+    return out
+
+
+def test_group_features_equal_a_float64_restatement(mb):
+    """The features the fused selection computes -- by one thread for short groups and by a
+    warp for groups of more than 32 hits -- equal a float64 restatement from the sorted hits
+    (to float32 rounding and the device's log2f)."""
+    import os
+    from golden_cases import load
+    d, _ = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    ctx = mb.Context()
+    ctx.set_filter_params(14, 6, 0, 35)
+    ctx.new_align_spec(0.70, 100, A.freq)
+    ctx.set_globals(2000, False, 32 << 30)
+    ctx.load_block(0, A)
+    ctx.sort_kmers(0)
+    ctx.triage_reset()
+    ctx.triage_collect(True)
+    ctx.match_filter(0, 0, 1)
+    ctx.triage_collect(False)
+    feat, rec, cells = ctx.triage_groups()
+    hits = ctx.get_hits()
+    ctx.close()
+    # binshift 6 (-w6), minover 2000 (the context's global: 2 x -l1000), minhit 3 (-h35, -k14)
+    ref = _features_f64(hits, A.rlen, A.rlen, 6, 2000, 3, 0)
+    assert feat.shape[0] > 100
+    n = np.rint(np.exp2(feat[:, 0].astype(np.float64))).astype(np.int64)
+    assert (n > 32).sum() > 10, "the case should hold groups long enough for the warp path"
+    for row, ni in zip(feat, n):
+        key = (int(ni), int(round(2.0 ** float(row[1]))), int(round(2.0 ** float(row[2]))))
+        cands = ref.get(key, [])
+        assert any(np.allclose(row, c, rtol=2e-6, atol=2e-6) for c in cands), (key, row, cands[:2])
