@@ -2128,6 +2128,17 @@ int64_t gd_get_overlaps(gd_context* c, gd_overlap* recs, uint8_t* trace, int64_t
     int64_t m = std::min<int64_t>(rcap, (int64_t)c->srt_n);
     if (m <= 0)
         return 0;
+    if (m == (int64_t)c->srt_n && (uint64_t)tcap >= c->srt_tb)
+    {
+        // everything fits: the records and the trace bytes (laid out in record order) in two
+        // back-to-back copies
+        GD_CUDA(cudaMemcpyAsync(recs, c->srt_rec.p, (size_t)m * sizeof(gd_overlap), cudaMemcpyDeviceToHost, c->s));
+        if (c->srt_tb)
+            GD_CUDA(cudaMemcpyAsync(trace, c->srt_tr.p, c->srt_tb, cudaMemcpyDeviceToHost, c->s));
+        GD_CUDA(cudaStreamSynchronize(c->s));
+        return m;
+    }
+    // the leading records whose traces fit in tcap
     GD_CUDA(cudaMemcpyAsync(recs, c->srt_rec.p, (size_t)m * sizeof(gd_overlap), cudaMemcpyDeviceToHost, c->s));
     GD_CUDA(cudaStreamSynchronize(c->s));
     int tbytes = c->tspace <= 125 ? 1 : 2;

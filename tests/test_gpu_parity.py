@@ -304,3 +304,32 @@ def test_length_class_schedule_gives_the_same_output(mb, name, kinds, tmp_path):
     for n in names:
         ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
         assert ok, f"{name} {n}: {msg}"
+
+
+def test_get_overlaps_copies_whole_buffer_or_the_leading_records_that_fit(mb):
+    """gd_get_overlaps with room for everything copies the whole sorted buffer; with fewer
+    record slots or trace bytes it copies the leading records whose traces fit, and their
+    traces, unchanged."""
+    d, meta = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    ctx = _ctx(mb, A)
+    mb.daligner_block(ctx, A)
+    n, tb = ctx.sort_overlaps()
+    assert n > 10 and tb > 0
+    L = mb.lib()
+    full_r = np.zeros(n, mb.OVL_DTYPE)
+    full_t = np.zeros(tb, np.uint8)
+    assert L.gd_get_overlaps(ctx.h, full_r.ctypes.data, full_t.ctypes.data, n, tb) == n
+    bpt = 1  # -s100: one byte per trace value
+    ends = full_r["toff"].astype(np.int64) + full_r["tlen"].astype(np.int64) * bpt
+    assert ends[-1] == tb
+    for rcap, tcap in ((n // 2, tb), (n, tb // 2), (n // 3, tb // 3)):
+        want = int(min(rcap, np.searchsorted(ends, tcap, side="right")))
+        r = np.zeros(max(rcap, 1), mb.OVL_DTYPE)
+        t = np.zeros(max(tcap, 1), np.uint8)
+        k = L.gd_get_overlaps(ctx.h, r.ctypes.data, t.ctypes.data, rcap, tcap)
+        assert k == want
+        assert (r[:k] == full_r[:k]).all()
+        used = int(ends[k - 1]) if k else 0
+        assert (t[:used] == full_t[:used]).all()
+    ctx.close()
