@@ -172,7 +172,7 @@ int gd_set_wave_limit(gd_context* ctx, int limit);
  * class's kernel instance: 0 = a warp per alignment with 128-diagonal wave rings, 4 warps
  * per CTA (a group whose band outgrows 128 is redone by the wide instance), 1 = the wide
  * instance, 512-diagonal rings, one warp per CTA, 2 = the duo instance, two 16-lane teams
- * per warp, each aligning its own pair group with 64-diagonal rings (wider bands are redone
+ * per warp, each aligning its own pair group with 128-diagonal rings (wider bands are redone
  * by the wide instance; daligner2's report runs instance 0 in its place).  The autotuner
  * (marvel_b200/autotune.py) sets it; the output is the same for every schedule. */
 int gd_set_align_schedule(gd_context* ctx, int nedges, const int32_t* edges, const int32_t* kind);

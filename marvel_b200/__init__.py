@@ -350,7 +350,7 @@ class Context:
         """() = one persistent aligner launch over all pair groups (default); else one launch
         per length class split at these alen + blen edges (bp); kinds (one per class, longest
         first): 0 = the 128-diagonal warp instance, 1 = the 512-diagonal instance, 2 = the duo
-        instance (two 16-lane teams per warp, 64-diagonal rings).  With no edges, kinds holds the
+        instance (two 16-lane teams per warp, 128-diagonal rings).  With no edges, kinds holds the
         one persistent launch's instance."""
         e = np.ascontiguousarray(edges, np.int32)
         k = None if kinds is None else np.ascontiguousarray(kinds, np.int32)

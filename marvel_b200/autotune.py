@@ -12,8 +12,8 @@ keeps the fastest:
   (4 warps per CTA, 6 CTAs per SM; a group whose band outgrows 128 diagonals is redone by the
   wide instance), the wide instance (512-diagonal rings, one warp per CTA), which takes such
   groups in one pass, or the duo instance (two 16-lane teams per warp, each on its own pair
-  group with 64-diagonal rings), which keeps twice the lanes busy on the narrow bands most
-  waves have.
+  group with 128-diagonal rings), meant to keep twice the lanes busy on the narrow bands most
+  waves have (it measures slower on every workload: the ring pairs halve the resident warps).
 
 Candidates are timed on the loaded blocks (the aligner's device time of both orientations,
 gd_stats.ms_align, best of `repeats` runs).  The radix sorts have no choice here: their
