@@ -2910,13 +2910,15 @@ __global__ void __launch_bounds__(warps_of<RG>() * 32, RG == WIDE_RING ? 1 : GD_
 // The duo instance: two pair groups per warp, one per half-warp team of 16 lanes.
 //
 // Most waves are narrow (a few to 20 diagonals), so a warp with lanes over diagonals leaves
-// most of its lanes idle; two teams of 16 keep them busy.  Each team runs its pair group as
-// a state machine: the warp takes one wave step of every team that is in a wave (the teams
-// run the same instructions on their own data, in either direction), then lets each team
-// that left its wave do everything up to its next wave -- the end of the wave, the next
-// seed, the next panel or pair group -- on its own.  Records, cells and seeds are those of
-// k_align_pairs: the per-team work is the same code at team width.  A group whose band
-// outgrows 128 diagonals goes to the wide list.
+// most of its lanes idle; two teams of 16 are meant to keep them busy.  Each team runs its
+// pair group as a state machine: the warp takes one wave of every team that is in a wave in
+// lockstep (wave_step_duo: the teams run the same instructions on their own data, in either
+// direction), then lets each team that left its wave do everything up to its next wave --
+// the end of the wave, the next seed, the next panel or pair group -- on its own.  Records,
+// cells and seeds are those of k_align_pairs: the per-team work is the same code at team
+// width.  A group whose band outgrows 128 diagonals goes to the wide list.  Measured, it is
+// slower than k_align_pairs: a lockstep step of two waves issues about twice a warp wave's
+// instructions, and two rings per warp halve the resident warps.
 // ------------------------------------------------------------------------------------------
 enum DuoState : int
 {

@@ -31,6 +31,18 @@ def test_gpu_matches_reference_daligner2_golden(mb, name, tmp_path):
         assert ok, f"{name} {n}: {msg}"
 
 
+@pytest.mark.parametrize("name", ["d2_self", "d2_pair_dust"])
+def test_duo_schedule_keeps_daligner2_on_the_warp_instance(mb, name, tmp_path):
+    """daligner2's report has no duo instance: a schedule asking for it runs the warp instance
+    in its place, and the .las files are still the reference's."""
+    d, meta = load(name)
+    names = daligner_run.run(d, meta["flags"], meta["blocks"], str(tmp_path), "gpu", variant=2,
+                             ctx_hook=lambda ctx: ctx.set_align_schedule([], [2]))
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(tmp_path / n), os.path.join(d, n))
+        assert ok, f"{name} {n}: {msg}"
+
+
 @pytest.mark.parametrize("name,k,t", [("d2_self", 14, 0), ("d2_self_k16_w5", 16, 0), ("d2_self_asym_t20", 14, 20),
                                       ("d2_pair_dust", 14, 0)])
 def test_d2_kmer_index_matches_oracle(mb, name, k, t):

@@ -196,3 +196,39 @@ def test_group_features_equal_a_float64_restatement(mb):
         key = (int(ni), int(round(2.0 ** float(row[1]))), int(round(2.0 ** float(row[2]))))
         cands = ref.get(key, [])
         assert any(np.allclose(row, c, rtol=2e-6, atol=2e-6) for c in cands), (key, row, cands[:2])
+
+
+def test_duo_instance_honours_the_skip_flags(mb):
+    """The triage's skip flags reach the duo aligner instance as they reach the warp instance:
+    the same groups skipped and the same records (a random model, thresholded at the median of
+    its outputs so that about half the groups are skipped)."""
+    import os
+    from golden_cases import load
+    d, _ = load("self_default")
+    A = dazzdb.open_block(os.path.join(d, "G.1"))
+    rng = np.random.default_rng(11)
+    _, params = _random_model(rng)
+
+    def ctx_for(kinds):
+        ctx = mb.Context()
+        ctx.set_filter_params(14, 6, 0, 35)
+        ctx.new_align_spec(0.70, 100, A.freq)
+        ctx.set_globals(2000, False, 32 << 30)
+        if kinds is not None:
+            ctx.set_align_schedule([], kinds)
+        return ctx
+
+    ctx = ctx_for(None)
+    _, _, feat, _, _ = _collect(mb, ctx, A)
+    thr = float(np.median(ctx.mlp_forward(params, feat)))
+    ctx.close()
+    out = []
+    for kinds in (None, [2]):
+        ctx = ctx_for(kinds)
+        ctx.triage_set_model(params, thr)
+        r, t = mb.daligner_block(ctx, A)
+        st = ctx.stats()
+        out.append((dazzdb.las_digest(r, t, r["toff"], 1), sum(st["skipped"]), sum(st["cells"])))
+        ctx.close()
+    assert out[0][1] > 0
+    assert out[0] == out[1]
