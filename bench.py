@@ -385,6 +385,10 @@ def run_gpu(args):
             "stages_ms": {"index": round(idx_ms, 3), "merge_hitsort": round(sum(st["ms_merge"]), 3),
                           "seed_scan_align": round(align_ms, 3)},
             "gcups": round(gcups, 2) if gcups else None,
+            # the last step's aligner work (both orientations): pair groups aligned, those whose
+            # band outgrew the 128-diagonal instance (redone on the wide one), seeds, wave cells
+            "aligner": {"pair_groups": int(sum(st["groups"])), "wide_groups": int(sum(st["wide"])),
+                        "seeds": int(sum(st["seeds"])), "wave_cells": int(sum(st["cells"]))},
             # per-stage rates of the last step (its stats): k-mers sorted, hits emitted and
             # sorted, Local_Alignment calls
             "rates": {"kmers_sorted_per_s": round(kmers / (idx_ms / 1e3), 1) if idx_ms > 0 else None,
