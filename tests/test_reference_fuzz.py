@@ -1,0 +1,87 @@
+"""Differential test against the reference daligner itself: seeded random genomes, read
+models and option sets beyond the fixed golden cases (k 10-16, w 4-8, h, e .70-.90, l, s
+on both sides of the one-byte trace limit, -M down to 1 GB, -I, -A, -t, block pairs), each run by the
+reference daligner built from source (oracle/_ref/daligner, oracle/Makefile) and by the
+device path (GPU) or the oracle (CPU) on the same database; every .las file must be
+identical.  Skipped where the reference binary is not built."""
+import dataclasses
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import daligner_run
+from marvel_b200 import dazzdb, synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref", "daligner")
+N_CASES = 40
+
+
+def _case(i):
+    """Option set, genome and read model of case i (seeded)."""
+    rng = np.random.default_rng(1000 + i)
+    k = int(rng.integers(10, 17))
+    w = int(rng.integers(4, 9))
+    h = int(rng.integers(max(k + 1, 20), 61))
+    e = float(rng.choice([0.70, 0.75, 0.80, 0.85, 0.90]))
+    l = int(rng.choice([300, 500, 800, 1000, 1500]))
+    s = int(rng.choice([25, 50, 100, 125, 126, 200, 255]))
+    flags = [f"-M{int(rng.choice([32, 4, 1]))}", f"-k{k}", f"-w{w}", f"-h{h}", f"-e{e:.2f}", f"-l{l}", f"-s{s}"]
+    if rng.random() < 0.3:
+        flags.append("-I")
+    if rng.random() < 0.3:
+        flags.append("-A")
+    if rng.random() < 0.3:
+        flags.append(f"-t{int(rng.integers(10, 40))}")
+    pair = rng.random() < 0.4
+    err = float(rng.uniform(0.04, 0.16))  # total error rate of the reads
+    genome = synth.GenomeModel(int(rng.integers(40_000, 90_000)),
+                               repeats=((int(rng.integers(0, 6)), int(rng.integers(1000, 4000)),
+                                         float(rng.uniform(0.0, 0.03))),))
+    reads = synth.ReadModel(int(rng.integers(8, 16)), int(rng.integers(2500, 7000)), 2000, 800, 15000,
+                            p_ins=err * 0.6, p_del=err * 0.3, p_sub=err * 0.1)
+    wl = synth.Workload(f"fuzz{i}", genome, reads, seed=2000 + i)
+    return wl, flags, pair
+
+
+def _reference_run(i, tmp_path):
+    """Case i's database under tmp_path/db and the reference daligner's .las files there;
+    returns (db dir, flags, blocks)."""
+    wl, flags, pair = _case(i)
+    reads, _ = synth.generate(wl)
+    total = sum(r.size for r in reads)
+    d = tmp_path / "db"
+    d.mkdir()
+    # a block pair: two blocks of about half the bases each
+    dazzdb.write_db(str(d / "G"), reads, (total / 2 + 1) / 1e6 if pair else 200)
+    blocks = ["G.1", "G.2"] if pair else ["G.1", "G.1"]
+    subprocess.run([REF, "-j4"] + flags + blocks, cwd=str(d), check=True, stdout=subprocess.DEVNULL)
+    return d, flags, blocks
+
+
+def _compare(i, impl, tmp_path):
+    d, flags, blocks = _reference_run(i, tmp_path)
+    names = daligner_run.run(str(d), flags, blocks, str(tmp_path / impl), impl)
+    assert names
+    for n in names:
+        assert os.path.exists(d / n), f"case {i} {flags}: the reference wrote no {n}"
+        ok, msg = dazzdb.las_equal(str(tmp_path / impl / n), str(d / n))
+        assert ok, f"case {i} {flags} {blocks}: {n}: {msg}"
+
+
+needs_ref = pytest.mark.skipif(not os.path.exists(REF), reason="the reference daligner is not built (make -C oracle ref)")
+
+
+@needs_ref
+@pytest.mark.parametrize("i", range(N_CASES))
+def test_oracle_equals_reference_daligner(i, tmp_path):
+    _compare(i, "oracle", tmp_path)
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("i", range(N_CASES))
+def test_device_path_equals_reference_daligner(i, tmp_path):
+    _compare(i, "gpu", tmp_path)
