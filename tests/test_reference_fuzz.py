@@ -1,7 +1,8 @@
 """Differential test against the reference daligner itself: seeded random genomes, read
 models and option sets beyond the fixed golden cases (k 10-16, w 4-8, h, e .70-.90, l, s
-on both sides of the one-byte trace limit, -M down to 1 GB, -I, -A, -t, block pairs), each run by the
-reference daligner built from source (oracle/_ref/daligner, oracle/Makefile) and by the
+on both sides of the one-byte trace limit, -M down to 1 GB, -I, -A, -t, -b, -mdust with the
+reference DBdust track, block pairs; and daligner2 with its -H), each run by the
+reference daligner (daligner2) built from source (oracle/_ref, oracle/Makefile) and by the
 device path (GPU) or the oracle (CPU) on the same database; every .las file must be
 identical.  Skipped where the reference binary is not built."""
 import dataclasses
@@ -16,12 +17,16 @@ from marvel_b200 import dazzdb, synth
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, "oracle", "_ref", "daligner")
+REF2 = os.path.join(ROOT, "oracle", "_ref", "daligner2")
+DUST = os.path.join(ROOT, "oracle", "_ref", "DBdust")
 N_CASES = 40
+N_CASES2 = 20  # daligner2 (modimizer seeds)
 
 
-def _case(i):
-    """Option set, genome and read model of case i (seeded)."""
-    rng = np.random.default_rng(1000 + i)
+def _case(i, variant=1):
+    """Option set, genome and read model of case i (seeded): daligner's options, or with
+    variant 2 daligner2's (its -H instead of -b)."""
+    rng = np.random.default_rng(1000 * variant + i)
     k = int(rng.integers(10, 17))
     w = int(rng.integers(4, 9))
     h = int(rng.integers(max(k + 1, 20), 61))
@@ -35,6 +40,12 @@ def _case(i):
         flags.append("-A")
     if rng.random() < 0.3:
         flags.append(f"-t{int(rng.integers(10, 40))}")
+    if variant == 1 and rng.random() < 0.25:
+        flags.append("-b")
+    if variant == 2 and rng.random() < 0.3:
+        flags.append(f"-H{int(rng.integers(2000, 8000))}")
+    if rng.random() < 0.25:
+        flags.append("-mdust")
     pair = rng.random() < 0.4
     err = float(rng.uniform(0.04, 0.16))  # total error rate of the reads
     genome = synth.GenomeModel(int(rng.integers(40_000, 90_000)),
@@ -42,14 +53,14 @@ def _case(i):
                                          float(rng.uniform(0.0, 0.03))),))
     reads = synth.ReadModel(int(rng.integers(8, 16)), int(rng.integers(2500, 7000)), 2000, 800, 15000,
                             p_ins=err * 0.6, p_del=err * 0.3, p_sub=err * 0.1)
-    wl = synth.Workload(f"fuzz{i}", genome, reads, seed=2000 + i)
+    wl = synth.Workload(f"fuzz{variant}_{i}", genome, reads, seed=2000 * variant + i)
     return wl, flags, pair
 
 
-def _reference_run(i, tmp_path):
-    """Case i's database under tmp_path/db and the reference daligner's .las files there;
-    returns (db dir, flags, blocks)."""
-    wl, flags, pair = _case(i)
+def _reference_run(i, tmp_path, variant=1):
+    """Case i's database under tmp_path/db and the reference daligner's (daligner2's) .las
+    files there; returns (db dir, flags, blocks)."""
+    wl, flags, pair = _case(i, variant)
     reads, _ = synth.generate(wl)
     total = sum(r.size for r in reads)
     d = tmp_path / "db"
@@ -57,13 +68,16 @@ def _reference_run(i, tmp_path):
     # a block pair: two blocks of about half the bases each
     dazzdb.write_db(str(d / "G"), reads, (total / 2 + 1) / 1e6 if pair else 200)
     blocks = ["G.1", "G.2"] if pair else ["G.1", "G.1"]
-    subprocess.run([REF, "-j4"] + flags + blocks, cwd=str(d), check=True, stdout=subprocess.DEVNULL)
+    if "-mdust" in flags:
+        subprocess.run([DUST, "G"], cwd=str(d), check=True, stdout=subprocess.DEVNULL)
+    cmd = [REF, "-j4"] if variant == 1 else [REF2, "-T4", "-Pout"]
+    subprocess.run(cmd + flags + blocks, cwd=str(d), check=True, stdout=subprocess.DEVNULL)
     return d, flags, blocks
 
 
-def _compare(i, impl, tmp_path):
-    d, flags, blocks = _reference_run(i, tmp_path)
-    names = daligner_run.run(str(d), flags, blocks, str(tmp_path / impl), impl)
+def _compare(i, impl, tmp_path, variant=1):
+    d, flags, blocks = _reference_run(i, tmp_path, variant)
+    names = daligner_run.run(str(d), flags, blocks, str(tmp_path / impl), impl, variant=variant)
     assert names
     for n in names:
         assert os.path.exists(d / n), f"case {i} {flags}: the reference wrote no {n}"
@@ -71,7 +85,8 @@ def _compare(i, impl, tmp_path):
         assert ok, f"case {i} {flags} {blocks}: {n}: {msg}"
 
 
-needs_ref = pytest.mark.skipif(not os.path.exists(REF), reason="the reference daligner is not built (make -C oracle ref)")
+needs_ref = pytest.mark.skipif(not (os.path.exists(REF) and os.path.exists(REF2) and os.path.exists(DUST)),
+                               reason="the reference daligner is not built (make -C oracle ref)")
 
 
 @needs_ref
@@ -85,3 +100,16 @@ def test_oracle_equals_reference_daligner(i, tmp_path):
 @pytest.mark.parametrize("i", range(N_CASES))
 def test_device_path_equals_reference_daligner(i, tmp_path):
     _compare(i, "gpu", tmp_path)
+
+
+@needs_ref
+@pytest.mark.parametrize("i", range(N_CASES2))
+def test_oracle_equals_reference_daligner2(i, tmp_path):
+    _compare(i, "oracle", tmp_path, variant=2)
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("i", range(N_CASES2))
+def test_device_path_equals_reference_daligner2(i, tmp_path):
+    _compare(i, "gpu", tmp_path, variant=2)
