@@ -113,3 +113,60 @@ def test_oracle_equals_reference_daligner2(i, tmp_path):
 @pytest.mark.parametrize("i", range(N_CASES2))
 def test_device_path_equals_reference_daligner2(i, tmp_path):
     _compare(i, "gpu", tmp_path, variant=2)
+
+
+# ---- DBdust: random databases and parameters against the reference DBdust's track
+
+N_DUST = 20
+
+
+def _dust_case(i):
+    rng = np.random.default_rng(5000 + i)
+    kw = dict(window=int(rng.choice([16, 32, 48, 64, 100, 128])), thresh=float(rng.choice([1.0, 1.5, 2.0, 2.5, 3.0])),
+              mflag=int(rng.choice([5, 8, 10, 15])), biased=bool(rng.random() < 0.3))
+    at = float(rng.uniform(0.25, 0.42))  # A and T share of the genome
+    genome = synth.GenomeModel(int(rng.integers(30_000, 80_000)), tandem_frac=float(rng.uniform(0.0, 0.25)),
+                               tandem_period=(2, int(rng.integers(3, 12))),
+                               base_probs=(at, 0.5 - at, 0.5 - at, at))
+    reads = synth.ReadModel(6, 4000, 2000, 800, 12000, **synth.PACBIO)
+    return synth.Workload(f"dust{i}", genome, reads, seed=6000 + i), kw
+
+
+def _dust_flags(kw):
+    f = [f"-w{kw['window']}", f"-t{kw['thresh']}", f"-m{kw['mflag']}"]
+    return f + (["-b"] if kw["biased"] else [])
+
+
+def _dust_reference(i, tmp_path):
+    wl, kw = _dust_case(i)
+    reads, _ = synth.generate(wl)
+    d = tmp_path / "db"
+    d.mkdir()
+    dazzdb.write_db(str(d / "G"), reads, 200)
+    subprocess.run([DUST] + _dust_flags(kw) + ["G"], cwd=str(d), check=True, stdout=subprocess.DEVNULL)
+    a = open(d / ".G.dust.anno", "rb").read()
+    anno = np.frombuffer(a[8:], "<i8")
+    data = np.fromfile(str(d / ".G.dust.data"), "<i4")
+    return dazzdb.open_block(str(d / "G.1")), kw, anno, data
+
+
+@needs_ref
+@pytest.mark.parametrize("i", range(N_DUST))
+def test_oracle_dust_equals_reference_dbdust(i, tmp_path):
+    import oracle
+    blk, kw, anno, data = _dust_reference(i, tmp_path)
+    oa, od = oracle.dust(blk, **kw)
+    assert np.array_equal(oa, anno) and np.array_equal(od, data), kw
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("i", range(N_DUST))
+def test_device_dust_equals_reference_dbdust(i, tmp_path):
+    import marvel_b200 as mb
+    blk, kw, anno, data = _dust_reference(i, tmp_path)
+    ctx = mb.Context()
+    ctx.load_block(0, blk)
+    ga, gd = ctx.dust(0, blk.freq, **kw)
+    ctx.close()
+    assert np.array_equal(ga, anno) and np.array_equal(gd, data), kw
