@@ -170,3 +170,70 @@ def test_device_dust_equals_reference_dbdust(i, tmp_path):
     ga, gd = ctx.dust(0, blk.freq, **kw)
     ctx.close()
     assert np.array_equal(ga, anno) and np.array_equal(gd, data), kw
+
+
+# ---- LAsort: the records of a random case's .las files, shuffled, against the reference LAsort
+
+LASORT = os.path.join(ROOT, "oracle", "_ref", "LAsort")
+N_LASORT = 10
+
+
+def _raw_records(path):
+    """(trace spacing, the byte string of each record: 40-byte header with its pad + trace)."""
+    data = open(path, "rb").read()
+    n = int(np.frombuffer(data[:8], "<i8")[0])
+    ts = int(np.frombuffer(data[8:12], "<i4")[0])
+    tb = 1 if ts <= 125 else 2
+    out, o = [], 12
+    for _ in range(n):
+        tlen = int(np.frombuffer(data[o:o + 4], "<i4")[0])
+        out.append(data[o:o + 40 + tlen * tb])
+        o += 40 + tlen * tb
+    return ts, out
+
+
+def _lasort_reference(i, tmp_path):
+    d, flags, blocks = _reference_run(i, tmp_path)
+    recs, ts = [], None
+    for root, _, files in os.walk(d):
+        for f in sorted(files):
+            if f.endswith(".las"):
+                ts, r = _raw_records(os.path.join(root, f))
+                recs += r
+    rng = np.random.default_rng(7000 + i)
+    recs = [recs[j] for j in rng.permutation(len(recs))]
+    src = tmp_path / "in.las"
+    with open(src, "wb") as f:
+        f.write(np.int64(len(recs)).tobytes())
+        f.write(np.int32(ts).tobytes())
+        for r in recs:
+            f.write(r)
+    subprocess.run([LASORT, "in.las"], cwd=str(tmp_path), check=True, stdout=subprocess.DEVNULL)
+    return src, tmp_path / "in.S.las"
+
+
+needs_lasort = pytest.mark.skipif(not (os.path.exists(REF) and os.path.exists(LASORT)),
+                                  reason="the reference LAsort is not built (make -C oracle ref)")
+
+
+@needs_lasort
+@pytest.mark.parametrize("i", range(N_LASORT))
+def test_oracle_las_sort_equals_reference_lasort(i, tmp_path):
+    import las_sort
+    src, want = _lasort_reference(i, tmp_path)
+    las_sort.las_sort(str(src), str(tmp_path / "o.las"))
+    ok, msg = dazzdb.las_equal(str(tmp_path / "o.las"), str(want), key="lasort", pad=True)
+    assert ok, msg
+
+
+@pytest.mark.gpu
+@needs_lasort
+@pytest.mark.parametrize("i", range(N_LASORT))
+def test_device_las_sort_equals_reference_lasort(i, tmp_path):
+    import marvel_b200 as mb
+    src, want = _lasort_reference(i, tmp_path)
+    ctx = mb.Context()
+    ctx.las_sort(str(src), str(tmp_path / "g.las"))
+    ctx.close()
+    ok, msg = dazzdb.las_equal(str(tmp_path / "g.las"), str(want), key="lasort", pad=True)
+    assert ok, msg
