@@ -237,3 +237,44 @@ def test_device_las_sort_equals_reference_lasort(i, tmp_path):
     ctx.close()
     ok, msg = dazzdb.las_equal(str(tmp_path / "g.las"), str(want), key="lasort", pad=True)
     assert ok, msg
+
+
+# ---- LAmerge: the per-block .las directories of a random multi-block run
+
+LAMERGE = os.path.join(ROOT, "oracle", "_ref", "LAmerge")
+N_LAMERGE = 6
+
+
+def _lamerge_reference(i, tmp_path):
+    wl, flags, _ = _case(100 + i)
+    flags = [f for f in flags if f != "-mdust"]
+    reads, _ = synth.generate(wl)
+    total = sum(r.size for r in reads)
+    d = tmp_path / "db"
+    d.mkdir()
+    dazzdb.write_db(str(d / "G"), reads, (total / 3 + 1) / 1e6)
+    nb = len(dazzdb.read_stub(str(d / "G.db"))[3]) - 1  # the blocks DBsplit's rule gave
+    for b in range(1, nb + 1):  # HPCdaligner's jobs: block b against itself and the blocks before it
+        subprocess.run([REF, "-r1", "-j4"] + flags + [f"G.{b}"] + [f"G.{c}" for c in range(b, 0, -1)], cwd=str(d),
+                       check=True, stdout=subprocess.DEVNULL)
+    for b in range(1, nb + 1):
+        subprocess.run([LAMERGE, "-n", "8", "G.db", f"G.{b}.las", "%03d_%05d" % (1, b)], cwd=str(d), check=True,
+                       stdout=subprocess.DEVNULL)
+    return d, nb
+
+
+needs_lamerge = pytest.mark.skipif(not (os.path.exists(REF) and os.path.exists(LAMERGE)),
+                                   reason="the reference LAmerge is not built (make -C oracle ref)")
+
+
+@pytest.mark.gpu
+@needs_lamerge
+@pytest.mark.parametrize("i", range(N_LAMERGE))
+def test_device_las_merge_equals_reference_lamerge(i, tmp_path):
+    from marvel_b200 import lamerge
+    d, nb = _lamerge_reference(i, tmp_path)
+    for b in range(1, nb + 1):
+        out = tmp_path / f"G.{b}.las"
+        assert lamerge.main(["-n", "8", str(d / "G.db"), str(out), str(d / ("%03d_%05d" % (1, b)))]) == 0
+        ok, msg = dazzdb.las_equal(str(out), str(d / f"G.{b}.las"), key="overlap", pad=True)
+        assert ok, f"case {i} block {b}: {msg}"
