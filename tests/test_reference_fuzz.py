@@ -278,3 +278,32 @@ def test_device_las_merge_equals_reference_lamerge(i, tmp_path):
         assert lamerge.main(["-n", "8", str(d / "G.db"), str(out), str(d / ("%03d_%05d" % (1, b)))]) == 0
         ok, msg = dazzdb.las_equal(str(out), str(d / f"G.{b}.las"), key="overlap", pad=True)
         assert ok, f"case {i} block {b}: {msg}"
+
+
+# ---- the reference's own driver linked against the library (the link-time drop-in)
+
+RELINKED = os.path.join(ROOT, "oracle", "_ref", "daligner_relinked")
+N_RELINK = 10
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(REF) and os.path.exists(RELINKED)),
+                    reason="oracle/_ref/daligner_relinked is not built (make -C oracle ref)")
+@pytest.mark.parametrize("i", range(N_RELINK))
+def test_relinked_reference_driver_equals_reference_daligner(i, tmp_path):
+    """dalign/daligner.c, unmodified, linked against libgpudalign.so in place of the
+    reference's filter.c and align.c: the same .las files as the reference daligner."""
+    import shutil
+    d, flags, blocks = _reference_run(200 + i, tmp_path)
+    g = tmp_path / "relinked"
+    g.mkdir()
+    for f in os.listdir(d):
+        if os.path.isfile(d / f):
+            shutil.copy(d / f, g / f)
+    r = subprocess.run([RELINKED, "-j4"] + flags + blocks, cwd=str(g), capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    names = [os.path.relpath(os.path.join(root, f), d) for root, _, fs in os.walk(d) for f in fs if f.endswith(".las")]
+    assert names
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(g / n), str(d / n))
+        assert ok, f"case {200 + i} {flags} {blocks}: {n}: {msg}"
