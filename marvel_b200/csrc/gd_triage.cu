@@ -25,6 +25,27 @@ namespace gd
 // f6 log2(1+diag sd)       f7 overlap length on the mean diagonal / (2*minover)
 // f8 hits per 64 bp of apos span                   f9 fraction of hits within one band of the mean diagonal
 // f10 orientation (comp)   f11 masked fraction of the A read
+// The twelve features from a group's sums: hits n, read lengths, a-position extent, the
+// diagonals' mean, variance, range and the hits near the mean, the masked bases of the A read.
+__device__ __forceinline__ void features_out(int n, float alen, float blen, int amin, int amax, double mean, double var,
+                                             int dmin, int dmax, int near, long long masked_bases, bool has_mask,
+                                             int comp, int minover, float f[TRI_NF])
+{
+    const double ovl = fmin((double)alen, (double)blen + mean) - fmax(0.0, mean);
+    f[0] = log2f((float)n);
+    f[1] = log2f(alen);
+    f[2] = log2f(blen);
+    f[3] = (float)(amax - amin) / alen;
+    f[4] = log2f(1.f + (float)(dmax - dmin));
+    f[5] = (float)(mean / alen);
+    f[6] = log2f(1.f + (float)sqrt(var));
+    f[7] = (float)(ovl / (2.0 * minover));
+    f[8] = 64.f * n / (float)(amax - amin + 1);
+    f[9] = (float)near / n;
+    f[10] = (float)comp;
+    f[11] = has_mask ? (float)masked_bases / alen : 0.f;
+}
+
 __device__ void group_features(const uint64_t* __restrict__ hkey, const uint32_t* __restrict__ hdiag, uint2 gr,
                                const HitBits& hb, const DevBlock& A, const DevBlock& B, int comp, int minover,
                                int binshift, const int64_t* __restrict__ anno, const int32_t* __restrict__ mdata,
@@ -51,27 +72,11 @@ __device__ void group_features(const uint64_t* __restrict__ hkey, const uint32_t
     int band = 1 << binshift, near = 0;
     for (int i = s; i < e; i++)
         near += fabs((double)(int)hdiag[i] - mean) <= band;
-    double ovl = fmin((double)alen, (double)blen + mean) - fmax(0.0, mean);
-    float masked = 0.f;
+    long long mb = 0;
     if (anno)
-    {
-        long long mb = 0;
         for (int64_t j = anno[ar]; j < anno[ar + 1]; j += 2)
             mb += mdata[j + 1] - mdata[j];
-        masked = (float)mb / alen;
-    }
-    f[0] = log2f((float)n);
-    f[1] = log2f(alen);
-    f[2] = log2f(blen);
-    f[3] = (float)(amax - amin) / alen;
-    f[4] = log2f(1.f + (float)(dmax - dmin));
-    f[5] = (float)(mean / alen);
-    f[6] = log2f(1.f + (float)sqrt(var));
-    f[7] = (float)(ovl / (2.0 * minover));
-    f[8] = 64.f * n / (float)(amax - amin + 1);
-    f[9] = (float)near / n;
-    f[10] = (float)comp;
-    f[11] = masked;
+    features_out(n, alen, blen, amin, amax, mean, var, dmin, dmax, near, mb, anno != nullptr, comp, minover, f);
 }
 
 // group_features with a warp's lanes over the group's hits (every lane returns the features).
@@ -114,29 +119,15 @@ __device__ void group_features_warp(const uint64_t* __restrict__ hkey, const uin
     for (int i = s + lane; i < e; i += 32)
         near += fabs((double)(int)hdiag[i] - mean) <= band;
     near = __reduce_add_sync(GD_FULL, near);
-    double ovl = fmin((double)alen, (double)blen + mean) - fmax(0.0, mean);
-    float masked = 0.f;
+    long long mb = 0;
     if (anno)
     {
-        long long mb = 0;
         for (int64_t j = anno[ar] + 2 * lane; j < anno[ar + 1]; j += 64)
             mb += mdata[j + 1] - mdata[j];
         for (int o = 16; o; o >>= 1)
             mb += __shfl_xor_sync(GD_FULL, mb, o);
-        masked = (float)mb / alen;
     }
-    f[0] = log2f((float)n);
-    f[1] = log2f(alen);
-    f[2] = log2f(blen);
-    f[3] = (float)(amax - amin) / alen;
-    f[4] = log2f(1.f + (float)(dmax - dmin));
-    f[5] = (float)(mean / alen);
-    f[6] = log2f(1.f + (float)sqrt(var));
-    f[7] = (float)(ovl / (2.0 * minover));
-    f[8] = 64.f * n / (float)(amax - amin + 1);
-    f[9] = (float)near / n;
-    f[10] = (float)comp;
-    f[11] = masked;
+    features_out(n, alen, blen, amin, amax, mean, var, dmin, dmax, near, mb, anno != nullptr, comp, minover, f);
 }
 
 // groups of more hits than this get their features from a whole warp (group_features_warp)
