@@ -307,3 +307,32 @@ def test_relinked_reference_driver_equals_reference_daligner(i, tmp_path):
     for n in names:
         ok, msg = dazzdb.las_equal(str(g / n), str(d / n))
         assert ok, f"case {200 + i} {flags} {blocks}: {n}: {msg}"
+
+
+# ---- the daligner command line of this package on the same random cases
+
+CLI = os.path.join(ROOT, "marvel_b200", "daligner_gpu")
+N_CLI = 10
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(REF) and os.path.exists(CLI)),
+                    reason="the reference daligner or marvel_b200/daligner_gpu is not built")
+@pytest.mark.parametrize("i", range(N_CLI))
+def test_command_line_equals_reference_daligner(i, tmp_path):
+    """marvel_b200/daligner_gpu, given the reference's command line, writes the reference
+    daligner's .las files (option parsing, mask tracks, file names and the two-file split)."""
+    import shutil
+    d, flags, blocks = _reference_run(300 + i, tmp_path)
+    g = tmp_path / "cli"
+    g.mkdir()
+    for f in os.listdir(d):
+        if os.path.isfile(d / f):
+            shutil.copy(d / f, g / f)
+    r = subprocess.run([CLI, "-j4"] + flags + blocks, cwd=str(g), capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    names = [os.path.relpath(os.path.join(root, f), d) for root, _, fs in os.walk(d) for f in fs if f.endswith(".las")]
+    assert names
+    for n in names:
+        ok, msg = dazzdb.las_equal(str(g / n), str(d / n))
+        assert ok, f"case {300 + i} {flags} {blocks}: {n}: {msg}"
