@@ -713,21 +713,25 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
             R.NB[cur][k & RM] = nb;
         }
 
-        // clip bookkeeping: bclip = first B-end in scan order, aclip = last A-end
-        unsigned bm = tballot(w, valid && bend);
-        if (bm)
+        // clip bookkeeping: bclip = first B-end in scan order, aclip = last A-end (a read end
+        // is rare: one vote for both first)
+        if (tany(w, valid && (bend || aend)))
         {
-            int pb = ch * TW + __ffs(bm) - 1;
-            int kb = FWD ? hgh - pb : low + pb;
-            bclip = FWD ? max(bclip, kb) : min(bclip, kb);
-            more = 0;
-        }
-        unsigned amk = tballot(w, valid && aend);
-        if (amk)
-        {
-            int pa = ch * TW + 31 - __clz(amk);
-            aclip = FWD ? hgh - pa : low + pa;
-            more = 0;
+            unsigned bm = tballot(w, valid && bend);
+            if (bm)
+            {
+                int pb = ch * TW + __ffs(bm) - 1;
+                int kb = FWD ? hgh - pb : low + pb;
+                bclip = FWD ? max(bclip, kb) : min(bclip, kb);
+                more = 0;
+            }
+            unsigned amk = tballot(w, valid && aend);
+            if (amk)
+            {
+                int pa = ch * TW + 31 - __clz(amk);
+                aclip = FWD ? hgh - pa : low + pa;
+                more = 0;
+            }
         }
 
         // best point: every new maximum in scan order is a record (align.c:880-897).  The
@@ -764,8 +768,12 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
                     trim[4] = hb;
                 }
             }
-            else
+            else if ((mq1 & ((1u << jm) - 1u)) && (!p1j || (mq2 & ((1u << jm) - 1u))))
             {
+                // only a q1 lane before jm can be a record that matters here (lasta when jm
+                // itself fails q1; the trim point when a q2 lane precedes it): without one the
+                // scan would change nothing, and that is most waves (on a 6 Mbp sample of the
+                // 1 Mbp model, every forward wave whose maximum fails the trim test)
                 // prefix max over the lanes before jm only (records lie before the maximum)
                 int incl = wv;
                 for (int o = 1; o < jm; o <<= 1)
