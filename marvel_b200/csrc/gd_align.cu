@@ -49,12 +49,43 @@ constexpr int ring_of()
     return RG & 0xffff;
 }
 
-// wave vectors: [dif & 1] holds wave dif, so a wave reads the previous one while it writes
+// Wave vectors by diagonal (k & RM).  The warp instances keep one ring per warp and update it
+// in place: within a chunk of 32 diagonals every lane reads its three predecessors before any
+// lane writes (the reads come before the chunk's first warp vote, the writes after a warp
+// barrier), and the one diagonal a chunk's first lane reads from the chunk before it (its kP,
+// and for a new band edge its NA/NB) is saved by that chunk's last lane before it writes
+// (ChunkEdge).  One ring instead of two halves the shared memory of a warp, which leaves the
+// SM a larger L1 for the reads' 2-bit words and the pebbles.  The duo instance's teams keep
+// two rings, [dif & 1] holding wave dif.
+template <int RG>
+constexpr int parities_of()
+{
+    return (RG >> 16) ? 2 : 1;
+}
+
+template <int RG>
+__device__ __forceinline__ int par(int dif)
+{
+    if constexpr (parities_of<RG>() == 2)
+        return dif & 1;
+    else
+        return 0;
+}
+
 template <int RG>
 struct WaveSmem
 {
-    unsigned long long T[2][ring_of<RG>()];
-    int V[2][ring_of<RG>()], HA[2][ring_of<RG>()], HB[2][ring_of<RG>()], NA[2][ring_of<RG>()], NB[2][ring_of<RG>()];
+    unsigned long long T[parities_of<RG>()][ring_of<RG>()];
+    int V[parities_of<RG>()][ring_of<RG>()], HA[parities_of<RG>()][ring_of<RG>()], HB[parities_of<RG>()][ring_of<RG>()],
+        NA[parities_of<RG>()][ring_of<RG>()], NB[parities_of<RG>()][ring_of<RG>()];
+};
+
+// The previous wave's values at the last diagonal of a 32-lane chunk, for the next chunk's
+// first lane (single-ring instances only)
+struct ChunkEdge
+{
+    unsigned long long t;
+    int v, ha, hb, na, nb, pad;
 };
 
 struct LAPath
@@ -71,6 +102,7 @@ struct WarpSmem
     int trim[5];  // the trim point (anti-diagonal, y, diffs, A and B pebble heads), written by its lane
     int clipm[6];  // the clip fallback: M count, anti-diagonal, y, diffs, A and B pebble heads
     int besty;    // y of the best anti-diagonal
+    ChunkEdge edge[ring_of<RG>() / 32 > 1 ? ring_of<RG>() / 32 - 1 : 1];  // [ch]: chunk ch's last diagonal
 };
 
 // The lanes that align one pair group together: a whole warp, or in the duo instance a
@@ -446,15 +478,15 @@ __device__ __forceinline__ void wave_begin(const bool FWD, WarpCtx<RG>& w, WaveV
                     hgh = aclip - 1;
                 else
                     low = aclip + 1;
-                int Mc = __popcll(R.T[dif & 1][aclip & RM] & MASK61);
+                int Mc = __popcll(R.T[par<RG>(dif)][aclip & RM] & MASK61);
                 if (lane == 0 && clipm[0] <= Mc)
                 {
                     clipm[0] = Mc;
-                    clipm[1] = R.V[dif & 1][aclip & RM];
+                    clipm[1] = R.V[par<RG>(dif)][aclip & RM];
                     clipm[2] = (clipm[1] - aclip) / 2;
                     clipm[3] = dif;
-                    clipm[4] = R.HA[dif & 1][aclip & RM];
-                    clipm[5] = R.HB[dif & 1][aclip & RM];
+                    clipm[4] = R.HA[par<RG>(dif)][aclip & RM];
+                    clipm[5] = R.HB[par<RG>(dif)][aclip & RM];
                 }
                 tsync(w);
             }
@@ -464,15 +496,15 @@ __device__ __forceinline__ void wave_begin(const bool FWD, WarpCtx<RG>& w, WaveV
                     low = bclip + 1;
                 else
                     hgh = bclip - 1;
-                int Mc = __popcll(R.T[dif & 1][bclip & RM] & MASK61);
+                int Mc = __popcll(R.T[par<RG>(dif)][bclip & RM] & MASK61);
                 if (lane == 0 && clipm[0] <= Mc)
                 {
                     clipm[0] = Mc;
-                    clipm[1] = R.V[dif & 1][bclip & RM];
+                    clipm[1] = R.V[par<RG>(dif)][bclip & RM];
                     clipm[2] = (clipm[1] - bclip) / 2;
                     clipm[3] = dif;
-                    clipm[4] = R.HA[dif & 1][bclip & RM];
-                    clipm[5] = R.HB[dif & 1][bclip & RM];
+                    clipm[4] = R.HA[par<RG>(dif)][bclip & RM];
+                    clipm[5] = R.HB[par<RG>(dif)][bclip & RM];
                 }
                 tsync(w);
             }
@@ -515,15 +547,15 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
                     hgh = aclip - 1;
                 else
                     low = aclip + 1;
-                int Mc = __popcll(R.T[dif & 1][aclip & RM] & MASK61);
+                int Mc = __popcll(R.T[par<RG>(dif)][aclip & RM] & MASK61);
                 if (lane == 0 && clipm[0] <= Mc)
                 {
                     clipm[0] = Mc;
-                    clipm[1] = R.V[dif & 1][aclip & RM];
+                    clipm[1] = R.V[par<RG>(dif)][aclip & RM];
                     clipm[2] = (clipm[1] - aclip) / 2;
                     clipm[3] = dif;
-                    clipm[4] = R.HA[dif & 1][aclip & RM];
-                    clipm[5] = R.HB[dif & 1][aclip & RM];
+                    clipm[4] = R.HA[par<RG>(dif)][aclip & RM];
+                    clipm[5] = R.HB[par<RG>(dif)][aclip & RM];
                 }
                 tsync(w);
             }
@@ -533,15 +565,15 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
                     low = bclip + 1;
                 else
                     hgh = bclip - 1;
-                int Mc = __popcll(R.T[dif & 1][bclip & RM] & MASK61);
+                int Mc = __popcll(R.T[par<RG>(dif)][bclip & RM] & MASK61);
                 if (lane == 0 && clipm[0] <= Mc)
                 {
                     clipm[0] = Mc;
-                    clipm[1] = R.V[dif & 1][bclip & RM];
+                    clipm[1] = R.V[par<RG>(dif)][bclip & RM];
                     clipm[2] = (clipm[1] - bclip) / 2;
                     clipm[3] = dif;
-                    clipm[4] = R.HA[dif & 1][bclip & RM];
-                    clipm[5] = R.HB[dif & 1][bclip & RM];
+                    clipm[4] = R.HA[par<RG>(dif)][bclip & RM];
+                    clipm[5] = R.HB[par<RG>(dif)][bclip & RM];
                 }
                 tsync(w);
             }
@@ -598,7 +630,8 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
     constexpr int TW = team_width<RG>();
     const int nch = (width + TW - 1) / TW;
     const int hgh0 = hgh, low0 = low;
-    const int cur = dif & 1, prv = cur ^ 1;
+    constexpr int NP = parities_of<RG>();
+    const int cur = par<RG>(dif), prv = par<RG>(dif - 1);
     int c0 = 0;  // chunk 0's new V, for the WAVE_LAG test
 #pragma unroll
     for (int ch = 0; ch < ring_of<RG>() / TW; ch++)
@@ -611,6 +644,11 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
         int c = 0, y = 0, ha = 0, hb = 0, na = 0, nb = 0;
         unsigned long long b = 0;
         bool bend = false, aend = false;
+        // single ring: the chunk before this one has written its diagonals, so the first lane
+        // takes its kP values from that chunk's saved edge
+        const bool fromedge = NP == 1 && ch > 0 && lane == 0;
+        if (NP == 1 && ch > 0)
+            tsync(w);
         if (valid)
         {
             // choose the furthest of the three predecessors (align.c:748-797)
@@ -618,6 +656,8 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
             int vP = (kP >= olow && kP <= ohgh) ? R.V[prv][kP & RM] : VNONE;
             int vC = (k >= olow && k <= ohgh) ? R.V[prv][k & RM] : VNONE;
             int vN = (kN >= olow && kN <= ohgh) ? R.V[prv][kN & RM] : VNONE;
+            if (fromedge)
+                vP = w.sm->edge[ch > 0 ? ch - 1 : 0].v;
             int wP = FWD ? vP : -vP, wC = FWD ? vC : -vC, wN = FWD ? vN : -vN;
             int ks, vs, step;
             if (wC < wN)
@@ -650,6 +690,13 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
             b = R.T[prv][ks & RM] << 1;
             ha = R.HA[prv][ks & RM];
             hb = R.HB[prv][ks & RM];
+            if (fromedge && ks == kP)
+            {
+                const ChunkEdge& e = w.sm->edge[ch > 0 ? ch - 1 : 0];
+                b = e.t << 1;
+                ha = e.ha;
+                hb = e.hb;
+            }
             y = (c - k) >> 1;
             int y0 = y;
             y = PK ? snake_pk(FWD, apk, ag, bpk, bg, y, k, alen, blen, bend, aend)
@@ -660,6 +707,23 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
             const int kn = k < olow ? olow : (k > ohgh ? ohgh : k);
             na = R.NA[prv][kn & RM];
             nb = R.NB[prv][kn & RM];
+            if (fromedge && kn == kP)  // a new band edge next to the chunk before
+            {
+                const ChunkEdge& e = w.sm->edge[ch > 0 ? ch - 1 : 0];
+                na = e.na;
+                nb = e.nb;
+            }
+            if (NP == 1 && ch + 1 < ring_of<RG>() / TW && lane == TW - 1 && ch + 1 < nch)
+            {
+                // the last lane saves its diagonal's previous values for the next chunk
+                ChunkEdge& e = w.sm->edge[ch];
+                e.v = vC;
+                e.t = R.T[prv][k & RM];
+                e.ha = R.HA[prv][k & RM];
+                e.hb = R.HB[prv][k & RM];
+                e.na = na;
+                e.nb = nb;
+            }
         }
         // trace points of A and B crossed by this extension (align.c:826-878)
         while (true)
@@ -703,6 +767,8 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
         }
         if (ch == 0)
             c0 = c;
+        if (NP == 1)
+            tsync(w);  // every lane of the chunk has read the ring
         if (valid)
         {
             R.V[cur][k & RM] = c;
@@ -3465,8 +3531,34 @@ void align_scratch_carve(AlignScratch* s, void* base, int nwarps, int pcap, int 
     s->btr = btcap ? (uint16_t*)p : nullptr;
 }
 
+// Prefer the smallest shared-memory carveout that holds ctas CTAs of kern: the rest of the SM's
+// 256 KB stays L1, which the aligner's reads of the 2-bit words, the pebbles and the trim tables
+// depend on
+static int prefer_l1(const void* kern, int ctas)
+{
+    cudaFuncAttributes fa;
+    int dev = 0, smsm = 0;
+    GD_CUDA(cudaFuncGetAttributes(&fa, kern));
+    GD_CUDA(cudaGetDevice(&dev));
+    GD_CUDA(cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    const long need = (long)ctas * ((long)fa.sharedSizeBytes + 1024);  // 1 KB per CTA is reserved
+    int pct = (int)((need * 100 + smsm - 1) / smsm);
+    pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+    GD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    return 0;
+}
+
 int align_grid(int* grid_out, int wide)
 {
+    static bool carved = false;  // once per process (the attribute stays with the kernel)
+    if (!carved)
+    {
+        if (prefer_l1((const void*)k_align_pairs<RING>, GD_ALIGN_MINB) ||
+            prefer_l1((const void*)k_align_pairs<RING, true>, GD_ALIGN_MINB) ||
+            prefer_l1((const void*)k_align_pairs<TEST_RING>, GD_ALIGN_MINB))
+            return -1;
+        carved = true;
+    }
     int dev = 0, nsm = 0, per = 0;
     GD_CUDA(cudaGetDevice(&dev));
     GD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
