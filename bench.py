@@ -72,8 +72,8 @@ def path_name():
 
 CACHE = os.environ.get("MARVEL_B200_CACHE", os.path.join(tempfile.gettempdir(), "marvel_b200_bench"))
 # k_align_pairs DRAM bytes (read + write) per wave cell, from the ncu capture of the cfg1
-# N-orientation launch (profiles/k_align_pairs_cfg1.md): 90.1 MB over 282 M cells
-ALIGN_DRAM_BYTES_PER_CELL = 90.1e6 / 282.0e6
+# N-orientation launch (profiles/k_align_pairs_cfg1.md): 85.0 MB over 282 M cells
+ALIGN_DRAM_BYTES_PER_CELL = 84.96e6 / 282.0e6
 # k-mer index build DRAM bytes per k-mer (extraction + 4 LSD passes), from the ncu capture of
 # the cfg1 index (profiles/filter_kernels_cfg1.md): 1,731 MB over 21.08 M k-mers
 INDEX_DRAM_BYTES_PER_KMER = 1731.2e6 / 21082465
@@ -402,9 +402,9 @@ def run_gpu(args):
                          "traffic_source": "bytes per launch: dram read+write per wave cell of the cfg1 ncu capture "
                                            "(profiles/k_align_pairs_cfg1.md) x this launch's cells",
                          "peak_source": "derived: 148 SM x 128 lanes/clk x median SM clock under load",
-                         "issue_slots_busy": 0.755,
+                         "issue_slots_busy": 0.781,
                          "issue_source": "smsp__issue_active of the cfg1 ncu capture (profiles/k_align_pairs_cfg1.md): "
-                                         "the kernel issues on 75 % of cycles; a wave is ~11 diagonals wide, so a "
+                                         "the kernel issues on 78 % of cycles; a wave is ~11 diagonals wide, so a "
                                          "warp instruction carries about a third of a warp of cells"},
             "roofline_filter": {"bound": "hbm", "kernel": "k-mer index (extract + 4 LSD passes)",
                                 "achieved": round(idx_bytes / (idx_ms / 1e3) / 1e9, 1),
