@@ -25,6 +25,7 @@
 #include "gd_align.cuh"
 
 #include <climits>
+#include <type_traits>
 
 namespace gd
 {
@@ -633,11 +634,10 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
     constexpr int NP = parities_of<RG>();
     const int cur = par<RG>(dif), prv = par<RG>(dif - 1);
     int c0 = 0;  // chunk 0's new V, for the WAVE_LAG test
-#pragma unroll
-    for (int ch = 0; ch < ring_of<RG>() / TW; ch++)
-    {
-        if (ch >= nch)
-            break;
+    // one chunk of 32 diagonals; true: the wave failed (w.err set, wvars stored).  Chunk 0 is
+    // specialised, the rare later chunks share one non-unrolled copy
+    auto chunk = [&](const int ch, auto first) -> bool {
+        constexpr bool FIRST = decltype(first)::value;
         const int p = ch * TW + lane;
         const bool valid = p < width;
         const int k = FWD ? hgh - p : low + p;
@@ -646,8 +646,8 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
         bool bend = false, aend = false;
         // single ring: the chunk before this one has written its diagonals, so the first lane
         // takes its kP values from that chunk's saved edge
-        const bool fromedge = NP == 1 && ch > 0 && lane == 0;
-        if (NP == 1 && ch > 0)
+        const bool fromedge = NP == 1 && !FIRST && lane == 0;
+        if (NP == 1 && !FIRST)
             tsync(w);
         if (valid)
         {
@@ -745,7 +745,7 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
                         gd_fail(w.st, GD_ERR_PEBBLES, w.item, w.pcap);
                     w.err = 1;
                     wvars.hgh = hgh; wvars.low = low; wvars.dif = dif; wvars.more = more; wvars.aclip = aclip; wvars.bclip = bclip; wvars.besta = besta; wvars.lasta = lasta; wvars.npeb = npeb;
-                    return false;
+                    return true;
                 }
                 if (cA)
                 {
@@ -765,7 +765,7 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
             if (needB)
                 nb += FWD ? TS : -TS;
         }
-        if (ch == 0)
+        if (FIRST)
             c0 = c;
         if (NP == 1)
             tsync(w);  // every lane of the chunk has read the ring
@@ -871,8 +871,14 @@ __device__ __forceinline__ bool wave_step(const bool FWD, WarpCtx<RG>& w, WaveVa
                 }
             }
             tsync(w);  // a later chunk's best point and trim point overwrite these
-        }
-    }
+        }        return false;
+    };
+    if (chunk(0, std::true_type{}))
+        return false;
+#pragma unroll 1
+    for (int ch = 1; ch < nch; ch++)
+        if (chunk(ch, std::false_type{}))
+            return false;
     tsync(w);
     clip_block();
 
